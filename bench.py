@@ -1,0 +1,379 @@
+"""Benchmark of the Strassen tensor-contraction path on B200.
+
+Workload (one step = one contraction call):
+    C(a,b,c,d) += A(e,f,a,c) * B(f,b,d,e)   FP64, column-major, U[-1,1] (seed 0)
+    with every extent 128, i.e. NIm = NJn = NPk = 16384, through
+    stra_tblis_tensor_mult (one-level Strassen, variant ABC).
+Metric: effective TFLOP/s = 2*NIm*NJn*NPk / t  (the reference's GFLOPS
+formula, test/test_strassen.cxx:228,355), for every Strassen level.
+
+The timed region runs exactly --steps contractions on device-resident
+operands, bracketed by barrier + synchronize, timed with CUDA events on the
+launching stream (max over ranks).  The operands (3 x 2 GiB) are far larger than
+the 126 MB L2, so no flush is needed between steps.  The same line also reports
+the plain L=0 kernel on the same GPU, the end-to-end figure through the C ABI
+with pinned host buffers (host<->device copies inside the timed region), the
+roofline of the dominant kernel against a cuBLAS DGEMM measured in the same
+run, clocks sampled during the timed region, and the reference's own CPU
+implementation timed on a bounded sample (rank 0, N=1).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "tblis-strassen_b200")
+sys.path.insert(0, ROOT)
+
+IDX_A, IDX_B, IDX_C = "efac", "fbde", "abcd"
+METRIC = "effective TFLOPS (2mnk/t) Strassen L1/L2 vs plain L=0 TC on 1 B200 at stated error"
+
+# DRAM traffic (read + write bytes) per launch of the dominant kernel, from the
+# ncu capture summarised in profiles/stra_dmma_kernel_fp64_L1.md, scaled by the
+# units processed (see that file).  None until a capture exists.
+NCU_TRAFFIC_BYTES = None
+
+
+def load_package():
+    name = "tblis_strassen_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(
+        name, os.path.join(PKG_DIR, "__init__.py"), submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def colmajor(torch, shape, device, gen=None, fill=None, pin=False):
+    """Column-major tensor of the given shape (U[-1,1] or constant)."""
+    rev = tuple(reversed(shape))
+    if device == "cpu":
+        t = torch.empty(rev, dtype=torch.float64, pin_memory=pin)
+    else:
+        t = torch.empty(rev, dtype=torch.float64, device=device)
+    if fill is None:
+        t.uniform_(-1.0, 1.0, generator=gen)
+    else:
+        t.fill_(fill)
+    return t.permute(*reversed(range(len(shape))))
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        load = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+def dgemm_peak(torch, device, n=8192, reps=5):
+    """cuBLAS DGEMM throughput (TFLOP/s) on this GPU: the FP64 roofline
+    denominator (MEASURED_PEAKS.json carries no FP64 figure)."""
+    a = torch.rand(n, n, dtype=torch.float64, device=device)
+    b = torch.rand(n, n, dtype=torch.float64, device=device)
+    c = torch.empty(n, n, dtype=torch.float64, device=device)
+    for _ in range(2):
+        torch.matmul(a, b, out=c)
+    torch.cuda.synchronize()
+    best = float("inf")
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b, out=c)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def cpu_reference(ext_sample: int, min_seconds: float, level: int, impl: int):
+    """The reference's own CPU implementation (oracle/_ref, compiled from its
+    sources) on a bounded sample: the same contraction pattern at extent
+    `ext_sample` per index, all host threads, min over repetitions (the
+    reference's run_kernel, test/test_strassen.cxx:74-95) until min_seconds of
+    CPU work.  Returns (TFLOP/s, threads, sample description, kind)."""
+    from oracle import oracle
+    import numpy as np
+    if not oracle.ref_available():
+        return None
+    threads = os.cpu_count() or 1
+    oracle.ref_set_threads(threads)
+    e = ext_sample
+    A = oracle.uniform((e,) * 4, 0)
+    B = oracle.uniform((e,) * 4, 1)
+    C = np.zeros((e,) * 4, order="F")
+    flops = 2.0 * float(e ** 2) ** 3
+    best, spent, reps = float("inf"), 0.0, 0
+    while spent < min_seconds or reps < 1:
+        t0 = time.perf_counter()
+        oracle.ref_mult(level, impl, 1.0, A, IDX_A, B, IDX_B, 1.0, C, IDX_C)
+        dt = time.perf_counter() - t0
+        best, spent, reps = min(best, dt), spent + dt, reps + 1
+        if reps >= 20:
+            break
+    sample = (f"reference stra_tblis_tensor_mult{'_2level' if level == 2 else ''} "
+              f"(L={level}, impl={impl}) on the same pattern at extent {e} "
+              f"(NIm=NJn=NPk={e * e}), min of {reps} reps ({spent:.1f} s CPU wall)")
+    if level == 0:
+        sample = sample.replace("stra_tblis_tensor_mult", "tblis_tensor_mult")
+    return flops / best / 1e12, threads, sample, "reference"
+
+
+def time_steps(torch, fn, steps, stream):
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(steps):
+        fn()
+    end.record(stream)
+    end.synchronize()
+    return start.elapsed_time(end) / 1e3
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--extent", type=int, default=128, help="extent of each of the six indices")
+    ap.add_argument("--level", type=int, default=1)
+    ap.add_argument("--variant", type=int, default=1, help="1 ABC, 2 AB, 3 Naive")
+    ap.add_argument("--cpu-sample-extent", type=int, default=64)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    e = args.extent
+    npk = e * e
+    flops = 2.0 * float(npk) ** 3
+    config = {"workload": f"C(abcd)+=A(efac)*B(fbde) FP64 col-major, extents {e} "
+                          f"(NIm=NJn=NPk={npk}), L={args.level} impl={args.variant}",
+              "NIm": npk, "NJn": npk, "NPk": npk, "level": args.level, "impl": args.variant,
+              "l2_flush": "inputs (3 x %.1f GiB) larger than L2" % (npk * npk * 8 / 2 ** 30),
+              "parallelism": f"replicas{world}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        r = cpu_reference(min(args.cpu_sample_extent, e), args.cpu_seconds * max(args.steps, 1) / 5.0,
+                          args.level, args.variant)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref not built"}))
+            return
+        val, cores, sample, kind = r
+        print(json.dumps({"impl": "reference", "metric": METRIC, "value": val, "unit": "TFLOP/s",
+                          "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                          "dtype": "f64", "data": "synthetic U[-1,1]", "config": config,
+                          "cpu_baseline": {"value": val, "unit": "TFLOP/s", "cores": cores, "kind": kind,
+                                           "sample": sample},
+                          "e2e": {"value": val, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+    tsb = load_package()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    device = torch.device(f"cuda:{local_rank}")
+    torch.cuda.set_device(device)
+    stream = torch.cuda.current_stream(device)
+
+    def barrier_sync():
+        torch.cuda.synchronize(device)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(device)
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    gen = torch.Generator(device=device).manual_seed(0 + rank)
+    shape = (e,) * 4
+    A = colmajor(torch, shape, device, gen)
+    B = colmajor(torch, shape, device, gen)
+    C = colmajor(torch, shape, device, fill=0.0)
+
+    def step(level=args.level, impl=args.variant):
+        tsb.contract(level, 1.0, A, IDX_A, B, IDX_B, 1.0, C, IDX_C, impl=impl, stream=stream)
+
+    # ---- headline: device-resident operands --------------------------------
+    for _ in range(args.warmup):
+        step()
+    barrier_sync()
+    sampler = ClockSampler(local_rank) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    launches0 = tsb.launch_count()
+    barrier_sync()
+    t = time_steps(torch, step, args.steps, stream)
+    barrier_sync()
+    launches = tsb.launch_count() - launches0
+    clocks = sampler.stop() if sampler else None
+    t = max_over_ranks(t)
+    ms_per_step = t / args.steps * 1e3
+    value = world * flops * args.steps / t / 1e12
+
+    # ---- same GPU, other levels (the plain L=0 kernel is the Strassen ratio's denominator)
+    levels = {}
+    for lv in sorted({0, 1, 2} - {args.level}) + [args.level]:
+        if lv == args.level:
+            levels[f"L{lv}"] = value / world
+            continue
+        for _ in range(2):
+            step(lv, 1)
+        barrier_sync()
+        tl = max_over_ranks(time_steps(torch, lambda: step(lv, 1), max(2, args.steps // 2), stream))
+        levels[f"L{lv}"] = flops * max(2, args.steps // 2) / tl / 1e12
+
+    # ---- accuracy of this run's result against the plain kernel -------------
+    C.zero_()
+    step()
+    C0 = colmajor(torch, shape, device, fill=0.0)
+    tsb.contract(0, 1.0, A, IDX_A, B, IDX_B, 0.0, C0, IDX_C, stream=stream)
+    torch.cuda.synchronize(device)
+    max_err = float((C - C0).abs().max())
+    # FP64 bound: 4 * 12^L * NPk * 2^-53 * max|A| * max|B|
+    bound = 4.0 * 12.0 ** args.level * npk * 2.0 ** -53 * float(A.abs().max()) * float(B.abs().max())
+    del C0
+
+    # ---- roofline of the dominant kernel ------------------------------------
+    peak = dgemm_peak(torch, device)
+    achieved = flops / (t / args.steps) / 1e12      # one launch per step (ABC)
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak,
+                "traffic": NCU_TRAFFIC_BYTES,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
+                "executed_frac": achieved * (7.0 / 8.0) ** args.level / peak,
+                "kernel": "stra_dmma_kernel<%d,%d>" % ((1, 1) if args.level == 0 else (2, 2) if args.level == 1 else (4, 4))}
+
+    # ---- end to end through the C ABI with pinned host buffers --------------
+    e2e = None
+    if not args.no_e2e:
+        del A, B, C
+        torch.cuda.empty_cache()
+        hA = colmajor(torch, shape, "cpu", pin=True, fill=0.5)
+        hB = colmajor(torch, shape, "cpu", pin=True, fill=0.25)
+        hC = colmajor(torch, shape, "cpu", pin=True, fill=0.0)
+        tsb.set_impl(args.variant)
+
+        def e2e_step():
+            tsb.contract(args.level, 1.0, hA, IDX_A, hB, IDX_B, 1.0, hC, IDX_C, drop_in=True)
+
+        e2e_step()
+        barrier_sync()
+        n2 = max(2, args.steps // 2)
+        t0 = time.perf_counter()
+        te = time_steps(torch, e2e_step, n2, torch.cuda.current_stream(device))
+        wall = time.perf_counter() - t0
+        te = max_over_ranks(max(te, wall))
+        tsb.set_impl(1)
+        nbytes = npk * npk * 8
+        e2e = {"value": world * flops * n2 / te / 1e12, "unit": "TFLOP/s",
+               "h2d_bytes_per_step": 3 * nbytes, "d2h_bytes_per_step": nbytes,
+               "path": "stra_tblis_tensor_mult with pinned host tensors (staged copies inside the call)"}
+        del hA, hB, hC
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        r = cpu_reference(args.cpu_sample_extent, args.cpu_seconds, args.level, args.variant)
+        if r is not None:
+            cpu = {"value": r[0], "unit": "TFLOP/s", "cores": r[1], "kind": r[3], "sample": r[2]}
+
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {"metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic U[-1,1] (seed 0)",
+            "config": config, "levels_tflops": levels,
+            "ratio_vs_L0": value / world / levels["L0"] if levels.get("L0") else None,
+            "max_err_vs_L0": max_err, "error_bound": bound,
+            "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
+            "gpu_launches": launches,
+            "measured_peaks_file": {k: measured_peaks().get(k) for k in ("hbm_gbs", "bf16_tflops")}}
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

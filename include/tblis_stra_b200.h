@@ -1,0 +1,182 @@
+/*
+ * tblis_stra_b200.h -- C ABI of the B200 (sm_100a) Strassen tensor-contraction
+ * library.  Drop-in for the contraction entry points of tblis-strassen:
+ *
+ *     C(idx_C) = alpha * A(idx_A) * B(idx_B) + beta * C(idx_C)
+ *
+ * with alpha = A->scalar * B->scalar and beta = C->scalar, exactly as the
+ * reference reads them (src/iface/3t/mult.cxx:128-129).  Every index label of
+ * a tensor names one mode; a label shared by A and B only is contracted, a
+ * label shared by A (or B) and C is a free row (column) index, a label in all
+ * three is a batch index, and a label in one tensor only is summed (A, B) or
+ * broadcast (C).  Repeated labels inside one tensor take the diagonal.
+ *
+ * Data pointers may be device memory (the fast path: stream-ordered, no
+ * copies) or host memory (the library stages through device memory and copies
+ * C back; the call is then synchronous).  The three drop-in symbols keep the
+ * reference's blocking `void` semantics and record a status readable through
+ * tblis_stra_last_status(); tblis_stra_mult() returns the status directly and
+ * is asynchronous on device pointers.
+ *
+ * Only FP64 (TYPE_DOUBLE) runs the plain double path (DMMA tensor cores).
+ * FP32 (TYPE_FLOAT) runs the split-BF16 tcgen05 path.
+ */
+#ifndef TBLIS_STRA_B200_H
+#define TBLIS_STRA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- types (layout-compatible with the reference) ----------------------- */
+
+/* Replaces src/util/basic_types.h:61-63 (configure defaults ptrdiff_t,
+ * ptrdiff_t, char; configure.ac:77-110). */
+typedef ptrdiff_t len_type;
+typedef ptrdiff_t stride_type;
+typedef char label_type;
+
+/* Replaces src/util/basic_types.h:52-59. */
+typedef enum
+{
+    TYPE_SINGLE   = 0,
+    TYPE_FLOAT    = TYPE_SINGLE,
+    TYPE_DOUBLE   = 1,
+    TYPE_SCOMPLEX = 2,
+    TYPE_DCOMPLEX = 3
+} type_t;
+
+/* Replaces src/util/basic_types.h:341-419 (same field order, sizes and
+ * alignment).  Strides are in elements and may be negative. */
+typedef struct tblis_tensor
+{
+    type_t type;
+    int conj;
+    char scalar[16] __attribute__((__aligned__(8)));
+    void* data;
+    unsigned ndim;
+    len_type* len;
+    stride_type* stride;
+} tblis_tensor;
+
+/* Opaque in this library.  The reference's tblis_comm is a TCI thread
+ * communicator (src/util/thread.h:7) and tblis_config a CPU kernel table
+ * (src/util/basic_types.h:37); both select CPU threading, which the GPU grid
+ * replaces, so any value (NULL included) is accepted and ignored. */
+typedef struct tci_comm tblis_comm;
+typedef struct tblis_config_s tblis_config;
+
+/* Replaces src/util/thread.h:8.  A non-null sentinel; passing it is the same
+ * as passing NULL. */
+extern const tblis_comm* const tblis_single;
+
+/* ---- drop-in contraction entry points ----------------------------------- */
+
+/* Plain (L=0) contraction.  Replaces tblis_tensor_mult,
+ * src/iface/3t/mult.h:17-20 / src/iface/3t/mult.cxx:15. */
+void tblis_tensor_mult(const tblis_comm* comm, const tblis_config* cfg,
+                       const tblis_tensor* A, const label_type* idx_A,
+                       const tblis_tensor* B, const label_type* idx_B,
+                             tblis_tensor* C, const label_type* idx_C);
+
+/* One-level Strassen (7 products).  Replaces stra_tblis_tensor_mult,
+ * src/stra_iface/3t/stra_mult.h:17-20 / src/stra_iface/3t/stra_mult.cxx:26. */
+void stra_tblis_tensor_mult(const tblis_comm* comm, const tblis_config* cfg,
+                            const tblis_tensor* A, const label_type* idx_A,
+                            const tblis_tensor* B, const label_type* idx_B,
+                                  tblis_tensor* C, const label_type* idx_C);
+
+/* Two-level Strassen (49 products).  Replaces stra_tblis_tensor_mult_2level,
+ * src/stra_iface/3t/stra_mult_2level.h:17-20 /
+ * src/stra_iface/3t/stra_mult_2level.cxx:26. */
+void stra_tblis_tensor_mult_2level(const tblis_comm* comm, const tblis_config* cfg,
+                                   const tblis_tensor* A, const label_type* idx_A,
+                                   const tblis_tensor* B, const label_type* idx_B,
+                                         tblis_tensor* C, const label_type* idx_C);
+
+/* Thread-count knobs of the reference (src/util/thread.h:13-15).  The GPU
+ * grid replaces CPU threads: the value is stored and reported, never used. */
+unsigned tblis_get_num_threads(void);
+void tblis_set_num_threads(unsigned num_threads);
+
+/* ---- status-returning / stream-ordered entry point ---------------------- */
+
+enum
+{
+    TBLIS_STRA_SUCCESS          = 0,
+    TBLIS_STRA_ERR_NULL         = 1,  /* null tensor, label or len/stride pointer */
+    TBLIS_STRA_ERR_TYPE         = 2,  /* type mismatch or unsupported element type */
+    TBLIS_STRA_ERR_EXTENT       = 3,  /* one label with different extents */
+    TBLIS_STRA_ERR_CONJ         = 4,  /* conj != 0 (real types only) */
+    TBLIS_STRA_ERR_ARG          = 5,  /* bad level, impl, ndim or negative extent */
+    TBLIS_STRA_ERR_CUDA         = 6,  /* a CUDA runtime call failed */
+    TBLIS_STRA_ERR_ALLOC        = 7,  /* device workspace could not be allocated */
+    TBLIS_STRA_ERR_TOO_LARGE    = 8,  /* sizes beyond what the kernels index */
+    TBLIS_STRA_ERR_UNSUPPORTED  = 9,  /* valid request this build does not run */
+    TBLIS_STRA_ERR_NO_DEVICE    = 10  /* no usable sm_100 device */
+};
+
+/* C(idx_C) = alpha*A*B + beta*C at Strassen level 0, 1 or 2 with the current
+ * variant (tblis_stra_set_impl).  `stream` is a cudaStream_t (NULL = the
+ * calling thread's stream from tblis_stra_set_stream, default the legacy
+ * stream).  With device pointers the call only enqueues work; with any host
+ * pointer it stages, computes and copies back before returning.  Replaces the
+ * three drop-in symbols above when the caller wants a status code: the
+ * reference returns void and aborts only in debug builds
+ * (src/util/assert.h:17-44). */
+int tblis_stra_mult(int level,
+                    const tblis_tensor* A, const label_type* idx_A,
+                    const tblis_tensor* B, const label_type* idx_B,
+                          tblis_tensor* C, const label_type* idx_C,
+                    void* stream);
+
+/* Strassen variant: 1 = ABC (sums fused into the loads, +-M fused into the
+ * epilogue, no workspace), 2 = AB (one M buffer, then a scatter-add pass),
+ * 3 = Naive (explicit S, T, M buffers).  Replaces the process-global
+ * tblis::internal::impl (src/internal/3t/mult.hpp:14-15) set by
+ * test/test_strassen.cxx:230-243; here it is per calling thread.  Level 0
+ * ignores it, as test/test_strassen.cxx:466-468 forces impl=1 there.
+ * Returns 0 or TBLIS_STRA_ERR_ARG. */
+int tblis_stra_set_impl(int impl);
+int tblis_stra_get_impl(void);
+
+/* Status of the calling thread's last contraction call; string form. */
+int tblis_stra_last_status(void);
+const char* tblis_stra_status_string(int status);
+
+/* The calling thread's default stream (a cudaStream_t; NULL = legacy). */
+int tblis_stra_set_stream(void* stream);
+void* tblis_stra_get_stream(void);
+
+/* Number of this library's kernels launched in this process so far. */
+unsigned long long tblis_stra_launch_count(void);
+
+/* Planning introspection; needs no GPU.  Runs the bundle analysis of a
+ * contraction (diagonal, label classes, fold; src/iface/3t/mult.cxx:21-126)
+ * and reports the batched matrix product it reduces to:
+ *   sizes[0..3] = m, n, k, batch;  ab[0..1] = alpha, beta;
+ * and, for each non-NULL array, the element-offset scatter vectors
+ *   rsA, rsC (length m), csB, csC (n), ksA, ksB (k), bA, bB, bC (batch),
+ * so that C[bC[b]+rsC[i]+csC[j]] = alpha * sum_p A[bA[b]+rsA[i]+ksA[p]] *
+ * B[bB[b]+ksB[p]+csB[j]] + beta * C[...].  This plays the role of the
+ * reference's matrify step (src/stra_nodes/stra_matrify.hpp:82-300).
+ * Returns a TBLIS_STRA_* status. */
+int tblis_stra_plan_query(const tblis_tensor* A, const label_type* idx_A,
+                          const tblis_tensor* B, const label_type* idx_B,
+                          const tblis_tensor* C, const label_type* idx_C,
+                          int64_t* sizes, double* ab,
+                          int64_t* rsA, int64_t* rsC, int64_t* csB, int64_t* csC,
+                          int64_t* ksA, int64_t* ksB,
+                          int64_t* bA, int64_t* bB, int64_t* bC);
+
+/* Library version string. */
+const char* tblis_stra_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TBLIS_STRA_B200_H */

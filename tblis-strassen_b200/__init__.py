@@ -1,0 +1,19 @@
+"""tblis-strassen for NVIDIA B200 (sm_100a).
+
+The library proper is ``libtblis_stra_b200.so`` (C ABI in
+``include/tblis_stra_b200.h``).  This package re-exports the Python mirror of
+the reference's contraction API (:mod:`.tblis_stra`).  The directory name
+contains a hyphen, so load it by path, e.g.::
+
+    import importlib.util, sys
+    spec = importlib.util.spec_from_file_location(
+        "tblis_strassen_b200", "tblis-strassen_b200/__init__.py",
+        submodule_search_locations=["tblis-strassen_b200"])
+    tsb = importlib.util.module_from_spec(spec); sys.modules[spec.name] = tsb
+    spec.loader.exec_module(tsb)
+"""
+from .tblis_stra import (  # noqa: F401
+    IMPL_AB, IMPL_ABC, IMPL_NAIVE, TYPE_DOUBLE, TYPE_FLOAT, TblisStraError, contract,
+    get_impl, launch_count, lib, mult, plan_query, set_impl, status_string, stra_mult,
+    stra_mult_2level, tblis_tensor, version,
+)

@@ -1,0 +1,137 @@
+// HBM-bound helper kernels of the contraction path.
+//
+//   scale_kernel        C = beta*C (beta == 0: C = 0 without reading C) for
+//                       alpha == 0 or an empty contracted range; replaces the
+//                       set/scale branch of src/stra_iface/3t/stra_mult.cxx:215-231.
+//   sum_gather_kernel   dense S = sum_t sign_t * X[block_t]: the explicit Strassen
+//                       operand sums of the Naive variant (straprim_naive2,
+//                       src/stra_internal/3t/straprim_common.hpp:70-157, which
+//                       forms them with add() into S and T buffers).
+//   scatter_add_kernel  C_q = (first ? beta*C_q : C_q) + sign_q*alpha*M for the
+//                       C blocks of one product: the M -> C update of the AB and
+//                       Naive variants (src/stra_internal/3t/straprim_common.hpp:
+//                       156, 187-203, tensor2matrix.hpp:390-830).
+//
+// All three are grid-stride loops over (batch, row, col) with the column index
+// fastest; the scatter vectors make the access pattern coalesced whenever the
+// fastest C (or X) mode is the column bundle's first mode.
+#include "kernels.cuh"
+
+#include <atomic>
+
+namespace tsb {
+
+extern std::atomic<unsigned long long> g_launches;
+
+namespace {
+
+constexpr int THREADS = 256;
+
+unsigned grid_for(int64_t total)
+{
+    int64_t blocks = (total + THREADS - 1) / THREADS;
+    const int64_t cap = 148 * 16;   // 16 resident blocks per SM on 148 SMs
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    return (unsigned)blocks;
+}
+
+__global__ void scale_kernel(const ScaleArgs a)
+{
+    const int64_t total = a.batch * a.m * a.n;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x)
+    {
+        const int64_t j = e % a.n;
+        const int64_t rest = e / a.n;
+        const int64_t i = rest % a.m;
+        const int64_t b = rest / a.m;
+        double* p = a.C + a.bC[b] + a.rsC[i] + a.csC[j];
+        *p = (a.beta == 0.0) ? 0.0 : a.beta * *p;
+    }
+}
+
+__global__ void sum_gather_kernel(const SumGatherArgs a)
+{
+    const int64_t total = a.batch * a.rows * a.cols;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x)
+    {
+        const int64_t j = e % a.cols;
+        const int64_t rest = e / a.cols;
+        const int64_t i = rest % a.rows;
+        const int64_t b = rest / a.rows;
+        double v = 0.0;
+        for (int t = 0; t < a.nt; t++)
+        {
+            const int64_t gi = a.t_r[t] * a.rows + i;
+            const int64_t gj = a.t_c[t] * a.cols + j;
+            if (gi < a.rows_full && gj < a.cols_full)
+            {
+                const double x = a.X[a.bX[b] + a.rsX[gi] + a.csX[gj]];
+                v += a.t_s[t] < 0 ? -x : x;
+            }
+        }
+        a.out[e] = v;
+    }
+}
+
+__global__ void scatter_add_kernel(const ScatterAddArgs a)
+{
+    const int64_t total = a.batch * a.ms * a.ns;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x)
+    {
+        const int64_t j = e % a.ns;
+        const int64_t rest = e / a.ns;
+        const int64_t i = rest % a.ms;
+        const int64_t b = rest / a.ms;
+        const double mv = a.M[e];
+        for (int q = 0; q < a.nc; q++)
+        {
+            const int64_t gi = a.c_r[q] * a.ms + i;
+            const int64_t gj = a.c_c[q] * a.ns + j;
+            if (gi >= a.m || gj >= a.n) continue;
+            double* p = a.C + a.bC[b] + a.rsC[gi] + a.csC[gj];
+            const double coef = a.c_s[q] < 0 ? -a.alpha : a.alpha;
+            double v = coef * mv;
+            if (!a.c_first[q]) v += *p;
+            else if (a.beta != 0.0) v += a.beta * *p;
+            *p = v;
+        }
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_scale(const ScaleArgs& a, cudaStream_t stream)
+{
+    const int64_t total = a.batch * a.m * a.n;
+    if (total <= 0) return cudaSuccess;
+    scale_kernel<<<grid_for(total), THREADS, 0, stream>>>(a);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) g_launches++;
+    return err;
+}
+
+cudaError_t launch_sum_gather(const SumGatherArgs& a, cudaStream_t stream)
+{
+    const int64_t total = a.batch * a.rows * a.cols;
+    if (total <= 0) return cudaSuccess;
+    sum_gather_kernel<<<grid_for(total), THREADS, 0, stream>>>(a);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) g_launches++;
+    return err;
+}
+
+cudaError_t launch_scatter_add(const ScatterAddArgs& a, cudaStream_t stream)
+{
+    const int64_t total = a.batch * a.ms * a.ns;
+    if (total <= 0) return cudaSuccess;
+    scatter_add_kernel<<<grid_for(total), THREADS, 0, stream>>>(a);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) g_launches++;
+    return err;
+}
+
+}  // namespace tsb

@@ -1,0 +1,516 @@
+// extern "C" boundary of the library and the host-side driver behind it.
+//
+//   tblis_tensor_mult              replaces src/iface/3t/mult.cxx:15
+//   stra_tblis_tensor_mult         replaces src/stra_iface/3t/stra_mult.cxx:26
+//   stra_tblis_tensor_mult_2level  replaces src/stra_iface/3t/stra_mult_2level.cxx:26
+//
+// Each call: plan the contraction (plan.cpp), fetch or build the device copy of
+// its scatter vectors (cached per shape/stride/label signature), stage host
+// operands through device memory when needed, and enqueue the kernels of the
+// requested level and variant on the caller's stream:
+//   ABC   one persistent DMMA launch running every product (no workspace);
+//   AB    per product: DMMA launch with fused operand sums into one M buffer,
+//         then a scatter-add of M into its C blocks;
+//   Naive per product: sum-gather S and T, DMMA launch M = S*T, scatter-add.
+// After the call C->scalar is 1 and C->conj 0, as the reference leaves them
+// (src/stra_iface/3t/stra_mult.cxx:251-252).
+#include "tblis_stra_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <list>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "plan.hpp"
+
+extern "C" {
+const tblis_comm* const tblis_single = reinterpret_cast<const tblis_comm*>(&tblis_single);
+}
+
+namespace tsb {
+namespace {
+
+thread_local int t_impl = 1;
+thread_local cudaStream_t t_stream = nullptr;
+thread_local int t_status = TBLIS_STRA_SUCCESS;
+unsigned g_num_threads = 1;
+
+// ---- device tables (cached) ------------------------------------------------
+
+struct DevPlan
+{
+    int device = -1;
+    void* mem = nullptr;
+    size_t bytes = 0;
+    const int64_t *rsA, *rsC, *csB, *csC, *ksA, *ksB, *bA, *bB, *bC;
+    ~DevPlan() { if (mem) cudaFree(mem); }
+};
+
+std::mutex g_cache_mu;
+std::list<std::pair<std::string, std::shared_ptr<DevPlan>>> g_cache;   // MRU first
+constexpr size_t CACHE_MAX = 32;
+
+std::string plan_key(int device, const tblis_tensor* const T[3], const label_type* const I[3])
+{
+    std::string k;
+    auto put = [&](const void* p, size_t n) { k.append(static_cast<const char*>(p), n); };
+    put(&device, sizeof device);
+    for (int t = 0; t < 3; t++)
+    {
+        put(&T[t]->type, sizeof T[t]->type);
+        put(&T[t]->ndim, sizeof T[t]->ndim);
+        if (T[t]->ndim)
+        {
+            put(T[t]->len, sizeof(len_type) * T[t]->ndim);
+            put(T[t]->stride, sizeof(stride_type) * T[t]->ndim);
+            put(I[t], sizeof(label_type) * T[t]->ndim);
+        }
+    }
+    return k;
+}
+
+int upload_plan(const GemmView& g, int device, std::shared_ptr<DevPlan>& out)
+{
+    auto dp = std::make_shared<DevPlan>();
+    dp->device = device;
+    const std::vector<int64_t>* parts[9] = {&g.rsA, &g.rsC, &g.csB, &g.csC, &g.ksA, &g.ksB,
+                                            &g.bA, &g.bB, &g.bC};
+    size_t total = 0;
+    for (auto* v : parts) total += std::max<size_t>(v->size(), 1);
+    std::vector<int64_t> host(total, 0);
+    size_t off[9], pos = 0;
+    for (int i = 0; i < 9; i++)
+    {
+        off[i] = pos;
+        std::copy(parts[i]->begin(), parts[i]->end(), host.begin() + (ptrdiff_t)pos);
+        pos += std::max<size_t>(parts[i]->size(), 1);
+    }
+    dp->bytes = total * sizeof(int64_t);
+    if (cudaMalloc(&dp->mem, dp->bytes) != cudaSuccess) { dp->mem = nullptr; return TBLIS_STRA_ERR_ALLOC; }
+    if (cudaMemcpy(dp->mem, host.data(), dp->bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+        return TBLIS_STRA_ERR_CUDA;
+    const int64_t* base = static_cast<const int64_t*>(dp->mem);
+    dp->rsA = base + off[0]; dp->rsC = base + off[1]; dp->csB = base + off[2];
+    dp->csC = base + off[3]; dp->ksA = base + off[4]; dp->ksB = base + off[5];
+    dp->bA = base + off[6]; dp->bB = base + off[7]; dp->bC = base + off[8];
+    out = dp;
+    return TBLIS_STRA_SUCCESS;
+}
+
+int get_plan(const tblis_tensor* const T[3], const label_type* const I[3], int device,
+             GemmView& g, std::shared_ptr<DevPlan>& dp)
+{
+    std::string key = plan_key(device, T, I);
+    {
+        std::lock_guard<std::mutex> lk(g_cache_mu);
+        for (auto it = g_cache.begin(); it != g_cache.end(); ++it)
+            if (it->first == key)
+            {
+                dp = it->second;
+                g_cache.splice(g_cache.begin(), g_cache, it);
+                // scalars and sizes still come from a (scatter-free) re-plan
+                return plan_contraction(T[0], I[0], T[1], I[1], T[2], I[2], g, false);
+            }
+    }
+    int st = plan_contraction(T[0], I[0], T[1], I[1], T[2], I[2], g, true);
+    if (st) return st;
+    st = upload_plan(g, device, dp);
+    if (st) return st;
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    g_cache.emplace_front(key, dp);
+    while (g_cache.size() > CACHE_MAX) g_cache.pop_back();
+    return TBLIS_STRA_SUCCESS;
+}
+
+int num_sms(int device)
+{
+    static std::mutex mu;
+    static std::map<int, int> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(device);
+    if (it != cache.end()) return it->second;
+    int v = 148;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device);
+    cache[device] = v;
+    return v;
+}
+
+bool is_device_ptr(const void* p)
+{
+    if (!p) return false;
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) { cudaGetLastError(); return false; }
+    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+// Stream-ordered device scratch (AB / Naive temporaries, staging).
+struct Scratch
+{
+    void* p = nullptr;
+    cudaStream_t s = nullptr;
+    ~Scratch() { if (p) cudaFreeAsync(p, s); }
+    int alloc(size_t bytes, cudaStream_t st)
+    {
+        s = st;
+        if (bytes == 0) bytes = 16;
+        return cudaMallocAsync(&p, bytes, st) == cudaSuccess ? TBLIS_STRA_SUCCESS : TBLIS_STRA_ERR_ALLOC;
+    }
+};
+
+DevProduct to_dev(const Product& p)
+{
+    DevProduct d{};
+    d.na = p.na; d.nb = p.nb; d.nc = p.nc;
+    for (int i = 0; i < 4; i++)
+    {
+        d.a_r[i] = p.a[i].r; d.a_c[i] = p.a[i].c; d.a_s[i] = p.a[i].sign;
+        d.b_r[i] = p.b[i].r; d.b_c[i] = p.b[i].c; d.b_s[i] = p.b[i].sign;
+        d.c_r[i] = p.c[i].r; d.c_c[i] = p.c[i].c; d.c_s[i] = p.c[i].sign;
+        d.c_first[i] = p.c_first[i];
+    }
+    return d;
+}
+
+int max_terms(const ProductTable& t)
+{
+    int m = 1;
+    for (auto& p : t.prod) m = std::max<int>(m, std::max<int>(p.na, p.nb));
+    return m;
+}
+
+inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+#define TSB_CUDA(x) do { if ((x) != cudaSuccess) return TBLIS_STRA_ERR_CUDA; } while (0)
+
+// Dense row-major temporaries of the AB / Naive variants: offset tables.
+struct DenseTables
+{
+    Scratch mem;
+    const int64_t* rows = nullptr;   // i * ld
+    const int64_t* cols = nullptr;   // j
+    const int64_t* bat = nullptr;    // b * rows_n * ld
+    int build(int64_t nr, int64_t ld, int64_t nbat, cudaStream_t st)
+    {
+        std::vector<int64_t> h((size_t)(nr + ld + nbat));
+        for (int64_t i = 0; i < nr; i++) h[(size_t)i] = i * ld;
+        for (int64_t j = 0; j < ld; j++) h[(size_t)(nr + j)] = j;
+        for (int64_t b = 0; b < nbat; b++) h[(size_t)(nr + ld + b)] = b * nr * ld;
+        int s = mem.alloc(h.size() * 8, st);
+        if (s) return s;
+        TSB_CUDA(cudaMemcpyAsync(mem.p, h.data(), h.size() * 8, cudaMemcpyHostToDevice, st));
+        TSB_CUDA(cudaStreamSynchronize(st));   // h is a local buffer
+        rows = static_cast<const int64_t*>(mem.p);
+        cols = rows + nr;
+        bat = cols + ld;
+        return TBLIS_STRA_SUCCESS;
+    }
+};
+
+DmmaArgs base_args(const GemmView& g, const DevPlan& t, const double* A, const double* B, double* C)
+{
+    DmmaArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.A = A; a.B = B; a.C = C;
+    a.rsA = t.rsA; a.ksA = t.ksA; a.ksB = t.ksB; a.csB = t.csB; a.rsC = t.rsC; a.csC = t.csC;
+    a.bA = t.bA; a.bB = t.bB; a.bC = t.bC;
+    a.m = g.m; a.n = g.n; a.k = g.k; a.mC = g.m; a.nC = g.n;
+    a.batch = g.batch;
+    a.alpha = g.alpha; a.beta = g.beta;
+    // Consecutive threads walk the operand dimension with the smaller stride.
+    a.a_kfast = (g.unit_ksA != 0 && (g.unit_rsA == 0 || g.unit_ksA < g.unit_rsA)) ? 1 : 0;
+    a.b_kfast = (g.unit_ksB != 0 && (g.unit_csB == 0 || g.unit_ksB < g.unit_csB)) ? 1 : 0;
+    return a;
+}
+
+void set_grid(DmmaArgs& a, int64_t ms, int64_t ns, int64_t ks)
+{
+    a.ms = ms; a.ns = ns; a.ks = ks;
+    a.tiles_m = (int)cdiv(ms, 128);
+    a.tiles_n = (int)cdiv(ns, 128);
+    a.work = a.batch * (int64_t)a.tiles_m * a.tiles_n;
+}
+
+int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
+             const double* A, const double* B, double* C, cudaStream_t st, int device)
+{
+    if (g.m == 0 || g.n == 0 || g.batch == 0) return TBLIS_STRA_SUCCESS;
+    if (g.alpha == 0.0 || g.k == 0)
+    {
+        ScaleArgs s{C, t.rsC, t.csC, t.bC, g.m, g.n, g.batch, g.beta};
+        TSB_CUDA(launch_scale(s, st));
+        return TBLIS_STRA_SUCCESS;
+    }
+    const ProductTable& tab = product_table(level);
+    const int H = tab.H;
+    const int64_t ms = cdiv(g.m, H), ns = cdiv(g.n, H), ks = cdiv(g.k, H);
+    const int sms = num_sms(device);
+
+    if (level == 0 || impl == 1)
+    {
+        DmmaArgs a = base_args(g, t, A, B, C);
+        set_grid(a, ms, ns, ks);
+        a.nprod = (int)tab.prod.size();
+        a.H = a.Hc = H;
+        for (int p = 0; p < a.nprod; p++) a.prod[p] = to_dev(tab.prod[p]);
+        TSB_CUDA(launch_dmma(a, max_terms(tab), st, sms));
+        return TBLIS_STRA_SUCCESS;
+    }
+
+    // AB / Naive: one M buffer (ms x ns per batch entry), products in order.
+    Scratch Mbuf;
+    int s = Mbuf.alloc((size_t)(g.batch * ms * ns) * sizeof(double), st);
+    if (s) return s;
+    double* M = static_cast<double*>(Mbuf.p);
+    DenseTables Mt;
+    if ((s = Mt.build(ms, ns, g.batch, st))) return s;
+
+    Scratch Sbuf, Tbuf;
+    DenseTables St, Tt;
+    if (impl == 3)
+    {
+        if ((s = Sbuf.alloc((size_t)(g.batch * ms * ks) * sizeof(double), st))) return s;
+        if ((s = Tbuf.alloc((size_t)(g.batch * ks * ns) * sizeof(double), st))) return s;
+        if ((s = St.build(ms, ks, g.batch, st))) return s;
+        if ((s = Tt.build(ks, ns, g.batch, st))) return s;
+    }
+
+    for (const Product& pr : tab.prod)
+    {
+        DmmaArgs a;
+        int terms = 1;
+        if (impl == 2)
+        {
+            a = base_args(g, t, A, B, M);
+            set_grid(a, ms, ns, ks);
+            a.H = H;
+            DevProduct d = to_dev(pr);
+            terms = std::max<int>(pr.na, pr.nb);
+            d.nc = 1; d.c_r[0] = 0; d.c_c[0] = 0; d.c_s[0] = 1; d.c_first[0] = 1;
+            a.prod[0] = d;
+        }
+        else
+        {
+            SumGatherArgs sa{};
+            sa.X = A; sa.rsX = t.rsA; sa.csX = t.ksA; sa.bX = t.bA;
+            sa.rows_full = g.m; sa.cols_full = g.k; sa.rows = ms; sa.cols = ks;
+            sa.batch = g.batch; sa.nt = pr.na; sa.out = static_cast<double*>(Sbuf.p);
+            for (int i = 0; i < pr.na; i++) { sa.t_r[i] = pr.a[i].r; sa.t_c[i] = pr.a[i].c; sa.t_s[i] = pr.a[i].sign; }
+            TSB_CUDA(launch_sum_gather(sa, st));
+            SumGatherArgs sb{};
+            sb.X = B; sb.rsX = t.ksB; sb.csX = t.csB; sb.bX = t.bB;
+            sb.rows_full = g.k; sb.cols_full = g.n; sb.rows = ks; sb.cols = ns;
+            sb.batch = g.batch; sb.nt = pr.nb; sb.out = static_cast<double*>(Tbuf.p);
+            for (int i = 0; i < pr.nb; i++) { sb.t_r[i] = pr.b[i].r; sb.t_c[i] = pr.b[i].c; sb.t_s[i] = pr.b[i].sign; }
+            TSB_CUDA(launch_sum_gather(sb, st));
+
+            std::memset(&a, 0, sizeof a);
+            a.A = static_cast<const double*>(Sbuf.p); a.B = static_cast<const double*>(Tbuf.p); a.C = M;
+            a.rsA = St.rows; a.ksA = St.cols; a.bA = St.bat;
+            a.ksB = Tt.rows; a.csB = Tt.cols; a.bB = Tt.bat;
+            a.m = ms; a.n = ns; a.k = ks; a.batch = g.batch;
+            a.a_kfast = 1; a.b_kfast = 0;
+            set_grid(a, ms, ns, ks);
+            a.H = 1;
+            DevProduct d{};
+            d.na = d.nb = d.nc = 1; d.a_s[0] = d.b_s[0] = d.c_s[0] = 1; d.c_first[0] = 1;
+            a.prod[0] = d;
+        }
+        a.rsC = Mt.rows; a.csC = Mt.cols; a.bC = Mt.bat;
+        a.mC = ms; a.nC = ns; a.Hc = 1;
+        a.alpha = 1.0; a.beta = 0.0;
+        a.nprod = 1;
+        TSB_CUDA(launch_dmma(a, terms, st, sms));
+
+        ScatterAddArgs sc{};
+        sc.C = C; sc.rsC = t.rsC; sc.csC = t.csC; sc.bC = t.bC;
+        sc.m = g.m; sc.n = g.n; sc.ms = ms; sc.ns = ns; sc.batch = g.batch;
+        sc.M = M; sc.alpha = g.alpha; sc.beta = g.beta; sc.nc = pr.nc;
+        for (int q = 0; q < pr.nc; q++)
+        {
+            sc.c_r[q] = pr.c[q].r; sc.c_c[q] = pr.c[q].c; sc.c_s[q] = pr.c[q].sign;
+            sc.c_first[q] = pr.c_first[q];
+        }
+        TSB_CUDA(launch_scatter_add(sc, st));
+    }
+    return TBLIS_STRA_SUCCESS;
+}
+
+int mult(int level, const tblis_tensor* A, const label_type* idx_A,
+         const tblis_tensor* B, const label_type* idx_B,
+         tblis_tensor* C, const label_type* idx_C, cudaStream_t st, bool blocking)
+{
+    if (level < 0 || level > 2) return TBLIS_STRA_ERR_ARG;
+    const int impl = t_impl;
+    if (!A || !B || !C) return TBLIS_STRA_ERR_NULL;
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) { cudaGetLastError(); return TBLIS_STRA_ERR_NO_DEVICE; }
+
+    const tblis_tensor* T[3] = {A, B, C};
+    const label_type* I[3] = {idx_A, idx_B, idx_C};
+    GemmView g;
+    std::shared_ptr<DevPlan> dp;
+    int s = get_plan(T, I, device, g, dp);
+    if (s) return s;
+    if (g.type != TYPE_DOUBLE) return TBLIS_STRA_ERR_UNSUPPORTED;
+
+    // Every element access is an aligned 8-byte load or store.
+    for (int t = 0; t < 3; t++)
+        if (reinterpret_cast<uintptr_t>(T[t]->data) % sizeof(double)) return TBLIS_STRA_ERR_ARG;
+
+    // Stage host operands through device memory.
+    const size_t es = sizeof(double);
+    void* dptr[3] = {A->data, B->data, C->data};
+    Scratch stage[3];
+    bool staged[3] = {false, false, false};
+    for (int t = 0; t < 3; t++)
+    {
+        if (g.hi[t] < g.lo[t]) continue;            // empty tensor
+        if (!T[t]->data) return TBLIS_STRA_ERR_NULL;
+        if (is_device_ptr(T[t]->data)) continue;
+        const size_t n = (size_t)(g.hi[t] - g.lo[t] + 1);
+        if ((s = stage[t].alloc(n * es, st))) return s;
+        const char* hsrc = static_cast<const char*>(T[t]->data) + g.lo[t] * (int64_t)es;
+        TSB_CUDA(cudaMemcpyAsync(stage[t].p, hsrc, n * es, cudaMemcpyHostToDevice, st));
+        dptr[t] = static_cast<char*>(stage[t].p) - g.lo[t] * (int64_t)es;
+        staged[t] = true;
+    }
+
+    s = run_fp64(level, impl, g, *dp, static_cast<const double*>(dptr[0]),
+                 static_cast<const double*>(dptr[1]), static_cast<double*>(dptr[2]), st, device);
+    if (s) return s;
+
+    if (staged[2])
+    {
+        const size_t n = (size_t)(g.hi[2] - g.lo[2] + 1);
+        char* hdst = static_cast<char*>(C->data) + g.lo[2] * (int64_t)es;
+        TSB_CUDA(cudaMemcpyAsync(hdst, stage[2].p, n * es, cudaMemcpyDeviceToHost, st));
+    }
+    if (blocking || staged[0] || staged[1] || staged[2])
+        TSB_CUDA(cudaStreamSynchronize(st));
+
+    double one = 1.0;
+    std::memcpy(C->scalar, &one, sizeof one);
+    C->conj = 0;
+    return TBLIS_STRA_SUCCESS;
+}
+
+}  // namespace
+}  // namespace tsb
+
+extern "C" {
+
+static void drop_in(int level, const tblis_tensor* A, const label_type* idx_A,
+                    const tblis_tensor* B, const label_type* idx_B,
+                    tblis_tensor* C, const label_type* idx_C)
+{
+    tsb::t_status = tsb::mult(level, A, idx_A, B, idx_B, C, idx_C, tsb::t_stream, true);
+}
+
+void tblis_tensor_mult(const tblis_comm*, const tblis_config*,
+                       const tblis_tensor* A, const label_type* idx_A,
+                       const tblis_tensor* B, const label_type* idx_B,
+                       tblis_tensor* C, const label_type* idx_C)
+{
+    drop_in(0, A, idx_A, B, idx_B, C, idx_C);
+}
+
+void stra_tblis_tensor_mult(const tblis_comm*, const tblis_config*,
+                            const tblis_tensor* A, const label_type* idx_A,
+                            const tblis_tensor* B, const label_type* idx_B,
+                            tblis_tensor* C, const label_type* idx_C)
+{
+    drop_in(1, A, idx_A, B, idx_B, C, idx_C);
+}
+
+void stra_tblis_tensor_mult_2level(const tblis_comm*, const tblis_config*,
+                                   const tblis_tensor* A, const label_type* idx_A,
+                                   const tblis_tensor* B, const label_type* idx_B,
+                                   tblis_tensor* C, const label_type* idx_C)
+{
+    drop_in(2, A, idx_A, B, idx_B, C, idx_C);
+}
+
+int tblis_stra_mult(int level, const tblis_tensor* A, const label_type* idx_A,
+                    const tblis_tensor* B, const label_type* idx_B,
+                    tblis_tensor* C, const label_type* idx_C, void* stream)
+{
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : tsb::t_stream;
+    tsb::t_status = tsb::mult(level, A, idx_A, B, idx_B, C, idx_C, st, false);
+    return tsb::t_status;
+}
+
+unsigned tblis_get_num_threads(void) { return tsb::g_num_threads; }
+void tblis_set_num_threads(unsigned n) { tsb::g_num_threads = n ? n : 1; }
+
+int tblis_stra_set_impl(int impl)
+{
+    if (impl < 1 || impl > 3) return TBLIS_STRA_ERR_ARG;
+    tsb::t_impl = impl;
+    return TBLIS_STRA_SUCCESS;
+}
+
+int tblis_stra_get_impl(void) { return tsb::t_impl; }
+
+int tblis_stra_last_status(void) { return tsb::t_status; }
+
+const char* tblis_stra_status_string(int s)
+{
+    switch (s)
+    {
+        case TBLIS_STRA_SUCCESS:         return "success";
+        case TBLIS_STRA_ERR_NULL:        return "null tensor, label, extent or stride pointer";
+        case TBLIS_STRA_ERR_TYPE:        return "mismatched or unsupported element type";
+        case TBLIS_STRA_ERR_EXTENT:      return "one label with different extents";
+        case TBLIS_STRA_ERR_CONJ:        return "conjugation requested on a real type";
+        case TBLIS_STRA_ERR_ARG:         return "invalid argument (level, impl, ndim or extent)";
+        case TBLIS_STRA_ERR_CUDA:        return "CUDA runtime error";
+        case TBLIS_STRA_ERR_ALLOC:       return "device workspace allocation failed";
+        case TBLIS_STRA_ERR_TOO_LARGE:   return "sizes beyond the kernels' index range";
+        case TBLIS_STRA_ERR_UNSUPPORTED: return "request not supported by this build";
+        case TBLIS_STRA_ERR_NO_DEVICE:   return "no usable CUDA device";
+        default:                         return "unknown status";
+    }
+}
+
+int tblis_stra_set_stream(void* stream)
+{
+    tsb::t_stream = static_cast<cudaStream_t>(stream);
+    return TBLIS_STRA_SUCCESS;
+}
+
+void* tblis_stra_get_stream(void) { return tsb::t_stream; }
+
+unsigned long long tblis_stra_launch_count(void) { return tsb::launches(); }
+
+const char* tblis_stra_version(void) { return "tblis-strassen-b200 0.1.0 (sm_100a)"; }
+
+int tblis_stra_plan_query(const tblis_tensor* A, const label_type* idx_A,
+                          const tblis_tensor* B, const label_type* idx_B,
+                          const tblis_tensor* C, const label_type* idx_C,
+                          int64_t* sizes, double* ab,
+                          int64_t* rsA, int64_t* rsC, int64_t* csB, int64_t* csC,
+                          int64_t* ksA, int64_t* ksB,
+                          int64_t* bA, int64_t* bB, int64_t* bC)
+{
+    tsb::GemmView g;
+    const bool want = rsA || rsC || csB || csC || ksA || ksB || bA || bB || bC;
+    int s = tsb::plan_contraction(A, idx_A, B, idx_B, C, idx_C, g, want);
+    if (s) return s;
+    if (sizes) { sizes[0] = g.m; sizes[1] = g.n; sizes[2] = g.k; sizes[3] = g.batch; }
+    if (ab) { ab[0] = g.alpha; ab[1] = g.beta; }
+    auto cp = [](int64_t* dst, const std::vector<int64_t>& v) {
+        if (dst) std::copy(v.begin(), v.end(), dst);
+    };
+    cp(rsA, g.rsA); cp(rsC, g.rsC); cp(csB, g.csB); cp(csC, g.csC);
+    cp(ksA, g.ksA); cp(ksB, g.ksB); cp(bA, g.bA); cp(bB, g.bB); cp(bC, g.bC);
+    return TBLIS_STRA_SUCCESS;
+}
+
+}  // extern "C"

@@ -1,0 +1,100 @@
+// Device-side interfaces shared by the kernels and the host launcher.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tsb {
+
+// Marks an out-of-range row, column or contracted index in the per-tile
+// offset tables: the loader zero-fills it and the epilogue skips it.
+constexpr int64_t OFF_INVALID = INT64_MIN;
+
+constexpr int MAX_PRODUCTS = 49;
+
+// One Strassen product on the device: signed sums of up to 4 A blocks
+// (row part, k part) and 4 B blocks (k part, col part); the result M is added,
+// with sign, into up to 4 C blocks (row part, col part).  c_first marks the
+// product that first touches a C block of the tile, where beta is applied.
+struct DevProduct
+{
+    int8_t na, nb, nc, pad;
+    int8_t a_r[4], a_c[4], a_s[4];
+    int8_t b_r[4], b_c[4], b_s[4];
+    int8_t c_r[4], c_c[4], c_s[4], c_first[4];
+};
+
+// Arguments of the FP64 Strassen/GEMM kernel.  Element (i, p) of A lives at
+// A[bA[b] + rsA[i] + ksA[p]], (p, j) of B at B[bB[b] + ksB[p] + csB[j]] and
+// (i, j) of C at C[bC[b] + rsC[i] + csC[j]].  The matrix is cut into an
+// H x H grid of blocks of ms x ks (A), ks x ns (B), ms x ns (C); indices past
+// m, n, k (the padding of a ragged split) read as zero and are not written.
+struct DmmaArgs
+{
+    const double* A;
+    const double* B;
+    double* C;
+    const int64_t* rsA; const int64_t* ksA;
+    const int64_t* ksB; const int64_t* csB;
+    const int64_t* rsC; const int64_t* csC;
+    const int64_t* bA; const int64_t* bB; const int64_t* bC;
+    int64_t m, n, k;        // extents seen by A and B
+    int64_t mC, nC;         // extents of the C side (m, n; or ms, ns for an M buffer)
+    int64_t ms, ns, ks;     // block extents
+    int64_t batch;
+    int tiles_m, tiles_n;
+    int64_t work;           // batch * tiles_m * tiles_n
+    double alpha, beta;
+    int a_kfast, b_kfast;   // loader thread mapping: 1 = consecutive threads walk k
+    int nprod, H, Hc;       // products; grid parts on the A/B side and the C side
+    DevProduct prod[MAX_PRODUCTS];
+};
+
+// Elementwise helpers for the AB and Naive variants and for alpha == 0.
+struct ScaleArgs
+{
+    double* C;
+    const int64_t* rsC; const int64_t* csC; const int64_t* bC;
+    int64_t m, n, batch;
+    double beta;
+};
+
+// Dense S = sum_t sign_t * X[block_t]  (rows x cols per batch, row-major) where
+// X(i, j) = X[bX[b] + rsX[i] + csX[j]].
+struct SumGatherArgs
+{
+    const double* X;
+    const int64_t* rsX; const int64_t* csX; const int64_t* bX;
+    int64_t rows_full, cols_full;  // bounds of the full index ranges
+    int64_t rows, cols;            // block extents (output is rows x cols)
+    int64_t batch;
+    int nt;
+    int8_t t_r[4], t_c[4], t_s[4];
+    double* out;
+};
+
+// C[block_q] = (first_q ? beta*C : C) + coef_q * alpha * M for q < nc.
+struct ScatterAddArgs
+{
+    double* C;
+    const int64_t* rsC; const int64_t* csC; const int64_t* bC;
+    int64_t m, n;                  // full C extents
+    int64_t ms, ns;                // block extents (M is ms x ns per batch)
+    int64_t batch;
+    const double* M;
+    double alpha, beta;
+    int nc;
+    int8_t c_r[4], c_c[4], c_s[4], c_first[4];
+};
+
+// Launchers (kernels.cu).  `terms` = largest number of blocks in one sum
+// (1, 2 or 4), selecting the kernel instance.  Return a cudaError_t.
+cudaError_t launch_dmma(const DmmaArgs& args, int terms, cudaStream_t stream, int num_sms);
+cudaError_t launch_scale(const ScaleArgs& args, cudaStream_t stream);
+cudaError_t launch_sum_gather(const SumGatherArgs& args, cudaStream_t stream);
+cudaError_t launch_scatter_add(const ScatterAddArgs& args, cudaStream_t stream);
+
+// Number of kernels this library has launched (all launchers count).
+unsigned long long launches();
+
+}  // namespace tsb

@@ -1,0 +1,402 @@
+// Contraction planning (see plan.hpp for the reference behaviour followed).
+#include "plan.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <numeric>
+
+namespace tsb {
+
+namespace {
+
+// Mode list of one tensor after diagonal(): label, extent, stride.
+struct Mode { label_type idx; int64_t len; int64_t stride; };
+
+// diagonal(), src/util/tensor.hpp:305-342: sort modes by label, merge a
+// repeated label into one mode whose stride is the sum (the extents must agree),
+// drop extent-1 modes.
+int diagonal(const tblis_tensor* T, const label_type* idx, std::vector<Mode>& out)
+{
+    out.clear();
+    std::vector<unsigned> order(T->ndim);
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](unsigned a, unsigned b) { return idx[a] < idx[b]; });
+    for (unsigned pos = 0; pos < T->ndim; pos++)
+    {
+        unsigned d = order[pos];
+        int64_t len = T->len[d];
+        if (len < 0) return TBLIS_STRA_ERR_ARG;
+        if (pos > 0 && idx[d] == idx[order[pos - 1]])
+        {
+            // repeated label: extents must agree; strides add
+            unsigned p = order[pos - 1];
+            if (T->len[p] != len) return TBLIS_STRA_ERR_EXTENT;
+            if (len != 1)
+            {
+                if (out.empty() || out.back().idx != idx[d]) return TBLIS_STRA_ERR_EXTENT;
+                out.back().stride += T->stride[d];
+            }
+            continue;
+        }
+        if (len != 1) out.push_back({idx[d], len, (int64_t)T->stride[d]});
+    }
+    return TBLIS_STRA_SUCCESS;
+}
+
+const Mode* find(const std::vector<Mode>& v, label_type l)
+{
+    for (auto& m : v) if (m.idx == l) return &m;
+    return nullptr;
+}
+
+// fold(), src/util/tensor.hpp:270-303: order modes by the first tensor's stride,
+// then merge mode i into the previous one when it is contiguous with it in
+// every tensor of the class.
+void fold(Bundle& b)
+{
+    const size_t nd = b.len.size();
+    if (nd == 0) return;
+    const size_t nt = b.stride.size();
+    std::vector<size_t> order(nd);
+    std::iota(order.begin(), order.end(), size_t(0));
+    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
+        return b.stride[0][x] < b.stride[0][y];
+    });
+    Bundle out;
+    out.stride.resize(nt);
+    for (size_t i = 0; i < nd; i++)
+    {
+        size_t d = order[i];
+        bool contiguous = false;
+        if (i != 0)
+        {
+            size_t p = order[i - 1];
+            contiguous = true;
+            for (size_t t = 0; t < nt; t++)
+                if (b.stride[t][d] != b.stride[t][p] * b.len[p]) contiguous = false;
+        }
+        if (contiguous)
+        {
+            out.len.back() *= b.len[d];
+        }
+        else
+        {
+            out.idx.push_back(b.idx[d]);
+            out.len.push_back(b.len[d]);
+            for (size_t t = 0; t < nt; t++) out.stride[t].push_back(b.stride[t][d]);
+        }
+    }
+    b = std::move(out);
+}
+
+// Reorder a bundle's modes by ascending |stride| of the given tensors in
+// priority order (the reference's sort_by_stride(stride_C_AC, stride_A_AC),
+// src/stra_internal/3t/stra_mult.cxx:336-338), so that flat index 0,1,2...
+// walks the fastest mode first.
+void sort_modes(Bundle& b, std::vector<int> prio)
+{
+    const size_t nd = b.len.size();
+    std::vector<size_t> order(nd);
+    std::iota(order.begin(), order.end(), size_t(0));
+    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
+        for (int t : prio)
+        {
+            int64_t sx = std::llabs(b.stride[t][x]), sy = std::llabs(b.stride[t][y]);
+            if (sx != sy) return sx < sy;
+        }
+        return false;
+    });
+    Bundle out;
+    out.stride.resize(b.stride.size());
+    for (size_t d : order)
+    {
+        out.idx.push_back(b.idx[d]);
+        out.len.push_back(b.len[d]);
+        for (size_t t = 0; t < b.stride.size(); t++) out.stride[t].push_back(b.stride[t][d]);
+    }
+    b = std::move(out);
+}
+
+int64_t prod_len(const std::vector<int64_t>& len)
+{
+    int64_t p = 1;
+    for (int64_t l : len) p *= l;
+    return p;
+}
+
+// Flattened offsets of every index of a mode list (fastest mode first).
+void scatter(const std::vector<int64_t>& len, const std::vector<int64_t>& stride,
+             std::vector<int64_t>& out)
+{
+    int64_t total = prod_len(len);
+    out.assign((size_t)total, 0);
+    if (total == 0) return;
+    std::vector<int64_t> digit(len.size(), 0);
+    int64_t off = 0;
+    for (int64_t i = 0; i < total; i++)
+    {
+        out[(size_t)i] = off;
+        for (size_t d = 0; d < len.size(); d++)
+        {
+            digit[d]++;
+            off += stride[d];
+            if (digit[d] < len[d]) break;
+            off -= stride[d] * len[d];
+            digit[d] = 0;
+        }
+    }
+}
+
+// Append the modes of `src` (with strides for tensors listed in `map`, a
+// missing tensor getting stride 0) to `dst` whose tensors are `dst_tensors`.
+void append_modes(std::vector<int64_t>& len, std::vector<std::vector<int64_t>>& strides,
+                  const Bundle& src, const std::vector<int>& src_slot_for_dst)
+{
+    for (size_t d = 0; d < src.len.size(); d++)
+    {
+        len.push_back(src.len[d]);
+        for (size_t t = 0; t < strides.size(); t++)
+        {
+            int s = src_slot_for_dst[t];
+            strides[t].push_back(s < 0 ? 0 : src.stride[(size_t)s][d]);
+        }
+    }
+}
+
+int64_t first_stride(const std::vector<int64_t>& len, const std::vector<int64_t>& stride)
+{
+    for (size_t d = 0; d < len.size(); d++) if (len[d] > 1) return std::llabs(stride[d]);
+    return 0;
+}
+
+}  // namespace
+
+void tensor_span(unsigned ndim, const len_type* len, const stride_type* stride,
+                 int64_t& lo, int64_t& hi)
+{
+    lo = 0; hi = 0;
+    for (unsigned d = 0; d < ndim; d++)
+    {
+        if (len[d] == 0) { lo = 0; hi = -1; return; }
+        int64_t ext = (int64_t)(len[d] - 1) * (int64_t)stride[d];
+        if (ext < 0) lo += ext; else hi += ext;
+    }
+}
+
+int plan_contraction(const tblis_tensor* A, const label_type* idx_A,
+                     const tblis_tensor* B, const label_type* idx_B,
+                     const tblis_tensor* C, const label_type* idx_C,
+                     GemmView& g, bool build_scatter)
+{
+    if (!A || !B || !C) return TBLIS_STRA_ERR_NULL;
+    const tblis_tensor* T[3] = {A, B, C};
+    const label_type* I[3] = {idx_A, idx_B, idx_C};
+    for (int t = 0; t < 3; t++)
+    {
+        if (T[t]->ndim > 0 && (!I[t] || !T[t]->len || !T[t]->stride)) return TBLIS_STRA_ERR_NULL;
+        if (T[t]->ndim > 64) return TBLIS_STRA_ERR_ARG;
+    }
+    if (A->type != B->type || A->type != C->type) return TBLIS_STRA_ERR_TYPE;
+    if (A->type != TYPE_DOUBLE && A->type != TYPE_FLOAT) return TBLIS_STRA_ERR_TYPE;
+    if (A->conj || B->conj || C->conj) return TBLIS_STRA_ERR_CONJ;
+
+    g = GemmView();
+    g.type = A->type;
+    if (A->type == TYPE_DOUBLE)
+    {
+        double a, b, c;
+        std::memcpy(&a, A->scalar, 8); std::memcpy(&b, B->scalar, 8); std::memcpy(&c, C->scalar, 8);
+        g.alpha = a * b; g.beta = c;
+    }
+    else
+    {
+        float a, b, c;
+        std::memcpy(&a, A->scalar, 4); std::memcpy(&b, B->scalar, 4); std::memcpy(&c, C->scalar, 4);
+        g.alpha = (double)(a * b); g.beta = (double)c;
+    }
+
+    std::vector<Mode> M[3];
+    for (int t = 0; t < 3; t++)
+    {
+        int st = diagonal(T[t], I[t], M[t]);
+        if (st) return st;
+        tensor_span(T[t]->ndim, T[t]->len, T[t]->stride, g.lo[t], g.hi[t]);
+    }
+
+    // Label classes (src/iface/3t/mult.cxx:43-86) with the extent checks of
+    // its TBLIS_ASSERTs turned into a status.
+    std::vector<label_type> labels;
+    for (int t = 0; t < 3; t++) for (auto& m : M[t]) labels.push_back(m.idx);
+    std::sort(labels.begin(), labels.end());
+    labels.erase(std::unique(labels.begin(), labels.end()), labels.end());
+
+    g.ABC.stride.resize(3); g.AB.stride.resize(2); g.AC.stride.resize(2);
+    g.BC.stride.resize(2); g.A_only.stride.resize(1); g.B_only.stride.resize(1);
+    g.C_only.stride.resize(1);
+    for (label_type l : labels)
+    {
+        const Mode* ma = find(M[0], l);
+        const Mode* mb = find(M[1], l);
+        const Mode* mc = find(M[2], l);
+        int64_t len = ma ? ma->len : mb ? mb->len : mc->len;
+        if ((ma && ma->len != len) || (mb && mb->len != len) || (mc && mc->len != len))
+            return TBLIS_STRA_ERR_EXTENT;
+        Bundle* b; std::vector<const Mode*> ms;
+        if (ma && mb && mc) { b = &g.ABC; ms = {ma, mb, mc}; }
+        else if (ma && mb)  { b = &g.AB;  ms = {ma, mb}; }
+        else if (ma && mc)  { b = &g.AC;  ms = {ma, mc}; }
+        else if (mb && mc)  { b = &g.BC;  ms = {mb, mc}; }
+        else if (ma)        { b = &g.A_only; ms = {ma}; }
+        else if (mb)        { b = &g.B_only; ms = {mb}; }
+        else                { b = &g.C_only; ms = {mc}; }
+        b->idx.push_back(l);
+        b->len.push_back(len);
+        for (size_t t = 0; t < ms.size(); t++) b->stride[t].push_back(ms[t]->stride);
+    }
+
+    // fold() each class (src/iface/3t/mult.cxx:120-126).
+    fold(g.ABC); fold(g.AB); fold(g.AC); fold(g.BC);
+    fold(g.A_only); fold(g.B_only); fold(g.C_only);
+
+    // Flattening order (src/stra_internal/3t/stra_mult.cxx:336-338):
+    // AC by (C, A) stride, BC by (C, B), AB by (A, B); batch by (C, A, B).
+    sort_modes(g.AC, {1, 0});
+    sort_modes(g.BC, {1, 0});
+    sort_modes(g.AB, {0, 1});
+    sort_modes(g.ABC, {2, 0, 1});
+
+    // Rows: AC.  Columns: BC.  Contracted: AB + A-only (B stride 0) + B-only
+    // (A stride 0).  Batch: ABC + C-only (A, B stride 0).
+    std::vector<int64_t> k_len = g.AB.len;
+    std::vector<std::vector<int64_t>> k_str = {g.AB.stride[0], g.AB.stride[1]};
+    append_modes(k_len, k_str, g.A_only, {0, -1});
+    append_modes(k_len, k_str, g.B_only, {-1, 0});
+    std::vector<int64_t> b_len = g.ABC.len;
+    std::vector<std::vector<int64_t>> b_str = {g.ABC.stride[0], g.ABC.stride[1], g.ABC.stride[2]};
+    append_modes(b_len, b_str, g.C_only, {-1, -1, 0});
+
+    g.m = prod_len(g.AC.len);
+    g.n = prod_len(g.BC.len);
+    g.k = prod_len(k_len);
+    g.batch = prod_len(b_len);
+    const int64_t lim = (int64_t)1 << 31;
+    if (g.m >= lim || g.n >= lim || g.k >= lim || g.batch >= lim) return TBLIS_STRA_ERR_TOO_LARGE;
+
+    g.unit_rsA = first_stride(g.AC.len, g.AC.stride[0]);
+    g.unit_rsC = first_stride(g.AC.len, g.AC.stride[1]);
+    g.unit_csB = first_stride(g.BC.len, g.BC.stride[0]);
+    g.unit_csC = first_stride(g.BC.len, g.BC.stride[1]);
+    g.unit_ksA = first_stride(k_len, k_str[0]);
+    g.unit_ksB = first_stride(k_len, k_str[1]);
+
+    if (build_scatter)
+    {
+        scatter(g.AC.len, g.AC.stride[0], g.rsA);
+        scatter(g.AC.len, g.AC.stride[1], g.rsC);
+        scatter(g.BC.len, g.BC.stride[0], g.csB);
+        scatter(g.BC.len, g.BC.stride[1], g.csC);
+        scatter(k_len, k_str[0], g.ksA);
+        scatter(k_len, k_str[1], g.ksB);
+        scatter(b_len, b_str[0], g.bA);
+        scatter(b_len, b_str[1], g.bB);
+        scatter(b_len, b_str[2], g.bC);
+    }
+    return TBLIS_STRA_SUCCESS;
+}
+
+// ---- Strassen product tables ---------------------------------------------
+
+namespace {
+
+// Strassen 〈2,2,2〉: rows are sub-block ids 0..3 ((0,0),(0,1),(1,0),(1,1)),
+// columns the 7 products; values from src/stra_internal/3t/strassen:1-14.
+const int U[4][7] = {{1, 0, 1, 0, 1, -1, 0},
+                     {0, 0, 0, 0, 1, 0, 1},
+                     {0, 1, 0, 0, 0, 1, 0},
+                     {1, 1, 0, 1, 0, 0, -1}};
+const int V[4][7] = {{1, 1, 0, -1, 0, 1, 0},
+                     {0, 0, 1, 0, 0, 1, 0},
+                     {0, 0, 0, 1, 0, 0, 1},
+                     {1, 0, -1, 0, 1, 0, 1}};
+const int W[4][7] = {{1, 0, 0, 1, -1, 0, 1},
+                     {0, 0, 1, 0, 1, 0, 0},
+                     {0, 1, 0, 1, 0, 0, 0},
+                     {1, -1, 1, 0, 0, 1, 0}};
+
+ProductTable make_table(int level)
+{
+    ProductTable t;
+    t.level = level;
+    t.H = 1 << level;
+    if (level == 0)
+    {
+        Product p;
+        p.na = p.nb = p.nc = 1;
+        p.a[0] = {0, 0, 1}; p.b[0] = {0, 0, 1}; p.c[0] = {0, 0, 1};
+        p.c_first[0] = 1;
+        t.prod.push_back(p);
+        return t;
+    }
+    // Level L product index p = p_outer * 7^(L-1) + ... ; sub-block (r, c) of
+    // the H x H grid has r = sum_l r_l * 2^(L-1-l) (outer level most
+    // significant), matching the 4x4 ids 4*row+col of
+    // src/stra_internal/3t/stra_mult_2level.cxx:341-353.
+    int np = 1;
+    for (int l = 0; l < level; l++) np *= 7;
+    for (int p = 0; p < np; p++)
+    {
+        int digits[2] = {0, 0};
+        int rem = p;
+        for (int l = level - 1; l >= 0; l--) { digits[l] = rem % 7; rem /= 7; }
+        Product pr;
+        auto expand = [&](const int (*Mx)[7], Term* out, int8_t& count) {
+            // Kronecker product of the per-level coefficient columns.
+            struct Acc { int r, c, s; };
+            std::vector<Acc> cur = {{0, 0, 1}};
+            for (int l = 0; l < level; l++)
+            {
+                std::vector<Acc> nxt;
+                for (auto& a : cur)
+                    for (int id = 0; id < 4; id++)
+                    {
+                        int v = Mx[id][digits[l]];
+                        if (!v) continue;
+                        nxt.push_back({a.r * 2 + id / 2, a.c * 2 + id % 2, a.s * v});
+                    }
+                cur = nxt;
+            }
+            count = (int8_t)cur.size();
+            for (size_t i = 0; i < cur.size(); i++)
+                out[i] = {(int8_t)cur[i].r, (int8_t)cur[i].c, (int8_t)cur[i].s};
+        };
+        expand(U, pr.a, pr.na);
+        expand(V, pr.b, pr.nb);
+        expand(W, pr.c, pr.nc);
+        t.prod.push_back(pr);
+    }
+    // Mark the first product touching each C block (beta applied there once).
+    std::vector<int> seen(t.H * t.H, 0);
+    for (auto& pr : t.prod)
+        for (int i = 0; i < pr.nc; i++)
+        {
+            int id = pr.c[i].r * t.H + pr.c[i].c;
+            pr.c_first[i] = seen[id] ? 0 : 1;
+            seen[id] = 1;
+        }
+    return t;
+}
+
+}  // namespace
+
+const ProductTable& product_table(int level)
+{
+    static const ProductTable t0 = make_table(0);
+    static const ProductTable t1 = make_table(1);
+    static const ProductTable t2 = make_table(2);
+    return level == 0 ? t0 : level == 1 ? t1 : t2;
+}
+
+}  // namespace tsb

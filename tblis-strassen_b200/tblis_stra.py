@@ -1,0 +1,245 @@
+"""Python mirror of the reference's contraction API over this library's C ABI.
+
+The reference exposes ``mult<T>``, ``stra_mult<T>`` and ``stra_mult_2level<T>``
+(src/iface/3t/mult.h:26-62, src/stra_iface/3t/stra_mult.h:26-62,
+src/stra_iface/3t/stra_mult_2level.h:26-62): ``(alpha, A, idx_A, B, idx_B,
+beta, C, idx_C)`` computing ``C = alpha*A*B + beta*C`` over index-label
+strings.  The functions here take the same arguments, with torch tensors (CUDA
+or CPU) or numpy arrays as the tensor views, and call the extern "C" entry
+points of ``libtblis_stra_b200.so`` through ctypes.  Errors the reference
+would abort on (debug builds) raise :class:`TblisStraError` here.
+
+The shared library is the product; this module only marshals arguments.  It
+raises at import time when the library has not been built, so nothing can run
+without the CUDA kernels.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libtblis_stra_b200.so")
+
+TYPE_FLOAT = 0
+TYPE_DOUBLE = 1
+
+IMPL_ABC, IMPL_AB, IMPL_NAIVE = 1, 2, 3
+
+
+class TblisStraError(RuntimeError):
+    """A contraction call returned a non-zero TBLIS_STRA_* status."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"tblis_stra status {status}: {message}")
+        self.status = status
+
+
+class tblis_tensor(ctypes.Structure):
+    """Layout of ``tblis_tensor`` (include/tblis_stra_b200.h)."""
+
+    _fields_ = [
+        ("type", ctypes.c_int),
+        ("conj", ctypes.c_int),
+        ("scalar", ctypes.c_double * 2),   # char[16], 8-byte aligned
+        ("data", ctypes.c_void_p),
+        ("ndim", ctypes.c_uint),
+        ("len", ctypes.POINTER(ctypes.c_ssize_t)),
+        ("stride", ctypes.POINTER(ctypes.c_ssize_t)),
+    ]
+
+
+def _load() -> ctypes.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build the CUDA library first "
+            "(make -C tblis-strassen_b200, or __graft_entry__.build())")
+    lib = ctypes.CDLL(LIB_PATH)
+    T = ctypes.POINTER(tblis_tensor)
+    S = ctypes.c_char_p
+    for name in ("tblis_tensor_mult", "stra_tblis_tensor_mult", "stra_tblis_tensor_mult_2level"):
+        fn = getattr(lib, name)
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, T, S, T, S, T, S]
+        fn.restype = None
+    lib.tblis_stra_mult.argtypes = [ctypes.c_int, T, S, T, S, T, S, ctypes.c_void_p]
+    lib.tblis_stra_mult.restype = ctypes.c_int
+    lib.tblis_stra_set_impl.argtypes = [ctypes.c_int]
+    lib.tblis_stra_set_impl.restype = ctypes.c_int
+    lib.tblis_stra_get_impl.restype = ctypes.c_int
+    lib.tblis_stra_last_status.restype = ctypes.c_int
+    lib.tblis_stra_status_string.argtypes = [ctypes.c_int]
+    lib.tblis_stra_status_string.restype = ctypes.c_char_p
+    lib.tblis_stra_set_stream.argtypes = [ctypes.c_void_p]
+    lib.tblis_stra_set_stream.restype = ctypes.c_int
+    lib.tblis_stra_get_stream.restype = ctypes.c_void_p
+    lib.tblis_stra_launch_count.restype = ctypes.c_ulonglong
+    lib.tblis_stra_version.restype = ctypes.c_char_p
+    P64 = ctypes.POINTER(ctypes.c_int64)
+    lib.tblis_stra_plan_query.argtypes = [T, S, T, S, T, S, P64, ctypes.POINTER(ctypes.c_double)] + [P64] * 9
+    lib.tblis_stra_plan_query.restype = ctypes.c_int
+    lib.tblis_get_num_threads.restype = ctypes.c_uint
+    lib.tblis_set_num_threads.argtypes = [ctypes.c_uint]
+    return lib
+
+
+lib = _load()
+
+
+def status_string(status: int) -> str:
+    return lib.tblis_stra_status_string(status).decode()
+
+
+def _check(status: int) -> None:
+    if status != 0:
+        raise TblisStraError(status, status_string(status))
+
+
+class _View:
+    """A tblis_tensor plus the ctypes arrays it points into."""
+
+    def __init__(self, obj, scalar: float, dtype_code: int | None = None):
+        shape, strides, ptr, code = _describe(obj)
+        if dtype_code is not None and code != dtype_code:
+            raise TypeError("operand element types differ")
+        self.obj = obj
+        n = len(shape)
+        self.len = (ctypes.c_ssize_t * max(n, 1))(*shape)
+        self.stride = (ctypes.c_ssize_t * max(n, 1))(*strides)
+        t = tblis_tensor()
+        t.type = code
+        t.conj = 0
+        if code == TYPE_DOUBLE:
+            t.scalar[0] = float(scalar)
+        else:
+            ctypes.memmove(ctypes.addressof(t.scalar), ctypes.byref(ctypes.c_float(scalar)), 4)
+        t.data = ptr
+        t.ndim = n
+        t.len = ctypes.cast(self.len, ctypes.POINTER(ctypes.c_ssize_t))
+        t.stride = ctypes.cast(self.stride, ctypes.POINTER(ctypes.c_ssize_t))
+        self.t = t
+        self.code = code
+
+
+def _describe(obj):
+    """(shape, element strides, data pointer, type code) of a torch tensor or numpy array."""
+    mod = type(obj).__module__
+    if mod.startswith("torch"):
+        import torch
+        if obj.dtype == torch.float64:
+            code = TYPE_DOUBLE
+        elif obj.dtype == torch.float32:
+            code = TYPE_FLOAT
+        else:
+            raise TypeError(f"unsupported dtype {obj.dtype}")
+        return list(obj.shape), list(obj.stride()), obj.data_ptr(), code
+    import numpy as np
+    arr = obj
+    if arr.dtype == np.float64:
+        code, es = TYPE_DOUBLE, 8
+    elif arr.dtype == np.float32:
+        code, es = TYPE_FLOAT, 4
+    else:
+        raise TypeError(f"unsupported dtype {arr.dtype}")
+    if any(s % es for s in arr.strides):
+        raise ValueError("strides must be whole elements")
+    return list(arr.shape), [s // es for s in arr.strides], arr.ctypes.data, code
+
+
+def _labels(idx: str, n: int) -> bytes:
+    if len(idx) != n:
+        raise ValueError(f"index string {idx!r} has {len(idx)} labels for a {n}-d tensor")
+    return idx.encode()
+
+
+def contract(level: int, alpha, A, idx_A: str, B, idx_B: str, beta, C, idx_C: str,
+             impl: int | None = None, stream=None, drop_in: bool = False) -> None:
+    """C = alpha*A*B + beta*C at Strassen level 0, 1 or 2.
+
+    ``drop_in=True`` calls the reference-named blocking ``void`` symbols and
+    reads the status afterwards; otherwise ``tblis_stra_mult`` is used
+    (asynchronous on device pointers, on ``stream`` -- a torch.cuda.Stream, a
+    raw handle or None for the thread's default).
+    """
+    va = _View(A, alpha)
+    vb = _View(B, 1.0, va.code)
+    vc = _View(C, beta, va.code)
+    ia, ib, ic = _labels(idx_A, va.t.ndim), _labels(idx_B, vb.t.ndim), _labels(idx_C, vc.t.ndim)
+    old_impl = None
+    if impl is not None:
+        old_impl = lib.tblis_stra_get_impl()
+        _check(lib.tblis_stra_set_impl(impl))
+    try:
+        if drop_in:
+            fn = (lib.tblis_tensor_mult, lib.stra_tblis_tensor_mult,
+                  lib.stra_tblis_tensor_mult_2level)[level]
+            fn(None, None, ctypes.byref(va.t), ia, ctypes.byref(vb.t), ib, ctypes.byref(vc.t), ic)
+            _check(lib.tblis_stra_last_status())
+        else:
+            handle = None
+            if stream is not None:
+                handle = getattr(stream, "cuda_stream", stream)
+            _check(lib.tblis_stra_mult(level, ctypes.byref(va.t), ia, ctypes.byref(vb.t), ib,
+                                       ctypes.byref(vc.t), ic, handle))
+    finally:
+        if old_impl is not None:
+            lib.tblis_stra_set_impl(old_impl)
+
+
+def mult(alpha, A, idx_A, B, idx_B, beta, C, idx_C, **kw) -> None:
+    """Plain (L=0) contraction; mirrors tblis::mult (src/iface/3t/mult.h:27)."""
+    contract(0, alpha, A, idx_A, B, idx_B, beta, C, idx_C, **kw)
+
+
+def stra_mult(alpha, A, idx_A, B, idx_B, beta, C, idx_C, **kw) -> None:
+    """One-level Strassen; mirrors tblis::stra_mult (src/stra_iface/3t/stra_mult.h:27)."""
+    contract(1, alpha, A, idx_A, B, idx_B, beta, C, idx_C, **kw)
+
+
+def stra_mult_2level(alpha, A, idx_A, B, idx_B, beta, C, idx_C, **kw) -> None:
+    """Two-level Strassen; mirrors tblis::stra_mult_2level (src/stra_iface/3t/stra_mult_2level.h:27)."""
+    contract(2, alpha, A, idx_A, B, idx_B, beta, C, idx_C, **kw)
+
+
+def set_impl(impl: int) -> None:
+    """1 ABC, 2 AB, 3 Naive (the -impl knob of test/test_strassen.cxx:230-243)."""
+    _check(lib.tblis_stra_set_impl(impl))
+
+
+def get_impl() -> int:
+    return lib.tblis_stra_get_impl()
+
+
+def launch_count() -> int:
+    return int(lib.tblis_stra_launch_count())
+
+
+def version() -> str:
+    return lib.tblis_stra_version().decode()
+
+
+def plan_query(A, idx_A, B, idx_B, C, idx_C, scatter: bool = True):
+    """Bundle analysis of a contraction, without a GPU.
+
+    Returns a dict with m, n, k, batch, alpha, beta and (if ``scatter``) the
+    scatter vectors rsA, rsC, csB, csC, ksA, ksB, bA, bB, bC as numpy arrays.
+    """
+    import numpy as np
+    va, vb, vc = _View(A, 1.0), _View(B, 1.0), _View(C, 0.0)
+    ia, ib, ic = _labels(idx_A, va.t.ndim), _labels(idx_B, vb.t.ndim), _labels(idx_C, vc.t.ndim)
+    sizes = (ctypes.c_int64 * 4)()
+    ab = (ctypes.c_double * 2)()
+    args = [ctypes.byref(va.t), ia, ctypes.byref(vb.t), ib, ctypes.byref(vc.t), ic, sizes, ab] + [None] * 9
+    _check(lib.tblis_stra_plan_query(*args))
+    m, n, k, b = (int(x) for x in sizes)
+    out = {"m": m, "n": n, "k": k, "batch": b}
+    if scatter:
+        names = ["rsA", "rsC", "csB", "csC", "ksA", "ksB", "bA", "bB", "bC"]
+        lens = [m, m, n, n, k, k, b, b, b]
+        arrs = [np.zeros(max(L, 1), dtype=np.int64) for L in lens]
+        ptrs = [a.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)) for a in arrs]
+        va2, vb2, vc2 = _View(A, 1.0), _View(B, 1.0), _View(C, 0.0)
+        _check(lib.tblis_stra_plan_query(ctypes.byref(va2.t), ia, ctypes.byref(vb2.t), ib,
+                                         ctypes.byref(vc2.t), ic, sizes, ab, *ptrs))
+        for nm, a, L in zip(names, arrs, lens):
+            out[nm] = a[:L]
+    return out

@@ -1,0 +1,88 @@
+"""The C-ABI library on a machine without a GPU: it loads, exports every
+function include/tblis_stra_b200.h declares, has the reference's struct
+layout, and reports errors as status codes instead of aborting."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "tblis_stra_b200.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b([A-Za-z_]\w*)\s*\(", src, flags=re.M)
+    return sorted(set(n for n in names if n not in ("if", "defined")))
+
+
+def test_every_declared_symbol_is_exported(tsb):
+    names = declared_functions()
+    assert "tblis_tensor_mult" in names and "stra_tblis_tensor_mult_2level" in names
+    for n in names:
+        assert hasattr(tsb.lib, n), n
+    # the data symbol too
+    ctypes.c_void_p.in_dll(tsb.lib, "tblis_single")
+
+
+def test_struct_layout_matches_header(tsb, tmp_path):
+    prog = tmp_path / "layout.c"
+    prog.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "tblis_stra_b200.h"\n'
+        'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(tblis_tensor),'
+        'offsetof(tblis_tensor,conj),offsetof(tblis_tensor,scalar),offsetof(tblis_tensor,data),'
+        'offsetof(tblis_tensor,ndim),offsetof(tblis_tensor,len),offsetof(tblis_tensor,stride));return 0;}\n')
+    exe = tmp_path / "layout"
+    subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), str(prog), "-o", str(exe)])
+    got = [int(x) for x in subprocess.check_output([str(exe)]).split()]
+    T = tsb.tblis_tensor
+    want = [ctypes.sizeof(T), T.conj.offset, T.scalar.offset, T.data.offset, T.ndim.offset,
+            T.len.offset, T.stride.offset]
+    assert got == want
+
+
+def test_impl_knob(tsb):
+    assert tsb.get_impl() == 1
+    for impl in (2, 3, 1):
+        tsb.set_impl(impl)
+        assert tsb.get_impl() == impl
+    with pytest.raises(tsb.TblisStraError):
+        tsb.set_impl(4)
+    assert tsb.get_impl() == 1
+
+
+def test_status_strings(tsb):
+    for s in range(11):
+        assert tsb.status_string(s) != "unknown status"
+    assert tsb.status_string(99) == "unknown status"
+
+
+def test_threads_knob_is_kept(tsb):
+    tsb.lib.tblis_set_num_threads(6)
+    assert tsb.lib.tblis_get_num_threads() == 6
+    tsb.lib.tblis_set_num_threads(1)
+
+
+def test_no_device_is_a_status_not_a_crash(tsb):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    A = np.ones((4, 4)); B = np.ones((4, 4)); C = np.zeros((4, 4))
+    with pytest.raises(tsb.TblisStraError) as e:
+        tsb.mult(1.0, A, "ik", B, "kj", 0.0, C, "ij")
+    assert e.value.status in (6, 10)
+    # drop-in void symbol: records the status instead
+    with pytest.raises(tsb.TblisStraError):
+        tsb.mult(1.0, A, "ik", B, "kj", 0.0, C, "ij", drop_in=True)
+    assert tsb.lib.tblis_stra_last_status() in (6, 10)
+
+
+def test_bad_level_is_rejected(tsb):
+    A = np.ones((2, 2)); C = np.zeros((2, 2))
+    with pytest.raises(tsb.TblisStraError) as e:
+        tsb.contract(3, 1.0, A, "ik", A, "kj", 0.0, C, "ij")
+    assert e.value.status == 5

@@ -1,0 +1,198 @@
+"""Parity of the CUDA path with the oracle and with the reference's own
+outputs (golden fixtures), through the C ABI, on the GPU.
+
+Bound (FP64):  max|C - Cref| <= 4 * 12^L * NPk * 2^-53 * max|A| * max|B|
+scaled by |alpha| and widened by the rounding of beta*C (4 * 2^-53 * |beta| *
+max|C0|), where NPk is the length of the summed index range.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+with open(os.path.join(GOLDEN, "manifest.json")) as f:
+    MANIFEST = json.load(f)
+
+
+def tol(level, k, A, B, alpha=1.0, beta=0.0, C0=None):
+    t = oracle.error_bound(level, max(k, 1), np.abs(A).max(), np.abs(B).max()) * max(abs(alpha), 1.0)
+    if beta != 0.0 and C0 is not None and C0.size:
+        t += 4 * 2.0 ** -53 * abs(beta) * np.abs(C0).max()
+    return t + 1e-300
+
+
+def to_dev(x, cuda):
+    import torch
+    # keep the numpy strides (column-major stays column-major)
+    out = torch.empty_strided(x.shape, [s // x.itemsize for s in x.strides], dtype=torch.float64, device=cuda)
+    out.copy_(torch.from_numpy(x))
+    return out
+
+
+def run_gpu(tsb, cuda, level, impl, alpha, A, ia, B, ib, beta, C0, ic):
+    import torch
+    dA, dB, dC = to_dev(A, cuda), to_dev(B, cuda), to_dev(C0, cuda)
+    tsb.contract(level, alpha, dA, ia, dB, ib, beta, dC, ic, impl=impl)
+    torch.cuda.synchronize()
+    return dC.cpu().numpy()
+
+
+def summed_len(ext, ic):
+    return int(np.prod([v for c, v in ext.items() if c not in ic])) if ext else 1
+
+
+@pytest.mark.parametrize("case", MANIFEST, ids=[c["name"] for c in MANIFEST])
+def test_golden_all_levels_and_impls(tsb, cuda, case):
+    d = np.load(os.path.join(GOLDEN, case["name"] + ".npz"))
+    A, B, C0 = (np.asfortranarray(d[x]) for x in ("A", "B", "C0"))
+    k = summed_len(case["extents"], case["idx_C"])
+    for level in (0, 1, 2):
+        for impl in ((1,) if level == 0 else (1, 2, 3)):
+            C = run_gpu(tsb, cuda, level, impl, case["alpha"], A, case["idx_A"], B, case["idx_B"],
+                        case["beta"], C0, case["idx_C"])
+            key = f"L{level}_impl{impl}" if level else "L0"
+            ref = d[key] if key in d.files else d["L0"]   # reference Strassen invalid -> judge against L=0
+            t = tol(level, k, A, B, case["alpha"], case["beta"], C0)
+            err = np.abs(C - ref).max()
+            assert err <= t, (key, err, t)
+
+
+def rand_case(seed):
+    rng = np.random.default_rng(seed)
+    labels = "abcdef"
+    ext = {c: int(rng.integers(3, 21)) for c in labels}
+    # I = {a, c}, J = {b, d}, P = {e, f}; random operand orders
+    ia = "".join(rng.permutation(list("acef")))
+    ib = "".join(rng.permutation(list("bdef")))
+    ic = "".join(rng.permutation(list("abcd")))
+    return ext, ia, ib, ic
+
+
+@pytest.mark.parametrize("seed", range(6))
+@pytest.mark.parametrize("level", [0, 1, 2])
+def test_random_4d_vs_oracle(tsb, cuda, seed, level):
+    ext, ia, ib, ic = rand_case(seed)
+    order = "F" if seed % 2 == 0 else "C"
+    A = oracle.uniform([ext[c] for c in ia], seed, order)
+    B = oracle.uniform([ext[c] for c in ib], seed + 50, order)
+    C0 = oracle.uniform([ext[c] for c in ic], seed + 99, order)
+    for alpha, beta in ((1.0, 1.0), (-2.0, 0.0), (0.5, 0.5)):
+        Co = C0.copy(order="K")
+        oracle.contract(alpha, A, ia, B, ib, beta, Co, ic)
+        for impl in ((1,) if level == 0 else (1, 2, 3)):
+            C = run_gpu(tsb, cuda, level, impl, alpha, A, ia, B, ib, beta, C0, ic)
+            t = tol(level, ext["e"] * ext["f"], A, B, alpha, beta, C0)
+            assert np.abs(C - Co).max() <= t, (impl, alpha, beta)
+
+
+@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (1, 7, 3), (5, 1, 9), (129, 130, 17), (257, 3, 300), (2, 2, 1)])
+@pytest.mark.parametrize("level", [0, 1, 2])
+def test_matrix_edges(tsb, cuda, m, n, k, level):
+    A = oracle.uniform((m, k), 1)
+    B = oracle.uniform((k, n), 2)
+    C0 = oracle.uniform((m, n), 3)
+    ref = 1.25 * (A @ B) + 0.75 * C0
+    for impl in ((1,) if level == 0 else (1, 2, 3)):
+        C = run_gpu(tsb, cuda, level, impl, 1.25, A, "ik", B, "kj", 0.75, C0, "ij")
+        assert np.abs(C - ref).max() <= tol(level, k, A, B, 1.25, 0.75, C0) + 1e-13
+
+
+def test_beta_zero_ignores_nan_in_c(tsb, cuda):
+    A = oracle.uniform((40, 30), 1)
+    B = oracle.uniform((30, 20), 2)
+    C0 = np.full((40, 20), np.nan)
+    for level in (0, 1, 2):
+        C = run_gpu(tsb, cuda, level, 1, 1.0, A, "ik", B, "kj", 0.0, C0, "ij")
+        assert np.isfinite(C).all()
+        assert np.abs(C - A @ B).max() < 1e-12
+
+
+def test_alpha_zero_and_empty_k(tsb, cuda):
+    A = oracle.uniform((6, 5), 1)
+    B = oracle.uniform((5, 4), 2)
+    C0 = oracle.uniform((6, 4), 3)
+    C = run_gpu(tsb, cuda, 1, 1, 0.0, A, "ik", B, "kj", 0.5, C0, "ij")
+    np.testing.assert_allclose(C, 0.5 * C0, rtol=0, atol=1e-15)
+    C = run_gpu(tsb, cuda, 1, 1, 0.0, A, "ik", B, "kj", 0.0, C0, "ij")
+    assert not C.any()
+    Ae = np.zeros((6, 0)); Be = np.zeros((0, 4))
+    C = run_gpu(tsb, cuda, 2, 1, 1.0, Ae, "ik", Be, "kj", 2.0, C0, "ij")
+    np.testing.assert_allclose(C, 2.0 * C0, rtol=0, atol=1e-15)
+
+
+def test_host_pointers_are_staged(tsb, cuda):
+    A = oracle.uniform((8, 8, 8, 8), 5)
+    B = oracle.uniform((8, 8, 8, 8), 6)
+    C = oracle.uniform((8, 8, 8, 8), 7)
+    Co = C.copy(order="F")
+    oracle.contract(1.0, A, "efac", B, "fbde", 1.0, Co, "abcd")
+    for level in (0, 1, 2):
+        Ch = C.copy(order="F")
+        tsb.contract(level, 1.0, A, "efac", B, "fbde", 1.0, Ch, "abcd", drop_in=True)
+        assert np.abs(Ch - Co).max() <= tol(level, 64, A, B, 1.0, 1.0, C)
+
+
+def test_strided_views_leave_gaps_untouched(tsb, cuda):
+    import torch
+    big = torch.full((20, 30), 7.0, dtype=torch.float64, device=cuda)
+    Cv = big[2:18:2, 3:27:3]          # 8 x 8 view with gaps
+    A = torch.rand(8, 5, dtype=torch.float64, device=cuda)
+    B = torch.rand(5, 8, dtype=torch.float64, device=cuda)
+    tsb.contract(1, 1.0, A, "ik", B, "kj", 0.0, Cv, "ij")
+    torch.cuda.synchronize()
+    assert torch.allclose(Cv, A @ B, atol=1e-13)
+    mask = torch.ones_like(big, dtype=torch.bool)
+    mask[2:18:2, 3:27:3] = False
+    assert bool((big[mask] == 7.0).all())
+
+
+def test_async_stream_entry_point(tsb, cuda):
+    import torch
+    s = torch.cuda.Stream()
+    A = torch.rand(300, 200, dtype=torch.float64, device=cuda)
+    B = torch.rand(200, 100, dtype=torch.float64, device=cuda)
+    C = torch.zeros(300, 100, dtype=torch.float64, device=cuda)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(s):
+        tsb.contract(1, 1.0, A, "ik", B, "kj", 0.0, C, "ij", stream=s)
+    s.synchronize()
+    assert torch.allclose(C, A @ B, atol=1e-12)
+
+
+def test_launch_counter_moves(tsb, cuda):
+    before = tsb.launch_count()
+    A = oracle.uniform((16, 16), 1)
+    run_gpu(tsb, cuda, 1, 1, 1.0, A, "ik", A, "kj", 0.0, A, "ij")
+    assert tsb.launch_count() == before + 1     # ABC: one persistent launch
+
+
+@pytest.mark.parametrize("level", [1, 2])
+def test_sampled_entries_at_config1_size(tsb, cuda, level):
+    """Config-1 pattern at extent 64 (NIm=NJn=NPk=4096): too large for the
+    oracle's loop, so 4096 sampled entries of C are checked against exact
+    dot products, and L vs L=0 on the GPU against the bound."""
+    import torch
+    e = 64
+    g = torch.Generator(device=cuda).manual_seed(0)
+    A = (torch.rand((e,) * 4, dtype=torch.float64, device=cuda, generator=g) * 2 - 1).permute(3, 2, 1, 0).contiguous().permute(3, 2, 1, 0)
+    B = (torch.rand((e,) * 4, dtype=torch.float64, device=cuda, generator=g) * 2 - 1).permute(3, 2, 1, 0).contiguous().permute(3, 2, 1, 0)
+    C0 = torch.zeros((e,) * 4, dtype=torch.float64, device=cuda).permute(3, 2, 1, 0).contiguous().permute(3, 2, 1, 0)
+    C0.zero_()
+    C1 = C0.clone(memory_format=torch.preserve_format)
+    tsb.contract(0, 1.0, A, "efac", B, "fbde", 0.0, C0, "abcd")
+    tsb.contract(level, 1.0, A, "efac", B, "fbde", 0.0, C1, "abcd")
+    torch.cuda.synchronize()
+    bound = oracle.error_bound(level, e * e, 1.0, 1.0)
+    assert float((C1 - C0).abs().max()) <= bound
+    rng = np.random.default_rng(1)
+    idx = rng.integers(0, e, size=(4096, 4))
+    An, Bn, Cn = A.cpu().numpy(), B.cpu().numpy(), C1.cpu().numpy()
+    for a, b, c, d in idx[:512]:
+        exact = np.sum(An[:, :, a, c] * Bn[:, b, d, :].T)
+        assert abs(Cn[a, b, c, d] - exact) <= bound
