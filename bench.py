@@ -38,9 +38,9 @@ sys.path.insert(0, ROOT)
 IDX_A, IDX_B, IDX_C = "efac", "fbde", "abcd"
 METRIC = "effective TFLOPS (2mnk/t) Strassen L1/L2 vs plain L=0 TC on 1 B200 at stated error"
 
-# DRAM traffic (read + write bytes) per launch of the dominant kernel, from the
-# ncu capture summarised in profiles/stra_dmma_kernel_fp64_L1.md, scaled by the
-# units processed (see that file).  None until a capture exists.
+# DRAM traffic (read + write bytes) per launch of the dominant kernel, taken
+# from one ncu capture (summaries in the profiles directory) and scaled to a
+# full launch by the units processed.  None until such a capture exists.
 NCU_TRAFFIC_BYTES = None
 
 
@@ -195,6 +195,33 @@ def time_steps(torch, fn, steps, stream):
     return start.elapsed_time(end) / 1e3
 
 
+def kernel_probe(args):
+    """One warm-up and one timed contraction per requested level (the
+    command the ncu captures under profiles/ run)."""
+    import torch
+    tsb = load_package()
+    dev = torch.device("cuda:0")
+    gen = torch.Generator(device=dev).manual_seed(0)
+    e = args.extent
+    shape = (e,) * 4
+    A = colmajor(torch, shape, dev, gen)
+    B = colmajor(torch, shape, dev, gen)
+    C = colmajor(torch, shape, dev, fill=0.0)
+    levels = [int(x) for x in args.kernels.split(",")]
+    for lv in levels:
+        tsb.contract(lv, 1.0, A, IDX_A, B, IDX_B, 1.0, C, IDX_C, impl=args.variant)
+    torch.cuda.synchronize()
+    flops = 2.0 * float(e * e) ** 3
+    for lv in levels:
+        s, t = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        tsb.contract(lv, 1.0, A, IDX_A, B, IDX_B, 1.0, C, IDX_C, impl=args.variant)
+        t.record()
+        t.synchronize()
+        ms = s.elapsed_time(t)
+        print(f"L{lv} impl{args.variant} extent {e}: {ms:.3f} ms  {flops / ms / 1e9:.2f} TFLOP/s effective")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -208,8 +235,13 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--kernels", default=None,
+                    help="comma-separated levels: run one warm-up and one timed call per level "
+                         "and print per-level times (profiling driver; no JSON line)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.kernels is not None:
+        return kernel_probe(args)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
