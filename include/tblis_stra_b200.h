@@ -172,6 +172,24 @@ int tblis_stra_plan_query(const tblis_tensor* A, const label_type* idx_A,
                           int64_t* ksA, int64_t* ksB,
                           int64_t* bA, int64_t* bB, int64_t* bC);
 
+/* Contraction that allocates no device memory (no counterpart in the
+ * reference, which allocates host workspace freely).  For callers that cannot
+ * call cudaMalloc: an application whose own pool has reserved the whole
+ * device, a host that forbids plug-ins from allocating device memory, or code
+ * that cannot afford cudaMalloc/cudaFree's implicit device synchronisation.
+ * Same arguments as tblis_stra_mult; always the ABC variant; A, B and C must
+ * be device memory (TBLIS_STRA_ERR_ARG otherwise); `stream` NULL = the legacy
+ * default stream.  The contraction's scatter vectors go into one static
+ * 2 MiB device array, so 2*m + 2*n + 2*k + 3*batch (the planned sizes) may not
+ * exceed 262144, else TBLIS_STRA_ERR_TOO_LARGE.  The first call on a device
+ * looks the array up (cudaGetSymbolAddress) and should come before any stream
+ * capture; calls whose work overlaps on the GPU share the array and race. */
+int tblis_stra_mult_noalloc(int level,
+                            const tblis_tensor* A, const label_type* idx_A,
+                            const tblis_tensor* B, const label_type* idx_B,
+                                  tblis_tensor* C, const label_type* idx_C,
+                            void* stream);
+
 /* Library version string. */
 const char* tblis_stra_version(void);
 
