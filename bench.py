@@ -207,6 +207,22 @@ def kernel_probe(args):
     A = colmajor(torch, shape, dev, gen)
     B = colmajor(torch, shape, dev, gen)
     C = colmajor(torch, shape, dev, fill=0.0)
+    if args.kernels == "dgemm":
+        # cuBLAS DGEMM at the same m = n = k, for side-by-side profiles
+        n = e * e
+        a = torch.rand(n, n, dtype=torch.float64, device=dev)
+        b = torch.rand(n, n, dtype=torch.float64, device=dev)
+        c = torch.empty(n, n, dtype=torch.float64, device=dev)
+        torch.matmul(a, b, out=c)
+        torch.cuda.synchronize()
+        s, t = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b, out=c)
+        t.record()
+        t.synchronize()
+        ms = s.elapsed_time(t)
+        print(f"cuBLAS DGEMM {n}^3: {ms:.3f} ms  {2.0 * n ** 3 / ms / 1e9:.2f} TFLOP/s")
+        return
     levels = [int(x) for x in args.kernels.split(",")]
     for lv in levels:
         tsb.contract(lv, 1.0, A, IDX_A, B, IDX_B, 1.0, C, IDX_C, impl=args.variant)
@@ -315,6 +331,7 @@ def main():
     if sampler:
         sampler.start()
     launches0 = tsb.launch_count()
+    tsb.set_kernel_timing(True)      # per-kernel CUDA events on the launch stream
     barrier_sync()
     t = time_steps(torch, step, args.steps, stream)
     barrier_sync()
@@ -323,6 +340,9 @@ def main():
     t = max_over_ranks(t)
     ms_per_step = t / args.steps * 1e3
     value = world * flops * args.steps / t / 1e12
+
+    kinds_snapshot = {k: tsb.kernel_timing(k) for k in ("fused", "pack", "packed_gemm", "aux")}
+    tsb.set_kernel_timing(False)
 
     # ---- same GPU, other levels (the plain L=0 kernel is the Strassen ratio's denominator)
     levels = {}
@@ -349,13 +369,24 @@ def main():
 
     # ---- roofline of the dominant kernel ------------------------------------
     peak = dgemm_peak(torch, device)
-    achieved = flops / (t / args.steps) / 1e12      # one launch per step (ABC)
+    kinds = kinds_snapshot
+    dom = max(kinds, key=lambda k: kinds[k][1])
+    n_launch, dom_ms = kinds[dom]
+    # Algorithmic work of one launch of the dominant kernel: the contraction's
+    # 2*NIm*NJn*NPk divided over the launches that carry it (one per Strassen
+    # product for the packed GEMM; one per contraction for the fused kernel).
+    per_launch_flops = flops * args.steps / max(n_launch, 1)
+    achieved = per_launch_flops / (dom_ms / max(n_launch, 1) / 1e3) / 1e12
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak,
                 "traffic": NCU_TRAFFIC_BYTES,
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
                 "executed_frac": achieved * (7.0 / 8.0) ** args.level / peak,
-                "kernel": "stra_dmma_kernel<%d,%d>" % ((1, 1) if args.level == 0 else (2, 2) if args.level == 1 else (4, 4))}
+                "kernel": {"fused": "stra_dmma_kernel", "pack": "pack_kernel",
+                           "packed_gemm": "packed_gemm_kernel", "aux": "aux"}[dom],
+                "launches_timed": n_launch, "kernel_ms_total": dom_ms,
+                "share_of_step": dom_ms / (t * 1e3),
+                "other_kernels_ms": {k: v[1] for k, v in kinds.items() if k != dom}}
 
     # ---- end to end through the C ABI with pinned host buffers --------------
     e2e = None

@@ -143,6 +143,17 @@ int tblis_stra_mult(int level,
 int tblis_stra_set_impl(int impl);
 int tblis_stra_get_impl(void);
 
+/* Device workspace (bytes) the ABC variant may use, per calling thread
+ * (default: unlimited).  Within the limit ABC packs the signed sums of each
+ * Strassen product into tile-ordered buffers (the reference's pack buffers,
+ * stra_pack_{two,four}_*, src/kernels/3m/gemm.hpp:504-816) and fuses the
+ * +-M update into the GEMM epilogue; with a limit below the needed
+ * 8*batch*(ceil(ms/128)+ceil(ns/128))*128*kpad bytes (0 included) it runs the
+ * fully fused kernel, which forms the sums inside the GEMM and allocates
+ * nothing beyond the scatter vectors. */
+int tblis_stra_set_workspace_limit(size_t bytes);
+size_t tblis_stra_get_workspace_limit(void);
+
 /* Status of the calling thread's last contraction call; string form. */
 int tblis_stra_last_status(void);
 const char* tblis_stra_status_string(int status);
@@ -189,6 +200,16 @@ int tblis_stra_mult_noalloc(int level,
                             const tblis_tensor* B, const label_type* idx_B,
                                   tblis_tensor* C, const label_type* idx_C,
                             void* stream);
+
+/* Per-kernel timing for profiling (no counterpart in the reference, which
+ * times whole calls with omp_get_wtime, test/test_strassen.cxx:74-95).  With
+ * timing on, every kernel launch is bracketed by CUDA events on its stream;
+ * tblis_stra_kernel_timing() waits for them and returns, for one kernel kind
+ * (0 fused DMMA, 1 pack, 2 packed DMMA GEMM, 3 elementwise helpers), the number
+ * of launches and their summed time since timing was (re)enabled.
+ * tblis_stra_set_kernel_timing() also clears the records. */
+int tblis_stra_set_kernel_timing(int on);
+int tblis_stra_kernel_timing(int kind, unsigned long long* launches, double* total_ms);
 
 /* Library version string. */
 const char* tblis_stra_version(void);

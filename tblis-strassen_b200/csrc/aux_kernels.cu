@@ -16,6 +16,7 @@
 // fastest; the scatter vectors make the access pattern coalesced whenever the
 // fastest C (or X) mode is the column bundle's first mode.
 #include "kernels.cuh"
+#include "timing.hpp"
 
 #include <atomic>
 
@@ -108,7 +109,9 @@ cudaError_t launch_scale(const ScaleArgs& a, cudaStream_t stream)
 {
     const int64_t total = a.batch * a.m * a.n;
     if (total <= 0) return cudaSuccess;
+    timing_begin(KK_AUX, stream);
     scale_kernel<<<grid_for(total), THREADS, 0, stream>>>(a);
+    timing_end(KK_AUX, stream);
     cudaError_t err = cudaGetLastError();
     if (err == cudaSuccess) g_launches++;
     return err;
@@ -118,7 +121,9 @@ cudaError_t launch_sum_gather(const SumGatherArgs& a, cudaStream_t stream)
 {
     const int64_t total = a.batch * a.rows * a.cols;
     if (total <= 0) return cudaSuccess;
+    timing_begin(KK_AUX, stream);
     sum_gather_kernel<<<grid_for(total), THREADS, 0, stream>>>(a);
+    timing_end(KK_AUX, stream);
     cudaError_t err = cudaGetLastError();
     if (err == cudaSuccess) g_launches++;
     return err;
@@ -128,7 +133,9 @@ cudaError_t launch_scatter_add(const ScatterAddArgs& a, cudaStream_t stream)
 {
     const int64_t total = a.batch * a.ms * a.ns;
     if (total <= 0) return cudaSuccess;
+    timing_begin(KK_AUX, stream);
     scatter_add_kernel<<<grid_for(total), THREADS, 0, stream>>>(a);
+    timing_end(KK_AUX, stream);
     cudaError_t err = cudaGetLastError();
     if (err == cudaSuccess) g_launches++;
     return err;

@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <cstring>
 #include <list>
 #include <map>
@@ -40,6 +41,7 @@ namespace {
 thread_local int t_impl = 1;
 thread_local cudaStream_t t_stream = nullptr;
 thread_local int t_status = TBLIS_STRA_SUCCESS;
+thread_local size_t t_ws_limit = SIZE_MAX;   // device workspace the ABC schedule may use
 unsigned g_num_threads = 1;
 
 // ---- device tables (cached) ------------------------------------------------
@@ -150,7 +152,30 @@ bool is_device_ptr(const void* p)
     return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
 }
 
-// Stream-ordered device scratch (AB / Naive temporaries, staging).
+// The library's own stream-ordered memory pool per device.  Its release
+// threshold is unlimited, so memory freed by one call is reused by the next
+// without returning to the driver at every synchronisation.
+cudaMemPool_t library_pool(int device)
+{
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = pools.find(device);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+    uint64_t threshold = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+    pools[device] = pool;
+    return pool;
+}
+
+// Stream-ordered device scratch (packed operands, AB / Naive temporaries, staging).
 struct Scratch
 {
     void* p = nullptr;
@@ -160,7 +185,12 @@ struct Scratch
     {
         s = st;
         if (bytes == 0) bytes = 16;
-        return cudaMallocAsync(&p, bytes, st) == cudaSuccess ? TBLIS_STRA_SUCCESS : TBLIS_STRA_ERR_ALLOC;
+        int device = 0;
+        if (cudaGetDevice(&device) != cudaSuccess) { cudaGetLastError(); return TBLIS_STRA_ERR_NO_DEVICE; }
+        cudaMemPool_t pool = library_pool(device);
+        cudaError_t e = pool ? cudaMallocFromPoolAsync(&p, bytes, pool, st) : cudaMallocAsync(&p, bytes, st);
+        if (e != cudaSuccess) { cudaGetLastError(); p = nullptr; return TBLIS_STRA_ERR_ALLOC; }
+        return TBLIS_STRA_SUCCESS;
     }
 };
 
@@ -237,6 +267,53 @@ void set_grid(DmmaArgs& a, int64_t ms, int64_t ns, int64_t ks)
     a.work = a.batch * (int64_t)a.tiles_m * a.tiles_n;
 }
 
+// Packed schedule of the ABC variant (see packed_kernels.cu).  S and T are
+// reused for every product, in stream order.
+int run_fp64_packed(const ProductTable& tab, const GemmView& g, const DevPlan& t,
+                    const double* A, const double* B, double* C, cudaStream_t st, int sms,
+                    int64_t ms, int64_t ns, int64_t ks, int64_t k_pad, int64_t tm, int64_t tn)
+{
+    Scratch Sbuf, Tbuf;
+    int s;
+    if ((s = Sbuf.alloc((size_t)(g.batch * tm * k_pad * PACK_TILE) * sizeof(double), st))) return s;
+    if ((s = Tbuf.alloc((size_t)(g.batch * tn * k_pad * PACK_TILE) * sizeof(double), st))) return s;
+    double* S = static_cast<double*>(Sbuf.p);
+    double* T = static_cast<double*>(Tbuf.p);
+    const bool a_kfast = g.unit_ksA != 0 && (g.unit_rsA == 0 || g.unit_ksA < g.unit_rsA);
+    const bool b_kfast = g.unit_ksB != 0 && (g.unit_csB == 0 || g.unit_ksB < g.unit_csB);
+    for (const Product& pr : tab.prod)
+    {
+        PackArgs pa{};
+        pa.X = A; pa.rs = t.rsA; pa.ks = t.ksA; pa.bX = t.bA;
+        pa.rows_full = g.m; pa.k_full = g.k; pa.rows_blk = ms; pa.k_blk = ks;
+        pa.nt = pr.na;
+        for (int i = 0; i < pr.na; i++) { pa.t_r[i] = pr.a[i].r; pa.t_c[i] = pr.a[i].c; pa.t_s[i] = pr.a[i].sign; }
+        pa.tiles = tm; pa.k_pad = k_pad; pa.batch = g.batch; pa.kfast = a_kfast; pa.out = S;
+        TSB_CUDA(launch_pack(pa, st));
+        PackArgs pb{};
+        pb.X = B; pb.rs = t.csB; pb.ks = t.ksB; pb.bX = t.bB;
+        pb.rows_full = g.n; pb.k_full = g.k; pb.rows_blk = ns; pb.k_blk = ks;
+        pb.nt = pr.nb;
+        for (int i = 0; i < pr.nb; i++) { pb.t_r[i] = pr.b[i].c; pb.t_c[i] = pr.b[i].r; pb.t_s[i] = pr.b[i].sign; }
+        pb.tiles = tn; pb.k_pad = k_pad; pb.batch = g.batch; pb.kfast = b_kfast; pb.out = T;
+        TSB_CUDA(launch_pack(pb, st));
+        PackedGemmArgs ga{};
+        ga.S = S; ga.T = T; ga.C = C;
+        ga.rsC = t.rsC; ga.csC = t.csC; ga.bC = t.bC;
+        ga.m = g.m; ga.n = g.n; ga.ms = ms; ga.ns = ns; ga.k_pad = k_pad;
+        ga.tiles_m = tm; ga.tiles_n = tn; ga.batch = g.batch;
+        ga.alpha = g.alpha; ga.beta = g.beta;
+        ga.nc = pr.nc;
+        for (int q = 0; q < pr.nc; q++)
+        {
+            ga.c_r[q] = pr.c[q].r; ga.c_c[q] = pr.c[q].c; ga.c_s[q] = pr.c[q].sign;
+            ga.c_first[q] = pr.c_first[q];
+        }
+        TSB_CUDA(launch_packed_gemm(ga, st, sms));
+    }
+    return TBLIS_STRA_SUCCESS;
+}
+
 int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
              const double* A, const double* B, double* C, cudaStream_t st, int device)
 {
@@ -254,6 +331,14 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
 
     if (level == 0 || impl == 1)
     {
+        // Packed schedule (per product: pack the operand sums, GEMM with the
+        // +-M update in its epilogue) when its workspace is allowed; else the
+        // fully fused kernel, which needs none.
+        const int64_t k_pad = cdiv(ks, PACK_KSTEP) * PACK_KSTEP;
+        const int64_t tm = cdiv(ms, PACK_TILE), tn = cdiv(ns, PACK_TILE);
+        const size_t ws = (size_t)(g.batch * (tm + tn) * k_pad * PACK_TILE) * sizeof(double);
+        if (ws <= t_ws_limit && g.batch * tm <= 65535 && g.batch * tn <= 65535)
+            return run_fp64_packed(tab, g, t, A, B, C, st, sms, ms, ns, ks, k_pad, tm, tn);
         DmmaArgs a = base_args(g, t, A, B, C);
         set_grid(a, ms, ns, ks);
         a.nprod = (int)tab.prod.size();
@@ -457,6 +542,14 @@ int tblis_stra_set_impl(int impl)
 }
 
 int tblis_stra_get_impl(void) { return tsb::t_impl; }
+
+int tblis_stra_set_workspace_limit(size_t bytes)
+{
+    tsb::t_ws_limit = bytes;
+    return TBLIS_STRA_SUCCESS;
+}
+
+size_t tblis_stra_get_workspace_limit(void) { return tsb::t_ws_limit; }
 
 int tblis_stra_last_status(void) { return tsb::t_status; }
 

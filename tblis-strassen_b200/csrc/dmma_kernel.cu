@@ -16,24 +16,23 @@
 //     so C blocks shared by several products need no atomics and no barrier,
 //     and beta is applied exactly once (by the first product touching a block).
 //
-// Tile: 128 x 128 per CTA, k-step 8, 8 warps as 2 (m) x 4 (n), 64 x 32 per warp
-// (4 x 4 m16n8k4 fragments).  A persistent grid walks (batch, tile) work items.
+// Tile shapes are template parameters (BM x BN per CTA, k-step BK, WM x WN
+// warps each owning a (BM/WM) x (BN/WN) tile of m16n8k4 fragments, STAGES deep
+// cp.async ring).  Shared-memory tiles are stored k-major, rows g and g+8 of
+// each 16-row group (columns for B) adjacent and swizzled per k (tile_pos), so
+// every fragment pair a thread needs is one 128-bit load and both the loads and
+// the cp.async writes are free of bank conflicts.
+// A persistent grid walks (batch, tile) work items.
 #include "kernels.cuh"
+#include "tile_layout.cuh"
+#include "timing.hpp"
 
 #include <atomic>
+#include <cstdlib>
 
 namespace tsb {
 
 namespace {
-
-constexpr int BM = 128;
-constexpr int BN = 128;
-constexpr int BK = 8;
-constexpr int NT = 256;
-constexpr int PAD = 4;            // doubles; row pitch 132*8 B = 32 mod 128 B: conflict-free fragments
-constexpr int LDA = BM + PAD;
-constexpr int LDB = BN + PAD;
-constexpr int HMAX = 4;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
 {
@@ -43,7 +42,7 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p)
 __device__ __forceinline__ void cp_async8(uint32_t dst, const void* src, int src_bytes)
 {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n"
-                 :: "r"(dst), "l"(src), "r"(src_bytes) : "memory");
+                 :: "r"(dst), "l"(src), "r"(src_bytes));
 }
 
 __device__ __forceinline__ void cp_async_commit()
@@ -59,51 +58,79 @@ __device__ __forceinline__ void cp_async_wait()
 
 __device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, double b0)
 {
-    asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 "
+    asm("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 "
                  "{%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
                  : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
                  : "d"(a0), "d"(a1), "d"(b0));
 }
 
-// Flip the sign of x when mask has the sign bit set (integer op, no FP64 multiply).
-__device__ __forceinline__ double apply_sign(double x, long long mask)
+template <int BM_, int BN_, int BK_, int WM_, int WN_, int STAGES_, int NA_, int NB_, int MINB_, int HM_>
+struct Cfg
 {
-    return __longlong_as_double(__double_as_longlong(x) ^ mask);
-}
-
-template <int NA, int NB, int STAGES>
-struct Smem
-{
-    static constexpr int R = STAGES + 1;   // ring of per-stage k offset tables
+    static constexpr int BM = BM_, BN = BN_, BK = BK_, WM = WM_, WN = WN_;
+    static constexpr int STAGES = STAGES_, NA = NA_, NB = NB_, MINB = MINB_;
+    static constexpr int HMAX = HM_;                       // largest block grid side H
+    static constexpr int NT = 32 * WM * WN;
+    static constexpr int WTM = BM / WM, WTN = BN / WN;     // warp tile
+    static constexpr int MI = WTM / 16, NI = WTN / 8;      // fragments per warp
+    static constexpr int LDA = BM, LDB = BN;               // rows 128-byte aligned (swizzled)
+    static constexpr int R = STAGES + 1;                   // k-offset table ring
     static constexpr size_t a_bytes = size_t(STAGES) * NA * BK * LDA * 8;
     static constexpr size_t b_bytes = size_t(STAGES) * NB * BK * LDB * 8;
     static constexpr size_t tab_bytes = size_t(HMAX) * (BM + BM + BN + BN) * 8;
     static constexpr size_t k_bytes = size_t(R) * HMAX * BK * 8 * 2;
-    static constexpr size_t total = a_bytes + b_bytes + tab_bytes + k_bytes;
+    static constexpr size_t smem = a_bytes + b_bytes + tab_bytes + k_bytes;
+    static_assert(WTM % 16 == 0 && WTN % 16 == 0, "warp tile must hold whole fragment pairs");
+    static_assert(BK % 8 == 0, "k-step is a multiple of 8 (loader lane map)");
+    static_assert(BM % 16 == 0 && BN % 16 == 0, "tiles are whole 16-row groups");
+    static_assert(2 * HMAX * BK <= NT, "one thread per k-table entry");
+    static_assert((BK * BM) % NT == 0 && (BK * BN) % NT == 0, "loader covers the tile");
 };
 
-template <int NA, int NB, int STAGES>
-__global__ void __launch_bounds__(NT, 1)
+// Loader lane maps: element e (= thread + x * threads) of a BK x BM tile.
+// k-fast: half-warps take 8 consecutive k of rows (m, m+8); row-fast: 16
+// consecutive rows of one k.
+template <int BK, int BM>
+__device__ __forceinline__ void lane_map(bool kfast, int e, int& kk, int& m)
+{
+    if (kfast)
+    {
+        kk = (e & 7) + 8 * ((e >> 4) % (BK / 8));
+        const int ridx = 2 * (e / (16 * (BK / 8))) + ((e >> 3) & 1);
+        m = (ridx & ~15) | ((ridx & 1) << 3) | ((ridx >> 1) & 7);
+    }
+    else
+    {
+        m = e % BM;
+        kk = e / BM;
+    }
+}
+
+template <class K, bool KA, bool KB>
+__global__ void __launch_bounds__(K::NT, K::MINB)
 stra_dmma_kernel(const __grid_constant__ DmmaArgs args)
 {
-    using S = Smem<NA, NB, STAGES>;
+    constexpr int BM = K::BM, BN = K::BN, BK = K::BK, NT = K::NT;
+    constexpr int NA = K::NA, NB = K::NB, STAGES = K::STAGES, R = K::R;
+    constexpr int LDA = K::LDA, LDB = K::LDB, MI = K::MI, NI = K::NI;
+    constexpr int HMAX = K::HMAX;
     extern __shared__ __align__(128) unsigned char smem[];
     double* As = reinterpret_cast<double*>(smem);
-    double* Bs = reinterpret_cast<double*>(smem + S::a_bytes);
-    int64_t* rowA = reinterpret_cast<int64_t*>(smem + S::a_bytes + S::b_bytes);
+    double* Bs = reinterpret_cast<double*>(smem + K::a_bytes);
+    int64_t* rowA = reinterpret_cast<int64_t*>(smem + K::a_bytes + K::b_bytes);
     int64_t* rowC = rowA + HMAX * BM;
     int64_t* colB = rowC + HMAX * BM;
     int64_t* colC = colB + HMAX * BN;
     int64_t* kA = colC + HMAX * BN;           // [R][HMAX][BK]
-    int64_t* kB = kA + S::R * HMAX * BK;      // [R][HMAX][BK]
+    int64_t* kB = kA + R * HMAX * BK;         // [R][HMAX][BK]
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
     const int g = lane >> 2;         // groupID
     const int t4 = lane & 3;         // threadID_in_group
-    const int wm = (warp >> 2) * 64; // 2 warps along m
-    const int wn = (warp & 3) * 32;  // 4 warps along n
+    const int wm = (warp / K::WN) * K::WTM;
+    const int wn = (warp % K::WN) * K::WTN;
 
     const int64_t tiles = (int64_t)args.tiles_m * args.tiles_n;
     const int64_t nk = (args.ks + BK - 1) / BK;
@@ -146,80 +173,102 @@ stra_dmma_kernel(const __grid_constant__ DmmaArgs args)
             const DevProduct& P = args.prod[p];
             const int na = P.na, nb = P.nb;
 
-            // k offset table of one stage: kX[slot][h][kk] for every k part h.
-            auto load_ktab = [&](int64_t stage, int64_t& va, int64_t& vb, int& sl, int& idx) {
-                // thread tid < HMAX*BK fills A entry, tid in [HMAX*BK, 2*HMAX*BK) fills B.
+            // k offset table of one stage: kX[slot][h][kk] for every k part h;
+            // threads [0, HMAX*BK) fill A entries, [HMAX*BK, 2*HMAX*BK) B entries.
+            auto load_ktab = [&](int64_t stage, int64_t& v) {
                 const int e = tid % (HMAX * BK);
                 const int h = e / BK, kk = e % BK;
                 const int64_t kl = stage * BK + kk, gk = h * args.ks + kl;
                 const bool ok = (h < H && kl < args.ks && gk < args.k);
-                sl = (int)(stage % S::R);
-                idx = e;
-                if (tid < HMAX * BK)       va = ok ? args.ksA[gk] : OFF_INVALID;
-                else if (tid < 2 * HMAX * BK) vb = ok ? args.ksB[gk] : OFF_INVALID;
+                v = OFF_INVALID;
+                if (ok)
+                {
+                    if (tid < HMAX * BK) v = args.ksA[gk];
+                    else if (tid < 2 * HMAX * BK) v = args.ksB[gk];
+                }
             };
-            auto store_ktab = [&](int sl, int idx, int64_t va, int64_t vb) {
-                if (tid < HMAX * BK)           kA[sl * HMAX * BK + idx] = va;
-                else if (tid < 2 * HMAX * BK)  kB[sl * HMAX * BK + idx] = vb;
+            auto store_ktab = [&](int64_t stage, int64_t v) {
+                const int sl = (int)(stage % R);
+                if (tid < HMAX * BK)           kA[sl * HMAX * BK + tid] = v;
+                else if (tid < 2 * HMAX * BK)  kB[sl * HMAX * BK + tid - HMAX * BK] = v;
             };
 
-            // Issue the cp.async gathers of one stage (all A and B terms).
-            auto issue_stage = [&](int64_t stage) {
-                const int buf = (int)(stage % STAGES);
-                const int sl = (int)(stage % S::R);
-                const int64_t* kAs = kA + sl * HMAX * BK;
-                const int64_t* kBs = kB + sl * HMAX * BK;
+            // Loader.  Element x of A term i lands on tile (row r, k kk); with
+            // KA consecutive threads walk k (coalesced when A is contiguous
+            // along k), otherwise rows.  B likewise with KB.
+            constexpr int EA = BK * BM / NT;        // A elements per thread per term
+            constexpr int EB = BK * BN / NT;
+            constexpr int EPS = NA * EA + NB * EB;  // elements per thread per stage
+            constexpr int Q = BK / 4;               // k4 steps per stage
+            constexpr int CH = (EPS + Q - 1) / Q;   // loader elements per k4 step
+            uint32_t rA[NA], rB[NB];                // row/col table of each term (smem)
+            int kofA[NA], kofB[NB];                 // its k part (offset into a k table)
+            uint32_t dA[NA], dB[NB];                // its tile in stage buffer 0 (smem)
 #pragma unroll
-                for (int i = 0; i < NA; i++)
+            for (int i = 0; i < NA; i++)
+            {
+                rA[i] = smem_u32(rowA + (i < na ? P.a_r[i] : 0) * BM);
+                kofA[i] = (i < na ? P.a_c[i] : 0) * BK;
+                dA[i] = smem_u32(As + (size_t)i * BK * LDA);
+            }
+#pragma unroll
+            for (int j = 0; j < NB; j++)
+            {
+                rB[j] = smem_u32(colB + (j < nb ? P.b_c[j] : 0) * BN);
+                kofB[j] = (j < nb ? P.b_r[j] : 0) * BK;
+                dB[j] = smem_u32(Bs + (size_t)j * BK * LDB);
+            }
+            auto lds64 = [](uint32_t addr) {
+                int64_t v;
+                asm volatile("ld.shared.s64 %0, [%1];\n" : "=l"(v) : "r"(addr));
+                return v;
+            };
+            auto issue_elem = [&](int j, int buf, const int64_t* kAs, const int64_t* kBs) {
+                if (j < NA * EA)
                 {
+                    const int i = j / EA, x = j % EA;
                     if (i < na)
                     {
-                        const int64_t* rtab = rowA + P.a_r[i] * BM;
-                        const int64_t* ktab = kAs + P.a_c[i] * BK;
-                        double* dst = As + ((size_t)buf * NA + i) * BK * LDA;
-#pragma unroll
-                        for (int x = 0; x < BK * BM / NT; x++)
-                        {
-                            const int e = tid + x * NT;
-                            const int r = args.a_kfast ? e / BK : e % BM;
-                            const int kk = args.a_kfast ? e % BK : e / BM;
-                            const int64_t ro = rtab[r], ko = ktab[kk];
-                            const bool ok = (ro != OFF_INVALID) && (ko != OFF_INVALID);
-                            const double* src = ok ? args.A + ro + ko : args.A;
-                            cp_async8(smem_u32(dst + kk * LDA + r), src, ok ? 8 : 0);
-                        }
+                        int kk, r;
+                        lane_map<BK, BM>(KA, tid + x * NT, kk, r);
+                        const int64_t ro = lds64(rA[i] + r * 8);
+                        const int64_t ko = kAs[kofA[i] + kk];
+                        const bool ok = (ro != OFF_INVALID) & (ko != OFF_INVALID);
+                        const uint32_t dst = dA[i] + (uint32_t)(buf * NA * BK * LDA + tile_pos(kk, r, LDA)) * 8;
+                        cp_async8(dst, ok ? args.A + (ro + ko) : args.A, ok ? 8 : 0);
                     }
                 }
-#pragma unroll
-                for (int j = 0; j < NB; j++)
+                else
                 {
-                    if (j < nb)
+                    const int jj = j - NA * EA;
+                    const int i = jj / EB, x = jj % EB;
+                    if (i < nb)
                     {
-                        const int64_t* ctab = colB + P.b_c[j] * BN;
-                        const int64_t* ktab = kBs + P.b_r[j] * BK;
-                        double* dst = Bs + ((size_t)buf * NB + j) * BK * LDB;
-#pragma unroll
-                        for (int x = 0; x < BK * BN / NT; x++)
-                        {
-                            const int e = tid + x * NT;
-                            const int c = args.b_kfast ? e / BK : e % BN;
-                            const int kk = args.b_kfast ? e % BK : e / BN;
-                            const int64_t co = ctab[c], ko = ktab[kk];
-                            const bool ok = (co != OFF_INVALID) && (ko != OFF_INVALID);
-                            const double* src = ok ? args.B + ko + co : args.B;
-                            cp_async8(smem_u32(dst + kk * LDB + c), src, ok ? 8 : 0);
-                        }
+                        int kk, c;
+                        lane_map<BK, BN>(KB, tid + x * NT, kk, c);
+                        const int64_t co = lds64(rB[i] + c * 8);
+                        const int64_t ko = kBs[kofB[i] + kk];
+                        const bool ok = (co != OFF_INVALID) & (ko != OFF_INVALID);
+                        const uint32_t dst = dB[i] + (uint32_t)(buf * NB * BK * LDB + tile_pos(kk, c, LDB)) * 8;
+                        cp_async8(dst, ok ? args.B + (ko + co) : args.B, ok ? 8 : 0);
                     }
                 }
+            };
+            auto issue_stage = [&](int64_t stage) {
+                const int buf = (int)(stage % STAGES);
+                const int sl = (int)(stage % R);
+#pragma unroll
+                for (int j = 0; j < EPS; j++)
+                    issue_elem(j, buf, kA + sl * HMAX * BK, kB + sl * HMAX * BK);
             };
 
             __syncthreads();   // previous product's last stage fully consumed
             // Prologue: k tables for stages 0..STAGES-1, then data for 0..STAGES-2.
             for (int64_t s = 0; s < STAGES; s++)
             {
-                int64_t va = 0, vb = 0; int sl = 0, idx = 0;
-                load_ktab(s, va, vb, sl, idx);
-                store_ktab(sl, idx, va, vb);
+                int64_t v;
+                load_ktab(s, v);
+                store_ktab(s, v);
             }
             __syncthreads();
             for (int64_t s = 0; s < STAGES - 1; s++)
@@ -228,81 +277,108 @@ stra_dmma_kernel(const __grid_constant__ DmmaArgs args)
                 cp_async_commit();
             }
 
-            double acc[4][4][4];
+            double acc[MI][NI][4];
 #pragma unroll
-            for (int mi = 0; mi < 4; mi++)
+            for (int mi = 0; mi < MI; mi++)
 #pragma unroll
-                for (int ni = 0; ni < 4; ni++)
+                for (int ni = 0; ni < NI; ni++)
 #pragma unroll
                     for (int e = 0; e < 4; e++) acc[mi][ni][e] = 0.0;
 
-            long long sa[NA], sb[NB];
+            // Each operand sum is formed as x_0 + sum_i rel_i * x_i with
+            // rel_i = sign_i * sign_0 in {+1, -1} (one exact FMA per term);
+            // sign_0 of A and B moves into the C coefficient.
+            double ra[NA], rb[NB];
 #pragma unroll
-            for (int i = 0; i < NA; i++) sa[i] = (i < na && P.a_s[i] < 0) ? (long long)0x8000000000000000ull : 0ll;
+            for (int i = 0; i < NA; i++) ra[i] = (i < na && P.a_s[i] * P.a_s[0] < 0) ? -1.0 : 1.0;
 #pragma unroll
-            for (int j = 0; j < NB; j++) sb[j] = (j < nb && P.b_s[j] < 0) ? (long long)0x8000000000000000ull : 0ll;
+            for (int j = 0; j < NB; j++) rb[j] = (j < nb && P.b_s[j] * P.b_s[0] < 0) ? -1.0 : 1.0;
+            const bool lead_neg = (P.a_s[0] * P.b_s[0]) < 0;
+
+            // Fragments of one k4 step: signed sums over the terms, read as
+            // 128-bit pairs from the permuted layouts.
+            auto load_frags = [&](const double* Ab, const double* Bb, int k4,
+                                  double (&af)[MI][2], double (&bf)[NI]) {
+                const int kr = k4 + t4;
+                const int pg = 2 * ((g + swz_c(kr)) & 7);   // swizzled pair of rows g, g+8
+#pragma unroll
+                for (int mi = 0; mi < MI; mi++)
+                {
+                    const int pos = kr * LDA + wm + mi * 16 + pg;
+                    double2 v = *reinterpret_cast<const double2*>(Ab + pos);
+                    double x0 = v.x, x1 = v.y;
+#pragma unroll
+                    for (int i = 1; i < NA; i++)
+                    {
+                        if (i < na)
+                        {
+                            double2 u = *reinterpret_cast<const double2*>(Ab + (size_t)i * BK * LDA + pos);
+                            x0 = fma(ra[i], u.x, x0);
+                            x1 = fma(ra[i], u.y, x1);
+                        }
+                    }
+                    af[mi][0] = x0; af[mi][1] = x1;
+                }
+#pragma unroll
+                for (int nj = 0; nj < NI / 2; nj++)
+                {
+                    const int pos = kr * LDB + wn + nj * 16 + pg;
+                    double2 v = *reinterpret_cast<const double2*>(Bb + pos);
+                    double y0 = v.x, y1 = v.y;
+#pragma unroll
+                    for (int j = 1; j < NB; j++)
+                    {
+                        if (j < nb)
+                        {
+                            double2 u = *reinterpret_cast<const double2*>(Bb + (size_t)j * BK * LDB + pos);
+                            y0 = fma(rb[j], u.x, y0);
+                            y1 = fma(rb[j], u.y, y1);
+                        }
+                    }
+                    bf[2 * nj] = y0; bf[2 * nj + 1] = y1;
+                }
+            };
 
             for (int64_t s = 0; s < nk; s++)
             {
                 cp_async_wait<STAGES - 2>();
                 __syncthreads();
-                // Refill: data of stage s+STAGES-1 (its k table is ready), and
-                // fetch the k table of stage s+STAGES into registers.
+                // This stage refills buffer (s+STAGES-1) % STAGES, whose k table
+                // is ready, spread over the k4 steps between the DMMA batches;
+                // the k table of stage s+STAGES is fetched into a register.
                 const int64_t sn = s + STAGES - 1;
-                if (sn < nk) issue_stage(sn);
-                cp_async_commit();
-                int64_t va = 0, vb = 0; int sl = 0, idx = 0;
-                load_ktab(s + STAGES, va, vb, sl, idx);
+                const bool refill = sn < nk;
+                const int nbuf = (int)(sn % STAGES);
+                const int nsl = (int)(sn % R);
+                const int64_t* kAs = kA + nsl * HMAX * BK;
+                const int64_t* kBs = kB + nsl * HMAX * BK;
+                int64_t kv;
+                load_ktab(s + STAGES, kv);
 
                 const int buf = (int)(s % STAGES);
                 const double* Ab = As + (size_t)buf * NA * BK * LDA;
                 const double* Bb = Bs + (size_t)buf * NB * BK * LDB;
+                double af[2][MI][2], bf[2][NI];
+                load_frags(Ab, Bb, 0, af[0], bf[0]);
 #pragma unroll
-                for (int k4 = 0; k4 < BK; k4 += 4)
+                for (int q = 0; q < Q; q++)
                 {
-                    double af[4][2], bf[4];
-                    const int kr = k4 + t4;
+                    const int cur = q & 1;
+                    if (q + 1 < Q) load_frags(Ab, Bb, (q + 1) * 4, af[cur ^ 1], bf[cur ^ 1]);
 #pragma unroll
-                    for (int mi = 0; mi < 4; mi++)
+                    for (int mi = 0; mi < MI; mi++)
+#pragma unroll
+                        for (int ni = 0; ni < NI; ni++)
+                            dmma(acc[mi][ni], af[cur][mi][0], af[cur][mi][1], bf[cur][ni]);
+                    if (refill)
                     {
-                        const int r0 = wm + mi * 16 + g;
-                        double x0 = apply_sign(Ab[kr * LDA + r0], sa[0]);
-                        double x1 = apply_sign(Ab[kr * LDA + r0 + 8], sa[0]);
 #pragma unroll
-                        for (int i = 1; i < NA; i++)
-                        {
-                            if (i < na)
-                            {
-                                const double* Ai = Ab + (size_t)i * BK * LDA;
-                                x0 += apply_sign(Ai[kr * LDA + r0], sa[i]);
-                                x1 += apply_sign(Ai[kr * LDA + r0 + 8], sa[i]);
-                            }
-                        }
-                        af[mi][0] = x0; af[mi][1] = x1;
+                        for (int c = 0; c < CH; c++)
+                            if (q * CH + c < EPS) issue_elem(q * CH + c, nbuf, kAs, kBs);
                     }
-#pragma unroll
-                    for (int ni = 0; ni < 4; ni++)
-                    {
-                        const int c0 = wn + ni * 8 + g;
-                        double y = apply_sign(Bb[kr * LDB + c0], sb[0]);
-#pragma unroll
-                        for (int j = 1; j < NB; j++)
-                        {
-                            if (j < nb)
-                            {
-                                const double* Bj = Bb + (size_t)j * BK * LDB;
-                                y += apply_sign(Bj[kr * LDB + c0], sb[j]);
-                            }
-                        }
-                        bf[ni] = y;
-                    }
-#pragma unroll
-                    for (int mi = 0; mi < 4; mi++)
-#pragma unroll
-                        for (int ni = 0; ni < 4; ni++)
-                            dmma(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
                 }
-                store_ktab(sl, idx, va, vb);
+                cp_async_commit();
+                store_ktab(s + STAGES, kv);
             }
             cp_async_wait<0>();
 
@@ -311,11 +387,11 @@ stra_dmma_kernel(const __grid_constant__ DmmaArgs args)
             {
                 const int64_t* rt = rowC + P.c_r[q] * BM;
                 const int64_t* ct = colC + P.c_c[q] * BN;
-                const double coef = P.c_s[q] < 0 ? -args.alpha : args.alpha;
+                const double coef = ((P.c_s[q] < 0) != lead_neg) ? -args.alpha : args.alpha;
                 const bool first = P.c_first[q] != 0;
                 const double beta = args.beta;
 #pragma unroll
-                for (int mi = 0; mi < 4; mi++)
+                for (int mi = 0; mi < MI; mi++)
                 {
 #pragma unroll
                     for (int hr = 0; hr < 2; hr++)
@@ -323,7 +399,7 @@ stra_dmma_kernel(const __grid_constant__ DmmaArgs args)
                         const int64_t ro = rt[wm + mi * 16 + g + hr * 8];
                         if (ro == OFF_INVALID) continue;
 #pragma unroll
-                        for (int ni = 0; ni < 4; ni++)
+                        for (int ni = 0; ni < NI; ni++)
                         {
 #pragma unroll
                             for (int hc = 0; hc < 2; hc++)
@@ -344,19 +420,48 @@ stra_dmma_kernel(const __grid_constant__ DmmaArgs args)
     }
 }
 
-template <int NA, int NB, int STAGES>
-cudaError_t launch_instance(const DmmaArgs& args, cudaStream_t stream, int num_sms)
+template <class K>
+cudaError_t launch_cfg(const DmmaArgs& in, cudaStream_t stream, int num_sms)
 {
-    using S = Smem<NA, NB, STAGES>;
-    auto kern = stra_dmma_kernel<NA, NB, STAGES>;
-    static_assert(S::total <= 227 * 1024, "shared memory budget");
-    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::total);
+    static_assert(K::smem <= 227 * 1024, "shared memory budget");
+    auto kern = in.a_kfast ? (in.b_kfast ? stra_dmma_kernel<K, true, true> : stra_dmma_kernel<K, true, false>)
+                           : (in.b_kfast ? stra_dmma_kernel<K, false, true> : stra_dmma_kernel<K, false, false>);
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::smem);
     if (err != cudaSuccess) return err;
-    int64_t grid = args.work < num_sms ? args.work : num_sms;
-    if (grid < 1) grid = 1;
-    kern<<<(unsigned)grid, NT, S::total, stream>>>(args);
+    DmmaArgs args = in;
+    args.tiles_m = (int)((args.ms + K::BM - 1) / K::BM);
+    args.tiles_n = (int)((args.ns + K::BN - 1) / K::BN);
+    args.work = args.batch * (int64_t)args.tiles_m * args.tiles_n;
+    if (args.work <= 0) return cudaSuccess;
+    int per_sm = 0;
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, K::NT, K::smem);
+    if (err != cudaSuccess) return err;
+    if (per_sm < 1) per_sm = 1;
+    int64_t grid = (int64_t)num_sms * per_sm;
+    if (args.work < grid) grid = args.work;
+    timing_begin(KK_FUSED, stream);
+    kern<<<(unsigned)grid, K::NT, K::smem, stream>>>(args);
+    timing_end(KK_FUSED, stream);
     return cudaGetLastError();
 }
+
+// Tile configurations: <BM, BN, BK, WM, WN, STAGES, NA, NB, min CTAs per SM, H max>.
+// 16 warps of 32 x 32 per SM keep the DMMA pipe fed (the register file then
+// holds 128 registers per thread); 1 CTA of 512 threads or 4 CTAs of 128.
+// Plain products on a 1 x 1 grid (ABC at level 0):
+using P0 = Cfg<128, 128, 16, 4, 4, 3, 1, 1, 1, 1>;
+using P1 = Cfg<64, 64, 16, 2, 2, 3, 1, 1, 4, 1>;
+using P2 = Cfg<128, 128, 16, 2, 4, 3, 1, 1, 1, 1>;
+// Single-term products on a block grid (AB / Naive GEMMs):
+using G0 = Cfg<128, 128, 16, 4, 4, 3, 1, 1, 1, 4>;
+// Two-term sums (level 1):
+using T0 = Cfg<128, 128, 8, 4, 4, 6, 2, 2, 1, 2>;
+using T1 = Cfg<128, 128, 16, 4, 4, 3, 2, 2, 1, 2>;
+using T2 = Cfg<128, 128, 8, 2, 4, 4, 2, 2, 1, 2>;
+// Four-term sums (level 2):
+using F0 = Cfg<128, 128, 8, 4, 4, 3, 4, 4, 1, 4>;
+using F1 = Cfg<64, 64, 8, 2, 2, 3, 4, 4, 2, 4>;
+using F2 = Cfg<128, 128, 8, 2, 4, 3, 4, 4, 1, 4>;
 
 }  // namespace
 
@@ -364,13 +469,52 @@ std::atomic<unsigned long long> g_launches{0};
 
 unsigned long long launches() { return g_launches.load(); }
 
-cudaError_t launch_dmma(const DmmaArgs& args, int terms, cudaStream_t stream, int num_sms)
+cudaError_t launch_dmma(const DmmaArgs& args, int terms, cudaStream_t stream, int num_sms, int config)
 {
-    if (args.work <= 0) return cudaSuccess;
+    if (args.batch <= 0 || args.ms <= 0 || args.ns <= 0) return cudaSuccess;
+    if (terms > 4 || args.H > 4 || args.Hc > 4) return cudaErrorInvalidValue;
+    if (config < 0)
+    {
+        // Development override for tile sweeps: TBLIS_STRA_DMMA_CONFIG=<id>.
+        static const int env = [] {
+            const char* s = std::getenv("TBLIS_STRA_DMMA_CONFIG");
+            return s ? std::atoi(s) : -1;
+        }();
+        config = env;
+    }
     cudaError_t err;
-    if (terms <= 1)      err = launch_instance<1, 1, 8>(args, stream, num_sms);
-    else if (terms <= 2) err = launch_instance<2, 2, 6>(args, stream, num_sms);
-    else                 err = launch_instance<4, 4, 3>(args, stream, num_sms);
+    if (terms <= 1 && args.H <= 1 && args.Hc <= 1)
+    {
+        switch (config)
+        {
+            case 1:  err = launch_cfg<P1>(args, stream, num_sms); break;
+            case 2:  err = launch_cfg<P2>(args, stream, num_sms); break;
+            default: err = launch_cfg<P0>(args, stream, num_sms); break;
+        }
+    }
+    else if (terms <= 1)
+    {
+        err = launch_cfg<G0>(args, stream, num_sms);   // block grid up to 4 x 4
+    }
+    else if (terms <= 2 && args.H <= 2 && args.Hc <= 2)
+    {
+        switch (config)
+        {
+            case 1:  err = launch_cfg<T1>(args, stream, num_sms); break;
+            case 2:  err = launch_cfg<T2>(args, stream, num_sms); break;
+            default: err = launch_cfg<T0>(args, stream, num_sms); break;
+        }
+    }
+    else
+    {
+        // up to 4 terms per sum on a block grid up to 4 x 4
+        switch (config)
+        {
+            case 1:  err = launch_cfg<F1>(args, stream, num_sms); break;
+            case 2:  err = launch_cfg<F2>(args, stream, num_sms); break;
+            default: err = launch_cfg<F0>(args, stream, num_sms); break;
+        }
+    }
     if (err == cudaSuccess) g_launches++;
     return err;
 }

@@ -87,9 +87,57 @@ struct ScatterAddArgs
     int8_t c_r[4], c_c[4], c_s[4], c_first[4];
 };
 
+// ---- packed operands -------------------------------------------------------
+//
+// A Strassen operand sum (or a plain operand) packed into tile order: for
+// batch b, tile t of PACK_TILE rows (A side) or columns (B side) and k in
+// [0, k_pad), the PACK_TILE values of that k sit contiguously at
+//   out[((b * tiles + t) * k_pad + k) * PACK_TILE + pack_pos(k, r)]
+// in exactly the swizzled order the GEMM kernel keeps in shared memory, so a
+// pipeline stage is a straight 16-byte-chunk copy.  Rows past the block and k
+// past the block are zero.
+constexpr int PACK_TILE = 128;
+constexpr int PACK_KSTEP = 32;     // k_pad is a multiple of this
+
+struct PackArgs
+{
+    const double* X;                           // X(i, p) = X[bX[b] + rs[i] + ks[p]]
+    const int64_t* rs; const int64_t* ks; const int64_t* bX;
+    int64_t rows_full, k_full;                 // bounds of the full index ranges
+    int64_t rows_blk, k_blk;                   // block extents
+    int nt;                                    // terms of the sum (1..4)
+    int8_t t_r[4], t_c[4], t_s[4];             // block row part, k part, sign
+    int64_t tiles, k_pad, batch;
+    int kfast;                                 // 1: X is contiguous along k
+    double* out;
+};
+
+// C_q = (first_q ? beta*C_q : C_q) + sign_q*alpha*(S*T) for the nc targets of
+// one product, S and T packed (PACK_TILE x k_pad tiles).
+struct PackedGemmArgs
+{
+    const double* S;
+    const double* T;
+    double* C;
+    const int64_t* rsC; const int64_t* csC; const int64_t* bC;
+    int64_t m, n;                              // full C extents
+    int64_t ms, ns;                            // block extents
+    int64_t k_pad;
+    int64_t tiles_m, tiles_n, batch;
+    double alpha, beta;
+    int nc;
+    int8_t c_r[4], c_c[4], c_s[4], c_first[4];
+};
+
+cudaError_t launch_pack(const PackArgs& args, cudaStream_t stream);
+cudaError_t launch_packed_gemm(const PackedGemmArgs& args, cudaStream_t stream, int num_sms,
+                               int config = -1);
+
 // Launchers (kernels.cu).  `terms` = largest number of blocks in one sum
 // (1, 2 or 4), selecting the kernel instance.  Return a cudaError_t.
-cudaError_t launch_dmma(const DmmaArgs& args, int terms, cudaStream_t stream, int num_sms);
+// `config` selects a tile configuration (-1: default for `terms`).
+cudaError_t launch_dmma(const DmmaArgs& args, int terms, cudaStream_t stream, int num_sms,
+                        int config = -1);
 cudaError_t launch_scale(const ScaleArgs& args, cudaStream_t stream);
 cudaError_t launch_sum_gather(const SumGatherArgs& args, cudaStream_t stream);
 cudaError_t launch_scatter_add(const ScatterAddArgs& args, cudaStream_t stream);

@@ -166,10 +166,70 @@ void append_modes(std::vector<int64_t>& len, std::vector<std::vector<int64_t>>& 
     }
 }
 
-int64_t first_stride(const std::vector<int64_t>& len, const std::vector<int64_t>& stride)
+// Smallest |stride| among the first `lead` modes of extent > 1 (0 if none):
+// the stride consecutive loader threads walk inside one k-step.
+int64_t first_stride(const std::vector<int64_t>& len, const std::vector<int64_t>& stride,
+                     int lead = 1)
 {
-    for (size_t d = 0; d < len.size(); d++) if (len[d] > 1) return std::llabs(stride[d]);
-    return 0;
+    int64_t best = 0;
+    int seen = 0;
+    for (size_t d = 0; d < len.size() && seen < lead; d++)
+    {
+        if (len[d] <= 1) continue;
+        int64_t s = std::llabs(stride[d]);
+        if (seen == 0 || s < best) best = s;
+        seen++;
+    }
+    return best;
+}
+
+// Contracted-index order for two operands whose fastest modes differ.
+//
+// The order of the contracted index set is free: any bijection gives the same
+// sum, and Strassen's halving is valid for any split of the index set into
+// equal parts.  When A's smallest-stride mode dA and B's smallest-stride mode
+// dB differ (e.g. A(e,f,..) and B(f,..,e) column-major: A runs along e, B
+// along f), a plain order leaves one operand with no contiguous run inside a
+// k-step.  This splits dA into (a, len/a) and dB into (b, len/b) and puts the
+// two short parts first, so every aligned chunk of a*b consecutive indices is
+// an a x b box: A reads runs of a elements and B runs of b elements (4 x 4 =
+// 16 = the k-step: one 32-byte sector per run for FP64).  Returns whether the
+// order was changed.
+bool block_interleave(std::vector<int64_t>& len, std::vector<std::vector<int64_t>>& str)
+{
+    const size_t nd = len.size();
+    if (nd < 2) return false;
+    auto smallest = [&](int t) {
+        size_t best = nd;
+        for (size_t d = 0; d < nd; d++)
+            if (len[d] > 1 && (best == nd || std::llabs(str[t][d]) < std::llabs(str[t][best]))) best = d;
+        return best;
+    };
+    const size_t dA = smallest(0), dB = smallest(1);
+    if (dA == nd || dB == nd || dA == dB) return false;
+    if (std::llabs(str[0][dA]) != 1 || std::llabs(str[1][dB]) != 1) return false;
+    static const int choices[][2] = {{4, 4}, {4, 2}, {2, 4}, {2, 2}};
+    for (auto& c : choices)
+    {
+        const int64_t a = c[0], b = c[1];
+        if (len[dA] % a || len[dB] % b || len[dA] == a || len[dB] == b) continue;
+        std::vector<int64_t> nl;
+        std::vector<std::vector<int64_t>> ns(str.size());
+        auto push = [&](int64_t l, size_t d, int64_t mult) {
+            nl.push_back(l);
+            for (size_t t = 0; t < str.size(); t++) ns[t].push_back(str[t][d] * mult);
+        };
+        push(a, dA, 1);
+        push(b, dB, 1);
+        push(len[dA] / a, dA, a);
+        push(len[dB] / b, dB, b);
+        for (size_t d = 0; d < nd; d++)
+            if (d != dA && d != dB) push(len[d], d, 1);
+        len = nl;
+        str = ns;
+        return true;
+    }
+    return false;
 }
 
 }  // namespace
@@ -274,6 +334,7 @@ int plan_contraction(const tblis_tensor* A, const label_type* idx_A,
     std::vector<std::vector<int64_t>> k_str = {g.AB.stride[0], g.AB.stride[1]};
     append_modes(k_len, k_str, g.A_only, {0, -1});
     append_modes(k_len, k_str, g.B_only, {-1, 0});
+    const bool k_blocked = block_interleave(k_len, k_str);
     std::vector<int64_t> b_len = g.ABC.len;
     std::vector<std::vector<int64_t>> b_str = {g.ABC.stride[0], g.ABC.stride[1], g.ABC.stride[2]};
     append_modes(b_len, b_str, g.C_only, {-1, -1, 0});
@@ -289,8 +350,8 @@ int plan_contraction(const tblis_tensor* A, const label_type* idx_A,
     g.unit_rsC = first_stride(g.AC.len, g.AC.stride[1]);
     g.unit_csB = first_stride(g.BC.len, g.BC.stride[0]);
     g.unit_csC = first_stride(g.BC.len, g.BC.stride[1]);
-    g.unit_ksA = first_stride(k_len, k_str[0]);
-    g.unit_ksB = first_stride(k_len, k_str[1]);
+    g.unit_ksA = first_stride(k_len, k_str[0], k_blocked ? 2 : 1);
+    g.unit_ksB = first_stride(k_len, k_str[1], k_blocked ? 2 : 1);
 
     if (build_scatter)
     {

@@ -77,6 +77,14 @@ def _load() -> ctypes.CDLL:
     P64 = ctypes.POINTER(ctypes.c_int64)
     lib.tblis_stra_plan_query.argtypes = [T, S, T, S, T, S, P64, ctypes.POINTER(ctypes.c_double)] + [P64] * 9
     lib.tblis_stra_plan_query.restype = ctypes.c_int
+    lib.tblis_stra_set_workspace_limit.argtypes = [ctypes.c_size_t]
+    lib.tblis_stra_set_workspace_limit.restype = ctypes.c_int
+    lib.tblis_stra_get_workspace_limit.restype = ctypes.c_size_t
+    lib.tblis_stra_set_kernel_timing.argtypes = [ctypes.c_int]
+    lib.tblis_stra_set_kernel_timing.restype = ctypes.c_int
+    lib.tblis_stra_kernel_timing.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong),
+                                             ctypes.POINTER(ctypes.c_double)]
+    lib.tblis_stra_kernel_timing.restype = ctypes.c_int
     lib.tblis_get_num_threads.restype = ctypes.c_uint
     lib.tblis_set_num_threads.argtypes = [ctypes.c_uint]
     return lib
@@ -207,6 +215,32 @@ def set_impl(impl: int) -> None:
 
 def get_impl() -> int:
     return lib.tblis_stra_get_impl()
+
+
+def set_workspace_limit(nbytes: int | None) -> None:
+    """Device workspace the ABC variant may use (None = unlimited, 0 = the
+    fully fused kernel that packs nothing)."""
+    _check(lib.tblis_stra_set_workspace_limit(ctypes.c_size_t(-1).value if nbytes is None else nbytes))
+
+
+def get_workspace_limit() -> int:
+    return int(lib.tblis_stra_get_workspace_limit())
+
+
+KERNEL_KINDS = {"fused": 0, "pack": 1, "packed_gemm": 2, "aux": 3}
+
+
+def set_kernel_timing(on: bool) -> None:
+    """Bracket every kernel launch with CUDA events (clears earlier records)."""
+    _check(lib.tblis_stra_set_kernel_timing(1 if on else 0))
+
+
+def kernel_timing(kind: str):
+    """(launches, total milliseconds) of one kernel kind since timing was enabled."""
+    n = ctypes.c_ulonglong()
+    ms = ctypes.c_double()
+    _check(lib.tblis_stra_kernel_timing(KERNEL_KINDS[kind], ctypes.byref(n), ctypes.byref(ms)))
+    return int(n.value), float(ms.value)
 
 
 def launch_count() -> int:

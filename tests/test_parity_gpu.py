@@ -35,6 +35,15 @@ def to_dev(x, cuda):
     return out
 
 
+@pytest.fixture(params=["packed", "fused"])
+def schedule(request, tsb):
+    """ABC runs packed operand sums (default) or, with no workspace, the fully
+    fused kernel; both must meet the same bound."""
+    tsb.set_workspace_limit(None if request.param == "packed" else 0)
+    yield request.param
+    tsb.set_workspace_limit(None)
+
+
 def run_gpu(tsb, cuda, level, impl, alpha, A, ia, B, ib, beta, C0, ic):
     import torch
     dA, dB, dC = to_dev(A, cuda), to_dev(B, cuda), to_dev(C0, cuda)
@@ -48,7 +57,7 @@ def summed_len(ext, ic):
 
 
 @pytest.mark.parametrize("case", MANIFEST, ids=[c["name"] for c in MANIFEST])
-def test_golden_all_levels_and_impls(tsb, cuda, case):
+def test_golden_all_levels_and_impls(tsb, cuda, case, schedule):
     d = np.load(os.path.join(GOLDEN, case["name"] + ".npz"))
     A, B, C0 = (np.asfortranarray(d[x]) for x in ("A", "B", "C0"))
     k = summed_len(case["extents"], case["idx_C"])
@@ -76,7 +85,7 @@ def rand_case(seed):
 
 @pytest.mark.parametrize("seed", range(6))
 @pytest.mark.parametrize("level", [0, 1, 2])
-def test_random_4d_vs_oracle(tsb, cuda, seed, level):
+def test_random_4d_vs_oracle(tsb, cuda, seed, level, schedule):
     ext, ia, ib, ic = rand_case(seed)
     order = "F" if seed % 2 == 0 else "C"
     A = oracle.uniform([ext[c] for c in ia], seed, order)
@@ -93,7 +102,7 @@ def test_random_4d_vs_oracle(tsb, cuda, seed, level):
 
 @pytest.mark.parametrize("m,n,k", [(1, 1, 1), (1, 7, 3), (5, 1, 9), (129, 130, 17), (257, 3, 300), (2, 2, 1)])
 @pytest.mark.parametrize("level", [0, 1, 2])
-def test_matrix_edges(tsb, cuda, m, n, k, level):
+def test_matrix_edges(tsb, cuda, m, n, k, level, schedule):
     A = oracle.uniform((m, k), 1)
     B = oracle.uniform((k, n), 2)
     C0 = oracle.uniform((m, n), 3)
@@ -166,14 +175,21 @@ def test_async_stream_entry_point(tsb, cuda):
 
 
 def test_launch_counter_moves(tsb, cuda):
-    before = tsb.launch_count()
     A = oracle.uniform((16, 16), 1)
+    tsb.set_workspace_limit(0)
+    try:
+        before = tsb.launch_count()
+        run_gpu(tsb, cuda, 1, 1, 1.0, A, "ik", A, "kj", 0.0, A, "ij")
+        assert tsb.launch_count() == before + 1     # fused ABC: one persistent launch
+    finally:
+        tsb.set_workspace_limit(None)
+    before = tsb.launch_count()
     run_gpu(tsb, cuda, 1, 1, 1.0, A, "ik", A, "kj", 0.0, A, "ij")
-    assert tsb.launch_count() == before + 1     # ABC: one persistent launch
+    assert tsb.launch_count() == before + 21        # packed ABC: 7 x (pack S, pack T, GEMM)
 
 
 @pytest.mark.parametrize("level", [1, 2])
-def test_sampled_entries_at_config1_size(tsb, cuda, level):
+def test_sampled_entries_at_config1_size(tsb, cuda, level, schedule):
     """Config-1 pattern at extent 64 (NIm=NJn=NPk=4096): too large for the
     oracle's loop, so 4096 sampled entries of C are checked against exact
     dot products, and L vs L=0 on the GPU against the bound."""
