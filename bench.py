@@ -207,6 +207,9 @@ def kernel_probe(args):
     A = colmajor(torch, shape, dev, gen)
     B = colmajor(torch, shape, dev, gen)
     C = colmajor(torch, shape, dev, fill=0.0)
+    if args.dtype == "f32":
+        A, B, C = A.float(), B.float(), C.float()
+        tsb.set_fp32_terms(args.terms)
     if args.kernels == "dgemm":
         # cuBLAS DGEMM at the same m = n = k, for side-by-side profiles
         n = e * e
@@ -230,12 +233,17 @@ def kernel_probe(args):
     flops = 2.0 * float(e * e) ** 3
     for lv in levels:
         s, t = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        tsb.set_kernel_timing(True)
         s.record()
         tsb.contract(lv, 1.0, A, IDX_A, B, IDX_B, 1.0, C, IDX_C, impl=args.variant)
         t.record()
         t.synchronize()
         ms = s.elapsed_time(t)
-        print(f"L{lv} impl{args.variant} extent {e}: {ms:.3f} ms  {flops / ms / 1e9:.2f} TFLOP/s effective")
+        parts = {k: tsb.kernel_timing(k) for k in ("fused", "pack", "packed_gemm", "aux", "split_gemm")}
+        tsb.set_kernel_timing(False)
+        print("   kernels: " + ", ".join(f"{k} {n}x {v:.2f} ms" for k, (n, v) in parts.items() if n))
+        print(f"L{lv} impl{args.variant} {args.dtype}{'/' + str(args.terms) + ' terms' if args.dtype == 'f32' else ''} "
+              f"extent {e}: {ms:.3f} ms  {flops / ms / 1e9:.2f} TFLOP/s effective")
 
 
 def main():
@@ -251,6 +259,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--dtype", choices=["f64", "f32"], default="f64",
+                    help="operand type of the --kernels probe (f32 = split-BF16 tcgen05 path)")
+    ap.add_argument("--terms", type=int, default=6, help="split-BF16 product terms for f32 (3 or 6)")
     ap.add_argument("--kernels", default=None,
                     help="comma-separated levels: run one warm-up and one timed call per level "
                          "and print per-level times (profiling driver; no JSON line)")

@@ -18,8 +18,9 @@
  * tblis_stra_last_status(); tblis_stra_mult() returns the status directly and
  * is asynchronous on device pointers.
  *
- * Only FP64 (TYPE_DOUBLE) runs the plain double path (DMMA tensor cores).
- * FP32 (TYPE_FLOAT) runs the split-BF16 tcgen05 path.
+ * FP64 (TYPE_DOUBLE) runs on the FP64 tensor cores (DMMA); FP32 (TYPE_FLOAT)
+ * runs the split-BF16 tcgen05 path (tblis_stra_set_fp32_terms).  Complex types
+ * return TBLIS_STRA_ERR_TYPE.
  */
 #ifndef TBLIS_STRA_B200_H
 #define TBLIS_STRA_B200_H
@@ -116,7 +117,8 @@ enum
     TBLIS_STRA_ERR_ALLOC        = 7,  /* device workspace could not be allocated */
     TBLIS_STRA_ERR_TOO_LARGE    = 8,  /* sizes beyond what the kernels index */
     TBLIS_STRA_ERR_UNSUPPORTED  = 9,  /* valid request this build does not run */
-    TBLIS_STRA_ERR_NO_DEVICE    = 10  /* no usable sm_100 device */
+    TBLIS_STRA_ERR_NO_DEVICE    = 10, /* no usable sm_100 device */
+    TBLIS_STRA_ERR_TIMEOUT      = 11  /* a kernel's bounded wait expired (reported on blocking calls) */
 };
 
 /* C(idx_C) = alpha*A*B + beta*C at Strassen level 0, 1 or 2 with the current
@@ -153,6 +155,15 @@ int tblis_stra_get_impl(void);
  * nothing beyond the scatter vectors. */
 int tblis_stra_set_workspace_limit(size_t bytes);
 size_t tblis_stra_get_workspace_limit(void);
+
+/* FP32 (TYPE_FLOAT) contractions run on the BF16 tensor cores with each
+ * operand split into bf16 planes (no counterpart in the reference, whose FP32
+ * path is its CPU micro-kernel): terms = 6 splits into hi+mid+lo and keeps the
+ * products hh, hm, mh, hl, mm, lh (about FP32 accuracy); terms = 3 splits into
+ * hi+mid and keeps hh, hm, mh (twice as fast, about 2^-16 relative).  Per
+ * calling thread; default 6.  Returns 0 or TBLIS_STRA_ERR_ARG. */
+int tblis_stra_set_fp32_terms(int terms);
+int tblis_stra_get_fp32_terms(void);
 
 /* Status of the calling thread's last contraction call; string form. */
 int tblis_stra_last_status(void);

@@ -37,6 +37,21 @@ unsigned grid_for(int64_t total)
     return (unsigned)blocks;
 }
 
+__global__ void scale_f32_kernel(const ScaleF32Args a)
+{
+    const int64_t total = a.batch * a.m * a.n;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x)
+    {
+        const int64_t j = e % a.n;
+        const int64_t rest = e / a.n;
+        const int64_t i = rest % a.m;
+        const int64_t b = rest / a.m;
+        float* p = a.C + a.bC[b] + a.rsC[i] + a.csC[j];
+        *p = (a.beta == 0.f) ? 0.f : a.beta * *p;
+    }
+}
+
 __global__ void scale_kernel(const ScaleArgs a)
 {
     const int64_t total = a.batch * a.m * a.n;
@@ -111,6 +126,18 @@ cudaError_t launch_scale(const ScaleArgs& a, cudaStream_t stream)
     if (total <= 0) return cudaSuccess;
     timing_begin(KK_AUX, stream);
     scale_kernel<<<grid_for(total), THREADS, 0, stream>>>(a);
+    timing_end(KK_AUX, stream);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) g_launches++;
+    return err;
+}
+
+cudaError_t launch_scale_f32(const ScaleF32Args& a, cudaStream_t stream)
+{
+    const int64_t total = a.batch * a.m * a.n;
+    if (total <= 0) return cudaSuccess;
+    timing_begin(KK_AUX, stream);
+    scale_f32_kernel<<<grid_for(total), THREADS, 0, stream>>>(a);
     timing_end(KK_AUX, stream);
     cudaError_t err = cudaGetLastError();
     if (err == cudaSuccess) g_launches++;

@@ -1,0 +1,537 @@
+// Split-BF16 path for FP32 contractions on the 5th-generation tensor cores
+// (tcgen05, accumulators in TMEM).  No counterpart kernel in the reference,
+// which computes FP32 contractions with its CPU micro-kernels; the Strassen
+// schedule around it is the reference's ABC one (see packed_kernels.cu).
+//
+// Per Strassen product:
+//   scale_kernel     per local row r (A side) / column c (B side) a power of two
+//                    2^-e with 2^-e * max|X(r,:)| in [0.5, 1), taken over all
+//                    blocks of that row index, so every block of one signed sum
+//                    shares it;
+//   split_pack_kernel  S = sum_i u_i A_i in FP32, times the row scale, split
+//                    into P bf16 planes hi + mid (+ lo) with x ~ hi + mid + lo,
+//                    written as 128 x 64 tiles in the K-major 128-byte-swizzled
+//                    layout the tcgen05 shared-memory descriptors read;
+//   split_gemm_kernel  for each 128 x 128 C tile, the bf16 products of the plane
+//                    pairs (hh, hm, mh for 3 terms; + hl, mm, lh for 6 terms)
+//                    accumulate in TMEM (FP32, hi*hi apart from the smaller
+//                    correction terms) over chunks of 256 k; drain warps
+//                    add each chunk into FP32 registers (keeping the FP32
+//                    rounding of the accumulation to chunk length) and finally
+//                    write C_q = (first ? beta*C_q : C_q) + sign*alpha*acc
+//                    / (row scale * column scale).
+//
+// Warp roles in split_gemm_kernel (192 threads, one CTA per SM):
+//   warp 0      one lane issues the bulk copies (cp.async.bulk, 1-D TMA) of
+//               each stage's plane tiles into shared memory;
+//   warp 1      allocates TMEM; one lane issues tcgen05.mma and commits;
+//   warps 2-5   read TMEM (tcgen05.ld), accumulate, write C.
+// Every wait on an mbarrier is bounded (about a second of clock cycles); on
+// expiry the kernel records an error code and every role returns.
+#include "kernels.cuh"
+#include "timing.hpp"
+
+#include <cuda_bf16.h>
+
+#include <atomic>
+
+namespace tsb {
+
+extern std::atomic<unsigned long long> g_launches;
+
+namespace {
+
+constexpr int ST = SPLIT_TILE;               // 128: tile rows (A side) / columns (B side)
+constexpr int SK = 64;                       // k per tile block (one 128-byte bf16 row)
+constexpr int BLK = ST * SK * 2;             // 16 KB per tile block
+constexpr int KCH = 4;                       // k blocks per TMEM accumulation chunk (256 k)
+constexpr long long WAIT_LIMIT = 2000000000LL;   // clock cycles (~1 s)
+
+// Byte offset of element (r, k) in a 128 x 64 bf16 block, K-major with the
+// 128-byte swizzle: 16-byte chunk k/8 of row r moves to chunk (k/8) ^ (r%8).
+__host__ __device__ __forceinline__ int sw128(int r, int k)
+{
+    return (r >> 3) * 1024 + (r & 7) * 128 + ((((k >> 3) ^ r) & 7) << 4) + (k & 7) * 2;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// ---- row scales -------------------------------------------------------------------
+
+__global__ void scale_kernel(const __grid_constant__ SplitScaleArgs a)
+{
+    const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (wid >= a.batch * a.rows_blk) return;
+    const int64_t b = wid / a.rows_blk, r = wid % a.rows_blk;
+    float m = 0.f;
+    for (int h = 0; h < a.parts; h++)
+    {
+        const int64_t gr = h * a.rows_blk + r;
+        if (gr >= a.rows_full) continue;
+        const int64_t base = a.bX[b] + a.rs[gr];
+        for (int64_t k = lane; k < a.k_full; k += 32) m = fmaxf(m, fabsf(a.X[base + a.ks[k]]));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0)
+    {
+        int e = 0;
+        if (m > 0.f && isfinite(m)) frexpf(m, &e);
+        e = max(-120, min(120, e));
+        a.scale[wid] = ldexpf(1.f, -e);
+        a.inv[wid] = ldexpf(1.f, e);
+    }
+}
+
+// ---- split pack -------------------------------------------------------------------
+
+__global__ void __launch_bounds__(256)
+split_pack_kernel(const __grid_constant__ SplitPackArgs a)
+{
+    __shared__ float buf[ST][SK + 1];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int64_t c = blockIdx.x;            // k block
+    const int64_t t = blockIdx.y;            // row tile
+    const int64_t b = blockIdx.z;
+    const int64_t r0 = t * ST, k0 = c * SK;
+    const int64_t xoff = a.bX[b];
+#pragma unroll 4
+    for (int x = 0; x < ST * SK / 256; x++)
+    {
+        int r, kk;
+        if (a.kfast) { kk = lane + 32 * (x & 1); r = warp + 8 * (x >> 1); }
+        else         { r = lane + 32 * (x & 3); kk = warp + 8 * (x >> 2); }
+        const int64_t lr = r0 + r, lk = k0 + kk;
+        float v = 0.f;
+        if (lr < a.rows_blk && lk < a.k_blk)
+        {
+            for (int q = 0; q < a.nt; q++)
+            {
+                const int64_t gr = a.t_r[q] * a.rows_blk + lr;
+                const int64_t gk = a.t_c[q] * a.k_blk + lk;
+                if (gr < a.rows_full && gk < a.k_full)
+                {
+                    const float e = a.X[xoff + a.rs[gr] + a.ks[gk]];
+                    v += a.t_s[q] < 0 ? -e : e;
+                }
+            }
+            v *= a.scale[b * a.rows_blk + lr];
+        }
+        buf[r][kk] = v;
+    }
+    __syncthreads();
+    // 16-byte chunks: row r, k group g (8 values) -> one chunk per plane.
+    const size_t plane_stride = (size_t)a.batch * a.tiles * a.nk * BLK;
+    unsigned char* blk = reinterpret_cast<unsigned char*>(a.out) + ((size_t)(b * a.tiles + t) * a.nk + c) * BLK;
+#pragma unroll
+    for (int i = 0; i < ST * 8 / 256; i++)
+    {
+        const int q = tid + 256 * i;
+        const int r = q >> 3, g = q & 7;
+        unsigned short hv[8], mv[8], lv[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+        {
+            const float x = buf[r][g * 8 + j];
+            const __nv_bfloat16 h = __float2bfloat16_rn(x);
+            const float r1 = x - __bfloat162float(h);
+            const __nv_bfloat16 m = __float2bfloat16_rn(r1);
+            const float r2 = r1 - __bfloat162float(m);
+            const __nv_bfloat16 l = __float2bfloat16_rn(r2);
+            hv[j] = __bfloat16_as_ushort(h);
+            mv[j] = __bfloat16_as_ushort(m);
+            lv[j] = __bfloat16_as_ushort(l);
+        }
+        const int off = sw128(r, g * 8);
+        auto pack = [](const unsigned short* v) {
+            return make_uint4(v[0] | (unsigned)v[1] << 16, v[2] | (unsigned)v[3] << 16,
+                              v[4] | (unsigned)v[5] << 16, v[6] | (unsigned)v[7] << 16);
+        };
+        *reinterpret_cast<uint4*>(blk + off) = pack(hv);
+        *reinterpret_cast<uint4*>(blk + plane_stride + off) = pack(mv);
+        if (a.planes > 2) *reinterpret_cast<uint4*>(blk + 2 * plane_stride + off) = pack(lv);
+    }
+}
+
+// ---- tcgen05 GEMM -------------------------------------------------------------------
+
+__device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" :: "r"(addr), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t addr)
+{
+    asm volatile("{\n.reg .b64 st;\nmbarrier.arrive.shared::cta.b64 st, [%0];\n}\n" :: "r"(addr) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t addr, uint32_t bytes)
+{
+    asm volatile("{\n.reg .b64 st;\nmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n"
+                 :: "r"(addr), "r"(bytes) : "memory");
+}
+
+// Bounded wait for the phase of the given parity; false on timeout or abort.
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity, volatile int* abort_flag,
+                                          int* err, int code)
+{
+    const long long start = clock64();
+    while (true)
+    {
+        uint32_t done;
+        asm volatile("{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                     "selp.u32 %0, 1, 0, p;\n}\n" : "=r"(done) : "r"(addr), "r"(parity) : "memory");
+        if (done) return true;
+        if (*abort_flag) return false;
+        if (clock64() - start > WAIT_LIMIT)
+        {
+            *abort_flag = 1;
+            if (err) atomicExch(err, code);
+            return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                 :: "r"(dst), "l"(src), "r"(bytes), "r"(mbar) : "memory");
+}
+
+// Shared-memory descriptor of a 128-row, K-major, 128-byte-swizzled block:
+// start >> 4, leading offset 16 B (unused when swizzled), stride 1024 B
+// between 8-row groups, fixed 0b001 at bit 46, swizzle mode 2 (128 B).
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr)
+{
+    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// Instruction descriptor, kind::f16: D = F32, A = B = BF16, both K-major,
+// N = 128 (>> 3 at bit 17), M = 128 (>> 4 at bit 24).
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ void mma_bf16(uint32_t d, uint64_t ad, uint64_t bd, uint32_t acc)
+{
+    asm volatile("{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                 :: "r"(d), "l"(ad), "l"(bd), "r"(IDESC), "r"(acc));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t mbar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                 :: "r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
+{
+    uint32_t r[32];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                 "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                   "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                   "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+                   "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+                   "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+template <int P>
+struct SG
+{
+    static constexpr int STAGES = P == 3 ? 2 : 3;
+    static constexpr int STAGE_BYTES = 2 * P * BLK;
+    static constexpr int TAB_BYTES = 4 * (ST + ST) * 8 + 2 * ST * 4;
+    static constexpr int CTRL_BYTES = 256;
+    static constexpr size_t smem = 1024 + size_t(STAGES) * STAGE_BYTES + CTRL_BYTES + TAB_BYTES;
+};
+
+template <int P>
+__global__ void __launch_bounds__(192, 1)
+split_gemm_kernel(const __grid_constant__ SplitGemmArgs a)
+{
+    using K = SG<P>;
+    constexpr int STAGES = K::STAGES;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char* stages = smem;                           // [STAGES][A planes | B planes]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * K::STAGE_BYTES);
+    // bars: full[0..3], empty[4..7], acc_full[8..9], acc_empty[10..11], mma drain[12]
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 16);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    int64_t* rowC = reinterpret_cast<int64_t*>(smem + STAGES * K::STAGE_BYTES + K::CTRL_BYTES);
+    int64_t* colC = rowC + 4 * ST;
+    float* invr = reinterpret_cast<float*>(colC + 4 * ST);
+    float* invc = invr + ST;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    auto bar = [&](int i) { return smem_u32(bars + i); };
+    if (tid == 0)
+    {
+        for (int s = 0; s < 4; s++) { mbar_init(bar(s), 1); mbar_init(bar(4 + s), 1); }
+        for (int s = 0; s < 2; s++) { mbar_init(bar(8 + s), 1); mbar_init(bar(10 + s), 128); }
+        mbar_init(bar(12), 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 1)
+    {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;\n"
+                     :: "r"(smem_u32(tmem_slot)) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    const int64_t tiles = a.tiles_m * a.tiles_n;
+    const int64_t work = a.batch * tiles;
+    const int64_t nk = a.nk;
+    auto decode = [&](int64_t w, int64_t& b, int64_t& tm, int64_t& tn) {
+        b = w / tiles;
+        const int64_t tw = w - b * tiles;
+        const int64_t GROUP = 8;
+        const int64_t group = tw / (GROUP * a.tiles_n);
+        const int64_t first_m = group * GROUP;
+        const int64_t gsize = (a.tiles_m - first_m) < GROUP ? (a.tiles_m - first_m) : GROUP;
+        tm = first_m + (tw % gsize);
+        tn = (tw % (GROUP * a.tiles_n)) / gsize;
+    };
+    const size_t planeA = (size_t)a.batch * a.tiles_m * nk * BLK;
+    const size_t planeB = (size_t)a.batch * a.tiles_n * nk * BLK;
+
+    if (warp == 0)
+    {
+        if (lane == 0)
+        {
+            uint32_t it = 0;
+            bool ok = true;
+            for (int64_t w = blockIdx.x; w < work && ok; w += gridDim.x)
+            {
+                int64_t b, tm, tn;
+                decode(w, b, tm, tn);
+                const unsigned char* srcA = reinterpret_cast<const unsigned char*>(a.A) +
+                                            ((size_t)(b * a.tiles_m + tm) * nk) * BLK;
+                const unsigned char* srcB = reinterpret_cast<const unsigned char*>(a.B) +
+                                            ((size_t)(b * a.tiles_n + tn) * nk) * BLK;
+                for (int64_t c = 0; c < nk; c++, it++)
+                {
+                    const int s = it % STAGES;
+                    const uint32_t ph = (it / STAGES) & 1;
+                    if (!mbar_wait(bar(4 + s), ph ^ 1, abort_flag, a.err, 1)) { ok = false; break; }
+                    mbar_expect_tx(bar(s), 2 * P * BLK);
+                    const uint32_t dst = smem_u32(stages + s * K::STAGE_BYTES);
+#pragma unroll
+                    for (int p = 0; p < P; p++)
+                    {
+                        bulk_copy(dst + p * BLK, srcA + p * planeA + c * BLK, BLK, bar(s));
+                        bulk_copy(dst + (P + p) * BLK, srcB + p * planeB + c * BLK, BLK, bar(s));
+                    }
+                }
+            }
+            // Copies still in flight land before the CTA leaves (bounded wait on
+            // the full barrier of each of the last STAGES stages issued).
+            volatile int never = 0;
+            for (uint32_t i = (it > STAGES ? it - STAGES : 0); i < it; i++)
+                mbar_wait(bar(i % STAGES), (i / STAGES) & 1, &never, nullptr, 0);
+        }
+    }
+    else if (warp == 1)
+    {
+        if (lane == 0)
+        {
+            uint32_t it = 0, u = 0;
+            bool ok = true;
+            for (int64_t w = blockIdx.x; w < work && ok; w += gridDim.x)
+            {
+                uint32_t dcol = 0;
+                for (int64_t c = 0; c < nk; c++, it++)
+                {
+                    if (c % KCH == 0)
+                    {
+                        const int bacc = u & 1;
+                        if (!mbar_wait(bar(10 + bacc), ((u >> 1) & 1) ^ 1, abort_flag, a.err, 2)) { ok = false; break; }
+                        fence_after();
+                        dcol = bacc * 2 * ST;
+                    }
+                    const int s = it % STAGES;
+                    if (!mbar_wait(bar(s), (it / STAGES) & 1, abort_flag, a.err, 3)) { ok = false; break; }
+                    fence_after();
+                    const uint32_t base = smem_u32(stages + s * K::STAGE_BYTES);
+#pragma unroll
+                    for (int t = 0; t < 2 * P; t++)
+                    {
+                        if (t >= a.nterms) break;
+                        const uint64_t ad = sdesc(base + a.ta[t] * BLK);
+                        const uint64_t bd = sdesc(base + (P + a.tb[t]) * BLK);
+                        // hi*hi accumulates in its own TMEM columns; the
+                        // smaller correction terms share the next 128.
+                        const uint32_t d = tmem + dcol + (t == 0 ? 0 : ST);
+                        const bool fresh = (c % KCH == 0) && (t <= 1);
+#pragma unroll
+                        for (int kk = 0; kk < SK / 16; kk++)
+                            mma_bf16(d, ad + 2 * kk, bd + 2 * kk, (fresh && kk == 0) ? 0u : 1u);
+                    }
+                    mma_commit(bar(4 + s));
+                    if (c % KCH == KCH - 1 || c == nk - 1)
+                    {
+                        mma_commit(bar(8 + (u & 1)));
+                        u++;
+                    }
+                }
+            }
+            // Every MMA issued completes before TMEM is freed.
+            mma_commit(bar(12));
+            volatile int never = 0;
+            mbar_wait(bar(12), 0, &never, nullptr, 0);
+        }
+    }
+    else
+    {
+        // Drain warps: thread owns tile row `row` (TMEM lane).
+        const int q = warp & 3;
+        const int row = q * 32 + lane;
+        const int dt = tid - 64;                 // 0..127
+        uint32_t u = 0;
+        bool ok = true;
+        for (int64_t w = blockIdx.x; w < work && ok; w += gridDim.x)
+        {
+            int64_t b, tm, tn;
+            decode(w, b, tm, tn);
+            asm volatile("bar.sync 1, 128;\n" ::: "memory");
+            for (int qq = 0; qq < 4; qq++)
+            {
+                const int64_t li = tm * ST + dt, lj = tn * ST + dt;
+                const int64_t gi = (qq < a.nc ? a.c_r[qq] : 0) * a.ms + li;
+                const int64_t gj = (qq < a.nc ? a.c_c[qq] : 0) * a.ns + lj;
+                rowC[qq * ST + dt] = (qq < a.nc && li < a.ms && gi < a.m) ? a.bC[b] + a.rsC[gi] : OFF_INVALID;
+                colC[qq * ST + dt] = (qq < a.nc && lj < a.ns && gj < a.n) ? a.csC[gj] : OFF_INVALID;
+            }
+            {
+                const int64_t li = tm * ST + dt, lj = tn * ST + dt;
+                invr[dt] = li < a.ms ? a.invA[b * a.ms + li] : 0.f;
+                invc[dt] = lj < a.ns ? a.invB[b * a.ns + lj] : 0.f;
+            }
+            asm volatile("bar.sync 1, 128;\n" ::: "memory");
+
+            float acc[ST];
+#pragma unroll
+            for (int j = 0; j < ST; j++) acc[j] = 0.f;
+            const int64_t nch = (nk + KCH - 1) / KCH;
+            for (int64_t ch = 0; ch < nch; ch++, u++)
+            {
+                const int bacc = u & 1;
+                if (!mbar_wait(bar(8 + bacc), (u >> 1) & 1, abort_flag, a.err, 4)) { ok = false; break; }
+                fence_after();
+#pragma unroll
+                for (int j = 0; j < ST / 32; j++)
+                {
+                    float hh[32], cr[32];
+                    const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + bacc * 2 * ST + j * 32;
+                    tmem_ld32(ta, hh);
+                    tmem_ld32(ta + ST, cr);
+#pragma unroll
+                    for (int i = 0; i < 32; i++) acc[j * 32 + i] += hh[i] + cr[i];
+                }
+                fence_before();
+                mbar_arrive(bar(10 + bacc));
+            }
+            if (!ok) break;
+            for (int qq = 0; qq < a.nc; qq++)
+            {
+                const int64_t ro = rowC[qq * ST + row];
+                if (ro == OFF_INVALID) continue;
+                const float coef = (a.c_s[qq] < 0 ? -a.alpha : a.alpha) * invr[row];
+                const bool first = a.c_first[qq] != 0;
+#pragma unroll
+                for (int j = 0; j < ST; j++)
+                {
+                    const int64_t co = colC[qq * ST + j];
+                    if (co == OFF_INVALID) continue;
+                    float* ptr = a.C + ro + co;
+                    float v = coef * acc[j] * invc[j];
+                    if (!first) v += *ptr;
+                    else if (a.beta != 0.f) v += a.beta * *ptr;
+                    *ptr = v;
+                }
+            }
+        }
+    }
+    fence_before();
+    __syncthreads();
+    if (warp == 1)
+    {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;\n" :: "r"(tmem) : "memory");
+    }
+}
+
+template <int P>
+cudaError_t launch_split_gemm_p(const SplitGemmArgs& a, cudaStream_t stream, int num_sms)
+{
+    auto kern = split_gemm_kernel<P>;
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SG<P>::smem);
+    if (err != cudaSuccess) return err;
+    const int64_t work = a.batch * a.tiles_m * a.tiles_n;
+    int64_t grid = num_sms;
+    if (work < grid) grid = work;
+    timing_begin(KK_SPLIT_GEMM, stream);
+    kern<<<(unsigned)grid, 192, SG<P>::smem, stream>>>(a);
+    timing_end(KK_SPLIT_GEMM, stream);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_split_scale(const SplitScaleArgs& a, cudaStream_t stream)
+{
+    const int64_t warps = a.batch * a.rows_blk;
+    if (warps <= 0) return cudaSuccess;
+    const int64_t blocks = (warps * 32 + 255) / 256;
+    timing_begin(KK_AUX, stream);
+    scale_kernel<<<(unsigned)blocks, 256, 0, stream>>>(a);
+    timing_end(KK_AUX, stream);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) g_launches++;
+    return err;
+}
+
+cudaError_t launch_split_pack(const SplitPackArgs& a, cudaStream_t stream)
+{
+    if (a.batch <= 0 || a.tiles <= 0 || a.nk <= 0) return cudaSuccess;
+    if (a.tiles > 65535 || a.batch > 65535 || (a.planes != 2 && a.planes != 3)) return cudaErrorInvalidValue;
+    dim3 grid((unsigned)a.nk, (unsigned)a.tiles, (unsigned)a.batch);
+    timing_begin(KK_PACK, stream);
+    split_pack_kernel<<<grid, 256, 0, stream>>>(a);
+    timing_end(KK_PACK, stream);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) g_launches++;
+    return err;
+}
+
+cudaError_t launch_split_gemm(const SplitGemmArgs& a, cudaStream_t stream, int num_sms)
+{
+    if (a.batch <= 0 || a.tiles_m <= 0 || a.tiles_n <= 0 || a.nk <= 0) return cudaSuccess;
+    if (a.nc < 1 || a.nc > 4 || a.nterms < 1 || a.nterms > 2 * a.planes) return cudaErrorInvalidValue;
+    cudaError_t err = a.planes == 3 ? launch_split_gemm_p<3>(a, stream, num_sms)
+                    : a.planes == 2 ? launch_split_gemm_p<2>(a, stream, num_sms)
+                                    : cudaErrorInvalidValue;
+    if (err == cudaSuccess) g_launches++;
+    return err;
+}
+
+}  // namespace tsb

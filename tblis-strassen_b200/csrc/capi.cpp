@@ -42,6 +42,7 @@ thread_local int t_impl = 1;
 thread_local cudaStream_t t_stream = nullptr;
 thread_local int t_status = TBLIS_STRA_SUCCESS;
 thread_local size_t t_ws_limit = SIZE_MAX;   // device workspace the ABC schedule may use
+thread_local int t_fp32_terms = 6;           // split-BF16 product terms for FP32 (3 or 6)
 unsigned g_num_threads = 1;
 
 // ---- device tables (cached) ------------------------------------------------
@@ -427,6 +428,97 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
     return TBLIS_STRA_SUCCESS;
 }
 
+// FP32 contraction: split-BF16 tcgen05 path (bf16_split.cu), Strassen products
+// in stream order like the packed FP64 schedule.
+int run_fp32(int level, const GemmView& g, const DevPlan& t, const float* A, const float* B,
+             float* C, cudaStream_t st, int device, bool blocking)
+{
+    if (g.m == 0 || g.n == 0 || g.batch == 0) return TBLIS_STRA_SUCCESS;
+    if (g.alpha == 0.0 || g.k == 0)
+    {
+        ScaleF32Args s{C, t.rsC, t.csC, t.bC, g.m, g.n, g.batch, (float)g.beta};
+        TSB_CUDA(launch_scale_f32(s, st));
+        return TBLIS_STRA_SUCCESS;
+    }
+    const ProductTable& tab = product_table(level);
+    const int H = tab.H;
+    const int64_t ms = cdiv(g.m, H), ns = cdiv(g.n, H), ks = cdiv(g.k, H);
+    const int64_t nk = cdiv(ks, SPLIT_K);
+    const int64_t tm = cdiv(ms, SPLIT_TILE), tn = cdiv(ns, SPLIT_TILE);
+    if (g.batch * tm > 65535 || g.batch * tn > 65535 || nk > 2147483647) return TBLIS_STRA_ERR_TOO_LARGE;
+    const int P = t_fp32_terms == 3 ? 2 : 3;
+    const int sms = num_sms(device);
+
+    Scratch scal, planesA, planesB, errbuf;
+    int s;
+    const size_t nsc = (size_t)g.batch * (ms + ns);
+    if ((s = scal.alloc(2 * nsc * sizeof(float), st))) return s;
+    const size_t blk = (size_t)SPLIT_TILE * SPLIT_K * 2;
+    if ((s = planesA.alloc((size_t)P * g.batch * tm * nk * blk, st))) return s;
+    if ((s = planesB.alloc((size_t)P * g.batch * tn * nk * blk, st))) return s;
+    if ((s = errbuf.alloc(sizeof(int), st))) return s;
+    TSB_CUDA(cudaMemsetAsync(errbuf.p, 0, sizeof(int), st));
+    float* scaleA = static_cast<float*>(scal.p);
+    float* invA = scaleA + g.batch * ms;
+    float* scaleB = invA + g.batch * ms;
+    float* invB = scaleB + g.batch * ns;
+
+    SplitScaleArgs sa{A, t.rsA, t.ksA, t.bA, g.m, g.k, ms, H, g.batch, scaleA, invA};
+    TSB_CUDA(launch_split_scale(sa, st));
+    SplitScaleArgs sb{B, t.csB, t.ksB, t.bB, g.n, g.k, ns, H, g.batch, scaleB, invB};
+    TSB_CUDA(launch_split_scale(sb, st));
+
+    const bool a_kfast = g.unit_ksA != 0 && (g.unit_rsA == 0 || g.unit_ksA < g.unit_rsA);
+    const bool b_kfast = g.unit_ksB != 0 && (g.unit_csB == 0 || g.unit_ksB < g.unit_csB);
+    static const int8_t TA6[6] = {0, 0, 1, 0, 1, 2}, TB6[6] = {0, 1, 0, 2, 1, 0};
+    for (const Product& pr : tab.prod)
+    {
+        SplitPackArgs pa{};
+        pa.X = A; pa.rs = t.rsA; pa.ks = t.ksA; pa.bX = t.bA;
+        pa.rows_full = g.m; pa.k_full = g.k; pa.rows_blk = ms; pa.k_blk = ks;
+        pa.nt = pr.na;
+        for (int i = 0; i < pr.na; i++) { pa.t_r[i] = pr.a[i].r; pa.t_c[i] = pr.a[i].c; pa.t_s[i] = pr.a[i].sign; }
+        pa.scale = scaleA; pa.tiles = tm; pa.nk = nk; pa.batch = g.batch; pa.planes = P;
+        pa.kfast = a_kfast; pa.out = planesA.p;
+        TSB_CUDA(launch_split_pack(pa, st));
+        SplitPackArgs pb{};
+        pb.X = B; pb.rs = t.csB; pb.ks = t.ksB; pb.bX = t.bB;
+        pb.rows_full = g.n; pb.k_full = g.k; pb.rows_blk = ns; pb.k_blk = ks;
+        pb.nt = pr.nb;
+        for (int i = 0; i < pr.nb; i++) { pb.t_r[i] = pr.b[i].c; pb.t_c[i] = pr.b[i].r; pb.t_s[i] = pr.b[i].sign; }
+        pb.scale = scaleB; pb.tiles = tn; pb.nk = nk; pb.batch = g.batch; pb.planes = P;
+        pb.kfast = b_kfast; pb.out = planesB.p;
+        TSB_CUDA(launch_split_pack(pb, st));
+
+        SplitGemmArgs ga{};
+        ga.A = planesA.p; ga.B = planesB.p; ga.C = C;
+        ga.rsC = t.rsC; ga.csC = t.csC; ga.bC = t.bC;
+        ga.invA = invA; ga.invB = invB;
+        ga.m = g.m; ga.n = g.n; ga.ms = ms; ga.ns = ns; ga.nk = nk;
+        ga.tiles_m = tm; ga.tiles_n = tn; ga.batch = g.batch;
+        ga.alpha = (float)g.alpha; ga.beta = (float)g.beta;
+        ga.nc = pr.nc;
+        for (int q = 0; q < pr.nc; q++)
+        {
+            ga.c_r[q] = pr.c[q].r; ga.c_c[q] = pr.c[q].c; ga.c_s[q] = pr.c[q].sign;
+            ga.c_first[q] = pr.c_first[q];
+        }
+        ga.planes = P;
+        ga.nterms = P == 3 ? 6 : 3;
+        for (int i = 0; i < 6; i++) { ga.ta[i] = TA6[i]; ga.tb[i] = TB6[i]; }
+        ga.err = static_cast<int*>(errbuf.p);
+        TSB_CUDA(launch_split_gemm(ga, st, sms));
+    }
+    if (blocking)
+    {
+        int err = 0;
+        TSB_CUDA(cudaMemcpyAsync(&err, errbuf.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        TSB_CUDA(cudaStreamSynchronize(st));
+        if (err) return TBLIS_STRA_ERR_TIMEOUT;
+    }
+    return TBLIS_STRA_SUCCESS;
+}
+
 int mult(int level, const tblis_tensor* A, const label_type* idx_A,
          const tblis_tensor* B, const label_type* idx_B,
          tblis_tensor* C, const label_type* idx_C, cudaStream_t st, bool blocking)
@@ -443,14 +535,14 @@ int mult(int level, const tblis_tensor* A, const label_type* idx_A,
     std::shared_ptr<DevPlan> dp;
     int s = get_plan(T, I, device, g, dp);
     if (s) return s;
-    if (g.type != TYPE_DOUBLE) return TBLIS_STRA_ERR_UNSUPPORTED;
+    const bool fp32 = g.type == TYPE_FLOAT;
+    const size_t es = fp32 ? sizeof(float) : sizeof(double);
 
-    // Every element access is an aligned 8-byte load or store.
+    // Every element access is an aligned load or store of the element size.
     for (int t = 0; t < 3; t++)
-        if (reinterpret_cast<uintptr_t>(T[t]->data) % sizeof(double)) return TBLIS_STRA_ERR_ARG;
+        if (reinterpret_cast<uintptr_t>(T[t]->data) % es) return TBLIS_STRA_ERR_ARG;
 
     // Stage host operands through device memory.
-    const size_t es = sizeof(double);
     void* dptr[3] = {A->data, B->data, C->data};
     Scratch stage[3];
     bool staged[3] = {false, false, false};
@@ -467,8 +559,13 @@ int mult(int level, const tblis_tensor* A, const label_type* idx_A,
         staged[t] = true;
     }
 
-    s = run_fp64(level, impl, g, *dp, static_cast<const double*>(dptr[0]),
-                 static_cast<const double*>(dptr[1]), static_cast<double*>(dptr[2]), st, device);
+    if (fp32)
+        s = run_fp32(level, g, *dp, static_cast<const float*>(dptr[0]), static_cast<const float*>(dptr[1]),
+                     static_cast<float*>(dptr[2]), st, device,
+                     blocking || staged[0] || staged[1] || staged[2]);
+    else
+        s = run_fp64(level, impl, g, *dp, static_cast<const double*>(dptr[0]),
+                     static_cast<const double*>(dptr[1]), static_cast<double*>(dptr[2]), st, device);
     if (s) return s;
 
     if (staged[2])
@@ -480,8 +577,16 @@ int mult(int level, const tblis_tensor* A, const label_type* idx_A,
     if (blocking || staged[0] || staged[1] || staged[2])
         TSB_CUDA(cudaStreamSynchronize(st));
 
-    double one = 1.0;
-    std::memcpy(C->scalar, &one, sizeof one);
+    if (fp32)
+    {
+        float one = 1.0f;
+        std::memcpy(C->scalar, &one, sizeof one);
+    }
+    else
+    {
+        double one = 1.0;
+        std::memcpy(C->scalar, &one, sizeof one);
+    }
     C->conj = 0;
     return TBLIS_STRA_SUCCESS;
 }
@@ -551,6 +656,15 @@ int tblis_stra_set_workspace_limit(size_t bytes)
 
 size_t tblis_stra_get_workspace_limit(void) { return tsb::t_ws_limit; }
 
+int tblis_stra_set_fp32_terms(int terms)
+{
+    if (terms != 3 && terms != 6) return TBLIS_STRA_ERR_ARG;
+    tsb::t_fp32_terms = terms;
+    return TBLIS_STRA_SUCCESS;
+}
+
+int tblis_stra_get_fp32_terms(void) { return tsb::t_fp32_terms; }
+
 int tblis_stra_last_status(void) { return tsb::t_status; }
 
 const char* tblis_stra_status_string(int s)
@@ -568,6 +682,7 @@ const char* tblis_stra_status_string(int s)
         case TBLIS_STRA_ERR_TOO_LARGE:   return "sizes beyond the kernels' index range";
         case TBLIS_STRA_ERR_UNSUPPORTED: return "request not supported by this build";
         case TBLIS_STRA_ERR_NO_DEVICE:   return "no usable CUDA device";
+        case TBLIS_STRA_ERR_TIMEOUT:     return "a kernel's bounded wait expired";
         default:                         return "unknown status";
     }
 }

@@ -59,6 +59,14 @@ struct ScaleArgs
     double beta;
 };
 
+struct ScaleF32Args
+{
+    float* C;
+    const int64_t* rsC; const int64_t* csC; const int64_t* bC;
+    int64_t m, n, batch;
+    float beta;
+};
+
 // Dense S = sum_t sign_t * X[block_t]  (rows x cols per batch, row-major) where
 // X(i, j) = X[bX[b] + rsX[i] + csX[j]].
 struct SumGatherArgs
@@ -129,6 +137,60 @@ struct PackedGemmArgs
     int8_t c_r[4], c_c[4], c_s[4], c_first[4];
 };
 
+// ---- split-BF16 (FP32 contractions on tcgen05) --------------------------------------
+//
+// Planes: P bf16 planes (hi, mid[, lo]) of a scaled FP32 operand sum, each
+// [batch][tiles][nk][128 x 64 block] with blocks in the K-major 128-byte
+// swizzled layout; nk = k_pad / 64.
+constexpr int SPLIT_TILE = 128;
+constexpr int SPLIT_K = 64;
+
+struct SplitScaleArgs
+{
+    const float* X;                            // X(i, p) = X[bX[b] + rs[i] + ks[p]]
+    const int64_t* rs; const int64_t* ks; const int64_t* bX;
+    int64_t rows_full, k_full, rows_blk;
+    int parts;                                 // row parts of the block grid (H)
+    int64_t batch;
+    float* scale;                              // [batch][rows_blk] power-of-two multipliers
+    float* inv;                                // their inverses
+};
+
+struct SplitPackArgs
+{
+    const float* X;
+    const int64_t* rs; const int64_t* ks; const int64_t* bX;
+    int64_t rows_full, k_full, rows_blk, k_blk;
+    int nt;
+    int8_t t_r[4], t_c[4], t_s[4];
+    const float* scale;                        // [batch][rows_blk]
+    int64_t tiles, nk, batch;
+    int planes;                                // 2 (3-term) or 3 (6-term)
+    int kfast;
+    void* out;                                 // bf16 planes
+};
+
+struct SplitGemmArgs
+{
+    const void* A;                             // bf16 planes, A side
+    const void* B;                             // bf16 planes, B side
+    float* C;
+    const int64_t* rsC; const int64_t* csC; const int64_t* bC;
+    const float* invA;                         // [batch][ms] inverse row scales
+    const float* invB;                         // [batch][ns] inverse column scales
+    int64_t m, n, ms, ns, nk, tiles_m, tiles_n, batch;
+    float alpha, beta;
+    int nc;
+    int8_t c_r[4], c_c[4], c_s[4], c_first[4];
+    int planes, nterms;
+    int8_t ta[6], tb[6];                       // plane pair of each product term
+    int* err;                                  // set on a timed-out wait (may be null)
+};
+
+cudaError_t launch_split_scale(const SplitScaleArgs& args, cudaStream_t stream);
+cudaError_t launch_split_pack(const SplitPackArgs& args, cudaStream_t stream);
+cudaError_t launch_split_gemm(const SplitGemmArgs& args, cudaStream_t stream, int num_sms);
+
 cudaError_t launch_pack(const PackArgs& args, cudaStream_t stream);
 cudaError_t launch_packed_gemm(const PackedGemmArgs& args, cudaStream_t stream, int num_sms,
                                int config = -1);
@@ -139,6 +201,7 @@ cudaError_t launch_packed_gemm(const PackedGemmArgs& args, cudaStream_t stream, 
 cudaError_t launch_dmma(const DmmaArgs& args, int terms, cudaStream_t stream, int num_sms,
                         int config = -1);
 cudaError_t launch_scale(const ScaleArgs& args, cudaStream_t stream);
+cudaError_t launch_scale_f32(const ScaleF32Args& args, cudaStream_t stream);
 cudaError_t launch_sum_gather(const SumGatherArgs& args, cudaStream_t stream);
 cudaError_t launch_scatter_add(const ScatterAddArgs& args, cudaStream_t stream);
 

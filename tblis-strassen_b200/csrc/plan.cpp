@@ -192,10 +192,10 @@ int64_t first_stride(const std::vector<int64_t>& len, const std::vector<int64_t>
 // along f), a plain order leaves one operand with no contiguous run inside a
 // k-step.  This splits dA into (a, len/a) and dB into (b, len/b) and puts the
 // two short parts first, so every aligned chunk of a*b consecutive indices is
-// an a x b box: A reads runs of a elements and B runs of b elements (4 x 4 =
-// 16 = the k-step: one 32-byte sector per run for FP64).  Returns whether the
-// order was changed.
-bool block_interleave(std::vector<int64_t>& len, std::vector<std::vector<int64_t>>& str)
+// an a x b box: A reads runs of a elements and B runs of b elements (a = b =
+// one 32-byte sector: 4 x 4 = 16 for FP64, 8 x 8 = 64 for FP32, the k-steps
+// of the kernels).  Returns whether the order was changed.
+bool block_interleave(std::vector<int64_t>& len, std::vector<std::vector<int64_t>>& str, int run)
 {
     const size_t nd = len.size();
     if (nd < 2) return false;
@@ -208,10 +208,12 @@ bool block_interleave(std::vector<int64_t>& len, std::vector<std::vector<int64_t
     const size_t dA = smallest(0), dB = smallest(1);
     if (dA == nd || dB == nd || dA == dB) return false;
     if (std::llabs(str[0][dA]) != 1 || std::llabs(str[1][dB]) != 1) return false;
-    static const int choices[][2] = {{4, 4}, {4, 2}, {2, 4}, {2, 2}};
+    // Runs of `run` elements = one 32-byte sector (4 doubles, 8 floats).
+    const int choices[][2] = {{run, run}, {run, run / 2}, {run / 2, run}, {run / 2, run / 2}, {2, 2}};
     for (auto& c : choices)
     {
         const int64_t a = c[0], b = c[1];
+        if (a < 2 || b < 2) continue;
         if (len[dA] % a || len[dB] % b || len[dA] == a || len[dB] == b) continue;
         std::vector<int64_t> nl;
         std::vector<std::vector<int64_t>> ns(str.size());
@@ -334,7 +336,7 @@ int plan_contraction(const tblis_tensor* A, const label_type* idx_A,
     std::vector<std::vector<int64_t>> k_str = {g.AB.stride[0], g.AB.stride[1]};
     append_modes(k_len, k_str, g.A_only, {0, -1});
     append_modes(k_len, k_str, g.B_only, {-1, 0});
-    const bool k_blocked = block_interleave(k_len, k_str);
+    const bool k_blocked = block_interleave(k_len, k_str, A->type == TYPE_FLOAT ? 8 : 4);
     std::vector<int64_t> b_len = g.ABC.len;
     std::vector<std::vector<int64_t>> b_str = {g.ABC.stride[0], g.ABC.stride[1], g.ABC.stride[2]};
     append_modes(b_len, b_str, g.C_only, {-1, -1, 0});

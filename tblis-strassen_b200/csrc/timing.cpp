@@ -14,7 +14,7 @@ struct Record { int kind; cudaEvent_t start, stop; };
 std::atomic<bool> g_on{false};
 std::mutex g_mu;
 std::vector<Record> g_records;
-thread_local cudaEvent_t t_open[KK_COUNT] = {nullptr, nullptr, nullptr, nullptr};
+thread_local cudaEvent_t t_open[KK_COUNT] = {};
 
 }  // namespace
 

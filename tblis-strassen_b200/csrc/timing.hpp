@@ -15,7 +15,8 @@ enum KernelKind
     KK_PACK = 1,         // pack_kernel
     KK_PACKED_GEMM = 2,  // packed_gemm_kernel
     KK_AUX = 3,          // scale / sum-gather / scatter-add
-    KK_COUNT = 4
+    KK_SPLIT_GEMM = 4,   // split_gemm_kernel (tcgen05, FP32 via bf16 planes)
+    KK_COUNT = 5
 };
 
 bool timing_enabled();

@@ -85,6 +85,9 @@ def _load() -> ctypes.CDLL:
     lib.tblis_stra_kernel_timing.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong),
                                              ctypes.POINTER(ctypes.c_double)]
     lib.tblis_stra_kernel_timing.restype = ctypes.c_int
+    lib.tblis_stra_set_fp32_terms.argtypes = [ctypes.c_int]
+    lib.tblis_stra_set_fp32_terms.restype = ctypes.c_int
+    lib.tblis_stra_get_fp32_terms.restype = ctypes.c_int
     lib.tblis_get_num_threads.restype = ctypes.c_uint
     lib.tblis_set_num_threads.argtypes = [ctypes.c_uint]
     return lib
@@ -227,7 +230,16 @@ def get_workspace_limit() -> int:
     return int(lib.tblis_stra_get_workspace_limit())
 
 
-KERNEL_KINDS = {"fused": 0, "pack": 1, "packed_gemm": 2, "aux": 3}
+KERNEL_KINDS = {"fused": 0, "pack": 1, "packed_gemm": 2, "aux": 3, "split_gemm": 4}
+
+
+def set_fp32_terms(terms: int) -> None:
+    """Split-BF16 product terms for FP32 contractions: 6 (hi/mid/lo) or 3 (hi/mid)."""
+    _check(lib.tblis_stra_set_fp32_terms(terms))
+
+
+def get_fp32_terms() -> int:
+    return int(lib.tblis_stra_get_fp32_terms())
 
 
 def set_kernel_timing(on: bool) -> None:

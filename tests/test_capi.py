@@ -56,7 +56,7 @@ def test_impl_knob(tsb):
 
 
 def test_status_strings(tsb):
-    for s in range(11):
+    for s in range(12):
         assert tsb.status_string(s) != "unknown status"
     assert tsb.status_string(99) == "unknown status"
 

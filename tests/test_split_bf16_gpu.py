@@ -1,0 +1,109 @@
+"""Precision form: FP32 contractions on the BF16 tensor cores (tcgen05) with
+each operand sum split into bf16 planes, checked against the FP64 oracle on
+the same FP32 values (normwise error ||C - Cref||_F / ||Cref||_F):
+
+  6 terms (hi/mid/lo: hh, hm, mh, hl, mm, lh):  <= 1e-6
+  3 terms (hi/mid:    hh, hm, mh):              <= 6e-5
+
+for entries uniform in [-1, 1] and log-uniform magnitudes in [1e-3, 1e3] with
+random sign, at Strassen levels 0, 1, 2."""
+import numpy as np
+import pytest
+
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+TOL = {6: 1e-6, 3: 6e-5}
+
+
+def draw(shape, seed, dist):
+    rng = np.random.default_rng(seed)
+    n = int(np.prod(shape))
+    if dist == "uniform":
+        x = rng.uniform(-1, 1, n)
+    else:
+        x = np.sign(rng.uniform(-1, 1, n)) * 10.0 ** rng.uniform(-3, 3, n)
+    return np.asfortranarray(x.reshape(shape, order="F").astype(np.float32))
+
+
+def to_dev(x, cuda):
+    import torch
+    out = torch.empty_strided(x.shape, [s // x.itemsize for s in x.strides], dtype=torch.float32, device=cuda)
+    out.copy_(torch.from_numpy(x))
+    return out
+
+
+def normwise(C, R):
+    d = np.linalg.norm((C.astype(np.float64) - R).ravel())
+    r = np.linalg.norm(R.ravel())
+    return d / r if r else d
+
+
+@pytest.fixture(params=[6, 3])
+def terms(request, tsb):
+    tsb.set_fp32_terms(request.param)
+    yield request.param
+    tsb.set_fp32_terms(6)
+
+
+@pytest.mark.parametrize("dist", ["uniform", "loguniform"])
+@pytest.mark.parametrize("level", [0, 1, 2])
+def test_fp32_4d_vs_fp64_oracle(tsb, cuda, terms, level, dist):
+    import torch
+    ext = dict(a=24, b=20, c=10, d=12, e=18, f=16)
+    ia, ib, ic = "efac", "fbde", "abcd"
+    A = draw([ext[c] for c in ia], 1, dist)
+    B = draw([ext[c] for c in ib], 2, dist)
+    C0 = draw([ext[c] for c in ic], 3, dist)
+    R = C0.astype(np.float64, order="F")
+    oracle.contract(1.5, A.astype(np.float64, order="F"), ia, B.astype(np.float64, order="F"), ib, 0.5, R, ic)
+    dC = to_dev(C0, cuda)
+    tsb.contract(level, 1.5, to_dev(A, cuda), ia, to_dev(B, cuda), ib, 0.5, dC, ic)
+    torch.cuda.synchronize()
+    err = normwise(dC.cpu().numpy(), R)
+    assert err <= TOL[terms], err
+
+
+@pytest.mark.parametrize("level", [0, 1, 2])
+def test_fp32_ragged_batch_and_beta0(tsb, cuda, terms, level):
+    import torch
+    ext = dict(i=131, j=67, k=150, z=3)
+    A = draw((ext["i"], ext["k"], ext["z"]), 4, "uniform")
+    B = draw((ext["k"], ext["j"], ext["z"]), 5, "uniform")
+    C0 = np.full((ext["i"], ext["j"], ext["z"]), np.nan, dtype=np.float32, order="F")
+    R = np.zeros(C0.shape, order="F")
+    oracle.contract(1.0, A.astype(np.float64, order="F"), "ikz", B.astype(np.float64, order="F"), "kjz", 0.0, R, "ijz")
+    dC = to_dev(C0, cuda)
+    tsb.contract(level, 1.0, to_dev(A, cuda), "ikz", to_dev(B, cuda), "kjz", 0.0, dC, "ijz")
+    torch.cuda.synchronize()
+    out = dC.cpu().numpy()
+    assert np.isfinite(out).all()
+    assert normwise(out, R) <= TOL[terms]
+
+
+@pytest.mark.parametrize("level", [0, 1, 2])
+def test_fp32_config1_size_vs_fp64_gpu(tsb, cuda, terms, level):
+    """NIm = NJn = NPk = 4096 (extents 64): the FP64 GPU path (itself checked
+    against the oracle bound) is the reference; log-uniform magnitudes."""
+    import torch
+    e = 64
+    A = draw((e,) * 4, 7, "loguniform")
+    B = draw((e,) * 4, 8, "loguniform")
+    dA, dB = to_dev(A, cuda), to_dev(B, cuda)
+    C32 = torch.zeros((e,) * 4, dtype=torch.float32, device=cuda)
+    C64 = torch.zeros((e,) * 4, dtype=torch.float64, device=cuda)
+    tsb.contract(level, 1.0, dA, "efac", dB, "fbde", 0.0, C32, "abcd")
+    tsb.contract(0, 1.0, dA.double(), "efac", dB.double(), "fbde", 0.0, C64, "abcd")
+    torch.cuda.synchronize()
+    err = float(torch.linalg.norm((C32.double() - C64).flatten()) / torch.linalg.norm(C64.flatten()))
+    assert err <= TOL[terms], err
+
+
+def test_fp32_host_pointers(tsb, cuda):
+    A = draw((40, 30), 9, "uniform")
+    B = draw((30, 20), 10, "uniform")
+    C = np.zeros((40, 20), dtype=np.float32, order="F")
+    tsb.contract(1, 1.0, A, "ik", B, "kj", 0.0, C, "ij", drop_in=True)
+    R = A.astype(np.float64) @ B.astype(np.float64)
+    assert normwise(C, R) <= 1e-6
