@@ -93,35 +93,57 @@ __global__ void __launch_bounds__(256)
 split_pack_kernel(const __grid_constant__ SplitPackArgs a)
 {
     __shared__ float buf[ST][SK + 1];
+    __shared__ int64_t rowoff[4][ST];            // per term: batch + row offset (or invalid)
+    __shared__ int64_t koff[4][SK];              // per term: k offset (or invalid)
+    __shared__ float rscale[ST];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int64_t c = blockIdx.x;            // k block
     const int64_t t = blockIdx.y;            // row tile
     const int64_t b = blockIdx.z;
     const int64_t r0 = t * ST, k0 = c * SK;
-    const int64_t xoff = a.bX[b];
-#pragma unroll 4
-    for (int x = 0; x < ST * SK / 256; x++)
+    const int nt = a.nt;
+    for (int i = tid; i < nt * ST; i += 256)
     {
-        int r, kk;
-        if (a.kfast) { kk = lane + 32 * (x & 1); r = warp + 8 * (x >> 1); }
-        else         { r = lane + 32 * (x & 3); kk = warp + 8 * (x >> 2); }
-        const int64_t lr = r0 + r, lk = k0 + kk;
-        float v = 0.f;
-        if (lr < a.rows_blk && lk < a.k_blk)
+        const int q = i / ST, r = i % ST;
+        const int64_t lr = r0 + r, gr = a.t_r[q] * a.rows_blk + lr;
+        rowoff[q][r] = (lr < a.rows_blk && gr < a.rows_full) ? a.bX[b] + a.rs[gr] : OFF_INVALID;
+    }
+    for (int i = tid; i < nt * SK; i += 256)
+    {
+        const int q = i / SK, kk = i % SK;
+        const int64_t lk = k0 + kk, gk = a.t_c[q] * a.k_blk + lk;
+        koff[q][kk] = (lk < a.k_blk && gk < a.k_full) ? a.ks[gk] : OFF_INVALID;
+    }
+    for (int i = tid; i < ST; i += 256)
+        rscale[i] = (r0 + i < a.rows_blk) ? a.scale[b * a.rows_blk + r0 + i] : 0.f;
+    __syncthreads();
+    // Terms outermost: all loads of one term are independent and in flight.
+    constexpr int E = ST * SK / 256;
+    float v[E];
+#pragma unroll
+    for (int x = 0; x < E; x++) v[x] = 0.f;
+    for (int q = 0; q < nt; q++)
+    {
+        const bool neg = a.t_s[q] < 0;
+#pragma unroll
+        for (int x = 0; x < E; x++)
         {
-            for (int q = 0; q < a.nt; q++)
+            const int r = a.kfast ? warp + 8 * (x >> 1) : lane + 32 * (x & 3);
+            const int kk = a.kfast ? lane + 32 * (x & 1) : warp + 8 * (x >> 2);
+            const int64_t ro = rowoff[q][r], ko = koff[q][kk];
+            if (ro != OFF_INVALID && ko != OFF_INVALID)
             {
-                const int64_t gr = a.t_r[q] * a.rows_blk + lr;
-                const int64_t gk = a.t_c[q] * a.k_blk + lk;
-                if (gr < a.rows_full && gk < a.k_full)
-                {
-                    const float e = a.X[xoff + a.rs[gr] + a.ks[gk]];
-                    v += a.t_s[q] < 0 ? -e : e;
-                }
+                const float e = a.X[ro + ko];
+                v[x] += neg ? -e : e;
             }
-            v *= a.scale[b * a.rows_blk + lr];
         }
-        buf[r][kk] = v;
+    }
+#pragma unroll
+    for (int x = 0; x < E; x++)
+    {
+        const int r = a.kfast ? warp + 8 * (x >> 1) : lane + 32 * (x & 3);
+        const int kk = a.kfast ? lane + 32 * (x & 1) : warp + 8 * (x >> 2);
+        buf[r][kk] = v[x] * rscale[r];
     }
     __syncthreads();
     // 16-byte chunks: row r, k group g (8 values) -> one chunk per plane.
@@ -451,22 +473,33 @@ split_gemm_kernel(const __grid_constant__ SplitGemmArgs a)
                 mbar_arrive(bar(10 + bacc));
             }
             if (!ok) break;
+            // C update in batches of 32 columns: all loads of a batch are
+            // issued before any store, so their latencies overlap.
             for (int qq = 0; qq < a.nc; qq++)
             {
                 const int64_t ro = rowC[qq * ST + row];
                 if (ro == OFF_INVALID) continue;
                 const float coef = (a.c_s[qq] < 0 ? -a.alpha : a.alpha) * invr[row];
                 const bool first = a.c_first[qq] != 0;
+                const bool read_c = !first || a.beta != 0.f;
+                const float cb = first ? a.beta : 1.f;
+                float* crow = a.C + ro;
 #pragma unroll
-                for (int j = 0; j < ST; j++)
+                for (int j0 = 0; j0 < ST; j0 += 32)
                 {
-                    const int64_t co = colC[qq * ST + j];
-                    if (co == OFF_INVALID) continue;
-                    float* ptr = a.C + ro + co;
-                    float v = coef * acc[j] * invc[j];
-                    if (!first) v += *ptr;
-                    else if (a.beta != 0.f) v += a.beta * *ptr;
-                    *ptr = v;
+                    float cv[32];
+#pragma unroll
+                    for (int i = 0; i < 32; i++)
+                    {
+                        const int64_t co = colC[qq * ST + j0 + i];
+                        cv[i] = (read_c && co != OFF_INVALID) ? crow[co] : 0.f;
+                    }
+#pragma unroll
+                    for (int i = 0; i < 32; i++)
+                    {
+                        const int64_t co = colC[qq * ST + j0 + i];
+                        if (co != OFF_INVALID) crow[co] = coef * acc[j0 + i] * invc[j0 + i] + cb * cv[i];
+                    }
                 }
             }
         }

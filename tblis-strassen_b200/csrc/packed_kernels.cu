@@ -38,37 +38,59 @@ __global__ void __launch_bounds__(PK_THREADS)
 pack_kernel(const __grid_constant__ PackArgs a)
 {
     __shared__ double buf[PACK_TILE][PK_K + 1];
+    __shared__ int64_t rowoff[4][PACK_TILE];     // per term: batch + row offset (or invalid)
+    __shared__ int64_t koff[4][PK_K];            // per term: k offset (or invalid)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int64_t k0 = (int64_t)blockIdx.x * PK_K;
     const int64_t t = blockIdx.y;
     const int64_t b = blockIdx.z;
     const int64_t r0 = t * PACK_TILE;
-    const int64_t xoff = a.bX[b];
+    const int nt = a.nt;
+
+    // Offset tables of this CTA's rows and k values, once per term.
+    for (int i = tid; i < nt * PACK_TILE; i += PK_THREADS)
+    {
+        const int q = i / PACK_TILE, r = i % PACK_TILE;
+        const int64_t lr = r0 + r, gr = a.t_r[q] * a.rows_blk + lr;
+        rowoff[q][r] = (lr < a.rows_blk && gr < a.rows_full) ? a.bX[b] + a.rs[gr] : OFF_INVALID;
+    }
+    for (int i = tid; i < nt * PK_K; i += PK_THREADS)
+    {
+        const int q = i / PK_K, kk = i % PK_K;
+        const int64_t lk = k0 + kk, gk = a.t_c[q] * a.k_blk + lk;
+        koff[q][kk] = (lk < a.k_blk && gk < a.k_full) ? a.ks[gk] : OFF_INVALID;
+    }
+    __syncthreads();
 
     // Gather and sum: with kfast the 32 lanes of a warp walk 32 consecutive k
-    // of one row, else 32 consecutive rows of one k.
-#pragma unroll 4
-    for (int x = 0; x < PACK_TILE * PK_K / PK_THREADS; x++)
+    // of one row, else 32 consecutive rows of one k.  Terms outermost, so all
+    // loads of one term are independent and in flight together.
+    constexpr int E = PACK_TILE * PK_K / PK_THREADS;
+    double v[E];
+#pragma unroll
+    for (int x = 0; x < E; x++) v[x] = 0.0;
+    for (int q = 0; q < nt; q++)
     {
-        int r, kk;
-        if (a.kfast) { kk = lane; r = warp + 8 * x; }
-        else         { r = lane + 32 * (x & 3); kk = warp + 8 * (x >> 2); }
-        const int64_t lr = r0 + r, lk = k0 + kk;
-        double v = 0.0;
-        if (lr < a.rows_blk && lk < a.k_blk)
+        const bool neg = a.t_s[q] < 0;
+#pragma unroll
+        for (int x = 0; x < E; x++)
         {
-            for (int q = 0; q < a.nt; q++)
+            const int r = a.kfast ? warp + 8 * x : lane + 32 * (x & 3);
+            const int kk = a.kfast ? lane : warp + 8 * (x >> 2);
+            const int64_t ro = rowoff[q][r], ko = koff[q][kk];
+            if (ro != OFF_INVALID && ko != OFF_INVALID)
             {
-                const int64_t gr = a.t_r[q] * a.rows_blk + lr;
-                const int64_t gk = a.t_c[q] * a.k_blk + lk;
-                if (gr < a.rows_full && gk < a.k_full)
-                {
-                    const double e = a.X[xoff + a.rs[gr] + a.ks[gk]];
-                    v += a.t_s[q] < 0 ? -e : e;
-                }
+                const double e = a.X[ro + ko];
+                v[x] += neg ? -e : e;
             }
         }
-        buf[r][kk] = v;
+    }
+#pragma unroll
+    for (int x = 0; x < E; x++)
+    {
+        const int r = a.kfast ? warp + 8 * x : lane + 32 * (x & 3);
+        const int kk = a.kfast ? lane : warp + 8 * (x >> 2);
+        buf[r][kk] = v[x];
     }
     __syncthreads();
     // Write tile rows (one k each) in the swizzled order: 128 consecutive
@@ -246,15 +268,34 @@ packed_gemm_kernel(const __grid_constant__ PackedGemmArgs a)
         }
         cp_async_wait<0>();
 
-        // Epilogue: C_q = (first ? beta*C_q : C_q) + sign_q*alpha*S*T.
+        // Epilogue: C_q = (first ? beta*C_q : C_q) + sign_q*alpha*S*T.  All
+        // loads of C are issued before the stores so their latencies overlap.
         for (int q = 0; q < a.nc; q++)
         {
             const int64_t* rt = rowC + q * BM;
             const int64_t* ct = colC + q * BN;
             const double coef = a.c_s[q] < 0 ? -a.alpha : a.alpha;
             const bool first = a.c_first[q] != 0;
+            const bool read_c = !first || a.beta != 0.0;
+            const double cb = first ? a.beta : 1.0;
 #pragma unroll
             for (int mi = 0; mi < MI; mi++)
+            {
+                double cv[2][NI][2];
+#pragma unroll
+                for (int hr = 0; hr < 2; hr++)
+                {
+                    const int64_t ro = rt[wm + mi * 16 + g + hr * 8];
+#pragma unroll
+                    for (int ni = 0; ni < NI; ni++)
+#pragma unroll
+                        for (int hc = 0; hc < 2; hc++)
+                        {
+                            const int64_t co = ct[wn + ni * 8 + t4 * 2 + hc];
+                            cv[hr][ni][hc] = (read_c && ro != OFF_INVALID && co != OFF_INVALID)
+                                                 ? a.C[ro + co] : 0.0;
+                        }
+                }
 #pragma unroll
                 for (int hr = 0; hr < 2; hr++)
                 {
@@ -267,13 +308,10 @@ packed_gemm_kernel(const __grid_constant__ PackedGemmArgs a)
                         {
                             const int64_t co = ct[wn + ni * 8 + t4 * 2 + hc];
                             if (co == OFF_INVALID) continue;
-                            double* ptr = a.C + ro + co;
-                            double v = coef * acc[mi][ni][hr * 2 + hc];
-                            if (!first) v += *ptr;
-                            else if (a.beta != 0.0) v += a.beta * *ptr;
-                            *ptr = v;
+                            a.C[ro + co] = coef * acc[mi][ni][hr * 2 + hc] + cb * cv[hr][ni][hc];
                         }
                 }
+            }
         }
     }
 }
