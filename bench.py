@@ -259,6 +259,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-precision", action="store_true", help="skip the FP32 split-BF16 lines")
     ap.add_argument("--dtype", choices=["f64", "f32"], default="f64",
                     help="operand type of the --kernels probe (f32 = split-BF16 tcgen05 path)")
     ap.add_argument("--terms", type=int, default=6, help="split-BF16 product terms for f32 (3 or 6)")
@@ -399,6 +400,35 @@ def main():
                 "share_of_step": dom_ms / (t * 1e3),
                 "other_kernels_ms": {k: v[1] for k, v in kinds.items() if k != dom}}
 
+    # ---- precision form: FP32 operands on the split-BF16 tcgen05 path -------
+    precision = None
+    if not args.no_precision:
+        A32, B32 = A.float(), B.float()
+        A64r, B64r = A32.double(), B32.double()      # the FP32 values, exactly, in FP64
+        Cref = colmajor(torch, shape, device, fill=0.0)
+        tsb.contract(0, 1.0, A64r, IDX_A, B64r, IDX_B, 0.0, Cref, IDX_C, stream=stream)
+        del A64r, B64r
+        precision = {"oracle": "this library's FP64 L=0 contraction of the same FP32 values",
+                     "tolerance_normwise": {"6": 1e-6, "3": 6e-5}}
+        nref = float(torch.linalg.norm(Cref.flatten()))
+        C32 = colmajor(torch, shape, device, fill=0.0).float()
+        for terms in (6, 3):
+            tsb.set_fp32_terms(terms)
+            for lv in (0, 1, 2):
+                def run32():
+                    tsb.contract(lv, 1.0, A32, IDX_A, B32, IDX_B, 0.0, C32, IDX_C, stream=stream)
+                for _ in range(2):
+                    run32()
+                barrier_sync()
+                tt = max_over_ranks(time_steps(torch, run32, 3, stream))
+                err = float(torch.linalg.norm((C32.double() - Cref).flatten())) / nref
+                precision[f"L{lv}_{terms}terms"] = {"tflops": flops * 3 / tt / 1e12, "normwise_err": err}
+        tsb.set_fp32_terms(6)
+        best6 = max(v["tflops"] for k, v in precision.items() if k.endswith("_6terms"))
+        precision["best_6terms_vs_fp64_L0"] = best6 / levels["L0"]
+        del A32, B32, C32, Cref
+        torch.cuda.empty_cache()
+
     # ---- end to end through the C ABI with pinned host buffers --------------
     e2e = None
     if not args.no_e2e:
@@ -444,6 +474,7 @@ def main():
             "ratio_vs_L0": value / world / levels["L0"] if levels.get("L0") else None,
             "max_err_vs_L0": max_err, "error_bound": bound,
             "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
+            "precision_form": precision,
             "gpu_launches": launches,
             "measured_peaks_file": {k: measured_peaks().get(k) for k in ("hbm_gbs", "bf16_tflops")}}
     print(json.dumps(line))
