@@ -184,6 +184,62 @@ def cpu_reference(ext_sample: int, min_seconds: float, level: int, impl: int):
     return flops / best / 1e12, threads, sample, "reference"
 
 
+def batched_form(torch, tsb, device, stream, count, barrier_sync, max_over_ranks):
+    """The batched uneven workload: `count` contractions with 2-4 indices per
+    bundle, extents uniform in 8..96, bundle products in [512, 8192], random
+    index orders per operand (seed 0), U[-1,1]; one batch plan (grouped
+    launches in one CUDA graph) with autotuned levels, timed against the same
+    batch forced to L=0; FP64, then FP32 (split-BF16, 6 terms)."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from batched_cases import draw_problem
+    rng = np.random.default_rng(0)
+    shapes = [draw_problem(rng) for _ in range(count)]
+    flops = 0.0
+    for ext, ia, ib, ic in shapes:
+        m = np.prod([ext[c] for c in ia if c in ic]); n = np.prod([ext[c] for c in ib if c in ic])
+        k = np.prod([ext[c] for c in ia if c in ib])
+        flops += 2.0 * float(m) * float(n) * float(k)
+    out = {"problems": count, "tflop_per_batch": flops / 1e12,
+           "workload": "2-4 indices per bundle, extents U{8..96}, bundle products in [512, 8192], random orders"}
+    for dtype, name in ((torch.float64, "fp64"), (torch.float32, "fp32_split6")):
+        g = torch.Generator(device=device).manual_seed(1)
+        tens = []
+        for ext, ia, ib, ic in shapes:
+            A = torch.empty([ext[c] for c in ia], dtype=dtype, device=device).uniform_(-1, 1, generator=g)
+            B = torch.empty([ext[c] for c in ib], dtype=dtype, device=device).uniform_(-1, 1, generator=g)
+            C = torch.zeros([ext[c] for c in ic], dtype=dtype, device=device)
+            tens.append((A, ia, B, ib, C, ic))
+        res = {}
+        for mode, lv in (("autotuned", -1), ("all_L0", 0)):
+            probs = [(1.0, A, ia, B, ib, 0.0, C, ic, lv) for A, ia, B, ib, C, ic in tens]
+            t0 = time.perf_counter()
+            batch = tsb.Batch(probs)
+            create_s = time.perf_counter() - t0
+            levels = batch.levels()
+            batch.execute(stream)
+            barrier_sync()
+            n = 3
+            tt = max_over_ranks(time_steps(torch, lambda: batch.execute(stream), n, stream))
+            res[mode] = {"tflops_effective": flops * n / tt / 1e12, "ms_per_batch": tt / n * 1e3,
+                         "create_s": create_s,
+                         "levels": {str(l): levels.count(l) for l in (0, 1, 2)}}
+            batch.close()
+        # spot check: a few problems against the single-call L=0 path
+        worst = 0.0
+        for A, ia, B, ib, C, ic in tens[:: max(1, len(tens) // 8)]:
+            R = torch.zeros_like(C, dtype=torch.float64)
+            tsb.contract(0, 1.0, A.double(), ia, B.double(), ib, 0.0, R, ic, stream=stream)
+            torch.cuda.synchronize()
+            worst = max(worst, float(torch.linalg.norm((C.double() - R).flatten()) / torch.linalg.norm(R.flatten())))
+        res["spot_normwise_err"] = worst
+        res["autotune_gain_vs_L0"] = res["autotuned"]["tflops_effective"] / res["all_L0"]["tflops_effective"]
+        out[name] = res
+        del tens
+        torch.cuda.empty_cache()
+    return out
+
+
 def time_steps(torch, fn, steps, stream):
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
@@ -260,6 +316,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP32 split-BF16 lines")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-form lines")
+    ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--dtype", choices=["f64", "f32"], default="f64",
                     help="operand type of the --kernels probe (f32 = split-BF16 tcgen05 path)")
     ap.add_argument("--terms", type=int, default=6, help="split-BF16 product terms for f32 (3 or 6)")
@@ -456,6 +514,10 @@ def main():
                "path": "stra_tblis_tensor_mult with pinned host tensors (staged copies inside the call)"}
         del hA, hB, hC
 
+    batched = None
+    if not args.no_batched:
+        batched = batched_form(torch, tsb, device, stream, args.batch_count, barrier_sync, max_over_ranks)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         r = cpu_reference(args.cpu_sample_extent, args.cpu_seconds, args.level, args.variant)
@@ -475,6 +537,7 @@ def main():
             "max_err_vs_L0": max_err, "error_bound": bound,
             "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
             "precision_form": precision,
+            "batched_form": batched,
             "gpu_launches": launches,
             "measured_peaks_file": {k: measured_peaks().get(k) for k in ("hbm_gbs", "bf16_tflops")}}
     print(json.dumps(line))

@@ -212,6 +212,33 @@ int tblis_stra_mult_noalloc(int level,
                                   tblis_tensor* C, const label_type* idx_C,
                             void* stream);
 
+/* ---- batched contractions (no counterpart in the reference) --------------
+ *
+ * Many independent contractions with uneven bundles and extents, planned
+ * once and executed as grouped persistent launches (one per kernel
+ * configuration; every Strassen product of every problem of that group in one
+ * grid) captured in one CUDA graph.  Each problem's level is given (0, 1, 2)
+ * or chosen by a measured-time autotuner (-1): every level is timed in a
+ * grouped launch filled with copies of the problem, writing to scratch memory
+ * (never to C), and the fastest is kept; results are cached per process by a
+ * rounded size signature.  All tensors must be device memory and of one
+ * element type per problem; data pointers and scalars are read at create
+ * time.  FP32 problems run the split-BF16 path with 6 terms. */
+typedef struct tblis_stra_problem
+{
+    const tblis_tensor* A; const label_type* idx_A;
+    const tblis_tensor* B; const label_type* idx_B;
+    tblis_tensor* C; const label_type* idx_C;
+    int level;                 /* 0, 1, 2, or -1 = autotuned */
+} tblis_stra_problem;
+
+typedef struct tblis_stra_batch_s* tblis_stra_batch;
+
+int tblis_stra_batch_create(int count, const tblis_stra_problem* problems, tblis_stra_batch* batch);
+int tblis_stra_batch_execute(tblis_stra_batch batch, void* stream);
+int tblis_stra_batch_levels(tblis_stra_batch batch, int* levels);    /* the level each problem runs */
+void tblis_stra_batch_destroy(tblis_stra_batch batch);
+
 /* Per-kernel timing for profiling (no counterpart in the reference, which
  * times whole calls with omp_get_wtime, test/test_strassen.cxx:74-95).  With
  * timing on, every kernel launch is bracketed by CUDA events on its stream;

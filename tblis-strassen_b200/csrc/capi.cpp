@@ -428,44 +428,49 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
     return TBLIS_STRA_SUCCESS;
 }
 
+}  // namespace
+
 // FP32 contraction: split-BF16 tcgen05 path (bf16_split.cu), Strassen products
-// in stream order like the packed FP64 schedule.
-int run_fp32(int level, const GemmView& g, const DevPlan& t, const float* A, const float* B,
-             float* C, cudaStream_t st, int device, bool blocking)
+// in stream order like the packed FP64 schedule.  Workspace layout: row and
+// column scales, A planes, B planes.
+size_t fp32_workspace_bytes(int level, const GemmView& g, int terms)
 {
-    if (g.m == 0 || g.n == 0 || g.batch == 0) return TBLIS_STRA_SUCCESS;
-    if (g.alpha == 0.0 || g.k == 0)
-    {
-        ScaleF32Args s{C, t.rsC, t.csC, t.bC, g.m, g.n, g.batch, (float)g.beta};
-        TSB_CUDA(launch_scale_f32(s, st));
-        return TBLIS_STRA_SUCCESS;
-    }
+    const ProductTable& tab = product_table(level);
+    const int H = tab.H;
+    const int64_t ms = cdiv(g.m, H), ns = cdiv(g.n, H), ks = cdiv(g.k, H);
+    const int64_t nk = cdiv(ks, SPLIT_K);
+    const int64_t tm = cdiv(ms, SPLIT_TILE), tn = cdiv(ns, SPLIT_TILE);
+    const int P = terms == 3 ? 2 : 3;
+    const size_t blk = (size_t)SPLIT_TILE * SPLIT_K * 2;
+    const size_t sc = ((size_t)g.batch * (ms + ns) * 2 * sizeof(float) + 255) / 256 * 256;
+    return sc + (size_t)P * g.batch * (tm + tn) * nk * blk;
+}
+
+int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], const float* A,
+                     const float* B, float* C, cudaStream_t st, int sms, void* ws, size_t ws_bytes,
+                     int terms, int* err)
+{
+    // tb: rsA, rsC, csB, csC, ksA, ksB, bA, bB, bC
     const ProductTable& tab = product_table(level);
     const int H = tab.H;
     const int64_t ms = cdiv(g.m, H), ns = cdiv(g.n, H), ks = cdiv(g.k, H);
     const int64_t nk = cdiv(ks, SPLIT_K);
     const int64_t tm = cdiv(ms, SPLIT_TILE), tn = cdiv(ns, SPLIT_TILE);
     if (g.batch * tm > 65535 || g.batch * tn > 65535 || nk > 2147483647) return TBLIS_STRA_ERR_TOO_LARGE;
-    const int P = t_fp32_terms == 3 ? 2 : 3;
-    const int sms = num_sms(device);
-
-    Scratch scal, planesA, planesB, errbuf;
-    int s;
-    const size_t nsc = (size_t)g.batch * (ms + ns);
-    if ((s = scal.alloc(2 * nsc * sizeof(float), st))) return s;
+    if (ws_bytes < fp32_workspace_bytes(level, g, terms)) return TBLIS_STRA_ERR_ALLOC;
+    const int P = terms == 3 ? 2 : 3;
     const size_t blk = (size_t)SPLIT_TILE * SPLIT_K * 2;
-    if ((s = planesA.alloc((size_t)P * g.batch * tm * nk * blk, st))) return s;
-    if ((s = planesB.alloc((size_t)P * g.batch * tn * nk * blk, st))) return s;
-    if ((s = errbuf.alloc(sizeof(int), st))) return s;
-    TSB_CUDA(cudaMemsetAsync(errbuf.p, 0, sizeof(int), st));
-    float* scaleA = static_cast<float*>(scal.p);
+    const size_t sc = ((size_t)g.batch * (ms + ns) * 2 * sizeof(float) + 255) / 256 * 256;
+    float* scaleA = static_cast<float*>(ws);
     float* invA = scaleA + g.batch * ms;
     float* scaleB = invA + g.batch * ms;
     float* invB = scaleB + g.batch * ns;
+    void* planesA = static_cast<char*>(ws) + sc;
+    void* planesB = static_cast<char*>(planesA) + (size_t)P * g.batch * tm * nk * blk;
 
-    SplitScaleArgs sa{A, t.rsA, t.ksA, t.bA, g.m, g.k, ms, H, g.batch, scaleA, invA};
+    SplitScaleArgs sa{A, tb[0], tb[4], tb[6], g.m, g.k, ms, H, g.batch, scaleA, invA};
     TSB_CUDA(launch_split_scale(sa, st));
-    SplitScaleArgs sb{B, t.csB, t.ksB, t.bB, g.n, g.k, ns, H, g.batch, scaleB, invB};
+    SplitScaleArgs sb{B, tb[2], tb[5], tb[7], g.n, g.k, ns, H, g.batch, scaleB, invB};
     TSB_CUDA(launch_split_scale(sb, st));
 
     const bool a_kfast = g.unit_ksA != 0 && (g.unit_rsA == 0 || g.unit_ksA < g.unit_rsA);
@@ -474,25 +479,25 @@ int run_fp32(int level, const GemmView& g, const DevPlan& t, const float* A, con
     for (const Product& pr : tab.prod)
     {
         SplitPackArgs pa{};
-        pa.X = A; pa.rs = t.rsA; pa.ks = t.ksA; pa.bX = t.bA;
+        pa.X = A; pa.rs = tb[0]; pa.ks = tb[4]; pa.bX = tb[6];
         pa.rows_full = g.m; pa.k_full = g.k; pa.rows_blk = ms; pa.k_blk = ks;
         pa.nt = pr.na;
         for (int i = 0; i < pr.na; i++) { pa.t_r[i] = pr.a[i].r; pa.t_c[i] = pr.a[i].c; pa.t_s[i] = pr.a[i].sign; }
         pa.scale = scaleA; pa.tiles = tm; pa.nk = nk; pa.batch = g.batch; pa.planes = P;
-        pa.kfast = a_kfast; pa.out = planesA.p;
+        pa.kfast = a_kfast; pa.out = planesA;
         TSB_CUDA(launch_split_pack(pa, st));
         SplitPackArgs pb{};
-        pb.X = B; pb.rs = t.csB; pb.ks = t.ksB; pb.bX = t.bB;
+        pb.X = B; pb.rs = tb[2]; pb.ks = tb[5]; pb.bX = tb[7];
         pb.rows_full = g.n; pb.k_full = g.k; pb.rows_blk = ns; pb.k_blk = ks;
         pb.nt = pr.nb;
         for (int i = 0; i < pr.nb; i++) { pb.t_r[i] = pr.b[i].c; pb.t_c[i] = pr.b[i].r; pb.t_s[i] = pr.b[i].sign; }
         pb.scale = scaleB; pb.tiles = tn; pb.nk = nk; pb.batch = g.batch; pb.planes = P;
-        pb.kfast = b_kfast; pb.out = planesB.p;
+        pb.kfast = b_kfast; pb.out = planesB;
         TSB_CUDA(launch_split_pack(pb, st));
 
         SplitGemmArgs ga{};
-        ga.A = planesA.p; ga.B = planesB.p; ga.C = C;
-        ga.rsC = t.rsC; ga.csC = t.csC; ga.bC = t.bC;
+        ga.A = planesA; ga.B = planesB; ga.C = C;
+        ga.rsC = tb[1]; ga.csC = tb[3]; ga.bC = tb[8];
         ga.invA = invA; ga.invB = invB;
         ga.m = g.m; ga.n = g.n; ga.ms = ms; ga.ns = ns; ga.nk = nk;
         ga.tiles_m = tm; ga.tiles_n = tn; ga.batch = g.batch;
@@ -506,9 +511,35 @@ int run_fp32(int level, const GemmView& g, const DevPlan& t, const float* A, con
         ga.planes = P;
         ga.nterms = P == 3 ? 6 : 3;
         for (int i = 0; i < 6; i++) { ga.ta[i] = TA6[i]; ga.tb[i] = TB6[i]; }
-        ga.err = static_cast<int*>(errbuf.p);
+        ga.err = err;
         TSB_CUDA(launch_split_gemm(ga, st, sms));
     }
+    return TBLIS_STRA_SUCCESS;
+}
+
+namespace {
+
+int run_fp32(int level, const GemmView& g, const DevPlan& t, const float* A, const float* B,
+             float* C, cudaStream_t st, int device, bool blocking)
+{
+    if (g.m == 0 || g.n == 0 || g.batch == 0) return TBLIS_STRA_SUCCESS;
+    if (g.alpha == 0.0 || g.k == 0)
+    {
+        ScaleF32Args s{C, t.rsC, t.csC, t.bC, g.m, g.n, g.batch, (float)g.beta};
+        TSB_CUDA(launch_scale_f32(s, st));
+        return TBLIS_STRA_SUCCESS;
+    }
+    const int terms = t_fp32_terms;
+    Scratch wsbuf, errbuf;
+    int s;
+    const size_t wsb = fp32_workspace_bytes(level, g, terms);
+    if ((s = wsbuf.alloc(wsb, st))) return s;
+    if ((s = errbuf.alloc(sizeof(int), st))) return s;
+    TSB_CUDA(cudaMemsetAsync(errbuf.p, 0, sizeof(int), st));
+    const int64_t* tb[9] = {t.rsA, t.rsC, t.csB, t.csC, t.ksA, t.ksB, t.bA, t.bB, t.bC};
+    s = run_fp32_enqueue(level, g, tb, A, B, C, st, num_sms(device), wsbuf.p, wsb, terms,
+                         static_cast<int*>(errbuf.p));
+    if (s) return s;
     if (blocking)
     {
         int err = 0;

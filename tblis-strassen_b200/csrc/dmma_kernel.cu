@@ -106,15 +106,14 @@ __device__ __forceinline__ void lane_map(bool kfast, int e, int& kk, int& m)
     }
 }
 
+// One (batch, tile) work item of a contraction: all of its Strassen products.
 template <class K, bool KA, bool KB>
-__global__ void __launch_bounds__(K::NT, K::MINB)
-stra_dmma_kernel(const __grid_constant__ DmmaArgs args)
+__device__ __forceinline__ void dmma_tile(const DmmaArgs& args, int64_t w, unsigned char* smem)
 {
     constexpr int BM = K::BM, BN = K::BN, BK = K::BK, NT = K::NT;
     constexpr int NA = K::NA, NB = K::NB, STAGES = K::STAGES, R = K::R;
     constexpr int LDA = K::LDA, LDB = K::LDB, MI = K::MI, NI = K::NI;
     constexpr int HMAX = K::HMAX;
-    extern __shared__ __align__(128) unsigned char smem[];
     double* As = reinterpret_cast<double*>(smem);
     double* Bs = reinterpret_cast<double*>(smem + K::a_bytes);
     int64_t* rowA = reinterpret_cast<int64_t*>(smem + K::a_bytes + K::b_bytes);
@@ -137,8 +136,6 @@ stra_dmma_kernel(const __grid_constant__ DmmaArgs args)
     const int H = args.H;
     const int Hc = args.Hc;
 
-    for (int64_t w = blockIdx.x; w < args.work; w += gridDim.x)
-    {
         const int64_t b = w / tiles;
         const int64_t tw = w - b * tiles;
         // Grouped raster (8 tile rows per group) so concurrent CTAs share panels in L2.
@@ -417,6 +414,45 @@ stra_dmma_kernel(const __grid_constant__ DmmaArgs args)
                 }
             }
         }
+}
+
+template <class K, bool KA, bool KB>
+__global__ void __launch_bounds__(K::NT, K::MINB)
+stra_dmma_kernel(const __grid_constant__ DmmaArgs args)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    for (int64_t w = blockIdx.x; w < args.work; w += gridDim.x)
+        dmma_tile<K, KA, KB>(args, w, smem);
+}
+
+// Grouped launch: the work items of many contractions (one descriptor each,
+// in global memory) in one persistent grid; work item w belongs to the
+// problem p with prefix[p] <= w < prefix[p+1].
+template <class K>
+__global__ void __launch_bounds__(K::NT, K::MINB)
+stra_dmma_grouped_kernel(const __grid_constant__ DmmaGroupArgs g)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    for (int64_t w = blockIdx.x; w < g.total; w += gridDim.x)
+    {
+        int lo = 0, hi = g.nprob - 1;
+        while (lo < hi)
+        {
+            const int mid = (lo + hi + 1) >> 1;
+            if (g.prefix[mid] <= w) lo = mid; else hi = mid - 1;
+        }
+        const DmmaArgs& a = g.probs[lo];
+        const int64_t local = w - g.prefix[lo];
+        if (a.a_kfast)
+        {
+            if (a.b_kfast) dmma_tile<K, true, true>(a, local, smem);
+            else           dmma_tile<K, true, false>(a, local, smem);
+        }
+        else
+        {
+            if (a.b_kfast) dmma_tile<K, false, true>(a, local, smem);
+            else           dmma_tile<K, false, false>(a, local, smem);
+        }
     }
 }
 
@@ -463,9 +499,78 @@ using F0 = Cfg<128, 128, 8, 4, 4, 3, 4, 4, 1, 4>;
 using F1 = Cfg<64, 64, 8, 2, 2, 3, 4, 4, 2, 4>;
 using F2 = Cfg<128, 128, 8, 2, 4, 3, 4, 4, 1, 4>;
 
+template <class K>
+cudaError_t launch_group_cfg(const DmmaGroupArgs& g, cudaStream_t stream, int num_sms)
+{
+    static_assert(K::smem <= 227 * 1024, "shared memory budget");
+    auto kern = stra_dmma_grouped_kernel<K>;
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::smem);
+    if (err != cudaSuccess) return err;
+    if (g.total <= 0 || g.nprob <= 0) return cudaSuccess;
+    int per_sm = 0;
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, K::NT, K::smem);
+    if (err != cudaSuccess) return err;
+    if (per_sm < 1) per_sm = 1;
+    int64_t grid = (int64_t)num_sms * per_sm;
+    if (g.total < grid) grid = g.total;
+    timing_begin(KK_FUSED, stream);
+    kern<<<(unsigned)grid, K::NT, K::smem, stream>>>(g);
+    timing_end(KK_FUSED, stream);
+    return cudaGetLastError();
+}
+
+// Configuration family for a request: P* (plain, 1 x 1 grid), G0 (single
+// terms on a grid), T* (two-term sums, grid <= 2), F* (up to four terms).
+int config_family(int terms, int H, int Hc)
+{
+    if (terms <= 1 && H <= 1 && Hc <= 1) return 0;
+    if (terms <= 1) return 1;
+    if (terms <= 2 && H <= 2 && Hc <= 2) return 2;
+    return 3;
+}
+
 }  // namespace
 
 std::atomic<unsigned long long> g_launches{0};
+
+void dmma_tile_shape(int terms, int H, int Hc, int config, int* bm, int* bn)
+{
+    int m = 128, n = 128;
+    switch (config_family(terms, H, Hc))
+    {
+        case 0: if (config == 1) { m = P1::BM; n = P1::BN; } else if (config == 2) { m = P2::BM; n = P2::BN; }
+                else { m = P0::BM; n = P0::BN; } break;
+        case 1: m = G0::BM; n = G0::BN; break;
+        case 2: if (config == 1) { m = T1::BM; n = T1::BN; } else if (config == 2) { m = T2::BM; n = T2::BN; }
+                else { m = T0::BM; n = T0::BN; } break;
+        default: if (config == 1) { m = F1::BM; n = F1::BN; } else if (config == 2) { m = F2::BM; n = F2::BN; }
+                 else { m = F0::BM; n = F0::BN; } break;
+    }
+    *bm = m;
+    *bn = n;
+}
+
+cudaError_t launch_dmma_grouped(const DmmaGroupArgs& g, int terms, int H, int Hc, int config,
+                                cudaStream_t stream, int num_sms)
+{
+    if (terms > 4 || H > 4 || Hc > 4) return cudaErrorInvalidValue;
+    cudaError_t err;
+    switch (config_family(terms, H, Hc))
+    {
+        case 0: err = config == 1 ? launch_group_cfg<P1>(g, stream, num_sms)
+                    : config == 2 ? launch_group_cfg<P2>(g, stream, num_sms)
+                                  : launch_group_cfg<P0>(g, stream, num_sms); break;
+        case 1: err = launch_group_cfg<G0>(g, stream, num_sms); break;
+        case 2: err = config == 1 ? launch_group_cfg<T1>(g, stream, num_sms)
+                    : config == 2 ? launch_group_cfg<T2>(g, stream, num_sms)
+                                  : launch_group_cfg<T0>(g, stream, num_sms); break;
+        default: err = config == 1 ? launch_group_cfg<F1>(g, stream, num_sms)
+                     : config == 2 ? launch_group_cfg<F2>(g, stream, num_sms)
+                                   : launch_group_cfg<F0>(g, stream, num_sms); break;
+    }
+    if (err == cudaSuccess) g_launches++;
+    return err;
+}
 
 unsigned long long launches() { return g_launches.load(); }
 

@@ -50,6 +50,17 @@ struct DmmaArgs
     DevProduct prod[MAX_PRODUCTS];
 };
 
+// Grouped launch of the fused kernel: many contractions (one DmmaArgs each,
+// with tiles_m, tiles_n and work already set for the chosen configuration)
+// in one persistent grid.  prefix[p] = work items before problem p.
+struct DmmaGroupArgs
+{
+    const DmmaArgs* probs;
+    const int64_t* prefix;
+    int nprob;
+    int64_t total;
+};
+
 // Elementwise helpers for the AB and Naive variants and for alpha == 0.
 struct ScaleArgs
 {
@@ -200,6 +211,11 @@ cudaError_t launch_packed_gemm(const PackedGemmArgs& args, cudaStream_t stream, 
 // `config` selects a tile configuration (-1: default for `terms`).
 cudaError_t launch_dmma(const DmmaArgs& args, int terms, cudaStream_t stream, int num_sms,
                         int config = -1);
+// Tile shape (rows x columns per CTA) of the fused-kernel configuration that
+// launch_dmma / launch_dmma_grouped pick for these parameters.
+void dmma_tile_shape(int terms, int H, int Hc, int config, int* bm, int* bn);
+cudaError_t launch_dmma_grouped(const DmmaGroupArgs& g, int terms, int H, int Hc, int config,
+                                cudaStream_t stream, int num_sms);
 cudaError_t launch_scale(const ScaleArgs& args, cudaStream_t stream);
 cudaError_t launch_scale_f32(const ScaleF32Args& args, cudaStream_t stream);
 cudaError_t launch_sum_gather(const SumGatherArgs& args, cudaStream_t stream);

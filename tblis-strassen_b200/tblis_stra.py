@@ -49,6 +49,17 @@ class tblis_tensor(ctypes.Structure):
     ]
 
 
+class tblis_stra_problem(ctypes.Structure):
+    """Layout of ``tblis_stra_problem`` (include/tblis_stra_b200.h)."""
+
+    _fields_ = [
+        ("A", ctypes.POINTER(tblis_tensor)), ("idx_A", ctypes.c_char_p),
+        ("B", ctypes.POINTER(tblis_tensor)), ("idx_B", ctypes.c_char_p),
+        ("C", ctypes.POINTER(tblis_tensor)), ("idx_C", ctypes.c_char_p),
+        ("level", ctypes.c_int),
+    ]
+
+
 def _load() -> ctypes.CDLL:
     if not os.path.exists(LIB_PATH):
         raise ImportError(
@@ -88,6 +99,15 @@ def _load() -> ctypes.CDLL:
     lib.tblis_stra_set_fp32_terms.argtypes = [ctypes.c_int]
     lib.tblis_stra_set_fp32_terms.restype = ctypes.c_int
     lib.tblis_stra_get_fp32_terms.restype = ctypes.c_int
+    PB = ctypes.POINTER(tblis_stra_problem)
+    lib.tblis_stra_batch_create.argtypes = [ctypes.c_int, PB, ctypes.POINTER(ctypes.c_void_p)]
+    lib.tblis_stra_batch_create.restype = ctypes.c_int
+    lib.tblis_stra_batch_execute.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    lib.tblis_stra_batch_execute.restype = ctypes.c_int
+    lib.tblis_stra_batch_levels.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+    lib.tblis_stra_batch_levels.restype = ctypes.c_int
+    lib.tblis_stra_batch_destroy.argtypes = [ctypes.c_void_p]
+    lib.tblis_stra_batch_destroy.restype = None
     lib.tblis_get_num_threads.restype = ctypes.c_uint
     lib.tblis_set_num_threads.argtypes = [ctypes.c_uint]
     return lib
@@ -228,6 +248,50 @@ def set_workspace_limit(nbytes: int | None) -> None:
 
 def get_workspace_limit() -> int:
     return int(lib.tblis_stra_get_workspace_limit())
+
+
+class Batch:
+    """Many contractions planned once and run as grouped launches in one CUDA
+    graph (tblis_stra_batch_*).  ``problems``: iterable of
+    ``(alpha, A, idx_A, B, idx_B, beta, C, idx_C, level)`` with device tensors;
+    level -1 lets the autotuner choose."""
+
+    def __init__(self, problems):
+        self._views = []
+        probs = []
+        for alpha, A, ia, B, ib, beta, C, ic, level in problems:
+            va = _View(A, alpha)
+            vb = _View(B, 1.0, va.code)
+            vc = _View(C, beta, va.code)
+            la, lb, lc = _labels(ia, va.t.ndim), _labels(ib, vb.t.ndim), _labels(ic, vc.t.ndim)
+            self._views.append((va, vb, vc, la, lb, lc))
+            probs.append(tblis_stra_problem(ctypes.pointer(va.t), la, ctypes.pointer(vb.t), lb,
+                                            ctypes.pointer(vc.t), lc, level))
+        self.count = len(probs)
+        arr = (tblis_stra_problem * max(self.count, 1))(*probs)
+        self._arr = arr
+        self._h = ctypes.c_void_p()
+        _check(lib.tblis_stra_batch_create(self.count, arr, ctypes.byref(self._h)))
+
+    def execute(self, stream=None) -> None:
+        handle = None if stream is None else getattr(stream, "cuda_stream", stream)
+        _check(lib.tblis_stra_batch_execute(self._h, handle))
+
+    def levels(self):
+        out = (ctypes.c_int * max(self.count, 1))()
+        _check(lib.tblis_stra_batch_levels(self._h, out))
+        return list(out)[: self.count]
+
+    def close(self) -> None:
+        if self._h:
+            lib.tblis_stra_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 KERNEL_KINDS = {"fused": 0, "pack": 1, "packed_gemm": 2, "aux": 3, "split_gemm": 4}

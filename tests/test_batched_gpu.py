@@ -1,0 +1,95 @@
+"""Batched uneven form: many contractions planned once (tblis_stra_batch_*),
+executed as grouped persistent launches captured in one CUDA graph, with
+autotuned and fixed Strassen levels; every problem checked against the
+library's single-contraction L=0 path (itself checked against the oracle)
+and two problems against the oracle directly."""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from tests.batched_cases import draw_problem
+
+pytestmark = pytest.mark.gpu
+
+
+def make_batch(cuda, n, seed, dtype, lo, hi, pmin, pmax, level):
+    import torch
+    rng = np.random.default_rng(seed)
+    g = torch.Generator(device=cuda).manual_seed(seed)
+    probs = []
+    for i in range(n):
+        ext, ia, ib, ic = draw_problem(rng, lo, hi, pmin, pmax)
+        A = torch.rand([ext[c] for c in ia], dtype=dtype, device=cuda, generator=g) * 2 - 1
+        B = torch.rand([ext[c] for c in ib], dtype=dtype, device=cuda, generator=g) * 2 - 1
+        C = torch.rand([ext[c] for c in ic], dtype=dtype, device=cuda, generator=g) * 2 - 1
+        lv = level if level != "mixed" else (-1 if i % 2 else i % 3)
+        probs.append((1.0 + 0.25 * (i % 3), A, ia, B, ib, 0.5 * (i % 2), C, ic, lv))
+    return probs
+
+
+@pytest.mark.parametrize("level", [-1, 0, 1, 2, "mixed"])
+def test_batched_fp64_matches_single_calls(tsb, cuda, level):
+    import torch
+    probs = make_batch(cuda, 24, 3, torch.float64, 4, 20, 64, 1024, level)
+    refs = []
+    for alpha, A, ia, B, ib, beta, C, ic, _ in probs:
+        R = C.clone()
+        tsb.contract(0, alpha, A, ia, B, ib, beta, R, ic)
+        refs.append(R)
+    batch = tsb.Batch(probs)
+    levels = batch.levels()
+    assert all(l in (0, 1, 2) for l in levels)
+    if level in (0, 1, 2):
+        assert levels == [level] * len(probs)
+    batch.execute()
+    torch.cuda.synchronize()
+    for (alpha, A, ia, B, ib, beta, C, ic, _), R, lv in zip(probs, refs, levels):
+        k = int(np.prod([s for c, s in zip(ia, A.shape) if c not in ic]))
+        bound = oracle.error_bound(lv, k, 1.0, 1.0) * 2 + 1e-13
+        assert float((C - R).abs().max()) <= bound, (ia, ib, ic, lv)
+    # a second execution of the same graph gives the same contraction again
+    before = [C.clone() for (_, _, _, _, _, _, C, _, _) in probs]
+    batch.execute()
+    torch.cuda.synchronize()
+    for (alpha, A, ia, B, ib, beta, C, ic, _), C1 in zip(probs, before):
+        R = C1.clone()
+        tsb.contract(0, alpha, A, ia, B, ib, beta, R, ic)
+        assert torch.allclose(C, R, atol=1e-10, rtol=0)
+    batch.close()
+
+
+def test_batched_against_oracle(tsb, cuda):
+    import torch
+    probs = make_batch(cuda, 6, 9, torch.float64, 3, 9, 16, 128, -1)
+    host = [(alpha, A.cpu().numpy(), ia, B.cpu().numpy(), ib, beta, C.cpu().numpy().copy(), ic)
+            for alpha, A, ia, B, ib, beta, C, ic, _ in probs]
+    batch = tsb.Batch(probs)
+    batch.execute()
+    torch.cuda.synchronize()
+    for (alpha, A, ia, B, ib, beta, C0, ic), p, lv in zip(host, probs, batch.levels()):
+        R = np.asarray(C0, dtype=np.float64).copy()
+        oracle.contract(alpha, np.ascontiguousarray(A), ia, np.ascontiguousarray(B), ib, beta, R, ic)
+        k = int(np.prod([s for c, s in zip(ia, A.shape) if c not in ic]))
+        assert np.abs(p[6].cpu().numpy() - R).max() <= oracle.error_bound(lv, k, 1.0, 1.0) * 2 + 1e-13
+
+
+def test_batched_fp32_split(tsb, cuda):
+    import torch
+    probs = make_batch(cuda, 8, 5, torch.float32, 4, 16, 64, 512, -1)
+    refs = []
+    for alpha, A, ia, B, ib, beta, C, ic, _ in probs:
+        R = C.double()
+        tsb.contract(0, alpha, A.double(), ia, B.double(), ib, beta, R, ic)
+        refs.append(R)
+    batch = tsb.Batch(probs)
+    batch.execute()
+    torch.cuda.synchronize()
+    for (alpha, A, ia, B, ib, beta, C, ic, _), R in zip(probs, refs):
+        err = float(torch.linalg.norm((C.double() - R).flatten()) / torch.linalg.norm(R.flatten()))
+        assert err <= 1e-6, err
+
+
+def test_batch_rejects_host_tensors(tsb):
+    A = np.ones((4, 4)); B = np.ones((4, 4)); C = np.zeros((4, 4))
+    with pytest.raises(tsb.TblisStraError):
+        tsb.Batch([(1.0, A, "ik", B, "kj", 0.0, C, "ij", 0)])
