@@ -211,19 +211,27 @@ def batched_form(torch, tsb, device, stream, count, barrier_sync, max_over_ranks
             C = torch.zeros([ext[c] for c in ic], dtype=dtype, device=device)
             tens.append((A, ia, B, ib, C, ic))
         res = {}
-        for mode, lv in (("autotuned", -1), ("all_L0", 0)):
+        # autotuned (level, variant, tile) vs the plain grouped fused launch at L=0
+        modes = [("autotuned", -1, None)]
+        if dtype == torch.float64:
+            modes.append(("fused_L0", 0, ["fused"]))
+        for mode, lv, allowed in modes:
             probs = [(1.0, A, ia, B, ib, 0.0, C, ic, lv) for A, ia, B, ib, C, ic in tens]
-            t0 = time.perf_counter()
-            batch = tsb.Batch(probs)
-            create_s = time.perf_counter() - t0
-            levels = batch.levels()
+            tsb.set_batch_schedules(allowed)
+            try:
+                batch = tsb.Batch(probs)
+            finally:
+                tsb.set_batch_schedules(None)
+            create_s, tune_s, timings = batch.stats()
+            levels, sched = batch.levels(), batch.schedule()
             batch.execute(stream)
             barrier_sync()
             n = 3
             tt = max_over_ranks(time_steps(torch, lambda: batch.execute(stream), n, stream))
             res[mode] = {"tflops_effective": flops * n / tt / 1e12, "ms_per_batch": tt / n * 1e3,
-                         "create_s": create_s,
-                         "levels": {str(l): levels.count(l) for l in (0, 1, 2)}}
+                         "create_s": create_s, "autotune_s": tune_s, "candidate_timings": timings,
+                         "levels": {str(l): levels.count(l) for l in (0, 1, 2) if levels.count(l)},
+                         "schedules": {k: sched.count(k) for k in sorted(set(sched))}}
             batch.close()
         # spot check: a few problems against the single-call L=0 path
         worst = 0.0
@@ -233,7 +241,8 @@ def batched_form(torch, tsb, device, stream, count, barrier_sync, max_over_ranks
             torch.cuda.synchronize()
             worst = max(worst, float(torch.linalg.norm((C.double() - R).flatten()) / torch.linalg.norm(R.flatten())))
         res["spot_normwise_err"] = worst
-        res["autotune_gain_vs_L0"] = res["autotuned"]["tflops_effective"] / res["all_L0"]["tflops_effective"]
+        if "fused_L0" in res:
+            res["autotuned_vs_fused_L0"] = res["autotuned"]["tflops_effective"] / res["fused_L0"]["tflops_effective"]
         out[name] = res
         del tens
         torch.cuda.empty_cache()

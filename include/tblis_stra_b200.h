@@ -168,6 +168,9 @@ int tblis_stra_get_fp32_terms(void);
 /* Status of the calling thread's last contraction call; string form. */
 int tblis_stra_last_status(void);
 const char* tblis_stra_status_string(int status);
+/* The CUDA call (file:line, expression, error name) behind this thread's
+ * last TBLIS_STRA_ERR_CUDA, or "" (valid until the thread's next call). */
+const char* tblis_stra_last_error_detail(void);
 
 /* The calling thread's default stream (a cudaStream_t; NULL = legacy). */
 int tblis_stra_set_stream(void* stream);
@@ -215,15 +218,33 @@ int tblis_stra_mult_noalloc(int level,
 /* ---- batched contractions (no counterpart in the reference) --------------
  *
  * Many independent contractions with uneven bundles and extents, planned
- * once and executed as grouped persistent launches (one per kernel
- * configuration; every Strassen product of every problem of that group in one
- * grid) captured in one CUDA graph.  Each problem's level is given (0, 1, 2)
- * or chosen by a measured-time autotuner (-1): every level is timed in a
- * grouped launch filled with copies of the problem, writing to scratch memory
- * (never to C), and the fastest is kept; results are cached per process by a
- * rounded size signature.  All tensors must be device memory and of one
- * element type per problem; data pointers and scalars are read at create
- * time.  FP32 problems run the split-BF16 path with 6 terms. */
+ * once and captured in one CUDA graph.  Every problem gets a schedule:
+ *
+ *   TBLIS_STRA_BATCH_FUSED          fused kernel (operand sums formed while
+ *                                   loading, no workspace); all problems of one
+ *                                   level and tile shape share one grouped
+ *                                   persistent launch over every product of
+ *                                   every problem;
+ *   TBLIS_STRA_BATCH_FUSED_SMALL    the same with 64 x 64 tiles;
+ *   TBLIS_STRA_BATCH_PACKED_GROUPED L = 0 only: operands packed into tile
+ *                                   order, problems in chunks of bounded
+ *                                   workspace, one grouped packed-GEMM launch
+ *                                   per chunk (packing of the next chunk
+ *                                   overlaps the current chunk's GEMM);
+ *   TBLIS_STRA_BATCH_PACKED         the packed ABC schedule, problem by problem;
+ *   TBLIS_STRA_BATCH_SPLIT          FP32: the split-BF16 schedule (6 terms),
+ *                                   problem by problem on two graph branches;
+ *   TBLIS_STRA_BATCH_SCALE          alpha == 0 or empty contracted range.
+ *
+ * A problem's level is given (0, 1, 2) or left to the autotuner (-1); the
+ * schedule (variant and tile shape) is always autotuned among the candidates
+ * of the allowed levels.  Candidates are timed with CUDA events on the
+ * problem itself, writing to scratch memory (never to C): grouped schedules
+ * in a grouped launch filled with copies of the problem (its cost inside a
+ * full launch), the others alone; the fastest is kept.  Results are cached
+ * per process by a rounded size signature.  All tensors must be device
+ * memory and of one element type per problem; problems must not write
+ * overlapping C; data pointers and scalars are read at create time. */
 typedef struct tblis_stra_problem
 {
     const tblis_tensor* A; const label_type* idx_A;
@@ -232,11 +253,30 @@ typedef struct tblis_stra_problem
     int level;                 /* 0, 1, 2, or -1 = autotuned */
 } tblis_stra_problem;
 
+enum
+{
+    TBLIS_STRA_BATCH_FUSED = 0,
+    TBLIS_STRA_BATCH_FUSED_SMALL = 1,
+    TBLIS_STRA_BATCH_PACKED_GROUPED = 2,
+    TBLIS_STRA_BATCH_PACKED = 3,
+    TBLIS_STRA_BATCH_SPLIT = 4,
+    TBLIS_STRA_BATCH_SCALE = 5
+};
+
 typedef struct tblis_stra_batch_s* tblis_stra_batch;
 
 int tblis_stra_batch_create(int count, const tblis_stra_problem* problems, tblis_stra_batch* batch);
 int tblis_stra_batch_execute(tblis_stra_batch batch, void* stream);
-int tblis_stra_batch_levels(tblis_stra_batch batch, int* levels);    /* the level each problem runs */
+int tblis_stra_batch_levels(tblis_stra_batch batch, int* levels);      /* the level each problem runs */
+int tblis_stra_batch_schedule(tblis_stra_batch batch, int* schedules); /* TBLIS_STRA_BATCH_* per problem */
+/* FP64 schedules the autotuner may choose on this thread: a mask of bits
+ * (1 << TBLIS_STRA_BATCH_FUSED) | ... over FUSED, FUSED_SMALL, PACKED_GROUPED
+ * and PACKED (default: all four).  A problem with no allowed candidate fails
+ * create with TBLIS_STRA_ERR_ARG. */
+int tblis_stra_set_batch_schedules(unsigned mask);
+unsigned tblis_stra_get_batch_schedules(void);
+/* Seconds spent in create: total and autotuning; candidate timings run. */
+int tblis_stra_batch_stats(tblis_stra_batch batch, double* create_s, double* tune_s, int* timings);
 void tblis_stra_batch_destroy(tblis_stra_batch batch);
 
 /* Per-kernel timing for profiling (no counterpart in the reference, which

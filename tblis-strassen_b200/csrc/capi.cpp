@@ -30,6 +30,7 @@
 
 #include "kernels.cuh"
 #include "plan.hpp"
+#include "schedule.hpp"
 
 extern "C" {
 const tblis_comm* const tblis_single = reinterpret_cast<const tblis_comm*>(&tblis_single);
@@ -44,6 +45,7 @@ thread_local int t_status = TBLIS_STRA_SUCCESS;
 thread_local size_t t_ws_limit = SIZE_MAX;   // device workspace the ABC schedule may use
 thread_local int t_fp32_terms = 6;           // split-BF16 product terms for FP32 (3 or 6)
 unsigned g_num_threads = 1;
+thread_local std::string t_detail;           // what the last failing CUDA call was
 
 // ---- device tables (cached) ------------------------------------------------
 
@@ -97,8 +99,8 @@ int upload_plan(const GemmView& g, int device, std::shared_ptr<DevPlan>& out)
     }
     dp->bytes = total * sizeof(int64_t);
     if (cudaMalloc(&dp->mem, dp->bytes) != cudaSuccess) { dp->mem = nullptr; return TBLIS_STRA_ERR_ALLOC; }
-    if (cudaMemcpy(dp->mem, host.data(), dp->bytes, cudaMemcpyHostToDevice) != cudaSuccess)
-        return TBLIS_STRA_ERR_CUDA;
+    const int s = upload_complete(dp->mem, host.data(), dp->bytes);
+    if (s) return s;
     const int64_t* base = static_cast<const int64_t*>(dp->mem);
     dp->rsA = base + off[0]; dp->rsC = base + off[1]; dp->csB = base + off[2];
     dp->csC = base + off[3]; dp->ksA = base + off[4]; dp->ksB = base + off[5];
@@ -218,7 +220,8 @@ int max_terms(const ProductTable& t)
 
 inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
-#define TSB_CUDA(x) do { if ((x) != cudaSuccess) return TBLIS_STRA_ERR_CUDA; } while (0)
+#define TSB_CUDA(x) do { const cudaError_t e_ = (x); \
+    if (e_ != cudaSuccess) { note_cuda_error(#x, e_, __FILE__, __LINE__); return TBLIS_STRA_ERR_CUDA; } } while (0)
 
 // Dense row-major temporaries of the AB / Naive variants: offset tables.
 struct DenseTables
@@ -268,51 +271,16 @@ void set_grid(DmmaArgs& a, int64_t ms, int64_t ns, int64_t ks)
     a.work = a.batch * (int64_t)a.tiles_m * a.tiles_n;
 }
 
-// Packed schedule of the ABC variant (see packed_kernels.cu).  S and T are
-// reused for every product, in stream order.
-int run_fp64_packed(const ProductTable& tab, const GemmView& g, const DevPlan& t,
-                    const double* A, const double* B, double* C, cudaStream_t st, int sms,
-                    int64_t ms, int64_t ns, int64_t ks, int64_t k_pad, int64_t tm, int64_t tn)
+// Packed schedule of the ABC variant (see packed_kernels.cu) on pool scratch.
+int run_fp64_packed(int level, const GemmView& g, const DevPlan& t, const double* A, const double* B,
+                    double* C, cudaStream_t st, int sms)
 {
-    Scratch Sbuf, Tbuf;
+    const size_t ws = fp64_packed_workspace_bytes(level, g);
+    Scratch buf;
     int s;
-    if ((s = Sbuf.alloc((size_t)(g.batch * tm * k_pad * PACK_TILE) * sizeof(double), st))) return s;
-    if ((s = Tbuf.alloc((size_t)(g.batch * tn * k_pad * PACK_TILE) * sizeof(double), st))) return s;
-    double* S = static_cast<double*>(Sbuf.p);
-    double* T = static_cast<double*>(Tbuf.p);
-    const bool a_kfast = g.unit_ksA != 0 && (g.unit_rsA == 0 || g.unit_ksA < g.unit_rsA);
-    const bool b_kfast = g.unit_ksB != 0 && (g.unit_csB == 0 || g.unit_ksB < g.unit_csB);
-    for (const Product& pr : tab.prod)
-    {
-        PackArgs pa{};
-        pa.X = A; pa.rs = t.rsA; pa.ks = t.ksA; pa.bX = t.bA;
-        pa.rows_full = g.m; pa.k_full = g.k; pa.rows_blk = ms; pa.k_blk = ks;
-        pa.nt = pr.na;
-        for (int i = 0; i < pr.na; i++) { pa.t_r[i] = pr.a[i].r; pa.t_c[i] = pr.a[i].c; pa.t_s[i] = pr.a[i].sign; }
-        pa.tiles = tm; pa.k_pad = k_pad; pa.batch = g.batch; pa.kfast = a_kfast; pa.out = S;
-        TSB_CUDA(launch_pack(pa, st));
-        PackArgs pb{};
-        pb.X = B; pb.rs = t.csB; pb.ks = t.ksB; pb.bX = t.bB;
-        pb.rows_full = g.n; pb.k_full = g.k; pb.rows_blk = ns; pb.k_blk = ks;
-        pb.nt = pr.nb;
-        for (int i = 0; i < pr.nb; i++) { pb.t_r[i] = pr.b[i].c; pb.t_c[i] = pr.b[i].r; pb.t_s[i] = pr.b[i].sign; }
-        pb.tiles = tn; pb.k_pad = k_pad; pb.batch = g.batch; pb.kfast = b_kfast; pb.out = T;
-        TSB_CUDA(launch_pack(pb, st));
-        PackedGemmArgs ga{};
-        ga.S = S; ga.T = T; ga.C = C;
-        ga.rsC = t.rsC; ga.csC = t.csC; ga.bC = t.bC;
-        ga.m = g.m; ga.n = g.n; ga.ms = ms; ga.ns = ns; ga.k_pad = k_pad;
-        ga.tiles_m = tm; ga.tiles_n = tn; ga.batch = g.batch;
-        ga.alpha = g.alpha; ga.beta = g.beta;
-        ga.nc = pr.nc;
-        for (int q = 0; q < pr.nc; q++)
-        {
-            ga.c_r[q] = pr.c[q].r; ga.c_c[q] = pr.c[q].c; ga.c_s[q] = pr.c[q].sign;
-            ga.c_first[q] = pr.c_first[q];
-        }
-        TSB_CUDA(launch_packed_gemm(ga, st, sms));
-    }
-    return TBLIS_STRA_SUCCESS;
+    if ((s = buf.alloc(ws, st))) return s;
+    const int64_t* tb[9] = {t.rsA, t.rsC, t.csB, t.csC, t.ksA, t.ksB, t.bA, t.bB, t.bC};
+    return run_fp64_packed_enqueue(level, g, tb, A, B, C, st, sms, buf.p, ws);
 }
 
 int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
@@ -335,11 +303,9 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
         // Packed schedule (per product: pack the operand sums, GEMM with the
         // +-M update in its epilogue) when its workspace is allowed; else the
         // fully fused kernel, which needs none.
-        const int64_t k_pad = cdiv(ks, PACK_KSTEP) * PACK_KSTEP;
-        const int64_t tm = cdiv(ms, PACK_TILE), tn = cdiv(ns, PACK_TILE);
-        const size_t ws = (size_t)(g.batch * (tm + tn) * k_pad * PACK_TILE) * sizeof(double);
-        if (ws <= t_ws_limit && g.batch * tm <= 65535 && g.batch * tn <= 65535)
-            return run_fp64_packed(tab, g, t, A, B, C, st, sms, ms, ns, ks, k_pad, tm, tn);
+        const PackGeom pg = pack_geom(level, g);
+        if (pg.fits && fp64_packed_workspace_bytes(level, g) <= t_ws_limit)
+            return run_fp64_packed(level, g, t, A, B, C, st, sms);
         DmmaArgs a = base_args(g, t, A, B, C);
         set_grid(a, ms, ns, ks);
         a.nprod = (int)tab.prod.size();
@@ -429,6 +395,129 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
 }
 
 }  // namespace
+
+PackGeom pack_geom(int level, const GemmView& g)
+{
+    const int H = product_table(level).H;
+    PackGeom p;
+    p.ms = cdiv(g.m, H); p.ns = cdiv(g.n, H); p.ks = cdiv(g.k, H);
+    p.k_pad = cdiv(p.ks, PACK_KSTEP) * PACK_KSTEP;
+    p.tm = cdiv(p.ms, PACK_TILE); p.tn = cdiv(p.ns, PACK_TILE);
+    p.s_elems = (size_t)(g.batch * p.tm * p.k_pad * PACK_TILE);
+    p.t_elems = (size_t)(g.batch * p.tn * p.k_pad * PACK_TILE);
+    p.fits = p.tm <= 65535 && p.tn <= 65535 && g.batch <= 65535 && g.batch * p.tm <= 65535 &&
+             g.batch * p.tn <= 65535;
+    return p;
+}
+
+size_t fp64_packed_workspace_bytes(int level, const GemmView& g)
+{
+    const PackGeom p = pack_geom(level, g);
+    return (p.s_elems + p.t_elems) * sizeof(double);
+}
+
+int enqueue_pack_product(const Product& pr, const GemmView& g, const PackGeom& pg,
+                         const int64_t* const tb[9], const double* A, const double* B,
+                         double* S, double* T, cudaStream_t st)
+{
+    const bool a_kfast = g.unit_ksA != 0 && (g.unit_rsA == 0 || g.unit_ksA < g.unit_rsA);
+    const bool b_kfast = g.unit_ksB != 0 && (g.unit_csB == 0 || g.unit_ksB < g.unit_csB);
+    PackArgs pa{};
+    pa.X = A; pa.rs = tb[0]; pa.ks = tb[4]; pa.bX = tb[6];
+    pa.rows_full = g.m; pa.k_full = g.k; pa.rows_blk = pg.ms; pa.k_blk = pg.ks;
+    pa.nt = pr.na;
+    for (int i = 0; i < pr.na; i++) { pa.t_r[i] = pr.a[i].r; pa.t_c[i] = pr.a[i].c; pa.t_s[i] = pr.a[i].sign; }
+    pa.tiles = pg.tm; pa.k_pad = pg.k_pad; pa.batch = g.batch; pa.kfast = a_kfast; pa.out = S;
+    TSB_CUDA(launch_pack(pa, st));
+    PackArgs pb{};
+    pb.X = B; pb.rs = tb[2]; pb.ks = tb[5]; pb.bX = tb[7];
+    pb.rows_full = g.n; pb.k_full = g.k; pb.rows_blk = pg.ns; pb.k_blk = pg.ks;
+    pb.nt = pr.nb;
+    for (int i = 0; i < pr.nb; i++) { pb.t_r[i] = pr.b[i].c; pb.t_c[i] = pr.b[i].r; pb.t_s[i] = pr.b[i].sign; }
+    pb.tiles = pg.tn; pb.k_pad = pg.k_pad; pb.batch = g.batch; pb.kfast = b_kfast; pb.out = T;
+    TSB_CUDA(launch_pack(pb, st));
+    return TBLIS_STRA_SUCCESS;
+}
+
+PackedGemmArgs packed_product_args(const Product& pr, const GemmView& g, const PackGeom& pg,
+                                   const int64_t* const tb[9], const double* S, const double* T,
+                                   double* C)
+{
+    PackedGemmArgs ga{};
+    ga.S = S; ga.T = T; ga.C = C;
+    ga.rsC = tb[1]; ga.csC = tb[3]; ga.bC = tb[8];
+    ga.m = g.m; ga.n = g.n; ga.ms = pg.ms; ga.ns = pg.ns; ga.k_pad = pg.k_pad;
+    ga.tiles_m = pg.tm; ga.tiles_n = pg.tn; ga.batch = g.batch;
+    ga.alpha = g.alpha; ga.beta = g.beta;
+    ga.nc = pr.nc;
+    for (int q = 0; q < pr.nc; q++)
+    {
+        ga.c_r[q] = pr.c[q].r; ga.c_c[q] = pr.c[q].c; ga.c_s[q] = pr.c[q].sign;
+        ga.c_first[q] = pr.c_first[q];
+    }
+    return ga;
+}
+
+// S and T are reused for every product, in stream order.
+int run_fp64_packed_enqueue(int level, const GemmView& g, const int64_t* const tb[9],
+                            const double* A, const double* B, double* C, cudaStream_t st, int sms,
+                            void* ws, size_t ws_bytes)
+{
+    const PackGeom pg = pack_geom(level, g);
+    if (!pg.fits) return TBLIS_STRA_ERR_TOO_LARGE;
+    if (ws_bytes < (pg.s_elems + pg.t_elems) * sizeof(double)) return TBLIS_STRA_ERR_ALLOC;
+    double* S = static_cast<double*>(ws);
+    double* T = S + pg.s_elems;
+    for (const Product& pr : product_table(level).prod)
+    {
+        int s = enqueue_pack_product(pr, g, pg, tb, A, B, S, T, st);
+        if (s) return s;
+        TSB_CUDA(launch_packed_gemm(packed_product_args(pr, g, pg, tb, S, T, C), st, sms));
+    }
+    return TBLIS_STRA_SUCCESS;
+}
+
+// Host -> device copy that has landed when this returns.  cudaMemcpy from
+// pageable memory may return before its DMA completes, and kernels on
+// non-blocking streams are not ordered after it, so tables read by such
+// kernels go through a private non-blocking stream per device, synchronised.
+int upload_complete(void* dst, const void* src, size_t bytes)
+{
+    static std::mutex mu;
+    static std::map<int, cudaStream_t> streams;
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) { cudaGetLastError(); return TBLIS_STRA_ERR_NO_DEVICE; }
+    cudaStream_t st = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = streams.find(device);
+        if (it == streams.end())
+        {
+            if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
+            {
+                cudaGetLastError();
+                return TBLIS_STRA_ERR_CUDA;
+            }
+            streams[device] = st;
+        }
+        else st = it->second;
+    }
+    TSB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+    TSB_CUDA(cudaStreamSynchronize(st));
+    return TBLIS_STRA_SUCCESS;
+}
+
+void note_cuda_error(const char* what, cudaError_t e, const char* file, int line)
+{
+    const char* base = std::strrchr(file, '/');
+    t_detail = std::string(base ? base + 1 : file) + ":" + std::to_string(line) + " " + what + ": " +
+               cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    cudaGetLastError();
+}
+
+void note_detail(const std::string& what) { t_detail = what; }
+
+void clear_detail() { t_detail.clear(); }
 
 // FP32 contraction: split-BF16 tcgen05 path (bf16_split.cu), Strassen products
 // in stream order like the packed FP64 schedule.  Workspace layout: row and
@@ -554,6 +643,7 @@ int mult(int level, const tblis_tensor* A, const label_type* idx_A,
          const tblis_tensor* B, const label_type* idx_B,
          tblis_tensor* C, const label_type* idx_C, cudaStream_t st, bool blocking)
 {
+    clear_detail();
     if (level < 0 || level > 2) return TBLIS_STRA_ERR_ARG;
     const int impl = t_impl;
     if (!A || !B || !C) return TBLIS_STRA_ERR_NULL;
@@ -697,6 +787,8 @@ int tblis_stra_set_fp32_terms(int terms)
 int tblis_stra_get_fp32_terms(void) { return tsb::t_fp32_terms; }
 
 int tblis_stra_last_status(void) { return tsb::t_status; }
+
+const char* tblis_stra_last_error_detail(void) { return tsb::t_detail.c_str(); }
 
 const char* tblis_stra_status_string(int s)
 {

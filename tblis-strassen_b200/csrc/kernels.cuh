@@ -146,6 +146,16 @@ struct PackedGemmArgs
     double alpha, beta;
     int nc;
     int8_t c_r[4], c_c[4], c_s[4], c_first[4];
+    int pad_;                                  // 8-byte multiple (copied as words)
+};
+
+// Grouped packed GEMM: many problems' tiles in one persistent launch.
+struct PackedGroupArgs
+{
+    const PackedGemmArgs* probs;   // device array [nprob]
+    const int64_t* prefix;         // device array [nprob + 1]: work prefix sums
+    int nprob;
+    int64_t total;
 };
 
 // ---- split-BF16 (FP32 contractions on tcgen05) --------------------------------------
@@ -205,6 +215,7 @@ cudaError_t launch_split_gemm(const SplitGemmArgs& args, cudaStream_t stream, in
 cudaError_t launch_pack(const PackArgs& args, cudaStream_t stream);
 cudaError_t launch_packed_gemm(const PackedGemmArgs& args, cudaStream_t stream, int num_sms,
                                int config = -1);
+cudaError_t launch_packed_gemm_grouped(const PackedGroupArgs& args, cudaStream_t stream, int num_sms);
 
 // Launchers (kernels.cu).  `terms` = largest number of blocks in one sum
 // (1, 2 or 4), selecting the kernel instance.  Return a cudaError_t.

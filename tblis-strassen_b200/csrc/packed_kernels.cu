@@ -150,13 +150,12 @@ struct PCfg
     static_assert((BK * BM / 2) % NT == 0, "16-byte chunks per thread");
 };
 
+// One output tile (work item w of the problem `a`) of the packed GEMM.
 template <class K>
-__global__ void __launch_bounds__(K::NT, 1)
-packed_gemm_kernel(const __grid_constant__ PackedGemmArgs a)
+__device__ __forceinline__ void packed_tile(const PackedGemmArgs& a, int64_t w, unsigned char* smem)
 {
     constexpr int BM = K::BM, BN = K::BN, BK = K::BK, NT = K::NT, STAGES = K::STAGES;
     constexpr int MI = K::MI, NI = K::NI;
-    extern __shared__ __align__(128) unsigned char smem[];
     double* As = reinterpret_cast<double*>(smem);
     double* Bs = As + STAGES * BK * BM;
     int64_t* rowC = reinterpret_cast<int64_t*>(Bs + STAGES * BK * BN);
@@ -167,10 +166,8 @@ packed_gemm_kernel(const __grid_constant__ PackedGemmArgs a)
     const int wm = (warp / K::WN) * K::WTM;
     const int wn = (warp % K::WN) * K::WTN;
     const int64_t tiles = a.tiles_m * a.tiles_n;
-    const int64_t work = a.batch * tiles;
     const int64_t nk = a.k_pad / BK;
 
-    for (int64_t w = blockIdx.x; w < work; w += gridDim.x)
     {
         const int64_t b = w / tiles;
         const int64_t tw = w - b * tiles;
@@ -317,6 +314,48 @@ packed_gemm_kernel(const __grid_constant__ PackedGemmArgs a)
 }
 
 template <class K>
+__global__ void __launch_bounds__(K::NT, 1)
+packed_gemm_kernel(const __grid_constant__ PackedGemmArgs a)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int64_t work = a.batch * a.tiles_m * a.tiles_n;
+    for (int64_t w = blockIdx.x; w < work; w += gridDim.x) packed_tile<K>(a, w, smem);
+}
+
+// Grouped form: one persistent grid over the tiles of many problems (each
+// with its own packed S and T); work item w belongs to the problem p with
+// prefix[p] <= w < prefix[p + 1].  The problem's descriptor is staged in
+// shared memory whenever a CTA moves to another problem.
+template <class K>
+__global__ void __launch_bounds__(K::NT, 1)
+packed_gemm_grouped_kernel(const __grid_constant__ PackedGroupArgs g)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ PackedGemmArgs desc;
+    static_assert(sizeof(PackedGemmArgs) % 8 == 0, "descriptor copied as 8-byte words");
+    int cur = -1;
+    for (int64_t w = blockIdx.x; w < g.total; w += gridDim.x)
+    {
+        int lo = 0, hi = g.nprob - 1;
+        while (lo < hi)
+        {
+            const int mid = (lo + hi + 1) >> 1;
+            if (g.prefix[mid] <= w) lo = mid; else hi = mid - 1;
+        }
+        if (lo != cur)
+        {
+            __syncthreads();   // the previous tile no longer reads the descriptor
+            const int64_t* src = reinterpret_cast<const int64_t*>(g.probs + lo);
+            int64_t* dst = reinterpret_cast<int64_t*>(&desc);
+            for (int i = threadIdx.x; i < (int)(sizeof(PackedGemmArgs) / 8); i += blockDim.x) dst[i] = src[i];
+            __syncthreads();
+            cur = lo;
+        }
+        packed_tile<K>(desc, w - g.prefix[lo], smem);
+    }
+}
+
+template <class K>
 cudaError_t launch_packed_cfg(const PackedGemmArgs& a, cudaStream_t stream, int num_sms)
 {
     static_assert(K::smem <= 227 * 1024, "shared memory budget");
@@ -333,6 +372,26 @@ cudaError_t launch_packed_cfg(const PackedGemmArgs& a, cudaStream_t stream, int 
     if (work < grid) grid = work;
     timing_begin(KK_PACKED_GEMM, stream);
     kern<<<(unsigned)grid, K::NT, K::smem, stream>>>(a);
+    timing_end(KK_PACKED_GEMM, stream);
+    return cudaGetLastError();
+}
+
+template <class K>
+cudaError_t launch_packed_grouped_cfg(const PackedGroupArgs& g, cudaStream_t stream, int num_sms)
+{
+    constexpr size_t static_smem = sizeof(PackedGemmArgs);
+    static_assert(K::smem + static_smem <= 227 * 1024, "shared memory budget");
+    auto kern = packed_gemm_grouped_kernel<K>;
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::smem);
+    if (err != cudaSuccess) return err;
+    int per_sm = 0;
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, K::NT, K::smem);
+    if (err != cudaSuccess) return err;
+    if (per_sm < 1) per_sm = 1;
+    int64_t grid = (int64_t)num_sms * per_sm;
+    if (g.total < grid) grid = g.total;
+    timing_begin(KK_PACKED_GEMM, stream);
+    kern<<<(unsigned)grid, K::NT, K::smem, stream>>>(g);
     timing_end(KK_PACKED_GEMM, stream);
     return cudaGetLastError();
 }
@@ -378,6 +437,14 @@ cudaError_t launch_packed_gemm(const PackedGemmArgs& a, cudaStream_t stream, int
         case 3:  err = launch_packed_cfg<PG3>(a, stream, num_sms); break;
         default: err = launch_packed_cfg<PG0>(a, stream, num_sms); break;
     }
+    if (err == cudaSuccess) g_launches++;
+    return err;
+}
+
+cudaError_t launch_packed_gemm_grouped(const PackedGroupArgs& g, cudaStream_t stream, int num_sms)
+{
+    if (g.nprob <= 0 || g.total <= 0) return cudaSuccess;
+    const cudaError_t err = launch_packed_grouped_cfg<PG0>(g, stream, num_sms);
     if (err == cudaSuccess) g_launches++;
     return err;
 }

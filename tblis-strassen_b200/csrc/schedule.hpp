@@ -1,0 +1,62 @@
+// Host-side schedules shared by the single-call entry points (capi.cpp) and
+// the batched plans (batch.cpp).  Scatter-vector tables are passed as nine
+// device pointers in the order rsA, rsC, csB, csC, ksA, ksB, bA, bB, bC.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include "kernels.cuh"
+#include "plan.hpp"
+
+namespace tsb {
+
+// The failing CUDA call behind the last TBLIS_STRA_ERR_CUDA of this thread
+// (tblis_stra_last_error_detail); note_cuda_error also clears the runtime's
+// last-error state.
+void note_cuda_error(const char* what, cudaError_t e, const char* file, int line);
+void note_detail(const std::string& what);
+void clear_detail();
+
+// Host -> device copy complete on return (see capi.cpp).
+int upload_complete(void* dst, const void* src, size_t bytes);
+
+// Block and tile geometry of the packed FP64 schedule at one Strassen level.
+struct PackGeom
+{
+    int64_t ms, ns, ks;     // block extents (ceil(m / 2^L) ...)
+    int64_t k_pad;          // ks rounded up to the pack k-step
+    int64_t tm, tn;         // 128-row tiles of S and T per batch entry
+    size_t s_elems, t_elems;
+    bool fits;              // pack grid limits hold
+};
+PackGeom pack_geom(int level, const GemmView& g);
+
+// Bytes of S + T for the packed schedule (one product at a time).
+size_t fp64_packed_workspace_bytes(int level, const GemmView& g);
+
+// Pack product `pr`'s operand sums into S and T (two launches).
+int enqueue_pack_product(const Product& pr, const GemmView& g, const PackGeom& pg,
+                         const int64_t* const tb[9], const double* A, const double* B,
+                         double* S, double* T, cudaStream_t st);
+
+// Descriptor of product `pr`'s packed GEMM (+-alpha*S*T into its C blocks).
+PackedGemmArgs packed_product_args(const Product& pr, const GemmView& g, const PackGeom& pg,
+                                   const int64_t* const tb[9], const double* S, const double* T,
+                                   double* C);
+
+// Whole packed ABC schedule of one FP64 contraction on caller workspace.
+int run_fp64_packed_enqueue(int level, const GemmView& g, const int64_t* const tb[9],
+                            const double* A, const double* B, double* C, cudaStream_t st, int sms,
+                            void* ws, size_t ws_bytes);
+
+// Split-BF16 schedule of one FP32 contraction on caller workspace.
+size_t fp32_workspace_bytes(int level, const GemmView& g, int terms);
+int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], const float* A,
+                     const float* B, float* C, cudaStream_t st, int sms, void* ws, size_t ws_bytes,
+                     int terms, int* err);
+
+}  // namespace tsb

@@ -85,6 +85,7 @@ def _load() -> ctypes.CDLL:
     lib.tblis_stra_get_stream.restype = ctypes.c_void_p
     lib.tblis_stra_launch_count.restype = ctypes.c_ulonglong
     lib.tblis_stra_version.restype = ctypes.c_char_p
+    lib.tblis_stra_last_error_detail.restype = ctypes.c_char_p
     P64 = ctypes.POINTER(ctypes.c_int64)
     lib.tblis_stra_plan_query.argtypes = [T, S, T, S, T, S, P64, ctypes.POINTER(ctypes.c_double)] + [P64] * 9
     lib.tblis_stra_plan_query.restype = ctypes.c_int
@@ -106,6 +107,14 @@ def _load() -> ctypes.CDLL:
     lib.tblis_stra_batch_execute.restype = ctypes.c_int
     lib.tblis_stra_batch_levels.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
     lib.tblis_stra_batch_levels.restype = ctypes.c_int
+    lib.tblis_stra_batch_schedule.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+    lib.tblis_stra_batch_schedule.restype = ctypes.c_int
+    lib.tblis_stra_batch_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                           ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]
+    lib.tblis_stra_batch_stats.restype = ctypes.c_int
+    lib.tblis_stra_set_batch_schedules.argtypes = [ctypes.c_uint]
+    lib.tblis_stra_set_batch_schedules.restype = ctypes.c_int
+    lib.tblis_stra_get_batch_schedules.restype = ctypes.c_uint
     lib.tblis_stra_batch_destroy.argtypes = [ctypes.c_void_p]
     lib.tblis_stra_batch_destroy.restype = None
     lib.tblis_get_num_threads.restype = ctypes.c_uint
@@ -122,7 +131,11 @@ def status_string(status: int) -> str:
 
 def _check(status: int) -> None:
     if status != 0:
-        raise TblisStraError(status, status_string(status))
+        msg = status_string(status)
+        detail = lib.tblis_stra_last_error_detail()
+        if detail:
+            msg += " [" + detail.decode(errors="replace") + "]"
+        raise TblisStraError(status, msg)
 
 
 class _View:
@@ -250,6 +263,21 @@ def get_workspace_limit() -> int:
     return int(lib.tblis_stra_get_workspace_limit())
 
 
+SCHEDULES = {"fused": 0, "fused_small": 1, "packed_grouped": 2, "packed": 3, "split": 4, "scale": 5}
+SCHEDULE_NAMES = {v: k for k, v in SCHEDULES.items()}
+
+
+def set_batch_schedules(names) -> None:
+    """FP64 schedules the batch autotuner may pick on this thread (None = all):
+    any of "fused", "fused_small", "packed_grouped", "packed"."""
+    if names is None:
+        names = ["fused", "fused_small", "packed_grouped", "packed"]
+    mask = 0
+    for n in names:
+        mask |= 1 << SCHEDULES[n]
+    _check(lib.tblis_stra_set_batch_schedules(ctypes.c_uint(mask)))
+
+
 class Batch:
     """Many contractions planned once and run as grouped launches in one CUDA
     graph (tblis_stra_batch_*).  ``problems``: iterable of
@@ -281,6 +309,18 @@ class Batch:
         out = (ctypes.c_int * max(self.count, 1))()
         _check(lib.tblis_stra_batch_levels(self._h, out))
         return list(out)[: self.count]
+
+    def schedule(self):
+        """Schedule name of every problem (see SCHEDULES)."""
+        out = (ctypes.c_int * max(self.count, 1))()
+        _check(lib.tblis_stra_batch_schedule(self._h, out))
+        return [SCHEDULE_NAMES[v] for v in list(out)[: self.count]]
+
+    def stats(self):
+        """(create seconds, autotune seconds, candidate timings run)."""
+        c, t, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        _check(lib.tblis_stra_batch_stats(self._h, ctypes.byref(c), ctypes.byref(t), ctypes.byref(n)))
+        return c.value, t.value, n.value
 
     def close(self) -> None:
         if self._h:

@@ -89,6 +89,77 @@ def test_batched_fp32_split(tsb, cuda):
         assert err <= 1e-6, err
 
 
+@pytest.mark.parametrize("schedule", ["fused", "fused_small", "packed_grouped", "packed"])
+@pytest.mark.parametrize("level", [-1, 0, 1, 2])
+def test_batched_fp64_each_schedule(tsb, cuda, schedule, level):
+    """Every FP64 schedule, alone, against single L=0 calls; packed_grouped
+    with a 1 MiB chunk limit, so every problem is its own chunk and the two
+    chunk workspaces alternate (packing of chunk c waits for the GEMM of
+    chunk c-2)."""
+    import os
+    import torch
+    probs = make_batch(cuda, 12, 21, torch.float64, 4, 20, 64, 1024, level)
+    refs = []
+    for alpha, A, ia, B, ib, beta, C, ic, _ in probs:
+        R = C.clone()
+        tsb.contract(0, alpha, A, ia, B, ib, beta, R, ic)
+        refs.append(R)
+    os.environ["TBLIS_STRA_BATCH_CHUNK_BYTES"] = str(1 << 20)
+    try:
+        tsb.set_batch_schedules([schedule])
+        if (schedule == "fused_small" and level == 1) or (schedule == "packed_grouped" and level in (1, 2)):
+            with pytest.raises(tsb.TblisStraError):
+                tsb.Batch(probs)
+            return
+        batch = tsb.Batch(probs)
+    finally:
+        tsb.set_batch_schedules(None)
+        del os.environ["TBLIS_STRA_BATCH_CHUNK_BYTES"]
+    levels, sched = batch.levels(), batch.schedule()
+    assert set(sched) == {schedule}
+    if level >= 0:
+        assert levels == [level] * len(probs)
+    for rep in range(2):
+        if rep:   # the second execution starts from the first one's C
+            refs = []
+            for alpha, A, ia, B, ib, beta, C, ic, _ in probs:
+                R = C.clone()
+                tsb.contract(0, alpha, A, ia, B, ib, beta, R, ic)
+                refs.append(R)
+        batch.execute()
+        torch.cuda.synchronize()
+        for (alpha, A, ia, B, ib, beta, C, ic, _), R, lv in zip(probs, refs, levels):
+            k = int(np.prod([s for c, s in zip(ia, A.shape) if c not in ic]))
+            bound = oracle.error_bound(lv, k, 1.0, 1.0) * 2 + 1e-13
+            assert float((C - R).abs().max()) <= bound, (schedule, ia, ib, ic, lv, rep)
+    c, t, n = batch.stats()
+    assert c >= t >= 0.0 and n >= 0
+    batch.close()
+
+
+def test_batched_fp64_large_levels(tsb, cuda):
+    """Problems large enough for the tuner to consider L=1 (blocks of 1024 in
+    every dimension), mixed with small ones, against single L=0 calls."""
+    import torch
+    g = torch.Generator(device=cuda).manual_seed(4)
+    shapes = [((48, 48), (48, 48), (48, 48)), ((8, 16), (32, 8), (16, 16)), ((64, 40), (40, 64), (32, 64))]
+    probs, refs = [], []
+    for (m1, m2), (n1, n2), (k1, k2) in shapes:
+        A = torch.rand((m1, k1, m2, k2), dtype=torch.float64, device=cuda, generator=g) * 2 - 1
+        B = torch.rand((k2, n1, k1, n2), dtype=torch.float64, device=cuda, generator=g) * 2 - 1
+        C = torch.rand((n1, m1, m2, n2), dtype=torch.float64, device=cuda, generator=g) * 2 - 1
+        probs.append((1.0, A, "aibj", B, "jcid", 1.0, C, "cabd", -1))
+        R = C.clone()
+        tsb.contract(0, 1.0, A, "aibj", B, "jcid", 1.0, R, "cabd")
+        refs.append(R)
+    batch = tsb.Batch(probs)
+    batch.execute()
+    torch.cuda.synchronize()
+    for (_, A, ia, B, ib, _, C, ic, _), R, lv in zip(probs, refs, batch.levels()):
+        k = int(np.prod([s for c, s in zip(ia, A.shape) if c not in ic]))
+        assert float((C - R).abs().max()) <= oracle.error_bound(lv, k, 1.0, 1.0) * 2 + 1e-13
+
+
 def test_batch_rejects_host_tensors(tsb):
     A = np.ones((4, 4)); B = np.ones((4, 4)); C = np.zeros((4, 4))
     with pytest.raises(tsb.TblisStraError):

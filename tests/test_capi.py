@@ -86,3 +86,17 @@ def test_bad_level_is_rejected(tsb):
     with pytest.raises(tsb.TblisStraError) as e:
         tsb.contract(3, 1.0, A, "ik", A, "kj", 0.0, C, "ij")
     assert e.value.status == 5
+
+
+def test_batch_schedule_mask(tsb):
+    try:
+        tsb.set_batch_schedules(["packed_grouped", "fused"])
+        assert tsb.lib.tblis_stra_get_batch_schedules() == (1 << 2) | (1 << 0)
+        with pytest.raises(tsb.TblisStraError):
+            tsb.set_batch_schedules([])            # empty mask
+        with pytest.raises(tsb.TblisStraError):
+            tsb.set_batch_schedules(["split"])     # FP32 schedule is not selectable
+        assert tsb.lib.tblis_stra_get_batch_schedules() == (1 << 2) | (1 << 0)
+    finally:
+        tsb.set_batch_schedules(None)
+    assert tsb.lib.tblis_stra_get_batch_schedules() == 0b1111
