@@ -24,9 +24,10 @@
 // schedules are timed in a grouped launch holding enough copies of the
 // problem to fill the GPU twice (their cost inside a full grouped launch,
 // not their latency alone); problem-by-problem schedules run alone.  The
-// fastest candidate wins; the choice is cached per process by a size
-// signature (type, m, n, k rounded to half an octave, batch, loader mappings,
-// requested level, allowed schedules).
+// fastest candidate wins (a Strassen level by a 2 % margin); the choice is
+// cached per process by a size signature (type, m, n, k rounded to the
+// nearest power of two, batch, requested level, allowed schedules), so
+// problems of one size class share one set of timings.
 #include "tblis_stra_b200.h"
 
 #include <cuda_runtime.h>
@@ -174,45 +175,66 @@ struct DevBuf
     }
 };
 
-// Descriptors + work prefix of one grouped launch in one device allocation.
+// Descriptors + work prefix of one grouped launch, written into `mem`
+// (capacity `cap` bytes) and complete on return.
 template <class Desc>
-int upload_descs(const std::vector<Desc>& d, const std::vector<int64_t>& work, DevBuf& buf,
-                 const Desc*& probs, const int64_t*& prefix, int64_t& total)
+size_t descs_bytes(size_t n) { return (n * sizeof(Desc) + 15) / 16 * 16 + (n + 1) * sizeof(int64_t); }
+
+template <class Desc>
+int fill_descs(const std::vector<Desc>& d, const std::vector<int64_t>& work, void* mem, size_t cap,
+               const Desc*& probs, const int64_t*& prefix, int64_t& total)
 {
     std::vector<int64_t> pre(d.size() + 1, 0);
     for (size_t i = 0; i < d.size(); i++) pre[i + 1] = pre[i] + work[i];
     const size_t bytes_d = (d.size() * sizeof(Desc) + 15) / 16 * 16;
-    const size_t bytes = bytes_d + pre.size() * sizeof(int64_t);
-    int s = buf.alloc(bytes);
-    if (s) return s;
+    const size_t bytes = descs_bytes<Desc>(d.size());
+    if (bytes > cap) return TBLIS_STRA_ERR_ALLOC;
     std::vector<unsigned char> host(bytes, 0);
     std::memcpy(host.data(), d.data(), d.size() * sizeof(Desc));
     std::memcpy(host.data() + bytes_d, pre.data(), pre.size() * sizeof(int64_t));
-    if ((s = upload_complete(buf.p, host.data(), bytes))) return s;
-    probs = static_cast<const Desc*>(buf.p);
-    prefix = reinterpret_cast<const int64_t*>(static_cast<unsigned char*>(buf.p) + bytes_d);
+    int s = upload_complete(mem, host.data(), bytes);
+    if (s) return s;
+    probs = static_cast<const Desc*>(mem);
+    prefix = reinterpret_cast<const int64_t*>(static_cast<unsigned char*>(mem) + bytes_d);
     total = pre.back();
     return TBLIS_STRA_SUCCESS;
 }
 
-int upload_fused(const std::vector<DmmaArgs>& args, DevBuf& buf, DmmaGroupArgs& g)
+// The same into a new allocation owned by `buf`.
+template <class Desc>
+int upload_descs(const std::vector<Desc>& d, const std::vector<int64_t>& work, DevBuf& buf,
+                 const Desc*& probs, const int64_t*& prefix, int64_t& total)
+{
+    const size_t bytes = descs_bytes<Desc>(d.size());
+    int s = buf.alloc(bytes);
+    if (s) return s;
+    return fill_descs(d, work, buf.p, bytes, probs, prefix, total);
+}
+
+// Grouped-launch arguments of fused / packed descriptors: into `buf` (new
+// allocation) or, with buf == nullptr, into the existing `mem` of `cap` bytes.
+int upload_fused(const std::vector<DmmaArgs>& args, DevBuf* buf, DmmaGroupArgs& g, void* mem = nullptr,
+                 size_t cap = 0)
 {
     std::memset(&g, 0, sizeof g);
     if (args.empty()) return TBLIS_STRA_SUCCESS;
     std::vector<int64_t> work(args.size());
     for (size_t i = 0; i < args.size(); i++) work[i] = args[i].work;
     g.nprob = (int)args.size();
-    return upload_descs(args, work, buf, g.probs, g.prefix, g.total);
+    return buf ? upload_descs(args, work, *buf, g.probs, g.prefix, g.total)
+               : fill_descs(args, work, mem, cap, g.probs, g.prefix, g.total);
 }
 
-int upload_packed(const std::vector<PackedGemmArgs>& args, DevBuf& buf, PackedGroupArgs& g)
+int upload_packed(const std::vector<PackedGemmArgs>& args, DevBuf* buf, PackedGroupArgs& g,
+                  void* mem = nullptr, size_t cap = 0)
 {
     std::memset(&g, 0, sizeof g);
     if (args.empty()) return TBLIS_STRA_SUCCESS;
     std::vector<int64_t> work(args.size());
     for (size_t i = 0; i < args.size(); i++) work[i] = args[i].batch * args[i].tiles_m * args[i].tiles_n;
     g.nprob = (int)args.size();
-    return upload_descs(args, work, buf, g.probs, g.prefix, g.total);
+    return buf ? upload_descs(args, work, *buf, g.probs, g.prefix, g.total)
+               : fill_descs(args, work, mem, cap, g.probs, g.prefix, g.total);
 }
 
 int launch_fused_group(const DmmaGroupArgs& g, int level, int config, cudaStream_t st, int sms)
@@ -228,17 +250,15 @@ int launch_fused_group(const DmmaGroupArgs& g, int level, int config, cudaStream
 
 struct Choice { int level, variant; };
 
-using TuneKey = std::tuple<int, int, int, int, int64_t, int, int, int, unsigned>;
+using TuneKey = std::tuple<int, int, int, int, int64_t, int, unsigned>;
 std::mutex g_tune_mu;
 std::map<TuneKey, Choice> g_tune_cache;
 
 TuneKey tune_key(const Prob& pr)
 {
     const GemmView& g = pr.g;
-    auto q = [](int64_t x) { return x <= 0 ? -1 : (int)std::lround(2.0 * std::log2((double)x)); };
-    const int ak = (g.unit_ksA != 0 && (g.unit_rsA == 0 || g.unit_ksA < g.unit_rsA)) ? 1 : 0;
-    const int bk = (g.unit_ksB != 0 && (g.unit_csB == 0 || g.unit_ksB < g.unit_csB)) ? 1 : 0;
-    return std::make_tuple(g.type, q(g.m), q(g.n), q(g.k), g.batch, ak, bk, pr.level_req, t_variant_mask);
+    auto q = [](int64_t x) { return x <= 0 ? -1 : (int)std::lround(std::log2((double)x)); };
+    return std::make_tuple(g.type, q(g.m), q(g.n), q(g.k), g.batch, pr.level_req, t_variant_mask);
 }
 
 // Candidate schedules of a problem.  With the level left to the tuner, a
@@ -283,6 +303,8 @@ std::vector<Choice> candidates(const Prob& pr, bool prune = true)
     return c;
 }
 
+constexpr int MAX_COPIES = 64;
+
 struct Tuner
 {
     cudaStream_t st = nullptr;
@@ -290,6 +312,8 @@ struct Tuner
     DevBuf scratch;            // scratch C (largest C span)
     DevBuf ws;                 // packed / split workspace (largest candidate)
     size_t ws_bytes = 0;
+    DevBuf desc;               // grouped-launch descriptors of the copies
+    size_t desc_cap = 0;
     int* err = nullptr;
     int sms = 148;
     int timings = 0;
@@ -309,6 +333,8 @@ struct Tuner
         if ((s = scratch.alloc(c_bytes))) return s;
         if (cudaMemset(scratch.p, 0, c_bytes) != cudaSuccess) return TBLIS_STRA_ERR_CUDA;
         ws_bytes = w_bytes;
+        desc_cap = std::max(descs_bytes<DmmaArgs>(MAX_COPIES), descs_bytes<PackedGemmArgs>(MAX_COPIES));
+        if ((s = desc.alloc(desc_cap))) return s;
         return ws.alloc(w_bytes);
     }
     int failures = 0;
@@ -346,7 +372,7 @@ struct Tuner
     int copies_for(int64_t work) const
     {
         const int64_t fill = (int64_t)sms * 2;
-        return (int)std::max<int64_t>(1, std::min<int64_t>(64, (fill + work - 1) / work));
+        return (int)std::max<int64_t>(1, std::min<int64_t>(MAX_COPIES, (fill + work - 1) / work));
     }
 
     double time_choice(const Prob& pr, const int64_t* tab, const Choice& c)
@@ -361,9 +387,8 @@ struct Tuner
             if (one.work <= 0) return 0.0;
             const int copies = copies_for(one.work);
             std::vector<DmmaArgs> args(copies, one);
-            DevBuf buf;
             DmmaGroupArgs g;
-            if (upload_fused(args, buf, g)) return 1e30;
+            if (upload_fused(args, nullptr, g, desc.p, desc_cap)) return 1e30;
             return time([&] { return launch_fused_group(g, c.level, config, st, sms); }) / copies;
         }
         if (c.variant == V_PGROUP)
@@ -380,9 +405,8 @@ struct Tuner
                                                      static_cast<double*>(scratch.p) - shift);
             const int copies = copies_for(one.batch * one.tiles_m * one.tiles_n);
             std::vector<PackedGemmArgs> args(copies, one);
-            DevBuf buf;
             PackedGroupArgs g;
-            if (upload_packed(args, buf, g)) return 1e30;
+            if (upload_packed(args, nullptr, g, desc.p, desc_cap)) return 1e30;
             const double gemm_ms = time([&] {
                 return launch_packed_gemm_grouped(g, st, sms) == cudaSuccess ? 0 : (int)TBLIS_STRA_ERR_CUDA;
             });
@@ -414,13 +438,16 @@ struct Tuner
             auto it = g_tune_cache.find(key);
             if (it != g_tune_cache.end()) return it->second;
         }
+        // A Strassen level must beat the best lower-level candidate by 2 %:
+        // its timing stands for every problem of the size class, and a near
+        // tie does not repay the level's extra error.
         Choice best = cand[0];
         double best_t = 1e30;
         static const char* names[] = {"fused", "fused_small", "packed_grouped", "packed", "split", "scale"};
         for (const Choice& c : cand)
         {
             what = names[c.variant];
-            const double t = time_choice(pr, tab, c);
+            const double t = time_choice(pr, tab, c) * (c.level > best.level ? 1.02 : 1.0);
             if (t < best_t) { best_t = t; best = c; }
         }
         std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -608,7 +635,7 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
     {
         plan->descs.emplace_back();
         DmmaGroupArgs g;
-        TSB_TRY(upload_fused(kv.second, plan->descs.back(), g));
+        TSB_TRY(upload_fused(kv.second, &plan->descs.back(), g));
         fused_groups.emplace_back(kv.first.first, kv.first.second, g);
     }
     // 4b. problem-by-problem packed schedules share one workspace
@@ -656,7 +683,7 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
                                                static_cast<double*>(pr.C)));
         }
         plan->descs.emplace_back();
-        TSB_TRY(upload_packed(args, plan->descs.back(), cplans[c].g));
+        TSB_TRY(upload_packed(args, &plan->descs.back(), cplans[c].g));
     }
     // 4d. FP32 problems on two branches balanced by flops
     std::vector<int> f32_list[2];
