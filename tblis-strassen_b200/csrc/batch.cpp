@@ -402,11 +402,12 @@ struct Tuner
                                             static_cast<const double*>(pr.B), S, T, st);
             });
             PackedGemmArgs one = packed_product_args(p0, pr.g, pg, tb, S, T,
-                                                     static_cast<double*>(scratch.p) - shift);
+                                                     static_cast<double*>(scratch.p) - shift, err);
             const int copies = copies_for(one.batch * one.tiles_m * one.tiles_n);
             std::vector<PackedGemmArgs> args(copies, one);
             PackedGroupArgs g;
             if (upload_packed(args, nullptr, g, desc.p, desc_cap)) return 1e30;
+            g.err = err;
             const double gemm_ms = time([&] {
                 return launch_packed_gemm_grouped(g, st, sms) == cudaSuccess ? 0 : (int)TBLIS_STRA_ERR_CUDA;
             });
@@ -416,7 +417,8 @@ struct Tuner
             return time([&] {
                 return run_fp64_packed_enqueue(c.level, pr.g, tb, static_cast<const double*>(pr.A),
                                                static_cast<const double*>(pr.B),
-                                               static_cast<double*>(scratch.p) - shift, st, sms, ws.p, ws_bytes);
+                                               static_cast<double*>(scratch.p) - shift, st, sms, ws.p, ws_bytes,
+                                               err);
             });
         if (c.variant == V_SPLIT)
             return time([&] {
@@ -680,10 +682,11 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
             const int64_t* tb[9];
             pr.tables(tab, tb);
             args.push_back(packed_product_args(product_table(0).prod[0], pr.g, pg, tb, S, T,
-                                               static_cast<double*>(pr.C)));
+                                               static_cast<double*>(pr.C), err));
         }
         plan->descs.emplace_back();
         TSB_TRY(upload_packed(args, &plan->descs.back(), cplans[c].g));
+        cplans[c].g.err = err;
     }
     // 4d. FP32 problems on two branches balanced by flops
     std::vector<int> f32_list[2];
@@ -796,7 +799,7 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
             TSB_TRY(run_fp64_packed_enqueue(pr.level, pr.g, tb, static_cast<const double*>(pr.A),
                                             static_cast<const double*>(pr.B), static_cast<double*>(pr.C),
                                             cs.main, sms, plan->seq_ws.p,
-                                            fp64_packed_workspace_bytes(pr.level, pr.g)));
+                                            fp64_packed_workspace_bytes(pr.level, pr.g), err));
         }
         for (size_t c = 0; c < chunks.size(); c++)
         {

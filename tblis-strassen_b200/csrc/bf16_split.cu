@@ -29,6 +29,7 @@
 // Every wait on an mbarrier is bounded (about a second of clock cycles); on
 // expiry the kernel records an error code and every role returns.
 #include "kernels.cuh"
+#include "mbarrier.cuh"
 #include "timing.hpp"
 
 #include <cuda_bf16.h>
@@ -45,7 +46,6 @@ constexpr int ST = SPLIT_TILE;               // 128: tile rows (A side) / column
 constexpr int SK = 64;                       // k per tile block (one 128-byte bf16 row)
 constexpr int BLK = ST * SK * 2;             // 16 KB per tile block
 constexpr int KCH = 4;                       // k blocks per TMEM accumulation chunk (256 k)
-constexpr long long WAIT_LIMIT = 2000000000LL;   // clock cycles (~1 s)
 
 // Byte offset of element (r, k) in a 128 x 64 bf16 block, K-major with the
 // 128-byte swizzle: 16-byte chunk k/8 of row r moves to chunk (k/8) ^ (r%8).
@@ -181,49 +181,6 @@ split_pack_kernel(const __grid_constant__ SplitPackArgs a)
 
 // ---- tcgen05 GEMM -------------------------------------------------------------------
 
-__device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" :: "r"(addr), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint32_t addr)
-{
-    asm volatile("{\n.reg .b64 st;\nmbarrier.arrive.shared::cta.b64 st, [%0];\n}\n" :: "r"(addr) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t addr, uint32_t bytes)
-{
-    asm volatile("{\n.reg .b64 st;\nmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n"
-                 :: "r"(addr), "r"(bytes) : "memory");
-}
-
-// Bounded wait for the phase of the given parity; false on timeout or abort.
-__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity, volatile int* abort_flag,
-                                          int* err, int code)
-{
-    const long long start = clock64();
-    while (true)
-    {
-        uint32_t done;
-        asm volatile("{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-                     "selp.u32 %0, 1, 0, p;\n}\n" : "=r"(done) : "r"(addr), "r"(parity) : "memory");
-        if (done) return true;
-        if (*abort_flag) return false;
-        if (clock64() - start > WAIT_LIMIT)
-        {
-            *abort_flag = 1;
-            if (err) atomicExch(err, code);
-            return false;
-        }
-    }
-}
-
-__device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
-                 :: "r"(dst), "l"(src), "r"(bytes), "r"(mbar) : "memory");
-}
-
 // Shared-memory descriptor of a 128-row, K-major, 128-byte-swizzled block:
 // start >> 4, leading offset 16 B (unused when swizzled), stride 1024 B
 // between 8-row groups, fixed 0b001 at bit 46, swizzle mode 2 (128 B).
@@ -307,7 +264,7 @@ split_gemm_kernel(const __grid_constant__ SplitGemmArgs a)
         for (int s = 0; s < 2; s++) { mbar_init(bar(8 + s), 1); mbar_init(bar(10 + s), 128); }
         mbar_init(bar(12), 1);
         *abort_flag = 0;
-        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        mbar_init_fence();
     }
     if (warp == 1)
     {

@@ -272,19 +272,31 @@ void set_grid(DmmaArgs& a, int64_t ms, int64_t ns, int64_t ks)
 }
 
 // Packed schedule of the ABC variant (see packed_kernels.cu) on pool scratch.
+// Blocking calls read back the kernels' wait-timeout flag.
 int run_fp64_packed(int level, const GemmView& g, const DevPlan& t, const double* A, const double* B,
-                    double* C, cudaStream_t st, int sms)
+                    double* C, cudaStream_t st, int sms, bool blocking)
 {
     const size_t ws = fp64_packed_workspace_bytes(level, g);
-    Scratch buf;
+    Scratch buf, errbuf;
     int s;
     if ((s = buf.alloc(ws, st))) return s;
+    if ((s = errbuf.alloc(sizeof(int), st))) return s;
+    TSB_CUDA(cudaMemsetAsync(errbuf.p, 0, sizeof(int), st));
     const int64_t* tb[9] = {t.rsA, t.rsC, t.csB, t.csC, t.ksA, t.ksB, t.bA, t.bB, t.bC};
-    return run_fp64_packed_enqueue(level, g, tb, A, B, C, st, sms, buf.p, ws);
+    s = run_fp64_packed_enqueue(level, g, tb, A, B, C, st, sms, buf.p, ws, static_cast<int*>(errbuf.p));
+    if (s) return s;
+    if (blocking)
+    {
+        int err = 0;
+        TSB_CUDA(cudaMemcpyAsync(&err, errbuf.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        TSB_CUDA(cudaStreamSynchronize(st));
+        if (err) return TBLIS_STRA_ERR_TIMEOUT;
+    }
+    return TBLIS_STRA_SUCCESS;
 }
 
 int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
-             const double* A, const double* B, double* C, cudaStream_t st, int device)
+             const double* A, const double* B, double* C, cudaStream_t st, int device, bool blocking)
 {
     if (g.m == 0 || g.n == 0 || g.batch == 0) return TBLIS_STRA_SUCCESS;
     if (g.alpha == 0.0 || g.k == 0)
@@ -305,7 +317,7 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
         // fully fused kernel, which needs none.
         const PackGeom pg = pack_geom(level, g);
         if (pg.fits && fp64_packed_workspace_bytes(level, g) <= t_ws_limit)
-            return run_fp64_packed(level, g, t, A, B, C, st, sms);
+            return run_fp64_packed(level, g, t, A, B, C, st, sms, blocking);
         DmmaArgs a = base_args(g, t, A, B, C);
         set_grid(a, ms, ns, ks);
         a.nprod = (int)tab.prod.size();
@@ -441,9 +453,10 @@ int enqueue_pack_product(const Product& pr, const GemmView& g, const PackGeom& p
 
 PackedGemmArgs packed_product_args(const Product& pr, const GemmView& g, const PackGeom& pg,
                                    const int64_t* const tb[9], const double* S, const double* T,
-                                   double* C)
+                                   double* C, int* err)
 {
     PackedGemmArgs ga{};
+    ga.err = err;
     ga.S = S; ga.T = T; ga.C = C;
     ga.rsC = tb[1]; ga.csC = tb[3]; ga.bC = tb[8];
     ga.m = g.m; ga.n = g.n; ga.ms = pg.ms; ga.ns = pg.ns; ga.k_pad = pg.k_pad;
@@ -461,7 +474,7 @@ PackedGemmArgs packed_product_args(const Product& pr, const GemmView& g, const P
 // S and T are reused for every product, in stream order.
 int run_fp64_packed_enqueue(int level, const GemmView& g, const int64_t* const tb[9],
                             const double* A, const double* B, double* C, cudaStream_t st, int sms,
-                            void* ws, size_t ws_bytes)
+                            void* ws, size_t ws_bytes, int* err)
 {
     const PackGeom pg = pack_geom(level, g);
     if (!pg.fits) return TBLIS_STRA_ERR_TOO_LARGE;
@@ -472,7 +485,7 @@ int run_fp64_packed_enqueue(int level, const GemmView& g, const int64_t* const t
     {
         int s = enqueue_pack_product(pr, g, pg, tb, A, B, S, T, st);
         if (s) return s;
-        TSB_CUDA(launch_packed_gemm(packed_product_args(pr, g, pg, tb, S, T, C), st, sms));
+        TSB_CUDA(launch_packed_gemm(packed_product_args(pr, g, pg, tb, S, T, C, err), st, sms));
     }
     return TBLIS_STRA_SUCCESS;
 }
@@ -686,7 +699,8 @@ int mult(int level, const tblis_tensor* A, const label_type* idx_A,
                      blocking || staged[0] || staged[1] || staged[2]);
     else
         s = run_fp64(level, impl, g, *dp, static_cast<const double*>(dptr[0]),
-                     static_cast<const double*>(dptr[1]), static_cast<double*>(dptr[2]), st, device);
+                     static_cast<const double*>(dptr[1]), static_cast<double*>(dptr[2]), st, device,
+                     blocking || staged[0] || staged[1] || staged[2]);
     if (s) return s;
 
     if (staged[2])

@@ -146,7 +146,7 @@ struct PackedGemmArgs
     double alpha, beta;
     int nc;
     int8_t c_r[4], c_c[4], c_s[4], c_first[4];
-    int pad_;                                  // 8-byte multiple (copied as words)
+    int* err;                                  // set on a timed-out wait (may be null)
 };
 
 // Grouped packed GEMM: many problems' tiles in one persistent launch.
@@ -156,6 +156,7 @@ struct PackedGroupArgs
     const int64_t* prefix;         // device array [nprob + 1]: work prefix sums
     int nprob;
     int64_t total;
+    int* err;                      // set on a timed-out wait (may be null)
 };
 
 // ---- split-BF16 (FP32 contractions on tcgen05) --------------------------------------

@@ -17,6 +17,7 @@
 // bandwidth on every fragment read; the GEMM's loader becomes a plain copy of
 // contiguous 16-byte chunks.
 #include "kernels.cuh"
+#include "mbarrier.cuh"
 #include "tile_layout.cuh"
 #include "timing.hpp"
 
@@ -322,19 +323,54 @@ packed_gemm_kernel(const __grid_constant__ PackedGemmArgs a)
     for (int64_t w = blockIdx.x; w < work; w += gridDim.x) packed_tile<K>(a, w, smem);
 }
 
-// Grouped form: one persistent grid over the tiles of many problems (each
-// with its own packed S and T); work item w belongs to the problem p with
-// prefix[p] <= w < prefix[p + 1].  The problem's descriptor is staged in
-// shared memory whenever a CTA moves to another problem.
-template <class K>
-__global__ void __launch_bounds__(K::NT, 1)
-packed_gemm_grouped_kernel(const __grid_constant__ PackedGroupArgs g)
+// ---- warp-specialised packed GEMM ----------------------------------------------------
+//
+// The same tiles, fragments and epilogue as packed_tile, with the operand
+// ring filled by 1-D bulk copies (one 32 KB copy of S and one of T per
+// k-step: a packed tile's k-steps are contiguous) that complete on an
+// mbarrier, instead of every thread issuing 16-byte cp.async and the CTA
+// meeting at a barrier each k-step.  Thread 0 also produces: after each
+// k-step it refills the slot that step used once all 16 warps have released
+// it (one arrival per warp), so warps drift apart by up to STAGES - 1 steps
+// and the DMMA pipe does not drain at a block-wide barrier.  The producer
+// runs ahead across tile boundaries, loading the next tile's first steps
+// during the epilogue.  Every wait is bounded (mbarrier.cuh).
+
+// Thread 0's producer cursor and the ring's barriers (shared memory).
+struct WsCtrl
 {
-    extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ PackedGemmArgs desc;
-    static_assert(sizeof(PackedGemmArgs) % 8 == 0, "descriptor copied as 8-byte words");
-    int cur = -1;
-    for (int64_t w = blockIdx.x; w < g.total; w += gridDim.x)
+    uint64_t full[4], empty[4];    // per ring slot; STAGES <= 4
+    int64_t pw, ps, nk;            // producer: work item, k-step within it, k-steps of it
+    const double* sA;
+    const double* sB;
+    uint32_t pit;                  // k-steps issued
+    int abort;
+};
+
+// Work sources: one problem (kernel parameter) or a group of problems
+// (descriptors in global memory; work item w belongs to the problem p with
+// prefix[p] <= w < prefix[p + 1]).
+// The parameter is read through a pointer of unknown origin, so its fields
+// are loaded where they are used (as the group's descriptors are) instead of
+// being held in registers across the k loop.
+struct OneProblem
+{
+    const PackedGemmArgs* a;
+    __device__ int64_t total() const { return a->batch * a->tiles_m * a->tiles_n; }
+    __device__ const PackedGemmArgs& at(int64_t w, int64_t& local) const
+    {
+        local = w;
+        const PackedGemmArgs* p = a;
+        asm volatile("" : "+l"(p));
+        return *p;
+    }
+};
+
+struct ProblemGroup
+{
+    const PackedGroupArgs& g;
+    __device__ int64_t total() const { return g.total; }
+    __device__ const PackedGemmArgs& at(int64_t w, int64_t& local) const
     {
         int lo = 0, hi = g.nprob - 1;
         while (lo < hi)
@@ -342,17 +378,258 @@ packed_gemm_grouped_kernel(const __grid_constant__ PackedGroupArgs g)
             const int mid = (lo + hi + 1) >> 1;
             if (g.prefix[mid] <= w) lo = mid; else hi = mid - 1;
         }
-        if (lo != cur)
-        {
-            __syncthreads();   // the previous tile no longer reads the descriptor
-            const int64_t* src = reinterpret_cast<const int64_t*>(g.probs + lo);
-            int64_t* dst = reinterpret_cast<int64_t*>(&desc);
-            for (int i = threadIdx.x; i < (int)(sizeof(PackedGemmArgs) / 8); i += blockDim.x) dst[i] = src[i];
-            __syncthreads();
-            cur = lo;
-        }
-        packed_tile<K>(desc, w - g.prefix[lo], smem);
+        local = w - g.prefix[lo];
+        return g.probs[lo];
     }
+};
+
+// Tile (batch b, row tile tm, column tile tn) of work item w: groups of 8
+// row tiles walk the column tiles together so concurrent CTAs share panels.
+__device__ __forceinline__ void decode_tile(const PackedGemmArgs& a, int64_t w, int64_t& b, int64_t& tm,
+                                            int64_t& tn)
+{
+    const int64_t tiles = a.tiles_m * a.tiles_n;
+    b = w / tiles;
+    const int64_t tw = w - b * tiles;
+    const int64_t GROUP = 8;
+    const int64_t group = tw / (GROUP * a.tiles_n);
+    const int64_t first_m = group * GROUP;
+    const int64_t gsize = (a.tiles_m - first_m) < GROUP ? (a.tiles_m - first_m) : GROUP;
+    tm = first_m + (tw % gsize);
+    tn = (tw % (GROUP * a.tiles_n)) / gsize;
+}
+
+template <class K>
+constexpr size_t ws_smem()
+{
+    return K::STAGES * K::stage_bytes + size_t(4) * (K::BM + K::BN) * 8 + sizeof(WsCtrl);
+}
+
+template <class K, class Src>
+__device__ __forceinline__ void packed_ws_body(const Src& src, int* err, unsigned char* smem)
+{
+    constexpr int BM = K::BM, BN = K::BN, BK = K::BK, NT = K::NT, STAGES = K::STAGES;
+    constexpr int MI = K::MI, NI = K::NI, NW = NT / 32;
+    static_assert(STAGES <= 4, "WsCtrl holds 4 ring slots");
+    static_assert((BK * BM * 8) % 16 == 0 && (BK * BN * 8) % 16 == 0, "bulk copies of 16-byte multiples");
+    double* As = reinterpret_cast<double*>(smem);
+    double* Bs = As + STAGES * BK * BM;
+    int64_t* rowC = reinterpret_cast<int64_t*>(Bs + STAGES * BK * BN);
+    int64_t* colC = rowC + 4 * BM;
+    WsCtrl* ctl = reinterpret_cast<WsCtrl*>(colC + 4 * BN);
+    volatile int* abort_flag = &ctl->abort;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t4 = lane & 3;
+    const int wm = (warp / K::WN) * K::WTM;
+    const int wn = (warp % K::WN) * K::WTN;
+    const int64_t total = src.total();
+
+    if (tid == 0)
+    {
+        for (int s = 0; s < STAGES; s++)
+        {
+            mbar_init(smem_addr(&ctl->full[s]), 1);
+            mbar_init(smem_addr(&ctl->empty[s]), NW);
+        }
+        ctl->pw = blockIdx.x; ctl->ps = 0; ctl->nk = 0; ctl->pit = 0; ctl->abort = 0;
+        mbar_init_fence();
+    }
+    __syncthreads();
+
+    // Producer (thread 0): issue the next k-step of this CTA's work sequence
+    // into its ring slot, after the warps have released the slot's previous
+    // use.  False on a timed-out or aborted wait.
+    auto produce = [&]() -> bool {
+        while (ctl->pw < total)
+        {
+            if (ctl->ps == 0)
+            {
+                int64_t local;
+                const PackedGemmArgs& p = src.at(ctl->pw, local);
+                int64_t b, tm, tn;
+                decode_tile(p, local, b, tm, tn);
+                ctl->nk = p.k_pad / BK;
+                if (ctl->nk == 0) { ctl->pw += gridDim.x; continue; }
+                ctl->sA = p.S + ((b * p.tiles_m + tm) * p.k_pad) * BM;
+                ctl->sB = p.T + ((b * p.tiles_n + tn) * p.k_pad) * BN;
+            }
+            const uint32_t it = ctl->pit, slot = it % STAGES;
+            if (it >= (uint32_t)STAGES &&
+                !mbar_wait(smem_addr(&ctl->empty[slot]), ((it / STAGES) & 1) ^ 1, abort_flag, err, 1))
+                return false;
+            const uint32_t full = smem_addr(&ctl->full[slot]);
+            mbar_expect_tx(full, (uint32_t)((BK * BM + BK * BN) * 8));
+            bulk_copy(smem_addr(As + slot * BK * BM), ctl->sA + ctl->ps * BK * BM, BK * BM * 8, full);
+            bulk_copy(smem_addr(Bs + slot * BK * BN), ctl->sB + ctl->ps * BK * BN, BK * BN * 8, full);
+            ctl->pit = it + 1;
+            if (++ctl->ps == ctl->nk) { ctl->ps = 0; ctl->pw += gridDim.x; }
+            return true;
+        }
+        return true;
+    };
+    bool ok = true;
+    if (tid == 0)
+        for (int s = 0; s < STAGES && ok; s++) ok = produce();
+
+    auto load_frags = [&](const double* Ab, const double* Bb, int k4, double (&af)[MI][2], double (&bf)[NI]) {
+        const int kr = k4 + t4;
+        const int pg = 2 * ((g + swz_c(kr)) & 7);
+#pragma unroll
+        for (int mi = 0; mi < MI; mi++)
+        {
+            const double2 v = *reinterpret_cast<const double2*>(Ab + kr * BM + wm + mi * 16 + pg);
+            af[mi][0] = v.x; af[mi][1] = v.y;
+        }
+#pragma unroll
+        for (int nj = 0; nj < NI / 2; nj++)
+        {
+            const double2 v = *reinterpret_cast<const double2*>(Bb + kr * BN + wn + nj * 16 + pg);
+            bf[2 * nj] = v.x; bf[2 * nj + 1] = v.y;
+        }
+    };
+
+    uint32_t cit = 0;   // k-steps consumed
+    for (int64_t w = blockIdx.x; w < total; w += gridDim.x)
+    {
+        // Every thread takes part in every tile's barriers; a failed wait
+        // anywhere ends the loop for all of them here.
+        if (__syncthreads_or(!ok)) break;
+        int64_t local;
+        const PackedGemmArgs& a = src.at(w, local);
+        int64_t b, tm, tn;
+        decode_tile(a, local, b, tm, tn);
+        const int64_t nk = a.k_pad / BK;
+        for (int i = tid; i < 4 * BM; i += NT)
+        {
+            const int q = i / BM, r = i % BM;
+            const int64_t loc = tm * BM + r;
+            const int64_t gi = (q < a.nc ? a.c_r[q] : 0) * a.ms + loc;
+            rowC[i] = (q < a.nc && loc < a.ms && gi < a.m) ? a.bC[b] + a.rsC[gi] : OFF_INVALID;
+        }
+        for (int i = tid; i < 4 * BN; i += NT)
+        {
+            const int q = i / BN, c = i % BN;
+            const int64_t loc = tn * BN + c;
+            const int64_t gj = (q < a.nc ? a.c_c[q] : 0) * a.ns + loc;
+            colC[i] = (q < a.nc && loc < a.ns && gj < a.n) ? a.csC[gj] : OFF_INVALID;
+        }
+        __syncthreads();
+
+        double acc[MI][NI][4];
+#pragma unroll
+        for (int mi = 0; mi < MI; mi++)
+#pragma unroll
+            for (int ni = 0; ni < NI; ni++)
+#pragma unroll
+                for (int e = 0; e < 4; e++) acc[mi][ni][e] = 0.0;
+
+        for (int64_t s = 0; s < nk; s++)
+        {
+            const uint32_t slot = cit % STAGES;
+            // warp-uniform outcome, so the warp stays converged
+            ok = __all_sync(0xffffffffu,
+                            mbar_wait(smem_addr(&ctl->full[slot]), (cit / STAGES) & 1, abort_flag, err, 2));
+            if (!ok) break;
+            const double* Ab = As + slot * BK * BM;
+            const double* Bb = Bs + slot * BK * BN;
+            double af[2][MI][2], bf[2][NI];
+            load_frags(Ab, Bb, 0, af[0], bf[0]);
+#pragma unroll
+            for (int q = 0; q < BK / 4; q++)
+            {
+                const int cur = q & 1;
+                if (q + 1 < BK / 4) load_frags(Ab, Bb, (q + 1) * 4, af[cur ^ 1], bf[cur ^ 1]);
+#pragma unroll
+                for (int mi = 0; mi < MI; mi++)
+#pragma unroll
+                    for (int ni = 0; ni < NI; ni++)
+                        dmma(acc[mi][ni], af[cur][mi][0], af[cur][mi][1], bf[cur][ni]);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_addr(&ctl->empty[slot]));
+            cit++;
+            if (warp == 0)
+            {
+                bool pok = true;
+                if (lane == 0) pok = produce();
+                ok = __shfl_sync(0xffffffffu, pok, 0);
+                if (!ok) break;
+            }
+        }
+        if (!ok) continue;   // the barrier at the top ends the loop
+
+        // Epilogue: C_q = (first ? beta*C_q : C_q) + sign_q*alpha*S*T, all
+        // loads of a row pair issued before its stores.
+        for (int q = 0; q < a.nc; q++)
+        {
+            const int64_t* rt = rowC + q * BM;
+            const int64_t* ct = colC + q * BN;
+            const double coef = a.c_s[q] < 0 ? -a.alpha : a.alpha;
+            const bool first = a.c_first[q] != 0;
+            const bool read_c = !first || a.beta != 0.0;
+            const double cb = first ? a.beta : 1.0;
+#pragma unroll
+            for (int mi = 0; mi < MI; mi++)
+            {
+                double cv[2][NI][2];
+#pragma unroll
+                for (int hr = 0; hr < 2; hr++)
+                {
+                    const int64_t ro = rt[wm + mi * 16 + g + hr * 8];
+#pragma unroll
+                    for (int ni = 0; ni < NI; ni++)
+#pragma unroll
+                        for (int hc = 0; hc < 2; hc++)
+                        {
+                            const int64_t co = ct[wn + ni * 8 + t4 * 2 + hc];
+                            cv[hr][ni][hc] = (read_c && ro != OFF_INVALID && co != OFF_INVALID)
+                                                 ? a.C[ro + co] : 0.0;
+                        }
+                }
+#pragma unroll
+                for (int hr = 0; hr < 2; hr++)
+                {
+                    const int64_t ro = rt[wm + mi * 16 + g + hr * 8];
+                    if (ro == OFF_INVALID) continue;
+#pragma unroll
+                    for (int ni = 0; ni < NI; ni++)
+#pragma unroll
+                        for (int hc = 0; hc < 2; hc++)
+                        {
+                            const int64_t co = ct[wn + ni * 8 + t4 * 2 + hc];
+                            if (co == OFF_INVALID) continue;
+                            a.C[ro + co] = coef * acc[mi][ni][hr * 2 + hc] + cb * cv[hr][ni][hc];
+                        }
+                }
+            }
+        }
+    }
+    // Copies still in flight (after an abort) land before the CTA leaves:
+    // bounded waits on the last STAGES k-steps issued.
+    if (tid == 0)
+    {
+        volatile int never = 0;
+        const uint32_t pit = ctl->pit;
+        for (uint32_t i = (pit > (uint32_t)STAGES ? pit - STAGES : 0); i < pit; i++)
+            mbar_wait(smem_addr(&ctl->full[i % STAGES]), (i / STAGES) & 1, &never, nullptr, 0);
+    }
+}
+
+template <class K>
+__global__ void __launch_bounds__(K::NT, 1)
+packed_gemm_ws_kernel(const __grid_constant__ PackedGemmArgs a)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    packed_ws_body<K>(OneProblem{&a}, a.err, smem);
+}
+
+template <class K>
+__global__ void __launch_bounds__(K::NT, 1)
+packed_gemm_grouped_kernel(const __grid_constant__ PackedGroupArgs g)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    packed_ws_body<K>(ProblemGroup{g}, g.err, smem);
 }
 
 template <class K>
@@ -377,21 +654,33 @@ cudaError_t launch_packed_cfg(const PackedGemmArgs& a, cudaStream_t stream, int 
 }
 
 template <class K>
+cudaError_t launch_packed_ws_cfg(const PackedGemmArgs& a, cudaStream_t stream, int num_sms)
+{
+    static_assert(ws_smem<K>() <= 227 * 1024, "shared memory budget");
+    if (a.k_pad % K::BK) return cudaErrorInvalidValue;
+    auto kern = packed_gemm_ws_kernel<K>;
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ws_smem<K>());
+    if (err != cudaSuccess) return err;
+    const int64_t work = a.batch * a.tiles_m * a.tiles_n;
+    int64_t grid = num_sms;
+    if (work < grid) grid = work;
+    timing_begin(KK_PACKED_GEMM, stream);
+    kern<<<(unsigned)grid, K::NT, ws_smem<K>(), stream>>>(a);
+    timing_end(KK_PACKED_GEMM, stream);
+    return cudaGetLastError();
+}
+
+template <class K>
 cudaError_t launch_packed_grouped_cfg(const PackedGroupArgs& g, cudaStream_t stream, int num_sms)
 {
-    constexpr size_t static_smem = sizeof(PackedGemmArgs);
-    static_assert(K::smem + static_smem <= 227 * 1024, "shared memory budget");
+    static_assert(ws_smem<K>() <= 227 * 1024, "shared memory budget");
     auto kern = packed_gemm_grouped_kernel<K>;
-    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::smem);
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ws_smem<K>());
     if (err != cudaSuccess) return err;
-    int per_sm = 0;
-    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, K::NT, K::smem);
-    if (err != cudaSuccess) return err;
-    if (per_sm < 1) per_sm = 1;
-    int64_t grid = (int64_t)num_sms * per_sm;
+    int64_t grid = num_sms;
     if (g.total < grid) grid = g.total;
     timing_begin(KK_PACKED_GEMM, stream);
-    kern<<<(unsigned)grid, K::NT, K::smem, stream>>>(g);
+    kern<<<(unsigned)grid, K::NT, ws_smem<K>(), stream>>>(g);
     timing_end(KK_PACKED_GEMM, stream);
     return cudaGetLastError();
 }
@@ -430,12 +719,15 @@ cudaError_t launch_packed_gemm(const PackedGemmArgs& a, cudaStream_t stream, int
         config = env;
     }
     cudaError_t err;
+    // 0 (default): warp-specialised bulk-copy ring; 1-4: cp.async rings with a
+    // block barrier per k-step (4 = the same tile shape as the default).
     switch (config)
     {
         case 1:  err = launch_packed_cfg<PG1>(a, stream, num_sms); break;
         case 2:  err = launch_packed_cfg<PG2>(a, stream, num_sms); break;
         case 3:  err = launch_packed_cfg<PG3>(a, stream, num_sms); break;
-        default: err = launch_packed_cfg<PG0>(a, stream, num_sms); break;
+        case 4:  err = launch_packed_cfg<PG0>(a, stream, num_sms); break;
+        default: err = launch_packed_ws_cfg<PG0>(a, stream, num_sms); break;
     }
     if (err == cudaSuccess) g_launches++;
     return err;

@@ -43,15 +43,16 @@ int enqueue_pack_product(const Product& pr, const GemmView& g, const PackGeom& p
                          const int64_t* const tb[9], const double* A, const double* B,
                          double* S, double* T, cudaStream_t st);
 
-// Descriptor of product `pr`'s packed GEMM (+-alpha*S*T into its C blocks).
+// Descriptor of product `pr`'s packed GEMM (+-alpha*S*T into its C blocks);
+// `err` (device int, may be null) records a timed-out wait.
 PackedGemmArgs packed_product_args(const Product& pr, const GemmView& g, const PackGeom& pg,
                                    const int64_t* const tb[9], const double* S, const double* T,
-                                   double* C);
+                                   double* C, int* err);
 
 // Whole packed ABC schedule of one FP64 contraction on caller workspace.
 int run_fp64_packed_enqueue(int level, const GemmView& g, const int64_t* const tb[9],
                             const double* A, const double* B, double* C, cudaStream_t st, int sms,
-                            void* ws, size_t ws_bytes);
+                            void* ws, size_t ws_bytes, int* err);
 
 // Split-BF16 schedule of one FP32 contraction on caller workspace.
 size_t fp32_workspace_bytes(int level, const GemmView& g, int terms);
