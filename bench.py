@@ -466,7 +466,8 @@ def main():
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
                 "executed_frac": achieved * (7.0 / 8.0) ** args.level / peak,
                 "kernel": {"fused": "stra_dmma_kernel", "pack": "pack_kernel",
-                           "packed_gemm": "packed_gemm_kernel", "aux": "aux"}[dom],
+                           "packed_gemm": ("packed_gemm_kernel" if os.environ.get("TBLIS_STRA_PACKED_CONFIG", "0") in ("1", "2", "3", "4")
+                                           else "packed_gemm_ws_kernel"), "aux": "aux"}[dom],
                 "launches_timed": n_launch, "kernel_ms_total": dom_ms,
                 "share_of_step": dom_ms / (t * 1e3),
                 "other_kernels_ms": {k: v[1] for k, v in kinds.items() if k != dom}}

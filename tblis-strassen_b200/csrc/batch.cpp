@@ -24,7 +24,7 @@
 // schedules are timed in a grouped launch holding enough copies of the
 // problem to fill the GPU twice (their cost inside a full grouped launch,
 // not their latency alone); problem-by-problem schedules run alone.  The
-// fastest candidate wins (a Strassen level by a 2 % margin); the choice is
+// fastest candidate wins (a later one by a 2 % margin); the choice is
 // cached per process by a size signature (type, m, n, k rounded to the
 // nearest power of two, batch, requested level, allowed schedules), so
 // problems of one size class share one set of timings.
@@ -440,16 +440,18 @@ struct Tuner
             auto it = g_tune_cache.find(key);
             if (it != g_tune_cache.end()) return it->second;
         }
-        // A Strassen level must beat the best lower-level candidate by 2 %:
-        // its timing stands for every problem of the size class, and a near
-        // tie does not repay the level's extra error.
+        // A later candidate must beat the best so far by 2 %: its timing
+        // stands for every problem of the size class, so near ties go to the
+        // earlier candidate, which is the grouped launch at L = 0 (timed as a
+        // share of a full launch, whose tail it removes for the whole chunk)
+        // and the lower level otherwise (less rounding error).
         Choice best = cand[0];
         double best_t = 1e30;
         static const char* names[] = {"fused", "fused_small", "packed_grouped", "packed", "split", "scale"};
         for (const Choice& c : cand)
         {
             what = names[c.variant];
-            const double t = time_choice(pr, tab, c) * (c.level > best.level ? 1.02 : 1.0);
+            const double t = time_choice(pr, tab, c) * (best_t < 1e30 ? 1.02 : 1.0);
             if (t < best_t) { best_t = t; best = c; }
         }
         std::lock_guard<std::mutex> lk(g_tune_mu);
