@@ -591,7 +591,7 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
             need = true;
             for (const Choice& x : c)
                 tune_ws = std::max(tune_ws, x.variant == V_SPLIT ? fp32_workspace_bytes(x.level, pr.g, FP32_TERMS)
-                                                                 : fp64_packed_workspace_bytes(x.level, pr.g));
+                                                                 : fp64_packed_group_workspace_bytes(x.level, pr.g));
         }
         Tuner tuner;
         if (need) TSB_TRY(tuner.init((size_t)max_c_span * sizeof(double), tune_ws, err, sms));
@@ -645,7 +645,7 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
     // 4b. problem-by-problem packed schedules share one workspace
     size_t seq_bytes = 0;
     for (auto& pr : probs)
-        if (pr.variant == V_PACKED) seq_bytes = std::max(seq_bytes, fp64_packed_workspace_bytes(pr.level, pr.g));
+        if (pr.variant == V_PACKED) seq_bytes = std::max(seq_bytes, fp64_packed_group_workspace_bytes(pr.level, pr.g));
     if (seq_bytes) TSB_TRY(plan->seq_ws.alloc(seq_bytes));
     // 4c. chunks of grouped packed problems (consecutive, at most chunk_bytes()
     // of packed operands unless one problem needs more)
@@ -801,7 +801,7 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
             TSB_TRY(run_fp64_packed_enqueue(pr.level, pr.g, tb, static_cast<const double*>(pr.A),
                                             static_cast<const double*>(pr.B), static_cast<double*>(pr.C),
                                             cs.main, sms, plan->seq_ws.p,
-                                            fp64_packed_workspace_bytes(pr.level, pr.g), err));
+                                            fp64_packed_group_workspace_bytes(pr.level, pr.g), err));
         }
         for (size_t c = 0; c < chunks.size(); c++)
         {

@@ -276,7 +276,8 @@ void set_grid(DmmaArgs& a, int64_t ms, int64_t ns, int64_t ks)
 int run_fp64_packed(int level, const GemmView& g, const DevPlan& t, const double* A, const double* B,
                     double* C, cudaStream_t st, int sms, bool blocking)
 {
-    const size_t ws = fp64_packed_workspace_bytes(level, g);
+    const size_t ws_group = fp64_packed_group_workspace_bytes(level, g);
+    const size_t ws = ws_group <= t_ws_limit ? ws_group : fp64_packed_workspace_bytes(level, g);
     Scratch buf, errbuf;
     int s;
     if ((s = buf.alloc(ws, st))) return s;
@@ -428,6 +429,60 @@ size_t fp64_packed_workspace_bytes(int level, const GemmView& g)
     return (p.s_elems + p.t_elems) * sizeof(double);
 }
 
+size_t fp64_packed_group_workspace_bytes(int level, const GemmView& g)
+{
+    const size_t one = fp64_packed_workspace_bytes(level, g);
+    return level >= 1 && pack_group(level, 0, 0) ? 7 * one : one;
+}
+
+namespace {
+
+// Pack the 7 sums of product group G of one operand (0 = A, 1 = B) into out[].
+int enqueue_pack_group(int level, int operand, int G, const GemmView& g, const PackGeom& pg,
+                       const int64_t* const tb[9], const double* X, double* const out[7], cudaStream_t st)
+{
+    const PackGroup* grp = pack_group(level, operand, G);
+    if (!grp) return TBLIS_STRA_ERR_UNSUPPORTED;
+    PackMultiArgs a{};
+    a.X = X;
+    if (operand == 0)
+    {
+        a.rs = tb[0]; a.ks = tb[4]; a.bX = tb[6];
+        a.rows_full = g.m; a.rows_blk = pg.ms; a.tiles = pg.tm;
+        a.kfast = g.unit_ksA != 0 && (g.unit_rsA == 0 || g.unit_ksA < g.unit_rsA);
+    }
+    else
+    {
+        a.rs = tb[2]; a.ks = tb[5]; a.bX = tb[7];
+        a.rows_full = g.n; a.rows_blk = pg.ns; a.tiles = pg.tn;
+        a.kfast = g.unit_ksB != 0 && (g.unit_csB == 0 || g.unit_ksB < g.unit_csB);
+    }
+    a.k_full = g.k; a.k_blk = pg.ks; a.k_pad = pg.k_pad; a.batch = g.batch;
+    a.nt = grp->nt;
+    for (int c = 0; c < grp->nt; c++)
+    {
+        a.t_s[c] = grp->t_s[c];
+        for (int j = 0; j < 4; j++)
+        {
+            // block (row[j/2], col[j%2]) of the operand; B is packed n-major
+            const int br = grp->row[c][j / 2], bc = grp->col[c][j % 2];
+            a.prow[c][j] = (int8_t)(operand == 0 ? br : bc);
+            a.pk[c][j] = (int8_t)(operand == 0 ? bc : br);
+        }
+    }
+    a.nout = 7;
+    for (int q = 0; q < 7; q++)
+    {
+        a.o_n[q] = grp->o_n[q];
+        for (int i = 0; i < grp->o_n[q]; i++) { a.o_j[q][i] = grp->o_j[q][i]; a.o_s[q][i] = grp->o_s[q][i]; }
+        a.out[q] = out[q];
+    }
+    TSB_CUDA(launch_pack_multi(a, st));
+    return TBLIS_STRA_SUCCESS;
+}
+
+}  // namespace
+
 int enqueue_pack_product(const Product& pr, const GemmView& g, const PackGeom& pg,
                          const int64_t* const tb[9], const double* A, const double* B,
                          double* S, double* T, cudaStream_t st)
@@ -479,9 +534,34 @@ int run_fp64_packed_enqueue(int level, const GemmView& g, const int64_t* const t
     const PackGeom pg = pack_geom(level, g);
     if (!pg.fits) return TBLIS_STRA_ERR_TOO_LARGE;
     if (ws_bytes < (pg.s_elems + pg.t_elems) * sizeof(double)) return TBLIS_STRA_ERR_ALLOC;
+    const ProductTable& tab = product_table(level);
+    if (level >= 1 && fp64_packed_group_workspace_bytes(level, g) > fp64_packed_workspace_bytes(level, g) &&
+        ws_bytes >= fp64_packed_group_workspace_bytes(level, g))
+    {
+        // Grouped sums: per group of 7 products, one pass over A and one over
+        // B form all 14 operand sums, then the 7 GEMMs in product order.
+        double* S[7];
+        double* T[7];
+        for (int q = 0; q < 7; q++)
+        {
+            S[q] = static_cast<double*>(ws) + (size_t)q * pg.s_elems;
+            T[q] = static_cast<double*>(ws) + 7 * pg.s_elems + (size_t)q * pg.t_elems;
+        }
+        const int groups = (int)tab.prod.size() / 7;
+        for (int G = 0; G < groups; G++)
+        {
+            int s;
+            if ((s = enqueue_pack_group(level, 0, G, g, pg, tb, A, S, st))) return s;
+            if ((s = enqueue_pack_group(level, 1, G, g, pg, tb, B, T, st))) return s;
+            for (int q = 0; q < 7; q++)
+                TSB_CUDA(launch_packed_gemm(packed_product_args(tab.prod[(size_t)(G * 7 + q)], g, pg, tb, S[q],
+                                                                T[q], C, err), st, sms));
+        }
+        return TBLIS_STRA_SUCCESS;
+    }
     double* S = static_cast<double*>(ws);
     double* T = S + pg.s_elems;
-    for (const Product& pr : product_table(level).prod)
+    for (const Product& pr : tab.prod)
     {
         int s = enqueue_pack_product(pr, g, pg, tb, A, B, S, T, st);
         if (s) return s;

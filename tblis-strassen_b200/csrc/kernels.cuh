@@ -149,6 +149,27 @@ struct PackedGemmArgs
     int* err;                                  // set on a timed-out wait (may be null)
 };
 
+// Seven packed operand sums in one pass (pack_multi_kernel): the blocks of
+// the group's coarse sum are read once; X_j = sum_t sign_t * block(t, j)
+// (j = 0..3), output o = sum_i o_s[o][i] * X_{o_j[o][i]}, each written in the
+// layout of PackArgs::out.  Block (t, j) sits at packed-row block prow[t][j]
+// and k block pk[t][j].
+struct PackMultiArgs
+{
+    const double* X;
+    const int64_t* rs; const int64_t* ks; const int64_t* bX;
+    int64_t rows_full, k_full;
+    int64_t rows_blk, k_blk;
+    int nt;                                    // coarse terms (1 or 2)
+    int8_t t_s[2];
+    int8_t prow[2][4], pk[2][4];
+    int nout;                                  // outputs (<= 7)
+    int8_t o_n[7], o_j[7][2], o_s[7][2];
+    double* out[7];
+    int64_t tiles, k_pad, batch;
+    int kfast;
+};
+
 // Grouped packed GEMM: many problems' tiles in one persistent launch.
 struct PackedGroupArgs
 {
@@ -214,6 +235,7 @@ cudaError_t launch_split_pack(const SplitPackArgs& args, cudaStream_t stream);
 cudaError_t launch_split_gemm(const SplitGemmArgs& args, cudaStream_t stream, int num_sms);
 
 cudaError_t launch_pack(const PackArgs& args, cudaStream_t stream);
+cudaError_t launch_pack_multi(const PackMultiArgs& args, cudaStream_t stream);
 cudaError_t launch_packed_gemm(const PackedGemmArgs& args, cudaStream_t stream, int num_sms,
                                int config = -1);
 cudaError_t launch_packed_gemm_grouped(const PackedGroupArgs& args, cudaStream_t stream, int num_sms);

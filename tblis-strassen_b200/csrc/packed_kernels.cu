@@ -107,6 +107,99 @@ pack_kernel(const __grid_constant__ PackArgs a)
     }
 }
 
+// Seven sums of one product group per pass (L >= 1): each CTA reads its
+// 128-row x 32-k window of every block of the group's coarse sum once, forms
+// the four sub-block sums X_j in registers, then writes each output's signed
+// combination through the shared-memory transpose of pack_kernel.  At L=2 this
+// reads each block of A (and B) once per group instead of once per product
+// that uses it: 48 instead of 144 block reads per operand.
+constexpr int PM_THREADS = 512;
+
+__global__ void __launch_bounds__(PM_THREADS)
+pack_multi_kernel(const __grid_constant__ PackMultiArgs a)
+{
+    __shared__ double buf[PACK_TILE][PK_K + 1];
+    __shared__ int64_t rowoff[8][PACK_TILE];     // per block (t, j): batch + row offset (or invalid)
+    __shared__ int64_t koff[8][PK_K];            // per block (t, j): k offset (or invalid)
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int64_t k0 = (int64_t)blockIdx.x * PK_K;
+    const int64_t t = blockIdx.y;
+    const int64_t b = blockIdx.z;
+    const int64_t r0 = t * PACK_TILE;
+    const int nblk = a.nt * 4;
+
+    for (int i = tid; i < nblk * PACK_TILE; i += PM_THREADS)
+    {
+        const int q = i / PACK_TILE, r = i % PACK_TILE;
+        const int64_t lr = r0 + r, gr = a.prow[q >> 2][q & 3] * a.rows_blk + lr;
+        rowoff[q][r] = (lr < a.rows_blk && gr < a.rows_full) ? a.bX[b] + a.rs[gr] : OFF_INVALID;
+    }
+    for (int i = tid; i < nblk * PK_K; i += PM_THREADS)
+    {
+        const int q = i / PK_K, kk = i % PK_K;
+        const int64_t lk = k0 + kk, gk = a.pk[q >> 2][q & 3] * a.k_blk + lk;
+        koff[q][kk] = (lk < a.k_blk && gk < a.k_full) ? a.ks[gk] : OFF_INVALID;
+    }
+    __syncthreads();
+
+    // Element e of this thread: with kfast the 32 lanes of a warp walk 32
+    // consecutive k of one row, else 32 consecutive rows of one k.
+    constexpr int E = PACK_TILE * PK_K / PM_THREADS;
+    double x[4][E];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+        for (int e = 0; e < E; e++) x[j][e] = 0.0;
+    for (int c = 0; c < a.nt; c++)
+    {
+        const bool neg = a.t_s[c] < 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int e = 0; e < E; e++)
+            {
+                const int r = a.kfast ? warp + 16 * e : lane + 32 * (e & 3);
+                const int kk = a.kfast ? lane : warp + 16 * (e >> 2);
+                const int64_t ro = rowoff[c * 4 + j][r], ko = koff[c * 4 + j][kk];
+                if (ro != OFF_INVALID && ko != OFF_INVALID)
+                {
+                    const double v = a.X[ro + ko];
+                    x[j][e] += neg ? -v : v;
+                }
+            }
+    }
+    for (int o = 0; o < a.nout; o++)
+    {
+        int cf[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            cf[j] = (a.o_n[o] > 0 && a.o_j[o][0] == j ? a.o_s[o][0] : 0) +
+                    (a.o_n[o] > 1 && a.o_j[o][1] == j ? a.o_s[o][1] : 0);
+        __syncthreads();   // the previous output's tile has left buf
+#pragma unroll
+        for (int e = 0; e < E; e++)
+        {
+            double v = 0.0;
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (cf[j]) v += cf[j] > 0 ? x[j][e] : -x[j][e];
+            const int r = a.kfast ? warp + 16 * e : lane + 32 * (e & 3);
+            const int kk = a.kfast ? lane : warp + 16 * (e >> 2);
+            buf[r][kk] = v;
+        }
+        __syncthreads();
+        double* out = a.out[o] + ((b * a.tiles + t) * a.k_pad + k0) * PACK_TILE;
+#pragma unroll
+        for (int e = 0; e < E; e++)
+        {
+            const int r = lane + 32 * (e & 3);
+            const int kk = warp + 16 * (e >> 2);
+            if (k0 + kk < a.k_pad)
+                out[(int64_t)kk * PACK_TILE + tile_pos((int)((k0 + kk) & 7), r, 0)] = buf[r][kk];
+        }
+    }
+}
+
 // ---- packed GEMM ------------------------------------------------------------------
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
@@ -700,6 +793,20 @@ cudaError_t launch_pack(const PackArgs& a, cudaStream_t stream)
     if (a.tiles > 65535 || a.batch > 65535) return cudaErrorInvalidValue;
     timing_begin(KK_PACK, stream);
     pack_kernel<<<grid, PK_THREADS, 0, stream>>>(a);
+    timing_end(KK_PACK, stream);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) g_launches++;
+    return err;
+}
+
+cudaError_t launch_pack_multi(const PackMultiArgs& a, cudaStream_t stream)
+{
+    if (a.batch <= 0 || a.tiles <= 0 || a.k_pad <= 0 || a.nout <= 0) return cudaSuccess;
+    if (a.k_pad % PK_K || a.nt < 1 || a.nt > 2 || a.nout > 7) return cudaErrorInvalidValue;
+    if (a.tiles > 65535 || a.batch > 65535) return cudaErrorInvalidValue;
+    dim3 grid((unsigned)(a.k_pad / PK_K), (unsigned)a.tiles, (unsigned)a.batch);
+    timing_begin(KK_PACK, stream);
+    pack_multi_kernel<<<grid, PM_THREADS, 0, stream>>>(a);
     timing_end(KK_PACK, stream);
     cudaError_t err = cudaGetLastError();
     if (err == cudaSuccess) g_launches++;

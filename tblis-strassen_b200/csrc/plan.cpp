@@ -6,6 +6,8 @@
 #include <limits>
 #include <map>
 #include <numeric>
+#include <tuple>
+#include <vector>
 
 namespace tsb {
 
@@ -460,6 +462,96 @@ const ProductTable& product_table(int level)
     static const ProductTable t1 = make_table(1);
     static const ProductTable t2 = make_table(2);
     return level == 0 ? t0 : level == 1 ? t1 : t2;
+}
+
+namespace {
+
+// Factored sums of one group from the coefficient matrix M (U for A, V for B).
+PackGroup make_group(int level, const int (*M)[7], int group)
+{
+    PackGroup pg;
+    if (level == 1)
+    {
+        pg.nt = 1;
+        pg.t_s[0] = 1;
+        for (int h = 0; h < 2; h++) { pg.row[0][h] = (int8_t)h; pg.col[0][h] = (int8_t)h; }
+    }
+    else
+    {
+        for (int id = 0; id < 4; id++)
+        {
+            if (!M[id][group]) continue;
+            const int t = pg.nt++;
+            pg.t_s[t] = (int8_t)M[id][group];
+            for (int h = 0; h < 2; h++)
+            {
+                pg.row[t][h] = (int8_t)(2 * (id / 2) + h);
+                pg.col[t][h] = (int8_t)(2 * (id % 2) + h);
+            }
+        }
+    }
+    for (int q = 0; q < 7; q++)
+        for (int id = 0; id < 4; id++)
+            if (M[id][q])
+            {
+                const int i = pg.o_n[q]++;
+                pg.o_j[q][i] = (int8_t)id;
+                pg.o_s[q][i] = (int8_t)M[id][q];
+            }
+    return pg;
+}
+
+// Expand a group's sums and compare them with the product table's terms.
+bool group_matches(const PackGroup& pg, int level, int operand, int group)
+{
+    const ProductTable& t = product_table(level);
+    for (int q = 0; q < 7; q++)
+    {
+        const Product& pr = t.prod[(size_t)(group * 7 + q)];
+        const Term* want = operand == 0 ? pr.a : pr.b;
+        const int nwant = operand == 0 ? pr.na : pr.nb;
+        std::vector<std::tuple<int, int, int>> got, exp;
+        for (int i = 0; i < pg.o_n[q]; i++)
+        {
+            const int j = pg.o_j[q][i];
+            for (int c = 0; c < pg.nt; c++)
+                got.emplace_back(pg.row[c][j / 2], pg.col[c][j % 2], pg.t_s[c] * pg.o_s[q][i]);
+        }
+        for (int i = 0; i < nwant; i++) exp.emplace_back(want[i].r, want[i].c, want[i].sign);
+        std::sort(got.begin(), got.end());
+        std::sort(exp.begin(), exp.end());
+        if (got != exp) return false;
+    }
+    return true;
+}
+
+}  // namespace
+
+const PackGroup* pack_group(int level, int operand, int group)
+{
+    struct Groups
+    {
+        std::vector<PackGroup> g[3][2];
+        bool ok[3] = {false, false, false};
+        Groups()
+        {
+            for (int level = 1; level <= 2; level++)
+            {
+                const int ngroups = level == 1 ? 1 : 7;
+                ok[level] = true;
+                for (int op = 0; op < 2; op++)
+                    for (int G = 0; G < ngroups; G++)
+                    {
+                        g[level][op].push_back(make_group(level, op == 0 ? U : V, G));
+                        ok[level] = ok[level] && group_matches(g[level][op].back(), level, op, G);
+                    }
+            }
+        }
+    };
+    static const Groups groups;
+    if (level < 1 || level > 2 || !groups.ok[level] || operand < 0 || operand > 1) return nullptr;
+    if (group < 0 || group >= (int)groups.g[level][operand].size()) return nullptr;
+    return &groups.g[level][operand][(size_t)group];
 }
 
 }  // namespace tsb

@@ -99,4 +99,22 @@ struct ProductTable
 // (the 49-product grid of src/stra_internal/3t/stra_mult_2level.cxx:341-1485).
 const ProductTable& product_table(int level);
 
+// The operand sums of 7 consecutive products (all of L=1, or products
+// 7G .. 7G+6 of L=2) in factored form, so one pass over the operand forms all
+// seven: X_j = sum_t sign_t * block(row[t][j/2], col[t][j%2]) for the 4
+// sub-blocks j of the group's coarse sum, and sum q = sum_i s[q][i] * X_{j[q][i]}.
+// Blocks are positions in the H x H grid of the operand as the product table
+// addresses it (A: (m-block, k-block); B: (k-block, n-block)).  Expanding
+// reproduces product_table(level)'s terms exactly (checked when built).
+struct PackGroup
+{
+    int nt = 0;                  // coarse terms (1 or 2)
+    int8_t t_s[2] = {0, 0};
+    int8_t row[2][2] = {}, col[2][2] = {};
+    int8_t o_n[7] = {}, o_j[7][2] = {}, o_s[7][2] = {};
+};
+// operand 0 = A, 1 = B; group in [0, 7^(level-1)); nullptr if level is 0 or
+// the factored form failed its check against the product table.
+const PackGroup* pack_group(int level, int operand, int group);
+
 }  // namespace tsb

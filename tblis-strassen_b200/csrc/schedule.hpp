@@ -35,8 +35,12 @@ struct PackGeom
 };
 PackGeom pack_geom(int level, const GemmView& g);
 
-// Bytes of S + T for the packed schedule (one product at a time).
+// Bytes of S + T for the packed schedule one product at a time, and for
+// the grouped-sum form (L >= 1: the 7 sums of a product group formed in one
+// pass, 7 S and 7 T held at once).  run_fp64_packed_enqueue uses the grouped
+// form whenever ws_bytes allows it.
 size_t fp64_packed_workspace_bytes(int level, const GemmView& g);
+size_t fp64_packed_group_workspace_bytes(int level, const GemmView& g);
 
 // Pack product `pr`'s operand sums into S and T (two launches).
 int enqueue_pack_product(const Product& pr, const GemmView& g, const PackGeom& pg,

@@ -35,13 +35,37 @@ def to_dev(x, cuda):
     return out
 
 
-@pytest.fixture(params=["packed", "fused"])
-def schedule(request, tsb):
-    """ABC runs packed operand sums (default) or, with no workspace, the fully
-    fused kernel; both must meet the same bound."""
-    tsb.set_workspace_limit(None if request.param == "packed" else 0)
+@pytest.fixture(params=["packed", "packed_single", "fused"])
+def schedule(request, tsb, monkeypatch):
+    """ABC runs packed operand sums (default: at L >= 1 the 7 sums of a product
+    group formed in one pass), packed sums one product at a time (workspace
+    limited to one product's S and T), or, with no workspace, the fully fused
+    kernel; all must meet the same bound."""
+    if request.param == "packed_single":
+        orig = tsb.contract
+
+        def contract(level, alpha, A, ia, B, ib, beta, C, ic, **kw):
+            tsb.set_workspace_limit(single_product_bytes(tsb, level, A, ia, B, ib, C, ic))
+            try:
+                return orig(level, alpha, A, ia, B, ib, beta, C, ic, **kw)
+            finally:
+                tsb.set_workspace_limit(None)
+
+        monkeypatch.setattr(tsb, "contract", contract)
+    else:
+        tsb.set_workspace_limit(None if request.param == "packed" else 0)
     yield request.param
     tsb.set_workspace_limit(None)
+
+
+def single_product_bytes(tsb, level, A, ia, B, ib, C, ic):
+    """Workspace of one product's packed S and T (tile rows 128, k padded to 32)."""
+    q = tsb.plan_query(A, ia, B, ib, C, ic, scatter=False)
+    H = 1 << level
+    cdiv = lambda a, b: -(-a // b)
+    ms, ns, ks = cdiv(q["m"], H), cdiv(q["n"], H), cdiv(q["k"], H)
+    kpad = cdiv(ks, 32) * 32
+    return 8 * q["batch"] * (cdiv(ms, 128) + cdiv(ns, 128)) * 128 * kpad
 
 
 def run_gpu(tsb, cuda, level, impl, alpha, A, ia, B, ib, beta, C0, ic):
@@ -185,7 +209,14 @@ def test_launch_counter_moves(tsb, cuda):
         tsb.set_workspace_limit(None)
     before = tsb.launch_count()
     run_gpu(tsb, cuda, 1, 1, 1.0, A, "ik", A, "kj", 0.0, A, "ij")
-    assert tsb.launch_count() == before + 21        # packed ABC: 7 x (pack S, pack T, GEMM)
+    assert tsb.launch_count() == before + 9         # packed ABC: pack 7 S, pack 7 T, 7 GEMMs
+    tsb.set_workspace_limit(single_product_bytes(tsb, 1, A, "ik", A, "kj", A, "ij"))
+    try:
+        before = tsb.launch_count()
+        run_gpu(tsb, cuda, 1, 1, 1.0, A, "ik", A, "kj", 0.0, A, "ij")
+        assert tsb.launch_count() == before + 21    # one product at a time: 7 x (pack S, pack T, GEMM)
+    finally:
+        tsb.set_workspace_limit(None)
 
 
 @pytest.mark.parametrize("level", [1, 2])
