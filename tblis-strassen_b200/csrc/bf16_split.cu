@@ -43,15 +43,20 @@ extern std::atomic<unsigned long long> g_launches;
 namespace {
 
 constexpr int ST = SPLIT_TILE;               // 128: tile rows (A side) / columns (B side)
-constexpr int SK = 64;                       // k per tile block (one 128-byte bf16 row)
+constexpr int SK = SPLIT_K;                  // k per tile block (one 128-byte bf16 row)
 constexpr int BLK = ST * SK * 2;             // 16 KB per tile block
-constexpr int KCH = 4;                       // k blocks per TMEM accumulation chunk (256 k)
+constexpr int KCH = 256 / SK;                // k blocks per TMEM accumulation chunk (256 k)
+constexpr int ROWB = SK * 2;                 // bytes per block row
+static_assert(SK == 32 || SK == 64, "64- or 128-byte swizzled rows");
 
-// Byte offset of element (r, k) in a 128 x 64 bf16 block, K-major with the
-// 128-byte swizzle: 16-byte chunk k/8 of row r moves to chunk (k/8) ^ (r%8).
-__host__ __device__ __forceinline__ int sw128(int r, int k)
+// Byte offset of element (r, k) in a 128 x SK bf16 block, K-major with the
+// swizzle of its row length (16-byte chunk c = k/8 of row r):
+//   64-byte rows (SWIZZLE_64B):   chunk c ^ ((r / 2) % 4), 8-row groups of 512 B;
+//   128-byte rows (SWIZZLE_128B): chunk c ^ (r % 8),       8-row groups of 1024 B.
+__host__ __device__ __forceinline__ int swz(int r, int k)
 {
-    return (r >> 3) * 1024 + (r & 7) * 128 + ((((k >> 3) ^ r) & 7) << 4) + (k & 7) * 2;
+    const int c = SK == 32 ? ((k >> 3) ^ (r >> 1)) & 3 : ((k >> 3) ^ r) & 7;
+    return (r >> 3) * (8 * ROWB) + (r & 7) * ROWB + (c << 4) + (k & 7) * 2;
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
@@ -89,22 +94,27 @@ __global__ void scale_kernel(const __grid_constant__ SplitScaleArgs a)
 
 // ---- split pack -------------------------------------------------------------------
 
+// Each CTA packs half a tile block (PR = 64 of its 128 rows x SK k), so a
+// CTA's shared memory stays small and several CTAs per SM keep loads in flight.
+constexpr int PR = ST / 2;
+
 __global__ void __launch_bounds__(256)
 split_pack_kernel(const __grid_constant__ SplitPackArgs a)
 {
-    __shared__ float buf[ST][SK + 1];
-    __shared__ int64_t rowoff[4][ST];            // per term: batch + row offset (or invalid)
+    __shared__ float buf[PR][SK + 1];
+    __shared__ int64_t rowoff[4][PR];            // per term: batch + row offset (or invalid)
     __shared__ int64_t koff[4][SK];              // per term: k offset (or invalid)
-    __shared__ float rscale[ST];
+    __shared__ float rscale[PR];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int64_t c = blockIdx.x;            // k block
-    const int64_t t = blockIdx.y;            // row tile
+    const int64_t t = blockIdx.y >> 1;       // row tile
+    const int half = blockIdx.y & 1;         // its rows [64 half, 64 half + 64)
     const int64_t b = blockIdx.z;
-    const int64_t r0 = t * ST, k0 = c * SK;
+    const int64_t r0 = t * ST + half * PR, k0 = c * SK;
     const int nt = a.nt;
-    for (int i = tid; i < nt * ST; i += 256)
+    for (int i = tid; i < nt * PR; i += 256)
     {
-        const int q = i / ST, r = i % ST;
+        const int q = i / PR, r = i % PR;
         const int64_t lr = r0 + r, gr = a.t_r[q] * a.rows_blk + lr;
         rowoff[q][r] = (lr < a.rows_blk && gr < a.rows_full) ? a.bX[b] + a.rs[gr] : OFF_INVALID;
     }
@@ -114,11 +124,15 @@ split_pack_kernel(const __grid_constant__ SplitPackArgs a)
         const int64_t lk = k0 + kk, gk = a.t_c[q] * a.k_blk + lk;
         koff[q][kk] = (lk < a.k_blk && gk < a.k_full) ? a.ks[gk] : OFF_INVALID;
     }
-    for (int i = tid; i < ST; i += 256)
+    for (int i = tid; i < PR; i += 256)
         rscale[i] = (r0 + i < a.rows_blk) ? a.scale[b * a.rows_blk + r0 + i] : 0.f;
     __syncthreads();
     // Terms outermost: all loads of one term are independent and in flight.
-    constexpr int E = ST * SK / 256;
+    // With kfast the 32 lanes of a warp walk 32 consecutive k of one row,
+    // else 32 consecutive rows of one k.
+    constexpr int E = PR * SK / 256;
+    auto row_of = [&](int x) { return a.kfast ? warp + 8 * (x / (SK / 32)) : lane + 32 * (x % (PR / 32)); };
+    auto k_of = [&](int x) { return a.kfast ? lane + 32 * (x % (SK / 32)) : warp + 8 * (x / (PR / 32)); };
     float v[E];
 #pragma unroll
     for (int x = 0; x < E; x++) v[x] = 0.f;
@@ -128,9 +142,7 @@ split_pack_kernel(const __grid_constant__ SplitPackArgs a)
 #pragma unroll
         for (int x = 0; x < E; x++)
         {
-            const int r = a.kfast ? warp + 8 * (x >> 1) : lane + 32 * (x & 3);
-            const int kk = a.kfast ? lane + 32 * (x & 1) : warp + 8 * (x >> 2);
-            const int64_t ro = rowoff[q][r], ko = koff[q][kk];
+            const int64_t ro = rowoff[q][row_of(x)], ko = koff[q][k_of(x)];
             if (ro != OFF_INVALID && ko != OFF_INVALID)
             {
                 const float e = a.X[ro + ko];
@@ -141,19 +153,18 @@ split_pack_kernel(const __grid_constant__ SplitPackArgs a)
 #pragma unroll
     for (int x = 0; x < E; x++)
     {
-        const int r = a.kfast ? warp + 8 * (x >> 1) : lane + 32 * (x & 3);
-        const int kk = a.kfast ? lane + 32 * (x & 1) : warp + 8 * (x >> 2);
-        buf[r][kk] = v[x] * rscale[r];
+        const int r = row_of(x);
+        buf[r][k_of(x)] = v[x] * rscale[r];
     }
     __syncthreads();
     // 16-byte chunks: row r, k group g (8 values) -> one chunk per plane.
     const size_t plane_stride = (size_t)a.batch * a.tiles * a.nk * BLK;
     unsigned char* blk = reinterpret_cast<unsigned char*>(a.out) + ((size_t)(b * a.tiles + t) * a.nk + c) * BLK;
 #pragma unroll
-    for (int i = 0; i < ST * 8 / 256; i++)
+    for (int i = 0; i < PR * (SK / 8) / 256; i++)
     {
         const int q = tid + 256 * i;
-        const int r = q >> 3, g = q & 7;
+        const int r = q / (SK / 8), g = q % (SK / 8);
         unsigned short hv[8], mv[8], lv[8];
 #pragma unroll
         for (int j = 0; j < 8; j++)
@@ -168,7 +179,7 @@ split_pack_kernel(const __grid_constant__ SplitPackArgs a)
             mv[j] = __bfloat16_as_ushort(m);
             lv[j] = __bfloat16_as_ushort(l);
         }
-        const int off = sw128(r, g * 8);
+        const int off = swz(half * PR + r, g * 8);
         auto pack = [](const unsigned short* v) {
             return make_uint4(v[0] | (unsigned)v[1] << 16, v[2] | (unsigned)v[3] << 16,
                               v[4] | (unsigned)v[5] << 16, v[6] | (unsigned)v[7] << 16);
@@ -181,13 +192,15 @@ split_pack_kernel(const __grid_constant__ SplitPackArgs a)
 
 // ---- tcgen05 GEMM -------------------------------------------------------------------
 
-// Shared-memory descriptor of a 128-row, K-major, 128-byte-swizzled block:
-// start >> 4, leading offset 16 B (unused when swizzled), stride 1024 B
-// between 8-row groups, fixed 0b001 at bit 46, swizzle mode 2 (128 B).
+// Shared-memory descriptor of a 128-row, K-major, swizzled block (swz):
+// start >> 4, leading offset 16 B (unused when swizzled), stride 8 rows
+// between 8-row groups, fixed 0b001 at bit 46, swizzle mode 4 (64 B rows) or
+// 2 (128 B rows) at bit 61.
 __device__ __forceinline__ uint64_t sdesc(uint32_t addr)
 {
-    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
-           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+    constexpr uint64_t mode = SK == 32 ? 4 : 2;
+    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)((8 * ROWB) >> 4) << 32) |
+           ((uint64_t)1 << 46) | (mode << 61);
 }
 
 // Instruction descriptor, kind::f16: D = F32, A = B = BF16, both K-major,
@@ -227,11 +240,17 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
     for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// Barrier slots of the split GEMM: full[s], empty[s] per ring stage, then
+// two accumulator-full, two accumulator-empty and the MMA drain barrier.
+constexpr int MAX_STAGES = 6;
+constexpr int BAR_FULL = 0, BAR_EMPTY = MAX_STAGES, BAR_ACCF = 2 * MAX_STAGES, BAR_ACCE = 2 * MAX_STAGES + 2,
+              BAR_DRAIN = 2 * MAX_STAGES + 4, NBARS = 2 * MAX_STAGES + 5;
+
 template <int P>
 struct SG
 {
-    static constexpr int STAGES = P == 3 ? 2 : 3;
     static constexpr int STAGE_BYTES = 2 * P * BLK;
+    static constexpr int STAGES = (192 * 1024) / STAGE_BYTES < MAX_STAGES ? (192 * 1024) / STAGE_BYTES : MAX_STAGES;
     static constexpr int TAB_BYTES = 4 * (ST + ST) * 8 + 2 * ST * 4;
     static constexpr int CTRL_BYTES = 256;
     static constexpr size_t smem = 1024 + size_t(STAGES) * STAGE_BYTES + CTRL_BYTES + TAB_BYTES;
@@ -248,8 +267,8 @@ split_gemm_kernel(const __grid_constant__ SplitGemmArgs a)
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     unsigned char* stages = smem;                           // [STAGES][A planes | B planes]
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * K::STAGE_BYTES);
-    // bars: full[0..3], empty[4..7], acc_full[8..9], acc_empty[10..11], mma drain[12]
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 16);
+    static_assert(NBARS * 8 + 8 <= K::CTRL_BYTES, "barriers, TMEM slot and abort flag");
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + NBARS);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
     int64_t* rowC = reinterpret_cast<int64_t*>(smem + STAGES * K::STAGE_BYTES + K::CTRL_BYTES);
     int64_t* colC = rowC + 4 * ST;
@@ -260,9 +279,9 @@ split_gemm_kernel(const __grid_constant__ SplitGemmArgs a)
     auto bar = [&](int i) { return smem_u32(bars + i); };
     if (tid == 0)
     {
-        for (int s = 0; s < 4; s++) { mbar_init(bar(s), 1); mbar_init(bar(4 + s), 1); }
-        for (int s = 0; s < 2; s++) { mbar_init(bar(8 + s), 1); mbar_init(bar(10 + s), 128); }
-        mbar_init(bar(12), 1);
+        for (int s = 0; s < STAGES; s++) { mbar_init(bar(BAR_FULL + s), 1); mbar_init(bar(BAR_EMPTY + s), 1); }
+        for (int s = 0; s < 2; s++) { mbar_init(bar(BAR_ACCF + s), 1); mbar_init(bar(BAR_ACCE + s), 128); }
+        mbar_init(bar(BAR_DRAIN), 1);
         *abort_flag = 0;
         mbar_init_fence();
     }
@@ -311,14 +330,14 @@ split_gemm_kernel(const __grid_constant__ SplitGemmArgs a)
                 {
                     const int s = it % STAGES;
                     const uint32_t ph = (it / STAGES) & 1;
-                    if (!mbar_wait(bar(4 + s), ph ^ 1, abort_flag, a.err, 1)) { ok = false; break; }
-                    mbar_expect_tx(bar(s), 2 * P * BLK);
+                    if (!mbar_wait(bar(BAR_EMPTY + s), ph ^ 1, abort_flag, a.err, 1)) { ok = false; break; }
+                    mbar_expect_tx(bar(BAR_FULL + s), 2 * P * BLK);
                     const uint32_t dst = smem_u32(stages + s * K::STAGE_BYTES);
 #pragma unroll
                     for (int p = 0; p < P; p++)
                     {
-                        bulk_copy(dst + p * BLK, srcA + p * planeA + c * BLK, BLK, bar(s));
-                        bulk_copy(dst + (P + p) * BLK, srcB + p * planeB + c * BLK, BLK, bar(s));
+                        bulk_copy(dst + p * BLK, srcA + p * planeA + c * BLK, BLK, bar(BAR_FULL + s));
+                        bulk_copy(dst + (P + p) * BLK, srcB + p * planeB + c * BLK, BLK, bar(BAR_FULL + s));
                     }
                 }
             }
@@ -326,7 +345,7 @@ split_gemm_kernel(const __grid_constant__ SplitGemmArgs a)
             // the full barrier of each of the last STAGES stages issued).
             volatile int never = 0;
             for (uint32_t i = (it > STAGES ? it - STAGES : 0); i < it; i++)
-                mbar_wait(bar(i % STAGES), (i / STAGES) & 1, &never, nullptr, 0);
+                mbar_wait(bar(BAR_FULL + i % STAGES), (i / STAGES) & 1, &never, nullptr, 0);
         }
     }
     else if (warp == 1)
@@ -343,12 +362,12 @@ split_gemm_kernel(const __grid_constant__ SplitGemmArgs a)
                     if (c % KCH == 0)
                     {
                         const int bacc = u & 1;
-                        if (!mbar_wait(bar(10 + bacc), ((u >> 1) & 1) ^ 1, abort_flag, a.err, 2)) { ok = false; break; }
+                        if (!mbar_wait(bar(BAR_ACCE + bacc), ((u >> 1) & 1) ^ 1, abort_flag, a.err, 2)) { ok = false; break; }
                         fence_after();
                         dcol = bacc * 2 * ST;
                     }
                     const int s = it % STAGES;
-                    if (!mbar_wait(bar(s), (it / STAGES) & 1, abort_flag, a.err, 3)) { ok = false; break; }
+                    if (!mbar_wait(bar(BAR_FULL + s), (it / STAGES) & 1, abort_flag, a.err, 3)) { ok = false; break; }
                     fence_after();
                     const uint32_t base = smem_u32(stages + s * K::STAGE_BYTES);
 #pragma unroll
@@ -365,18 +384,18 @@ split_gemm_kernel(const __grid_constant__ SplitGemmArgs a)
                         for (int kk = 0; kk < SK / 16; kk++)
                             mma_bf16(d, ad + 2 * kk, bd + 2 * kk, (fresh && kk == 0) ? 0u : 1u);
                     }
-                    mma_commit(bar(4 + s));
+                    mma_commit(bar(BAR_EMPTY + s));
                     if (c % KCH == KCH - 1 || c == nk - 1)
                     {
-                        mma_commit(bar(8 + (u & 1)));
+                        mma_commit(bar(BAR_ACCF + (u & 1)));
                         u++;
                     }
                 }
             }
             // Every MMA issued completes before TMEM is freed.
-            mma_commit(bar(12));
+            mma_commit(bar(BAR_DRAIN));
             volatile int never = 0;
-            mbar_wait(bar(12), 0, &never, nullptr, 0);
+            mbar_wait(bar(BAR_DRAIN), 0, &never, nullptr, 0);
         }
     }
     else
@@ -414,7 +433,7 @@ split_gemm_kernel(const __grid_constant__ SplitGemmArgs a)
             for (int64_t ch = 0; ch < nch; ch++, u++)
             {
                 const int bacc = u & 1;
-                if (!mbar_wait(bar(8 + bacc), (u >> 1) & 1, abort_flag, a.err, 4)) { ok = false; break; }
+                if (!mbar_wait(bar(BAR_ACCF + bacc), (u >> 1) & 1, abort_flag, a.err, 4)) { ok = false; break; }
                 fence_after();
 #pragma unroll
                 for (int j = 0; j < ST / 32; j++)
@@ -427,7 +446,7 @@ split_gemm_kernel(const __grid_constant__ SplitGemmArgs a)
                     for (int i = 0; i < 32; i++) acc[j * 32 + i] += hh[i] + cr[i];
                 }
                 fence_before();
-                mbar_arrive(bar(10 + bacc));
+                mbar_arrive(bar(BAR_ACCE + bacc));
             }
             if (!ok) break;
             // C update in batches of 32 columns: all loads of a batch are
@@ -503,8 +522,8 @@ cudaError_t launch_split_scale(const SplitScaleArgs& a, cudaStream_t stream)
 cudaError_t launch_split_pack(const SplitPackArgs& a, cudaStream_t stream)
 {
     if (a.batch <= 0 || a.tiles <= 0 || a.nk <= 0) return cudaSuccess;
-    if (a.tiles > 65535 || a.batch > 65535 || (a.planes != 2 && a.planes != 3)) return cudaErrorInvalidValue;
-    dim3 grid((unsigned)a.nk, (unsigned)a.tiles, (unsigned)a.batch);
+    if (2 * a.tiles > 65535 || a.batch > 65535 || (a.planes != 2 && a.planes != 3)) return cudaErrorInvalidValue;
+    dim3 grid((unsigned)a.nk, (unsigned)(2 * a.tiles), (unsigned)a.batch);
     timing_begin(KK_PACK, stream);
     split_pack_kernel<<<grid, 256, 0, stream>>>(a);
     timing_end(KK_PACK, stream);
