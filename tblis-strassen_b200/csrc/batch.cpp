@@ -590,7 +590,7 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
             if (c.size() < 2) continue;
             need = true;
             for (const Choice& x : c)
-                tune_ws = std::max(tune_ws, x.variant == V_SPLIT ? fp32_workspace_bytes(x.level, pr.g, FP32_TERMS)
+                tune_ws = std::max(tune_ws, x.variant == V_SPLIT ? fp32_group_workspace_bytes(x.level, pr.g, FP32_TERMS)
                                                                  : fp64_packed_group_workspace_bytes(x.level, pr.g));
         }
         Tuner tuner;
@@ -701,7 +701,7 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
             const int b = load[0] <= load[1] ? 0 : 1;
             f32_list[b].push_back(i);
             load[b] += probs[i].flops();
-            need[b] = std::max(need[b], fp32_workspace_bytes(probs[i].level, probs[i].g, FP32_TERMS));
+            need[b] = std::max(need[b], fp32_group_workspace_bytes(probs[i].level, probs[i].g, FP32_TERMS));
         }
         for (int b = 0; b < 2; b++)
             if (need[b]) TSB_TRY(plan->f32_ws[b].alloc(need[b]));
@@ -768,7 +768,7 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
                 TSB_TRY(run_fp32_enqueue(pr.level, pr.g, tb, static_cast<const float*>(pr.A),
                                          static_cast<const float*>(pr.B), static_cast<float*>(pr.C),
                                          cs.f32[b], sms, plan->f32_ws[b].p,
-                                         fp32_workspace_bytes(pr.level, pr.g, FP32_TERMS), FP32_TERMS, err));
+                                         fp32_group_workspace_bytes(pr.level, pr.g, FP32_TERMS), FP32_TERMS, err));
             }
             if (use_f32[b]) TSB_CU(cudaEventRecord(ev_f32[b], cs.f32[b]));
         }

@@ -94,9 +94,49 @@ __global__ void scale_kernel(const __grid_constant__ SplitScaleArgs a)
 
 // ---- split pack -------------------------------------------------------------------
 
+constexpr int PR = ST / 2;
+
+// Split the scaled FP32 values of buf (rows [64 half, 64 half + 64) of one
+// 128 x SK block) into bf16 planes hi = bf16(x), mid = bf16(x - hi),
+// lo = bf16(x - hi - mid), written as 16-byte chunks (8 k of one row) at
+// their swizzled offsets; plane p of the block is at out + p * plane_stride +
+// block_off.
+__device__ __forceinline__ void write_planes(const float (*buf)[SK + 1], void* out, size_t plane_stride,
+                                             size_t block_off, int half, int planes, int tid)
+{
+    unsigned char* blk = reinterpret_cast<unsigned char*>(out) + block_off;
+#pragma unroll
+    for (int i = 0; i < PR * (SK / 8) / 256; i++)
+    {
+        const int q = tid + 256 * i;
+        const int r = q / (SK / 8), g = q % (SK / 8);
+        unsigned short hv[8], mv[8], lv[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+        {
+            const float x = buf[r][g * 8 + j];
+            const __nv_bfloat16 h = __float2bfloat16_rn(x);
+            const float r1 = x - __bfloat162float(h);
+            const __nv_bfloat16 m = __float2bfloat16_rn(r1);
+            const float r2 = r1 - __bfloat162float(m);
+            const __nv_bfloat16 l = __float2bfloat16_rn(r2);
+            hv[j] = __bfloat16_as_ushort(h);
+            mv[j] = __bfloat16_as_ushort(m);
+            lv[j] = __bfloat16_as_ushort(l);
+        }
+        const int off = swz(half * PR + r, g * 8);
+        auto pack = [](const unsigned short* v) {
+            return make_uint4(v[0] | (unsigned)v[1] << 16, v[2] | (unsigned)v[3] << 16,
+                              v[4] | (unsigned)v[5] << 16, v[6] | (unsigned)v[7] << 16);
+        };
+        *reinterpret_cast<uint4*>(blk + off) = pack(hv);
+        *reinterpret_cast<uint4*>(blk + plane_stride + off) = pack(mv);
+        if (planes > 2) *reinterpret_cast<uint4*>(blk + 2 * plane_stride + off) = pack(lv);
+    }
+}
+
 // Each CTA packs half a tile block (PR = 64 of its 128 rows x SK k), so a
 // CTA's shared memory stays small and several CTAs per SM keep loads in flight.
-constexpr int PR = ST / 2;
 
 __global__ void __launch_bounds__(256)
 split_pack_kernel(const __grid_constant__ SplitPackArgs a)
@@ -157,36 +197,88 @@ split_pack_kernel(const __grid_constant__ SplitPackArgs a)
         buf[r][k_of(x)] = v[x] * rscale[r];
     }
     __syncthreads();
-    // 16-byte chunks: row r, k group g (8 values) -> one chunk per plane.
-    const size_t plane_stride = (size_t)a.batch * a.tiles * a.nk * BLK;
-    unsigned char* blk = reinterpret_cast<unsigned char*>(a.out) + ((size_t)(b * a.tiles + t) * a.nk + c) * BLK;
-#pragma unroll
-    for (int i = 0; i < PR * (SK / 8) / 256; i++)
+    write_planes(buf, a.out, (size_t)a.batch * a.tiles * a.nk * BLK,
+                 ((size_t)(b * a.tiles + t) * a.nk + c) * BLK, half, a.planes, tid);
+}
+
+// Seven split sums of one product group per pass (L >= 1), the FP32 form of
+// pack_multi_kernel: the CTA's 64-row x SK window of every block of the
+// group's coarse sum is read once, the four sub-block sums X_j stay in
+// registers, and each output's signed combination is scaled and split.
+__global__ void __launch_bounds__(256)
+split_pack_multi_kernel(const __grid_constant__ SplitPackMultiArgs a)
+{
+    __shared__ float buf[PR][SK + 1];
+    __shared__ int64_t rowoff[8][PR];            // per block (t, j): batch + row offset (or invalid)
+    __shared__ int64_t koff[8][SK];              // per block (t, j): k offset (or invalid)
+    __shared__ float rscale[PR];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int64_t c = blockIdx.x;
+    const int64_t t = blockIdx.y >> 1;
+    const int half = blockIdx.y & 1;
+    const int64_t b = blockIdx.z;
+    const int64_t r0 = t * ST + half * PR, k0 = c * SK;
+    const int nblk = a.nt * 4;
+    for (int i = tid; i < nblk * PR; i += 256)
     {
-        const int q = tid + 256 * i;
-        const int r = q / (SK / 8), g = q % (SK / 8);
-        unsigned short hv[8], mv[8], lv[8];
+        const int q = i / PR, r = i % PR;
+        const int64_t lr = r0 + r, gr = a.prow[q >> 2][q & 3] * a.rows_blk + lr;
+        rowoff[q][r] = (lr < a.rows_blk && gr < a.rows_full) ? a.bX[b] + a.rs[gr] : OFF_INVALID;
+    }
+    for (int i = tid; i < nblk * SK; i += 256)
+    {
+        const int q = i / SK, kk = i % SK;
+        const int64_t lk = k0 + kk, gk = a.pk[q >> 2][q & 3] * a.k_blk + lk;
+        koff[q][kk] = (lk < a.k_blk && gk < a.k_full) ? a.ks[gk] : OFF_INVALID;
+    }
+    for (int i = tid; i < PR; i += 256)
+        rscale[i] = (r0 + i < a.rows_blk) ? a.scale[b * a.rows_blk + r0 + i] : 0.f;
+    __syncthreads();
+    constexpr int E = PR * SK / 256;
+    auto row_of = [&](int x) { return a.kfast ? warp + 8 * (x / (SK / 32)) : lane + 32 * (x % (PR / 32)); };
+    auto k_of = [&](int x) { return a.kfast ? lane + 32 * (x % (SK / 32)) : warp + 8 * (x / (PR / 32)); };
+    float xs[4][E];
 #pragma unroll
-        for (int j = 0; j < 8; j++)
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+        for (int x = 0; x < E; x++) xs[j][x] = 0.f;
+    for (int q = 0; q < a.nt; q++)
+    {
+        const bool neg = a.t_s[q] < 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int x = 0; x < E; x++)
+            {
+                const int64_t ro = rowoff[q * 4 + j][row_of(x)], ko = koff[q * 4 + j][k_of(x)];
+                if (ro != OFF_INVALID && ko != OFF_INVALID)
+                {
+                    const float e = a.X[ro + ko];
+                    xs[j][x] += neg ? -e : e;
+                }
+            }
+    }
+    for (int o = 0; o < a.nout; o++)
+    {
+        int cf[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            cf[j] = (a.o_n[o] > 0 && a.o_j[o][0] == j ? a.o_s[o][0] : 0) +
+                    (a.o_n[o] > 1 && a.o_j[o][1] == j ? a.o_s[o][1] : 0);
+        __syncthreads();   // the previous output's tile has left buf
+#pragma unroll
+        for (int x = 0; x < E; x++)
         {
-            const float x = buf[r][g * 8 + j];
-            const __nv_bfloat16 h = __float2bfloat16_rn(x);
-            const float r1 = x - __bfloat162float(h);
-            const __nv_bfloat16 m = __float2bfloat16_rn(r1);
-            const float r2 = r1 - __bfloat162float(m);
-            const __nv_bfloat16 l = __float2bfloat16_rn(r2);
-            hv[j] = __bfloat16_as_ushort(h);
-            mv[j] = __bfloat16_as_ushort(m);
-            lv[j] = __bfloat16_as_ushort(l);
+            float v = 0.f;
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (cf[j]) v += cf[j] > 0 ? xs[j][x] : -xs[j][x];
+            const int r = row_of(x);
+            buf[r][k_of(x)] = v * rscale[r];
         }
-        const int off = swz(half * PR + r, g * 8);
-        auto pack = [](const unsigned short* v) {
-            return make_uint4(v[0] | (unsigned)v[1] << 16, v[2] | (unsigned)v[3] << 16,
-                              v[4] | (unsigned)v[5] << 16, v[6] | (unsigned)v[7] << 16);
-        };
-        *reinterpret_cast<uint4*>(blk + off) = pack(hv);
-        *reinterpret_cast<uint4*>(blk + plane_stride + off) = pack(mv);
-        if (a.planes > 2) *reinterpret_cast<uint4*>(blk + 2 * plane_stride + off) = pack(lv);
+        __syncthreads();
+        write_planes(buf, a.out[o], (size_t)a.batch * a.tiles * a.nk * BLK,
+                     ((size_t)(b * a.tiles + t) * a.nk + c) * BLK, half, a.planes, tid);
     }
 }
 
@@ -526,6 +618,20 @@ cudaError_t launch_split_pack(const SplitPackArgs& a, cudaStream_t stream)
     dim3 grid((unsigned)a.nk, (unsigned)(2 * a.tiles), (unsigned)a.batch);
     timing_begin(KK_PACK, stream);
     split_pack_kernel<<<grid, 256, 0, stream>>>(a);
+    timing_end(KK_PACK, stream);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) g_launches++;
+    return err;
+}
+
+cudaError_t launch_split_pack_multi(const SplitPackMultiArgs& a, cudaStream_t stream)
+{
+    if (a.batch <= 0 || a.tiles <= 0 || a.nk <= 0 || a.nout <= 0) return cudaSuccess;
+    if (2 * a.tiles > 65535 || a.batch > 65535 || (a.planes != 2 && a.planes != 3)) return cudaErrorInvalidValue;
+    if (a.nt < 1 || a.nt > 2 || a.nout > 7) return cudaErrorInvalidValue;
+    dim3 grid((unsigned)a.nk, (unsigned)(2 * a.tiles), (unsigned)a.batch);
+    timing_begin(KK_PACK, stream);
+    split_pack_multi_kernel<<<grid, 256, 0, stream>>>(a);
     timing_end(KK_PACK, stream);
     cudaError_t err = cudaGetLastError();
     if (err == cudaSuccess) g_launches++;

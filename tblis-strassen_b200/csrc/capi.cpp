@@ -628,6 +628,16 @@ size_t fp32_workspace_bytes(int level, const GemmView& g, int terms)
     return sc + (size_t)P * g.batch * (tm + tn) * nk * blk;
 }
 
+size_t fp32_group_workspace_bytes(int level, const GemmView& g, int terms)
+{
+    const size_t one = fp32_workspace_bytes(level, g, terms);
+    if (level < 1 || !pack_group(level, 0, 0)) return one;
+    const int H = product_table(level).H;
+    const int64_t ms = cdiv(g.m, H), ns = cdiv(g.n, H);
+    const size_t sc = ((size_t)g.batch * (ms + ns) * 2 * sizeof(float) + 255) / 256 * 256;
+    return sc + 7 * (one - sc);
+}
+
 int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], const float* A,
                      const float* B, float* C, cudaStream_t st, int sms, void* ws, size_t ws_bytes,
                      int terms, int* err)
@@ -640,6 +650,8 @@ int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], c
     const int64_t tm = cdiv(ms, SPLIT_TILE), tn = cdiv(ns, SPLIT_TILE);
     if (g.batch * tm > 65535 || g.batch * tn > 65535 || nk > 2147483647) return TBLIS_STRA_ERR_TOO_LARGE;
     if (ws_bytes < fp32_workspace_bytes(level, g, terms)) return TBLIS_STRA_ERR_ALLOC;
+    const bool grouped = level >= 1 && fp32_group_workspace_bytes(level, g, terms) > fp32_workspace_bytes(level, g, terms) &&
+                         ws_bytes >= fp32_group_workspace_bytes(level, g, terms);
     const int P = terms == 3 ? 2 : 3;
     const size_t blk = (size_t)SPLIT_TILE * SPLIT_K * 2;
     const size_t sc = ((size_t)g.batch * (ms + ns) * 2 * sizeof(float) + 255) / 256 * 256;
@@ -658,6 +670,87 @@ int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], c
     const bool a_kfast = g.unit_ksA != 0 && (g.unit_rsA == 0 || g.unit_ksA < g.unit_rsA);
     const bool b_kfast = g.unit_ksB != 0 && (g.unit_csB == 0 || g.unit_ksB < g.unit_csB);
     static const int8_t TA6[6] = {0, 0, 1, 0, 1, 2}, TB6[6] = {0, 1, 0, 2, 1, 0};
+    auto gemm = [&](const Product& pr, const void* pA, const void* pB) -> int {
+        SplitGemmArgs ga{};
+        ga.A = pA; ga.B = pB; ga.C = C;
+        ga.rsC = tb[1]; ga.csC = tb[3]; ga.bC = tb[8];
+        ga.invA = invA; ga.invB = invB;
+        ga.m = g.m; ga.n = g.n; ga.ms = ms; ga.ns = ns; ga.nk = nk;
+        ga.tiles_m = tm; ga.tiles_n = tn; ga.batch = g.batch;
+        ga.alpha = (float)g.alpha; ga.beta = (float)g.beta;
+        ga.nc = pr.nc;
+        for (int q = 0; q < pr.nc; q++)
+        {
+            ga.c_r[q] = pr.c[q].r; ga.c_c[q] = pr.c[q].c; ga.c_s[q] = pr.c[q].sign;
+            ga.c_first[q] = pr.c_first[q];
+        }
+        ga.planes = P;
+        ga.nterms = P == 3 ? 6 : 3;
+        for (int i = 0; i < 6; i++) { ga.ta[i] = TA6[i]; ga.tb[i] = TB6[i]; }
+        ga.err = err;
+        TSB_CUDA(launch_split_gemm(ga, st, sms));
+        return TBLIS_STRA_SUCCESS;
+    };
+    if (grouped)
+    {
+        // Per group of 7 products: one pass over A and one over B form the 14
+        // split sums (7 plane sets each), then the 7 GEMMs in product order.
+        const size_t bytesA = (size_t)P * g.batch * tm * nk * blk, bytesB = (size_t)P * g.batch * tn * nk * blk;
+        char* base = static_cast<char*>(ws) + sc;
+        void* outA[7];
+        void* outB[7];
+        for (int q = 0; q < 7; q++)
+        {
+            outA[q] = base + q * bytesA;
+            outB[q] = base + 7 * bytesA + q * bytesB;
+        }
+        for (int G = 0; G < (int)tab.prod.size() / 7; G++)
+        {
+            for (int operand = 0; operand < 2; operand++)
+            {
+                const PackGroup* grp = pack_group(level, operand, G);
+                if (!grp) return TBLIS_STRA_ERR_UNSUPPORTED;
+                SplitPackMultiArgs m{};
+                if (operand == 0)
+                {
+                    m.X = A; m.rs = tb[0]; m.ks = tb[4]; m.bX = tb[6];
+                    m.rows_full = g.m; m.rows_blk = ms; m.scale = scaleA; m.tiles = tm; m.kfast = a_kfast;
+                }
+                else
+                {
+                    m.X = B; m.rs = tb[2]; m.ks = tb[5]; m.bX = tb[7];
+                    m.rows_full = g.n; m.rows_blk = ns; m.scale = scaleB; m.tiles = tn; m.kfast = b_kfast;
+                }
+                m.k_full = g.k; m.k_blk = ks; m.nk = nk; m.batch = g.batch; m.planes = P;
+                m.nt = grp->nt;
+                for (int c = 0; c < grp->nt; c++)
+                {
+                    m.t_s[c] = grp->t_s[c];
+                    for (int j = 0; j < 4; j++)
+                    {
+                        // block (row[j/2], col[j%2]) of the operand; B is packed n-major
+                        const int br = grp->row[c][j / 2], bc = grp->col[c][j % 2];
+                        m.prow[c][j] = (int8_t)(operand == 0 ? br : bc);
+                        m.pk[c][j] = (int8_t)(operand == 0 ? bc : br);
+                    }
+                }
+                m.nout = 7;
+                for (int q = 0; q < 7; q++)
+                {
+                    m.o_n[q] = grp->o_n[q];
+                    for (int i = 0; i < grp->o_n[q]; i++) { m.o_j[q][i] = grp->o_j[q][i]; m.o_s[q][i] = grp->o_s[q][i]; }
+                    m.out[q] = operand == 0 ? outA[q] : outB[q];
+                }
+                TSB_CUDA(launch_split_pack_multi(m, st));
+            }
+            for (int q = 0; q < 7; q++)
+            {
+                const int s = gemm(tab.prod[(size_t)(G * 7 + q)], outA[q], outB[q]);
+                if (s) return s;
+            }
+        }
+        return TBLIS_STRA_SUCCESS;
+    }
     for (const Product& pr : tab.prod)
     {
         SplitPackArgs pa{};
@@ -676,25 +769,8 @@ int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], c
         pb.scale = scaleB; pb.tiles = tn; pb.nk = nk; pb.batch = g.batch; pb.planes = P;
         pb.kfast = b_kfast; pb.out = planesB;
         TSB_CUDA(launch_split_pack(pb, st));
-
-        SplitGemmArgs ga{};
-        ga.A = planesA; ga.B = planesB; ga.C = C;
-        ga.rsC = tb[1]; ga.csC = tb[3]; ga.bC = tb[8];
-        ga.invA = invA; ga.invB = invB;
-        ga.m = g.m; ga.n = g.n; ga.ms = ms; ga.ns = ns; ga.nk = nk;
-        ga.tiles_m = tm; ga.tiles_n = tn; ga.batch = g.batch;
-        ga.alpha = (float)g.alpha; ga.beta = (float)g.beta;
-        ga.nc = pr.nc;
-        for (int q = 0; q < pr.nc; q++)
-        {
-            ga.c_r[q] = pr.c[q].r; ga.c_c[q] = pr.c[q].c; ga.c_s[q] = pr.c[q].sign;
-            ga.c_first[q] = pr.c_first[q];
-        }
-        ga.planes = P;
-        ga.nterms = P == 3 ? 6 : 3;
-        for (int i = 0; i < 6; i++) { ga.ta[i] = TA6[i]; ga.tb[i] = TB6[i]; }
-        ga.err = err;
-        TSB_CUDA(launch_split_gemm(ga, st, sms));
+        const int s = gemm(pr, planesA, planesB);
+        if (s) return s;
     }
     return TBLIS_STRA_SUCCESS;
 }
@@ -714,7 +790,8 @@ int run_fp32(int level, const GemmView& g, const DevPlan& t, const float* A, con
     const int terms = t_fp32_terms;
     Scratch wsbuf, errbuf;
     int s;
-    const size_t wsb = fp32_workspace_bytes(level, g, terms);
+    const size_t wsb_group = fp32_group_workspace_bytes(level, g, terms);
+    const size_t wsb = wsb_group <= t_ws_limit ? wsb_group : fp32_workspace_bytes(level, g, terms);
     if ((s = wsbuf.alloc(wsb, st))) return s;
     if ((s = errbuf.alloc(sizeof(int), st))) return s;
     TSB_CUDA(cudaMemsetAsync(errbuf.p, 0, sizeof(int), st));

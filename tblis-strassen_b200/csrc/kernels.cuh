@@ -213,6 +213,27 @@ struct SplitPackArgs
     void* out;                                 // bf16 planes
 };
 
+// Seven split sums of one product group in one pass (split_pack_multi_kernel;
+// the FP32 counterpart of PackMultiArgs): X_j = sum_t sign_t * block(t, j),
+// output o = sum_i o_s[o][i] * X_{o_j[o][i]}, scaled per row and split into
+// planes laid out as SplitPackArgs::out.
+struct SplitPackMultiArgs
+{
+    const float* X;
+    const int64_t* rs; const int64_t* ks; const int64_t* bX;
+    int64_t rows_full, k_full, rows_blk, k_blk;
+    int nt;
+    int8_t t_s[2];
+    int8_t prow[2][4], pk[2][4];
+    int nout;
+    int8_t o_n[7], o_j[7][2], o_s[7][2];
+    const float* scale;                        // [batch][rows_blk]
+    int64_t tiles, nk, batch;
+    int planes;
+    int kfast;
+    void* out[7];
+};
+
 struct SplitGemmArgs
 {
     const void* A;                             // bf16 planes, A side
@@ -232,6 +253,7 @@ struct SplitGemmArgs
 
 cudaError_t launch_split_scale(const SplitScaleArgs& args, cudaStream_t stream);
 cudaError_t launch_split_pack(const SplitPackArgs& args, cudaStream_t stream);
+cudaError_t launch_split_pack_multi(const SplitPackMultiArgs& args, cudaStream_t stream);
 cudaError_t launch_split_gemm(const SplitGemmArgs& args, cudaStream_t stream, int num_sms);
 
 cudaError_t launch_pack(const PackArgs& args, cudaStream_t stream);

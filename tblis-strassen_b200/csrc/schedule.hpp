@@ -60,6 +60,9 @@ int run_fp64_packed_enqueue(int level, const GemmView& g, const int64_t* const t
 
 // Split-BF16 schedule of one FP32 contraction on caller workspace.
 size_t fp32_workspace_bytes(int level, const GemmView& g, int terms);
+// The same with the 7 split sums of a product group held at once (L >= 1);
+// run_fp32_enqueue forms them in one pass whenever ws_bytes allows it.
+size_t fp32_group_workspace_bytes(int level, const GemmView& g, int terms);
 int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], const float* A,
                      const float* B, float* C, cudaStream_t st, int sms, void* ws, size_t ws_bytes,
                      int terms, int* err);

@@ -107,3 +107,41 @@ def test_fp32_host_pointers(tsb, cuda):
     tsb.contract(1, 1.0, A, "ik", B, "kj", 0.0, C, "ij", drop_in=True)
     R = A.astype(np.float64) @ B.astype(np.float64)
     assert normwise(C, R) <= 1e-6
+
+
+def fp32_single_product_bytes(tsb, level, A, ia, B, ib, C, ic, terms):
+    """Workspace of the split path with one product's planes at a time
+    (row scales + P planes of 128 x 64 bf16 blocks for S and T)."""
+    q = tsb.plan_query(A, ia, B, ib, C, ic, scatter=False)
+    H = 1 << level
+    cdiv = lambda a, b: -(-a // b)
+    ms, ns, ks = cdiv(q["m"], H), cdiv(q["n"], H), cdiv(q["k"], H)
+    sc = cdiv(q["batch"] * (ms + ns) * 2 * 4, 256) * 256
+    P = 2 if terms == 3 else 3
+    return sc + P * q["batch"] * (cdiv(ms, 128) + cdiv(ns, 128)) * cdiv(ks, 64) * 128 * 64 * 2
+
+
+@pytest.mark.parametrize("level", [1, 2])
+def test_fp32_per_product_packing(tsb, cuda, terms, level):
+    """With workspace for one product's planes only, the split sums are packed
+    product by product instead of seven per pass: same bound."""
+    import torch
+    ext = dict(a=24, b=20, c=10, d=12, e=18, f=16)
+    ia, ib, ic = "efac", "fbde", "abcd"
+    A = draw([ext[c] for c in ia], 11, "loguniform")
+    B = draw([ext[c] for c in ib], 12, "loguniform")
+    C0 = draw([ext[c] for c in ic], 13, "uniform")
+    R = C0.astype(np.float64, order="F")
+    oracle.contract(1.0, A.astype(np.float64, order="F"), ia, B.astype(np.float64, order="F"), ib, 1.0, R, ic)
+    dA, dB, dC = to_dev(A, cuda), to_dev(B, cuda), to_dev(C0, cuda)
+    tsb.set_workspace_limit(fp32_single_product_bytes(tsb, level, dA, ia, dB, ib, dC, ic, terms))
+    try:
+        before = tsb.launch_count()
+        tsb.contract(level, 1.0, dA, ia, dB, ib, 1.0, dC, ic)
+        torch.cuda.synchronize()
+        # 2 scale launches, then per product: pack S, pack T, GEMM
+        assert tsb.launch_count() - before == 2 + 3 * 7 ** level
+    finally:
+        tsb.set_workspace_limit(None)
+    err = normwise(dC.cpu().numpy(), R)
+    assert err <= TOL[terms], err
