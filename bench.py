@@ -216,9 +216,10 @@ def batched_form(torch, tsb, device, stream, count, barrier_sync, max_over_ranks
             tens.append((A, ia, B, ib, C, ic))
         res = {}
         # autotuned (level, variant, tile) vs the plain grouped fused launch at L=0
+        # FP64: against the plain grouped fused launch; FP32: against the
+        # split schedule problem by problem
         modes = [("autotuned", -1, None)]
-        if dtype == torch.float64:
-            modes.append(("fused_L0", 0, ["fused"]))
+        modes.append(("fused_L0", 0, ["fused"]) if dtype == torch.float64 else ("split_L0", 0, ["split"]))
         for mode, lv, allowed in modes:
             probs = [(1.0, A, ia, B, ib, 0.0, C, ic, lv) for A, ia, B, ib, C, ic in tens]
             tsb.set_batch_schedules(allowed)
@@ -245,8 +246,9 @@ def batched_form(torch, tsb, device, stream, count, barrier_sync, max_over_ranks
             torch.cuda.synchronize()
             worst = max(worst, float(torch.linalg.norm((C.double() - R).flatten()) / torch.linalg.norm(R.flatten())))
         res["spot_normwise_err"] = worst
-        if "fused_L0" in res:
-            res["autotuned_vs_fused_L0"] = res["autotuned"]["tflops_effective"] / res["fused_L0"]["tflops_effective"]
+        for base in ("fused_L0", "split_L0"):
+            if base in res:
+                res["autotuned_vs_" + base] = res["autotuned"]["tflops_effective"] / res[base]["tflops_effective"]
         out[name] = res
         del tens
         torch.cuda.empty_cache()

@@ -234,6 +234,9 @@ int tblis_stra_mult_noalloc(int level,
  *   TBLIS_STRA_BATCH_PACKED         the packed ABC schedule, problem by problem;
  *   TBLIS_STRA_BATCH_SPLIT          FP32: the split-BF16 schedule (6 terms),
  *                                   problem by problem on two graph branches;
+ *   TBLIS_STRA_BATCH_SPLIT_GROUPED  FP32, L = 0: split planes packed per chunk,
+ *                                   one grouped split-BF16 GEMM launch per chunk
+ *                                   (chunked and overlapped as PACKED_GROUPED);
  *   TBLIS_STRA_BATCH_SCALE          alpha == 0 or empty contracted range.
  *
  * A problem's level is given (0, 1, 2) or left to the autotuner (-1); the
@@ -260,7 +263,8 @@ enum
     TBLIS_STRA_BATCH_PACKED_GROUPED = 2,
     TBLIS_STRA_BATCH_PACKED = 3,
     TBLIS_STRA_BATCH_SPLIT = 4,
-    TBLIS_STRA_BATCH_SCALE = 5
+    TBLIS_STRA_BATCH_SCALE = 5,
+    TBLIS_STRA_BATCH_SPLIT_GROUPED = 6
 };
 
 typedef struct tblis_stra_batch_s* tblis_stra_batch;
@@ -269,10 +273,10 @@ int tblis_stra_batch_create(int count, const tblis_stra_problem* problems, tblis
 int tblis_stra_batch_execute(tblis_stra_batch batch, void* stream);
 int tblis_stra_batch_levels(tblis_stra_batch batch, int* levels);      /* the level each problem runs */
 int tblis_stra_batch_schedule(tblis_stra_batch batch, int* schedules); /* TBLIS_STRA_BATCH_* per problem */
-/* FP64 schedules the autotuner may choose on this thread: a mask of bits
- * (1 << TBLIS_STRA_BATCH_FUSED) | ... over FUSED, FUSED_SMALL, PACKED_GROUPED
- * and PACKED (default: all four).  A problem with no allowed candidate fails
- * create with TBLIS_STRA_ERR_ARG. */
+/* Schedules the autotuner may choose on this thread: a mask of bits
+ * (1 << TBLIS_STRA_BATCH_FUSED) | ... over FUSED, FUSED_SMALL, PACKED_GROUPED,
+ * PACKED (FP64), SPLIT and SPLIT_GROUPED (FP32); default: all six.  A problem
+ * with no allowed candidate fails create with TBLIS_STRA_ERR_ARG. */
 int tblis_stra_set_batch_schedules(unsigned mask);
 unsigned tblis_stra_get_batch_schedules(void);
 /* Seconds spent in create: total and autotuning; candidate timings run. */

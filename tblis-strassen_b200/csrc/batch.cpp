@@ -62,7 +62,8 @@ enum Variant
     V_PGROUP = TBLIS_STRA_BATCH_PACKED_GROUPED,
     V_PACKED = TBLIS_STRA_BATCH_PACKED,
     V_SPLIT = TBLIS_STRA_BATCH_SPLIT,
-    V_SCALE = TBLIS_STRA_BATCH_SCALE
+    V_SCALE = TBLIS_STRA_BATCH_SCALE,
+    V_SGROUP = TBLIS_STRA_BATCH_SPLIT_GROUPED
 };
 
 #define TSB_CU(x) do { const cudaError_t e_ = (x); \
@@ -70,9 +71,10 @@ enum Variant
 
 constexpr int FP32_TERMS = 6;
 
-// FP64 schedules the tuner may pick (bit v = variant v), per thread.
-constexpr unsigned FP64_VARIANTS = (1u << V_FUSED) | (1u << V_FUSED_SMALL) | (1u << V_PGROUP) | (1u << V_PACKED);
-thread_local unsigned t_variant_mask = FP64_VARIANTS;
+// Schedules the tuner may pick (bit v = variant v), per thread.
+constexpr unsigned ALL_VARIANTS = (1u << V_FUSED) | (1u << V_FUSED_SMALL) | (1u << V_PGROUP) | (1u << V_PACKED) |
+                                  (1u << V_SPLIT) | (1u << V_SGROUP);
+thread_local unsigned t_variant_mask = ALL_VARIANTS;
 // Packed operands per chunk of grouped packed problems (two chunk workspaces
 // in turn); TBLIS_STRA_BATCH_CHUNK_BYTES overrides it at create time.
 size_t chunk_bytes()
@@ -237,6 +239,18 @@ int upload_packed(const std::vector<PackedGemmArgs>& args, DevBuf* buf, PackedGr
                : fill_descs(args, work, mem, cap, g.probs, g.prefix, g.total);
 }
 
+int upload_split(const std::vector<SplitGemmArgs>& args, DevBuf* buf, SplitGroupArgs& g,
+                 void* mem = nullptr, size_t cap = 0)
+{
+    std::memset(&g, 0, sizeof g);
+    if (args.empty()) return TBLIS_STRA_SUCCESS;
+    std::vector<int64_t> work(args.size());
+    for (size_t i = 0; i < args.size(); i++) work[i] = args[i].batch * args[i].tiles_m * args[i].tiles_n;
+    g.nprob = (int)args.size();
+    return buf ? upload_descs(args, work, *buf, g.probs, g.prefix, g.total)
+               : fill_descs(args, work, mem, cap, g.probs, g.prefix, g.total);
+}
+
 int launch_fused_group(const DmmaGroupArgs& g, int level, int config, cudaStream_t st, int sms)
 {
     if (g.nprob == 0 || g.total == 0) return TBLIS_STRA_SUCCESS;
@@ -272,7 +286,7 @@ std::vector<Choice> candidates(const Prob& pr, bool prune = true)
     std::vector<Choice> c;
     const GemmView& g = pr.g;
     auto add = [&](int L, int v) {
-        if (v == V_SPLIT || (t_variant_mask >> v) & 1u) c.push_back({L, v});
+        if ((t_variant_mask >> v) & 1u) c.push_back({L, v});
     };
     const int64_t mnk = std::min(g.m, std::min(g.n, g.k));
     for (int L = 0; L <= 2; L++)
@@ -281,7 +295,9 @@ std::vector<Choice> candidates(const Prob& pr, bool prune = true)
         if (prune && pr.level_req < 0 && L > 0 && mnk < ((int64_t)1024 << L)) continue;
         if (g.type == TYPE_FLOAT)
         {
-            if (pack_geom(L, g).fits) add(L, V_SPLIT);
+            if (!pack_geom(L, g).fits) continue;
+            if (L == 0) add(0, V_SGROUP);
+            add(L, V_SPLIT);
             continue;
         }
         const bool packable = pack_geom(L, g).fits;
@@ -333,7 +349,8 @@ struct Tuner
         if ((s = scratch.alloc(c_bytes))) return s;
         if (cudaMemset(scratch.p, 0, c_bytes) != cudaSuccess) return TBLIS_STRA_ERR_CUDA;
         ws_bytes = w_bytes;
-        desc_cap = std::max(descs_bytes<DmmaArgs>(MAX_COPIES), descs_bytes<PackedGemmArgs>(MAX_COPIES));
+        desc_cap = std::max(std::max(descs_bytes<DmmaArgs>(MAX_COPIES), descs_bytes<PackedGemmArgs>(MAX_COPIES)),
+                            descs_bytes<SplitGemmArgs>(MAX_COPIES));
         if ((s = desc.alloc(desc_cap))) return s;
         return ws.alloc(w_bytes);
     }
@@ -420,6 +437,23 @@ struct Tuner
                                                static_cast<double*>(scratch.p) - shift, st, sms, ws.p, ws_bytes,
                                                err);
             });
+        if (c.variant == V_SGROUP)
+        {
+            SplitGemmArgs one{};
+            float* Cs = static_cast<float*>(scratch.p) - shift;
+            const double prep_ms = time([&] {
+                return run_fp32_enqueue(0, pr.g, tb, static_cast<const float*>(pr.A), static_cast<const float*>(pr.B),
+                                        Cs, st, sms, ws.p, ws_bytes, FP32_TERMS, err, &one, true);
+            });
+            std::vector<SplitGemmArgs> args(copies_for(one.batch * one.tiles_m * one.tiles_n), one);
+            SplitGroupArgs g;
+            if (upload_split(args, nullptr, g, desc.p, desc_cap)) return 1e30;
+            g.err = err;
+            const double gemm_ms = time([&] {
+                return launch_split_gemm_grouped(g, one.planes, st, sms) == cudaSuccess ? 0 : (int)TBLIS_STRA_ERR_CUDA;
+            });
+            return prep_ms + gemm_ms / (double)args.size();
+        }
         if (c.variant == V_SPLIT)
             return time([&] {
                 return run_fp32_enqueue(c.level, pr.g, tb, static_cast<const float*>(pr.A),
@@ -447,7 +481,8 @@ struct Tuner
         // and the lower level otherwise (less rounding error).
         Choice best = cand[0];
         double best_t = 1e30;
-        static const char* names[] = {"fused", "fused_small", "packed_grouped", "packed", "split", "scale"};
+        static const char* names[] = {"fused", "fused_small", "packed_grouped", "packed", "split", "scale",
+                                      "split_grouped"};
         for (const Choice& c : cand)
         {
             what = names[c.variant];
@@ -590,7 +625,8 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
             if (c.size() < 2) continue;
             need = true;
             for (const Choice& x : c)
-                tune_ws = std::max(tune_ws, x.variant == V_SPLIT ? fp32_group_workspace_bytes(x.level, pr.g, FP32_TERMS)
+                tune_ws = std::max(tune_ws, (x.variant == V_SPLIT || x.variant == V_SGROUP)
+                                                ? fp32_group_workspace_bytes(x.level, pr.g, FP32_TERMS)
                                                                  : fp64_packed_group_workspace_bytes(x.level, pr.g));
         }
         Tuner tuner;
@@ -599,7 +635,7 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
         {
             if (pr.empty || pr.scale) { pr.variant = V_SCALE; pr.level = 0; continue; }
             const std::vector<Choice> c = candidates(pr);
-            if (c.empty()) return t_variant_mask == FP64_VARIANTS ? TBLIS_STRA_ERR_TOO_LARGE : TBLIS_STRA_ERR_ARG;
+            if (c.empty()) return t_variant_mask == ALL_VARIANTS ? TBLIS_STRA_ERR_TOO_LARGE : TBLIS_STRA_ERR_ARG;
             const Choice ch = c.size() == 1 ? c[0] : tuner.choose(pr, tab);
             pr.level = ch.level;
             pr.variant = ch.variant;
@@ -647,48 +683,89 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
     for (auto& pr : probs)
         if (pr.variant == V_PACKED) seq_bytes = std::max(seq_bytes, fp64_packed_group_workspace_bytes(pr.level, pr.g));
     if (seq_bytes) TSB_TRY(plan->seq_ws.alloc(seq_bytes));
-    // 4c. chunks of grouped packed problems (consecutive, at most chunk_bytes()
-    // of packed operands unless one problem needs more)
-    std::vector<std::vector<int>> chunks;
+    // 4c. chunks of grouped problems: FP64 packed (V_PGROUP) and FP32 split
+    // (V_SGROUP) problems, each kind in consecutive chunks of at most
+    // chunk_bytes() of workspace (unless one problem needs more), packed into
+    // two chunk workspaces in turn.
+    struct Chunk
+    {
+        bool fp32 = false;
+        std::vector<int> probs;
+        std::vector<void*> ws;          // per problem: FP64 S (T follows), FP32 split workspace
+        PackedGroupArgs pg{};
+        SplitGroupArgs sg{};
+    };
+    auto chunk_need_of = [&](const Prob& pr) {
+        return pr.variant == V_PGROUP ? pgroup_bytes(pr.g) : round256(fp32_workspace_bytes(0, pr.g, FP32_TERMS));
+    };
+    std::vector<Chunk> chunks;
     size_t chunk_need = 0;
     {
         const size_t cap = chunk_bytes();
-        size_t used = 0;
-        for (int i = 0; i < count; i++)
+        for (int kind = 0; kind < 2; kind++)
         {
-            if (probs[i].variant != V_PGROUP) continue;
-            const size_t need = pgroup_bytes(probs[i].g);
-            if (chunks.empty() || (used > 0 && used + need > cap)) { chunks.emplace_back(); used = 0; }
-            chunks.back().push_back(i);
-            used += need;
-            chunk_need = std::max(chunk_need, used);
+            size_t used = 0;
+            bool open = false;
+            for (int i = 0; i < count; i++)
+            {
+                if (probs[i].variant != (kind ? V_SGROUP : V_PGROUP)) continue;
+                const size_t need = chunk_need_of(probs[i]);
+                if (!open || (used > 0 && used + need > cap))
+                {
+                    chunks.emplace_back();
+                    chunks.back().fp32 = kind == 1;
+                    used = 0;
+                    open = true;
+                }
+                chunks.back().probs.push_back(i);
+                used += need;
+                chunk_need = std::max(chunk_need, used);
+            }
         }
     }
-    struct ChunkPlan { std::vector<std::pair<double*, double*>> st; PackedGroupArgs g; };
-    std::vector<ChunkPlan> cplans(chunks.size());
     for (size_t b = 0; b < std::min<size_t>(chunks.size(), 2); b++) TSB_TRY(plan->chunk_ws[b].alloc(chunk_need));
     for (size_t c = 0; c < chunks.size(); c++)
     {
+        Chunk& ch = chunks[c];
         unsigned char* base = static_cast<unsigned char*>(plan->chunk_ws[c % 2].p);
         size_t off = 0;
-        std::vector<PackedGemmArgs> args;
-        for (int i : chunks[c])
+        std::vector<PackedGemmArgs> pargs;
+        std::vector<SplitGemmArgs> sargs;
+        for (int i : ch.probs)
         {
             const Prob& pr = probs[i];
-            const PackGeom pg = pack_geom(0, pr.g);
-            double* S = reinterpret_cast<double*>(base + off);
-            off += round256(pg.s_elems * sizeof(double));
-            double* T = reinterpret_cast<double*>(base + off);
-            off += round256(pg.t_elems * sizeof(double));
-            cplans[c].st.emplace_back(S, T);
             const int64_t* tb[9];
             pr.tables(tab, tb);
-            args.push_back(packed_product_args(product_table(0).prod[0], pr.g, pg, tb, S, T,
-                                               static_cast<double*>(pr.C), err));
+            ch.ws.push_back(base + off);
+            if (!ch.fp32)
+            {
+                const PackGeom pg = pack_geom(0, pr.g);
+                double* S = reinterpret_cast<double*>(base + off);
+                double* T = reinterpret_cast<double*>(base + off + round256(pg.s_elems * sizeof(double)));
+                pargs.push_back(packed_product_args(product_table(0).prod[0], pr.g, pg, tb, S, T,
+                                                    static_cast<double*>(pr.C), err));
+            }
+            else
+            {
+                SplitGemmArgs a{};
+                TSB_TRY(run_fp32_enqueue(0, pr.g, tb, static_cast<const float*>(pr.A), static_cast<const float*>(pr.B),
+                                         static_cast<float*>(pr.C), nullptr, sms, base + off, chunk_need_of(pr),
+                                         FP32_TERMS, err, &a, false));
+                sargs.push_back(a);
+            }
+            off += chunk_need_of(pr);
         }
         plan->descs.emplace_back();
-        TSB_TRY(upload_packed(args, &plan->descs.back(), cplans[c].g));
-        cplans[c].g.err = err;
+        if (!ch.fp32)
+        {
+            TSB_TRY(upload_packed(pargs, &plan->descs.back(), ch.pg));
+            ch.pg.err = err;
+        }
+        else
+        {
+            TSB_TRY(upload_split(sargs, &plan->descs.back(), ch.sg));
+            ch.sg.err = err;
+        }
     }
     // 4d. FP32 problems on two branches balanced by flops
     std::vector<int> f32_list[2];
@@ -732,21 +809,37 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
     // when chunk c+1 needs it.
     auto enqueue_pack = [&](size_t c) -> int {
         if (c >= 2) TSB_CU(cudaStreamWaitEvent(cs.pack, ev_gemm[c - 2], 0));
-        for (size_t j = 0; j < chunks[c].size(); j++)
+        const Chunk& ch = chunks[c];
+        for (size_t j = 0; j < ch.probs.size(); j++)
         {
-            const Prob& pr = probs[chunks[c][j]];
+            const Prob& pr = probs[ch.probs[j]];
             const int64_t* tb[9];
             pr.tables(tab, tb);
-            TSB_TRY(enqueue_pack_product(product_table(0).prod[0], pr.g, pack_geom(0, pr.g), tb,
-                                         static_cast<const double*>(pr.A), static_cast<const double*>(pr.B),
-                                         cplans[c].st[j].first, cplans[c].st[j].second, cs.pack));
+            if (!ch.fp32)
+            {
+                const PackGeom pg = pack_geom(0, pr.g);
+                double* S = static_cast<double*>(ch.ws[j]);
+                double* T = reinterpret_cast<double*>(static_cast<unsigned char*>(ch.ws[j]) +
+                                                      round256(pg.s_elems * sizeof(double)));
+                TSB_TRY(enqueue_pack_product(product_table(0).prod[0], pr.g, pg, tb,
+                                             static_cast<const double*>(pr.A), static_cast<const double*>(pr.B),
+                                             S, T, cs.pack));
+            }
+            else
+            {
+                SplitGemmArgs unused{};
+                TSB_TRY(run_fp32_enqueue(0, pr.g, tb, static_cast<const float*>(pr.A),
+                                         static_cast<const float*>(pr.B), static_cast<float*>(pr.C), cs.pack, sms,
+                                         ch.ws[j], chunk_need_of(pr), FP32_TERMS, err, &unused, true));
+            }
         }
         TSB_CU(cudaEventRecord(ev_pack[c], cs.pack));
         return TBLIS_STRA_SUCCESS;
     };
     auto enqueue_gemm = [&](size_t c) -> int {
         TSB_CU(cudaStreamWaitEvent(cs.main, ev_pack[c], 0));
-        TSB_CU(launch_packed_gemm_grouped(cplans[c].g, cs.main, sms));
+        if (!chunks[c].fp32) TSB_CU(launch_packed_gemm_grouped(chunks[c].pg, cs.main, sms));
+        else TSB_CU(launch_split_gemm_grouped(chunks[c].sg, FP32_TERMS == 6 ? 3 : 2, cs.main, sms));
         TSB_CU(cudaEventRecord(ev_gemm[c], cs.main));
         return TBLIS_STRA_SUCCESS;
     };
@@ -882,7 +975,7 @@ int tblis_stra_batch_schedule(tblis_stra_batch batch, int* schedules)
 
 int tblis_stra_set_batch_schedules(unsigned mask)
 {
-    if (mask == 0 || (mask & ~tsb::FP64_VARIANTS)) return TBLIS_STRA_ERR_ARG;
+    if (mask == 0 || (mask & ~tsb::ALL_VARIANTS)) return TBLIS_STRA_ERR_ARG;
     tsb::t_variant_mask = mask;
     return TBLIS_STRA_SUCCESS;
 }

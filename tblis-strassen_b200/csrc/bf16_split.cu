@@ -348,13 +348,46 @@ struct SG
     static constexpr size_t smem = 1024 + size_t(STAGES) * STAGE_BYTES + CTRL_BYTES + TAB_BYTES;
 };
 
-template <int P>
-__global__ void __launch_bounds__(192, 1)
-split_gemm_kernel(const __grid_constant__ SplitGemmArgs a)
+// Work sources of the split GEMM: one problem (the kernel parameter, read
+// through a pointer of unknown origin so its fields are loaded where used) or
+// a group of problems (descriptors in global memory; work item w belongs to
+// the problem p with prefix[p] <= w < prefix[p + 1]).  Every role resolves the
+// problem of each tile itself, since the roles run tiles apart.
+struct OneSplit
+{
+    const SplitGemmArgs* a;
+    __device__ int64_t total() const { return a->batch * a->tiles_m * a->tiles_n; }
+    __device__ const SplitGemmArgs& at(int64_t w, int64_t& local) const
+    {
+        local = w;
+        const SplitGemmArgs* p = a;
+        asm volatile("" : "+l"(p));
+        return *p;
+    }
+};
+
+struct SplitGroup
+{
+    const SplitGroupArgs& g;
+    __device__ int64_t total() const { return g.total; }
+    __device__ const SplitGemmArgs& at(int64_t w, int64_t& local) const
+    {
+        int lo = 0, hi = g.nprob - 1;
+        while (lo < hi)
+        {
+            const int mid = (lo + hi + 1) >> 1;
+            if (g.prefix[mid] <= w) lo = mid; else hi = mid - 1;
+        }
+        local = w - g.prefix[lo];
+        return g.probs[lo];
+    }
+};
+
+template <int P, class Src>
+__device__ __forceinline__ void split_gemm_body(const Src& src, int* err, unsigned char* smem_raw)
 {
     using K = SG<P>;
     constexpr int STAGES = K::STAGES;
-    extern __shared__ unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     unsigned char* stages = smem;                           // [STAGES][A planes | B planes]
@@ -388,10 +421,9 @@ split_gemm_kernel(const __grid_constant__ SplitGemmArgs a)
     fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    const int64_t tiles = a.tiles_m * a.tiles_n;
-    const int64_t work = a.batch * tiles;
-    const int64_t nk = a.nk;
-    auto decode = [&](int64_t w, int64_t& b, int64_t& tm, int64_t& tn) {
+    const int64_t work = src.total();
+    auto decode = [&](const SplitGemmArgs& a, int64_t w, int64_t& b, int64_t& tm, int64_t& tn) {
+        const int64_t tiles = a.tiles_m * a.tiles_n;
         b = w / tiles;
         const int64_t tw = w - b * tiles;
         const int64_t GROUP = 8;
@@ -401,8 +433,6 @@ split_gemm_kernel(const __grid_constant__ SplitGemmArgs a)
         tm = first_m + (tw % gsize);
         tn = (tw % (GROUP * a.tiles_n)) / gsize;
     };
-    const size_t planeA = (size_t)a.batch * a.tiles_m * nk * BLK;
-    const size_t planeB = (size_t)a.batch * a.tiles_n * nk * BLK;
 
     if (warp == 0)
     {
@@ -412,8 +442,12 @@ split_gemm_kernel(const __grid_constant__ SplitGemmArgs a)
             bool ok = true;
             for (int64_t w = blockIdx.x; w < work && ok; w += gridDim.x)
             {
-                int64_t b, tm, tn;
-                decode(w, b, tm, tn);
+                int64_t local, b, tm, tn;
+                const SplitGemmArgs& a = src.at(w, local);
+                decode(a, local, b, tm, tn);
+                const int64_t nk = a.nk;
+                const size_t planeA = (size_t)a.batch * a.tiles_m * nk * BLK;
+                const size_t planeB = (size_t)a.batch * a.tiles_n * nk * BLK;
                 const unsigned char* srcA = reinterpret_cast<const unsigned char*>(a.A) +
                                             ((size_t)(b * a.tiles_m + tm) * nk) * BLK;
                 const unsigned char* srcB = reinterpret_cast<const unsigned char*>(a.B) +
@@ -422,7 +456,7 @@ split_gemm_kernel(const __grid_constant__ SplitGemmArgs a)
                 {
                     const int s = it % STAGES;
                     const uint32_t ph = (it / STAGES) & 1;
-                    if (!mbar_wait(bar(BAR_EMPTY + s), ph ^ 1, abort_flag, a.err, 1)) { ok = false; break; }
+                    if (!mbar_wait(bar(BAR_EMPTY + s), ph ^ 1, abort_flag, err, 1)) { ok = false; break; }
                     mbar_expect_tx(bar(BAR_FULL + s), 2 * P * BLK);
                     const uint32_t dst = smem_u32(stages + s * K::STAGE_BYTES);
 #pragma unroll
@@ -448,18 +482,21 @@ split_gemm_kernel(const __grid_constant__ SplitGemmArgs a)
             bool ok = true;
             for (int64_t w = blockIdx.x; w < work && ok; w += gridDim.x)
             {
+                int64_t local;
+                const SplitGemmArgs& a = src.at(w, local);
+                const int64_t nk = a.nk;
                 uint32_t dcol = 0;
                 for (int64_t c = 0; c < nk; c++, it++)
                 {
                     if (c % KCH == 0)
                     {
                         const int bacc = u & 1;
-                        if (!mbar_wait(bar(BAR_ACCE + bacc), ((u >> 1) & 1) ^ 1, abort_flag, a.err, 2)) { ok = false; break; }
+                        if (!mbar_wait(bar(BAR_ACCE + bacc), ((u >> 1) & 1) ^ 1, abort_flag, err, 2)) { ok = false; break; }
                         fence_after();
                         dcol = bacc * 2 * ST;
                     }
                     const int s = it % STAGES;
-                    if (!mbar_wait(bar(BAR_FULL + s), (it / STAGES) & 1, abort_flag, a.err, 3)) { ok = false; break; }
+                    if (!mbar_wait(bar(BAR_FULL + s), (it / STAGES) & 1, abort_flag, err, 3)) { ok = false; break; }
                     fence_after();
                     const uint32_t base = smem_u32(stages + s * K::STAGE_BYTES);
 #pragma unroll
@@ -500,8 +537,10 @@ split_gemm_kernel(const __grid_constant__ SplitGemmArgs a)
         bool ok = true;
         for (int64_t w = blockIdx.x; w < work && ok; w += gridDim.x)
         {
-            int64_t b, tm, tn;
-            decode(w, b, tm, tn);
+            int64_t local, b, tm, tn;
+            const SplitGemmArgs& a = src.at(w, local);
+            decode(a, local, b, tm, tn);
+            const int64_t nk = a.nk;
             asm volatile("bar.sync 1, 128;\n" ::: "memory");
             for (int qq = 0; qq < 4; qq++)
             {
@@ -525,7 +564,7 @@ split_gemm_kernel(const __grid_constant__ SplitGemmArgs a)
             for (int64_t ch = 0; ch < nch; ch++, u++)
             {
                 const int bacc = u & 1;
-                if (!mbar_wait(bar(BAR_ACCF + bacc), (u >> 1) & 1, abort_flag, a.err, 4)) { ok = false; break; }
+                if (!mbar_wait(bar(BAR_ACCF + bacc), (u >> 1) & 1, abort_flag, err, 4)) { ok = false; break; }
                 fence_after();
 #pragma unroll
                 for (int j = 0; j < ST / 32; j++)
@@ -582,6 +621,22 @@ split_gemm_kernel(const __grid_constant__ SplitGemmArgs a)
 }
 
 template <int P>
+__global__ void __launch_bounds__(192, 1)
+split_gemm_kernel(const __grid_constant__ SplitGemmArgs a)
+{
+    extern __shared__ unsigned char smem_raw[];
+    split_gemm_body<P>(OneSplit{&a}, a.err, smem_raw);
+}
+
+template <int P>
+__global__ void __launch_bounds__(192, 1)
+split_gemm_grouped_kernel(const __grid_constant__ SplitGroupArgs g)
+{
+    extern __shared__ unsigned char smem_raw[];
+    split_gemm_body<P>(SplitGroup{g}, g.err, smem_raw);
+}
+
+template <int P>
 cudaError_t launch_split_gemm_p(const SplitGemmArgs& a, cudaStream_t stream, int num_sms)
 {
     auto kern = split_gemm_kernel<P>;
@@ -592,6 +647,20 @@ cudaError_t launch_split_gemm_p(const SplitGemmArgs& a, cudaStream_t stream, int
     if (work < grid) grid = work;
     timing_begin(KK_SPLIT_GEMM, stream);
     kern<<<(unsigned)grid, 192, SG<P>::smem, stream>>>(a);
+    timing_end(KK_SPLIT_GEMM, stream);
+    return cudaGetLastError();
+}
+
+template <int P>
+cudaError_t launch_split_grouped_p(const SplitGroupArgs& g, cudaStream_t stream, int num_sms)
+{
+    auto kern = split_gemm_grouped_kernel<P>;
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SG<P>::smem);
+    if (err != cudaSuccess) return err;
+    int64_t grid = num_sms;
+    if (g.total < grid) grid = g.total;
+    timing_begin(KK_SPLIT_GEMM, stream);
+    kern<<<(unsigned)grid, 192, SG<P>::smem, stream>>>(g);
     timing_end(KK_SPLIT_GEMM, stream);
     return cudaGetLastError();
 }
@@ -645,6 +714,16 @@ cudaError_t launch_split_gemm(const SplitGemmArgs& a, cudaStream_t stream, int n
     cudaError_t err = a.planes == 3 ? launch_split_gemm_p<3>(a, stream, num_sms)
                     : a.planes == 2 ? launch_split_gemm_p<2>(a, stream, num_sms)
                                     : cudaErrorInvalidValue;
+    if (err == cudaSuccess) g_launches++;
+    return err;
+}
+
+cudaError_t launch_split_gemm_grouped(const SplitGroupArgs& g, int planes, cudaStream_t stream, int num_sms)
+{
+    if (g.nprob <= 0 || g.total <= 0) return cudaSuccess;
+    cudaError_t err = planes == 3 ? launch_split_grouped_p<3>(g, stream, num_sms)
+                    : planes == 2 ? launch_split_grouped_p<2>(g, stream, num_sms)
+                                  : cudaErrorInvalidValue;
     if (err == cudaSuccess) g_launches++;
     return err;
 }

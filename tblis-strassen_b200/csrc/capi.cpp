@@ -640,9 +640,10 @@ size_t fp32_group_workspace_bytes(int level, const GemmView& g, int terms)
 
 int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], const float* A,
                      const float* B, float* C, cudaStream_t st, int sms, void* ws, size_t ws_bytes,
-                     int terms, int* err)
+                     int terms, int* err, SplitGemmArgs* defer, bool enqueue)
 {
     // tb: rsA, rsC, csB, csC, ksA, ksB, bA, bB, bC
+    if (defer && level != 0) return TBLIS_STRA_ERR_ARG;
     const ProductTable& tab = product_table(level);
     const int H = tab.H;
     const int64_t ms = cdiv(g.m, H), ns = cdiv(g.n, H), ks = cdiv(g.k, H);
@@ -662,10 +663,13 @@ int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], c
     void* planesA = static_cast<char*>(ws) + sc;
     void* planesB = static_cast<char*>(planesA) + (size_t)P * g.batch * tm * nk * blk;
 
-    SplitScaleArgs sa{A, tb[0], tb[4], tb[6], g.m, g.k, ms, H, g.batch, scaleA, invA};
-    TSB_CUDA(launch_split_scale(sa, st));
-    SplitScaleArgs sb{B, tb[2], tb[5], tb[7], g.n, g.k, ns, H, g.batch, scaleB, invB};
-    TSB_CUDA(launch_split_scale(sb, st));
+    if (enqueue)
+    {
+        SplitScaleArgs sa{A, tb[0], tb[4], tb[6], g.m, g.k, ms, H, g.batch, scaleA, invA};
+        TSB_CUDA(launch_split_scale(sa, st));
+        SplitScaleArgs sb{B, tb[2], tb[5], tb[7], g.n, g.k, ns, H, g.batch, scaleB, invB};
+        TSB_CUDA(launch_split_scale(sb, st));
+    }
 
     const bool a_kfast = g.unit_ksA != 0 && (g.unit_rsA == 0 || g.unit_ksA < g.unit_rsA);
     const bool b_kfast = g.unit_ksB != 0 && (g.unit_csB == 0 || g.unit_ksB < g.unit_csB);
@@ -688,6 +692,7 @@ int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], c
         ga.nterms = P == 3 ? 6 : 3;
         for (int i = 0; i < 6; i++) { ga.ta[i] = TA6[i]; ga.tb[i] = TB6[i]; }
         ga.err = err;
+        if (defer) { *defer = ga; return TBLIS_STRA_SUCCESS; }
         TSB_CUDA(launch_split_gemm(ga, st, sms));
         return TBLIS_STRA_SUCCESS;
     };
@@ -760,7 +765,7 @@ int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], c
         for (int i = 0; i < pr.na; i++) { pa.t_r[i] = pr.a[i].r; pa.t_c[i] = pr.a[i].c; pa.t_s[i] = pr.a[i].sign; }
         pa.scale = scaleA; pa.tiles = tm; pa.nk = nk; pa.batch = g.batch; pa.planes = P;
         pa.kfast = a_kfast; pa.out = planesA;
-        TSB_CUDA(launch_split_pack(pa, st));
+        if (enqueue) TSB_CUDA(launch_split_pack(pa, st));
         SplitPackArgs pb{};
         pb.X = B; pb.rs = tb[2]; pb.ks = tb[5]; pb.bX = tb[7];
         pb.rows_full = g.n; pb.k_full = g.k; pb.rows_blk = ns; pb.k_blk = ks;
@@ -768,7 +773,7 @@ int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], c
         for (int i = 0; i < pr.nb; i++) { pb.t_r[i] = pr.b[i].c; pb.t_c[i] = pr.b[i].r; pb.t_s[i] = pr.b[i].sign; }
         pb.scale = scaleB; pb.tiles = tn; pb.nk = nk; pb.batch = g.batch; pb.planes = P;
         pb.kfast = b_kfast; pb.out = planesB;
-        TSB_CUDA(launch_split_pack(pb, st));
+        if (enqueue) TSB_CUDA(launch_split_pack(pb, st));
         const int s = gemm(pr, planesA, planesB);
         if (s) return s;
     }

@@ -251,10 +251,22 @@ struct SplitGemmArgs
     int* err;                                  // set on a timed-out wait (may be null)
 };
 
+// Grouped split GEMM: many problems' tiles in one persistent launch (all
+// with the same number of planes).
+struct SplitGroupArgs
+{
+    const SplitGemmArgs* probs;    // device array [nprob]
+    const int64_t* prefix;         // device array [nprob + 1]: work prefix sums
+    int nprob;
+    int64_t total;
+    int* err;                      // set on a timed-out wait (may be null)
+};
+
 cudaError_t launch_split_scale(const SplitScaleArgs& args, cudaStream_t stream);
 cudaError_t launch_split_pack(const SplitPackArgs& args, cudaStream_t stream);
 cudaError_t launch_split_pack_multi(const SplitPackMultiArgs& args, cudaStream_t stream);
 cudaError_t launch_split_gemm(const SplitGemmArgs& args, cudaStream_t stream, int num_sms);
+cudaError_t launch_split_gemm_grouped(const SplitGroupArgs& args, int planes, cudaStream_t stream, int num_sms);
 
 cudaError_t launch_pack(const PackArgs& args, cudaStream_t stream);
 cudaError_t launch_pack_multi(const PackMultiArgs& args, cudaStream_t stream);

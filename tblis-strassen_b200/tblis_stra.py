@@ -263,15 +263,17 @@ def get_workspace_limit() -> int:
     return int(lib.tblis_stra_get_workspace_limit())
 
 
-SCHEDULES = {"fused": 0, "fused_small": 1, "packed_grouped": 2, "packed": 3, "split": 4, "scale": 5}
+SCHEDULES = {"fused": 0, "fused_small": 1, "packed_grouped": 2, "packed": 3, "split": 4, "scale": 5,
+             "split_grouped": 6}
 SCHEDULE_NAMES = {v: k for k, v in SCHEDULES.items()}
 
 
 def set_batch_schedules(names) -> None:
-    """FP64 schedules the batch autotuner may pick on this thread (None = all):
-    any of "fused", "fused_small", "packed_grouped", "packed"."""
+    """Schedules the batch autotuner may pick on this thread (None = all):
+    any of "fused", "fused_small", "packed_grouped", "packed" (FP64) and
+    "split", "split_grouped" (FP32)."""
     if names is None:
-        names = ["fused", "fused_small", "packed_grouped", "packed"]
+        names = ["fused", "fused_small", "packed_grouped", "packed", "split", "split_grouped"]
     mask = 0
     for n in names:
         mask |= 1 << SCHEDULES[n]

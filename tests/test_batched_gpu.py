@@ -160,6 +160,35 @@ def test_batched_fp64_large_levels(tsb, cuda):
         assert float((C - R).abs().max()) <= oracle.error_bound(lv, k, 1.0, 1.0) * 2 + 1e-13
 
 
+@pytest.mark.parametrize("schedule", ["split", "split_grouped"])
+def test_batched_fp32_each_schedule(tsb, cuda, schedule):
+    """FP32 problems through one schedule, against single L=0 FP64 calls of the
+    same values; split_grouped with a 1 MiB chunk limit, so chunks alternate
+    between the two workspaces."""
+    import os
+    import torch
+    probs = make_batch(cuda, 10, 31, torch.float32, 4, 16, 64, 512, 0)
+    refs = []
+    for alpha, A, ia, B, ib, beta, C, ic, _ in probs:
+        R = C.double()
+        tsb.contract(0, alpha, A.double(), ia, B.double(), ib, beta, R, ic)
+        refs.append(R)
+    os.environ["TBLIS_STRA_BATCH_CHUNK_BYTES"] = str(1 << 20)
+    try:
+        tsb.set_batch_schedules([schedule])
+        batch = tsb.Batch(probs)
+    finally:
+        tsb.set_batch_schedules(None)
+        del os.environ["TBLIS_STRA_BATCH_CHUNK_BYTES"]
+    assert set(batch.schedule()) == {schedule}
+    batch.execute()
+    torch.cuda.synchronize()
+    for (alpha, A, ia, B, ib, beta, C, ic, _), R in zip(probs, refs):
+        err = float(torch.linalg.norm((C.double() - R).flatten()) / torch.linalg.norm(R.flatten()))
+        assert err <= 1e-6, (schedule, err)
+    batch.close()
+
+
 def test_batch_rejects_host_tensors(tsb):
     A = np.ones((4, 4)); B = np.ones((4, 4)); C = np.zeros((4, 4))
     with pytest.raises(tsb.TblisStraError):

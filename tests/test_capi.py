@@ -95,8 +95,10 @@ def test_batch_schedule_mask(tsb):
         with pytest.raises(tsb.TblisStraError):
             tsb.set_batch_schedules([])            # empty mask
         with pytest.raises(tsb.TblisStraError):
-            tsb.set_batch_schedules(["split"])     # FP32 schedule is not selectable
+            tsb.set_batch_schedules(["scale"])     # not a schedule the tuner chooses
         assert tsb.lib.tblis_stra_get_batch_schedules() == (1 << 2) | (1 << 0)
+        tsb.set_batch_schedules(["split_grouped"])
+        assert tsb.lib.tblis_stra_get_batch_schedules() == 1 << 6
     finally:
         tsb.set_batch_schedules(None)
-    assert tsb.lib.tblis_stra_get_batch_schedules() == 0b1111
+    assert tsb.lib.tblis_stra_get_batch_schedules() == 0b1011111
