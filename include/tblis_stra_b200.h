@@ -98,6 +98,40 @@ void stra_tblis_tensor_mult_2level(const tblis_comm* comm, const tblis_config* c
                                    const tblis_tensor* B, const label_type* idx_B,
                                          tblis_tensor* C, const label_type* idx_C);
 
+/* ---- matrix-level entry points ---------------------------------------------
+ *
+ * Replaces src/util/basic_types.h:264-272 (same field order, sizes and
+ * alignment): an m x n matrix with row stride rs and column stride cs, in
+ * elements.  C = alpha*A*B + beta*C with alpha = A.scalar*B.scalar and
+ * beta = C.scalar; afterwards C.scalar = 1 (as for tensors). */
+typedef struct tblis_matrix
+{
+    type_t type;
+    int conj;
+    char scalar[16] __attribute__((__aligned__(8)));
+    void* data;
+    len_type m, n;
+    stride_type rs, cs;
+} tblis_matrix;
+
+/* L=0: src/iface/3m/mult.h:17-19. */
+void tblis_matrix_mult(const tblis_comm* comm, const tblis_config* cfg,
+                       const tblis_matrix* A, const tblis_matrix* B, tblis_matrix* C);
+/* L=1, variants ABC / Naive / AB: src/stra_iface/3m/stra_mult.h:17-27. */
+void stra_tblis_matrix_mult(const tblis_comm* comm, const tblis_config* cfg,
+                            const tblis_matrix* A, const tblis_matrix* B, tblis_matrix* C);
+void stra_tblis_matrix_mult_naive(const tblis_comm* comm, const tblis_config* cfg,
+                                  const tblis_matrix* A, const tblis_matrix* B, tblis_matrix* C);
+void stra_tblis_matrix_mult_ab(const tblis_comm* comm, const tblis_config* cfg,
+                               const tblis_matrix* A, const tblis_matrix* B, tblis_matrix* C);
+/* L=2, variants ABC / Naive / AB: src/stra_iface/3m/stra_mult_2level.h:17-27. */
+void stra_tblis_matrix_mult_2level(const tblis_comm* comm, const tblis_config* cfg,
+                                   const tblis_matrix* A, const tblis_matrix* B, tblis_matrix* C);
+void stra_tblis_matrix_mult_2level_naive(const tblis_comm* comm, const tblis_config* cfg,
+                                         const tblis_matrix* A, const tblis_matrix* B, tblis_matrix* C);
+void stra_tblis_matrix_mult_2level_ab(const tblis_comm* comm, const tblis_config* cfg,
+                                      const tblis_matrix* A, const tblis_matrix* B, tblis_matrix* C);
+
 /* Thread-count knobs of the reference (src/util/thread.h:13-15).  The GPU
  * grid replaces CPU threads: the value is stored and reported, never used. */
 unsigned tblis_get_num_threads(void);

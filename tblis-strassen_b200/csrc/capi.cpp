@@ -888,10 +888,82 @@ int mult(int level, const tblis_tensor* A, const label_type* idx_A,
     return TBLIS_STRA_SUCCESS;
 }
 
+// Matrix-level calls: the 2-D special case of the contraction,
+// C(i,j) = alpha A(i,k) B(k,j) + beta C(i,j), with the variant given by the
+// entry point (src/stra_iface/3m/stra_mult.cxx:14-56 checks the same shapes
+// and calls internal::stra_mult / stra_mult_naive / stra_mult_ab).
+int matrix_mult(int level, int impl, const tblis_matrix* A, const tblis_matrix* B, tblis_matrix* C)
+{
+    if (!A || !B || !C) return TBLIS_STRA_ERR_NULL;
+    if (A->type != B->type || A->type != C->type) return TBLIS_STRA_ERR_TYPE;
+    if (A->conj || B->conj || C->conj) return TBLIS_STRA_ERR_CONJ;
+    if (A->m != C->m || B->n != C->n || A->n != B->m) return TBLIS_STRA_ERR_EXTENT;
+    len_type la[2] = {A->m, A->n}, lb[2] = {B->m, B->n}, lc[2] = {C->m, C->n};
+    stride_type sa[2] = {A->rs, A->cs}, sb[2] = {B->rs, B->cs}, sc[2] = {C->rs, C->cs};
+    tblis_tensor tA{A->type, 0, {0}, A->data, 2, la, sa};
+    tblis_tensor tB{B->type, 0, {0}, B->data, 2, lb, sb};
+    tblis_tensor tC{C->type, 0, {0}, C->data, 2, lc, sc};
+    std::memcpy(tA.scalar, A->scalar, sizeof tA.scalar);
+    std::memcpy(tB.scalar, B->scalar, sizeof tB.scalar);
+    std::memcpy(tC.scalar, C->scalar, sizeof tC.scalar);
+    const int saved = t_impl;
+    t_impl = impl;
+    const int s = mult(level, &tA, "ik", &tB, "kj", &tC, "ij", t_stream, true);
+    t_impl = saved;
+    if (s == TBLIS_STRA_SUCCESS)
+    {
+        std::memcpy(C->scalar, tC.scalar, sizeof C->scalar);
+        C->conj = 0;
+    }
+    return s;
+}
+
 }  // namespace
 }  // namespace tsb
 
 extern "C" {
+
+void tblis_matrix_mult(const tblis_comm*, const tblis_config*, const tblis_matrix* A, const tblis_matrix* B,
+                       tblis_matrix* C)
+{
+    tsb::t_status = tsb::matrix_mult(0, 1, A, B, C);
+}
+
+void stra_tblis_matrix_mult(const tblis_comm*, const tblis_config*, const tblis_matrix* A, const tblis_matrix* B,
+                            tblis_matrix* C)
+{
+    tsb::t_status = tsb::matrix_mult(1, 1, A, B, C);
+}
+
+void stra_tblis_matrix_mult_naive(const tblis_comm*, const tblis_config*, const tblis_matrix* A,
+                                  const tblis_matrix* B, tblis_matrix* C)
+{
+    tsb::t_status = tsb::matrix_mult(1, 3, A, B, C);
+}
+
+void stra_tblis_matrix_mult_ab(const tblis_comm*, const tblis_config*, const tblis_matrix* A,
+                               const tblis_matrix* B, tblis_matrix* C)
+{
+    tsb::t_status = tsb::matrix_mult(1, 2, A, B, C);
+}
+
+void stra_tblis_matrix_mult_2level(const tblis_comm*, const tblis_config*, const tblis_matrix* A,
+                                   const tblis_matrix* B, tblis_matrix* C)
+{
+    tsb::t_status = tsb::matrix_mult(2, 1, A, B, C);
+}
+
+void stra_tblis_matrix_mult_2level_naive(const tblis_comm*, const tblis_config*, const tblis_matrix* A,
+                                         const tblis_matrix* B, tblis_matrix* C)
+{
+    tsb::t_status = tsb::matrix_mult(2, 3, A, B, C);
+}
+
+void stra_tblis_matrix_mult_2level_ab(const tblis_comm*, const tblis_config*, const tblis_matrix* A,
+                                      const tblis_matrix* B, tblis_matrix* C)
+{
+    tsb::t_status = tsb::matrix_mult(2, 2, A, B, C);
+}
 
 static void drop_in(int level, const tblis_tensor* A, const label_type* idx_A,
                     const tblis_tensor* B, const label_type* idx_B,

@@ -49,6 +49,28 @@ class tblis_tensor(ctypes.Structure):
     ]
 
 
+class tblis_matrix(ctypes.Structure):
+    """Layout of ``tblis_matrix`` (include/tblis_stra_b200.h)."""
+
+    _fields_ = [
+        ("type", ctypes.c_int),
+        ("conj", ctypes.c_int),
+        ("scalar", ctypes.c_double * 2),   # char[16], 8-byte aligned
+        ("data", ctypes.c_void_p),
+        ("m", ctypes.c_ssize_t), ("n", ctypes.c_ssize_t),
+        ("rs", ctypes.c_ssize_t), ("cs", ctypes.c_ssize_t),
+    ]
+
+
+MATRIX_ENTRY = {
+    (0, IMPL_ABC): "tblis_matrix_mult",
+    (1, IMPL_ABC): "stra_tblis_matrix_mult", (1, IMPL_NAIVE): "stra_tblis_matrix_mult_naive",
+    (1, IMPL_AB): "stra_tblis_matrix_mult_ab",
+    (2, IMPL_ABC): "stra_tblis_matrix_mult_2level", (2, IMPL_NAIVE): "stra_tblis_matrix_mult_2level_naive",
+    (2, IMPL_AB): "stra_tblis_matrix_mult_2level_ab",
+}
+
+
 class tblis_stra_problem(ctypes.Structure):
     """Layout of ``tblis_stra_problem`` (include/tblis_stra_b200.h)."""
 
@@ -71,6 +93,11 @@ def _load() -> ctypes.CDLL:
     for name in ("tblis_tensor_mult", "stra_tblis_tensor_mult", "stra_tblis_tensor_mult_2level"):
         fn = getattr(lib, name)
         fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, T, S, T, S, T, S]
+        fn.restype = None
+    M = ctypes.POINTER(tblis_matrix)
+    for name in MATRIX_ENTRY.values():
+        fn = getattr(lib, name)
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, M, M, M]
         fn.restype = None
     lib.tblis_stra_mult.argtypes = [ctypes.c_int, T, S, T, S, T, S, ctypes.c_void_p]
     lib.tblis_stra_mult.restype = ctypes.c_int
@@ -395,3 +422,31 @@ def plan_query(A, idx_A, B, idx_B, C, idx_C, scatter: bool = True):
         for nm, a, L in zip(names, arrs, lens):
             out[nm] = a[:L]
     return out
+
+
+def matrix_mult(level: int, alpha, A, B, beta, C, impl: int = IMPL_ABC) -> None:
+    """C = alpha*A*B + beta*C through the matrix-level entry points
+    (``tblis_matrix_mult``, ``stra_tblis_matrix_mult[_naive|_ab]``,
+    ``stra_tblis_matrix_mult_2level[_naive|_ab]``); 2-D torch tensors or numpy
+    arrays of any strides.  Blocking, like the reference's calls."""
+    views = []
+    for X, s in ((A, alpha), (B, 1.0), (C, beta)):
+        shape, strides, ptr, code = _describe(X)
+        if len(shape) != 2:
+            raise ValueError("matrix_mult takes 2-D operands")
+        mtx = tblis_matrix()
+        mtx.type = code
+        mtx.conj = 0
+        if code == TYPE_DOUBLE:
+            mtx.scalar[0] = float(s)
+        else:
+            ctypes.memmove(ctypes.addressof(mtx.scalar), ctypes.byref(ctypes.c_float(s)), 4)
+        mtx.data = ptr
+        mtx.m, mtx.n = shape
+        mtx.rs, mtx.cs = strides
+        views.append(mtx)
+    name = MATRIX_ENTRY.get((level, impl if level else IMPL_ABC))
+    if name is None:
+        raise ValueError(f"no matrix entry point for level {level}, impl {impl}")
+    getattr(lib, name)(None, None, ctypes.byref(views[0]), ctypes.byref(views[1]), ctypes.byref(views[2]))
+    _check(lib.tblis_stra_last_status())

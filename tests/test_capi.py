@@ -102,3 +102,33 @@ def test_batch_schedule_mask(tsb):
     finally:
         tsb.set_batch_schedules(None)
     assert tsb.lib.tblis_stra_get_batch_schedules() == 0b1011111
+
+
+def test_matrix_struct_layout_matches_header(tsb, tmp_path):
+    prog = tmp_path / "mlayout.c"
+    prog.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "tblis_stra_b200.h"\n'
+        'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(tblis_matrix),'
+        'offsetof(tblis_matrix,conj),offsetof(tblis_matrix,scalar),offsetof(tblis_matrix,data),'
+        'offsetof(tblis_matrix,m),offsetof(tblis_matrix,n),offsetof(tblis_matrix,rs),'
+        'offsetof(tblis_matrix,cs));return 0;}\n')
+    exe = tmp_path / "mlayout"
+    subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), str(prog), "-o", str(exe)])
+    got = [int(x) for x in subprocess.check_output([str(exe)]).split()]
+    M = tsb.tblis_matrix
+    want = [ctypes.sizeof(M), M.conj.offset, M.scalar.offset, M.data.offset, M.m.offset, M.n.offset,
+            M.rs.offset, M.cs.offset]
+    assert got == want
+
+
+def test_matrix_shape_and_type_errors(tsb):
+    """Mismatched matrix shapes or element types are statuses (checked before
+    any device work, as src/stra_iface/3m/stra_mult.cxx:19-27 asserts them)."""
+    import numpy as np
+    A = np.zeros((4, 5)); B = np.zeros((6, 3)); C = np.zeros((4, 3))
+    with pytest.raises(tsb.TblisStraError) as e:
+        tsb.matrix_mult(1, 1.0, A, B, 0.0, C)
+    assert e.value.status == 3                       # TBLIS_STRA_ERR_EXTENT
+    with pytest.raises(tsb.TblisStraError) as e:
+        tsb.matrix_mult(0, 1.0, np.zeros((4, 5), np.float32), np.zeros((5, 3)), 0.0, C)
+    assert e.value.status == 2                       # TBLIS_STRA_ERR_TYPE
