@@ -274,30 +274,38 @@ void set_grid(DmmaArgs& a, int64_t ms, int64_t ns, int64_t ks)
 // Packed schedule of the ABC variant (see packed_kernels.cu) on pool scratch.
 // Blocking calls read back the kernels' wait-timeout flag.
 int run_fp64_packed(int level, const GemmView& g, const DevPlan& t, const double* A, const double* B,
-                    double* C, cudaStream_t st, int sms, bool blocking)
+                    double* C, cudaStream_t st, int sms, bool blocking, int* shared_err)
 {
     const size_t ws_group = fp64_packed_group_workspace_bytes(level, g);
     const size_t ws = ws_group <= t_ws_limit ? ws_group : fp64_packed_workspace_bytes(level, g);
     Scratch buf, errbuf;
     int s;
     if ((s = buf.alloc(ws, st))) return s;
-    if ((s = errbuf.alloc(sizeof(int), st))) return s;
-    TSB_CUDA(cudaMemsetAsync(errbuf.p, 0, sizeof(int), st));
-    const int64_t* tb[9] = {t.rsA, t.rsC, t.csB, t.csC, t.ksA, t.ksB, t.bA, t.bB, t.bC};
-    s = run_fp64_packed_enqueue(level, g, tb, A, B, C, st, sms, buf.p, ws, static_cast<int*>(errbuf.p));
-    if (s) return s;
-    if (blocking)
+    int* err = shared_err;
+    if (!err)
     {
-        int err = 0;
-        TSB_CUDA(cudaMemcpyAsync(&err, errbuf.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        if ((s = errbuf.alloc(sizeof(int), st))) return s;
+        TSB_CUDA(cudaMemsetAsync(errbuf.p, 0, sizeof(int), st));
+        err = static_cast<int*>(errbuf.p);
+    }
+    const int64_t* tb[9] = {t.rsA, t.rsC, t.csB, t.csC, t.ksA, t.ksB, t.bA, t.bB, t.bC};
+    s = run_fp64_packed_enqueue(level, g, tb, A, B, C, st, sms, buf.p, ws, err);
+    if (s) return s;
+    if (blocking && !shared_err)
+    {
+        int flag = 0;
+        TSB_CUDA(cudaMemcpyAsync(&flag, errbuf.p, sizeof(int), cudaMemcpyDeviceToHost, st));
         TSB_CUDA(cudaStreamSynchronize(st));
-        if (err) return TBLIS_STRA_ERR_TIMEOUT;
+        if (flag) return TBLIS_STRA_ERR_TIMEOUT;
     }
     return TBLIS_STRA_SUCCESS;
 }
 
+// shared_err (may be null): a device flag of the caller's that the kernels'
+// timed-out waits set; the caller then reads it, and `blocking` checks none.
 int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
-             const double* A, const double* B, double* C, cudaStream_t st, int device, bool blocking)
+             const double* A, const double* B, double* C, cudaStream_t st, int device, bool blocking,
+             int* shared_err = nullptr)
 {
     if (g.m == 0 || g.n == 0 || g.batch == 0) return TBLIS_STRA_SUCCESS;
     if (g.alpha == 0.0 || g.k == 0)
@@ -318,7 +326,7 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
         // fully fused kernel, which needs none.
         const PackGeom pg = pack_geom(level, g);
         if (pg.fits && fp64_packed_workspace_bytes(level, g) <= t_ws_limit)
-            return run_fp64_packed(level, g, t, A, B, C, st, sms, blocking);
+            return run_fp64_packed(level, g, t, A, B, C, st, sms, blocking, shared_err);
         DmmaArgs a = base_args(g, t, A, B, C);
         set_grid(a, ms, ns, ks);
         a.nprod = (int)tab.prod.size();
@@ -783,7 +791,7 @@ int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], c
 namespace {
 
 int run_fp32(int level, const GemmView& g, const DevPlan& t, const float* A, const float* B,
-             float* C, cudaStream_t st, int device, bool blocking)
+             float* C, cudaStream_t st, int device, bool blocking, int* shared_err = nullptr)
 {
     if (g.m == 0 || g.n == 0 || g.batch == 0) return TBLIS_STRA_SUCCESS;
     if (g.alpha == 0.0 || g.k == 0)
@@ -798,20 +806,250 @@ int run_fp32(int level, const GemmView& g, const DevPlan& t, const float* A, con
     const size_t wsb_group = fp32_group_workspace_bytes(level, g, terms);
     const size_t wsb = wsb_group <= t_ws_limit ? wsb_group : fp32_workspace_bytes(level, g, terms);
     if ((s = wsbuf.alloc(wsb, st))) return s;
-    if ((s = errbuf.alloc(sizeof(int), st))) return s;
-    TSB_CUDA(cudaMemsetAsync(errbuf.p, 0, sizeof(int), st));
-    const int64_t* tb[9] = {t.rsA, t.rsC, t.csB, t.csC, t.ksA, t.ksB, t.bA, t.bB, t.bC};
-    s = run_fp32_enqueue(level, g, tb, A, B, C, st, num_sms(device), wsbuf.p, wsb, terms,
-                         static_cast<int*>(errbuf.p));
-    if (s) return s;
-    if (blocking)
+    int* err = shared_err;
+    if (!err)
     {
-        int err = 0;
-        TSB_CUDA(cudaMemcpyAsync(&err, errbuf.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        if ((s = errbuf.alloc(sizeof(int), st))) return s;
+        TSB_CUDA(cudaMemsetAsync(errbuf.p, 0, sizeof(int), st));
+        err = static_cast<int*>(errbuf.p);
+    }
+    const int64_t* tb[9] = {t.rsA, t.rsC, t.csB, t.csC, t.ksA, t.ksB, t.bA, t.bB, t.bC};
+    s = run_fp32_enqueue(level, g, tb, A, B, C, st, num_sms(device), wsbuf.p, wsb, terms, err);
+    if (s) return s;
+    if (blocking && !shared_err)
+    {
+        int flag = 0;
+        TSB_CUDA(cudaMemcpyAsync(&flag, errbuf.p, sizeof(int), cudaMemcpyDeviceToHost, st));
         TSB_CUDA(cudaStreamSynchronize(st));
-        if (err) return TBLIS_STRA_ERR_TIMEOUT;
+        if (flag) return TBLIS_STRA_ERR_TIMEOUT;
     }
     return TBLIS_STRA_SUCCESS;
+}
+
+// ---- pipelined staging of host operands ----------------------------------------
+//
+// When A, B and C all live in host memory, the call splits the slowest label
+// of C that is also in exactly one of A and B into chunks: the other operand is
+// copied whole first, then chunk j of C and of the split operand is copied
+// in while chunk j-1 computes, and chunk j of C is copied back while chunk j+1
+// computes.  Each chunk is the same contraction on sub-views (the split label
+// restricted to the chunk's range), so every chunk is exact and C's chunks are
+// disjoint; beta applies once per element.
+
+struct CopyStreams { cudaStream_t in = nullptr, out = nullptr; };
+
+// Per-device non-blocking streams for the host <-> device copies.
+int copy_streams(int device, CopyStreams& cs)
+{
+    static std::mutex mu;
+    static std::map<int, CopyStreams> streams;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = streams.find(device);
+    if (it != streams.end()) { cs = it->second; return TBLIS_STRA_SUCCESS; }
+    CopyStreams c;
+    if (cudaStreamCreateWithFlags(&c.in, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c.out, cudaStreamNonBlocking) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return TBLIS_STRA_ERR_CUDA;
+    }
+    streams[device] = c;
+    cs = c;
+    return TBLIS_STRA_SUCCESS;
+}
+
+// Geometry of the slice [a, b) of the label at position `pos`: the labels
+// with smaller strides must tile [0, sigma) densely and those with larger
+// strides must be dense among themselves, so the slice is `height` rows of
+// (b - a) * sigma elements `pitch` apart, starting at element a * sigma.
+bool slice_geometry(const tblis_tensor* T, int pos, int64_t& sigma, int64_t& height, int64_t& pitch)
+{
+    const int64_t e = T->len[pos];
+    sigma = T->stride[pos];
+    if (sigma <= 0) return false;
+    std::vector<std::pair<int64_t, int64_t>> inner, outer;   // (stride, extent)
+    for (unsigned d = 0; d < T->ndim; d++)
+    {
+        if ((int)d == pos || T->len[d] == 1) continue;
+        if (T->stride[d] <= 0 || T->stride[d] == sigma) return false;
+        (T->stride[d] < sigma ? inner : outer).emplace_back(T->stride[d], T->len[d]);
+    }
+    std::sort(inner.begin(), inner.end());
+    int64_t run = 1;
+    for (auto& x : inner)
+    {
+        if (x.first != run) return false;
+        run *= x.second;
+    }
+    if (run != sigma) return false;
+    std::sort(outer.begin(), outer.end());
+    height = 1;
+    pitch = sigma * e;
+    if (!outer.empty())
+    {
+        pitch = outer[0].first;
+        if (pitch < sigma * e) return false;
+        int64_t r = pitch;
+        for (auto& x : outer)
+        {
+            if (x.first != r) return false;
+            r *= x.second;
+            height *= x.second;
+        }
+    }
+    return true;
+}
+
+constexpr size_t PIPELINE_MIN_BYTES = (size_t)64 << 20;
+constexpr int PIPELINE_CHUNKS = 4;
+constexpr int NOT_PIPELINED = -1;
+
+int run_plan(int level, int impl, const GemmView& g, const DevPlan& t, void* const dptr[3], cudaStream_t st,
+             int device, int* shared_err)
+{
+    if (g.type == TYPE_FLOAT)
+        return run_fp32(level, g, t, static_cast<const float*>(dptr[0]), static_cast<const float*>(dptr[1]),
+                        static_cast<float*>(dptr[2]), st, device, false, shared_err);
+    return run_fp64(level, impl, g, t, static_cast<const double*>(dptr[0]), static_cast<const double*>(dptr[1]),
+                    static_cast<double*>(dptr[2]), st, device, false, shared_err);
+}
+
+int mult_pipelined(int level, int impl, const tblis_tensor* const T[3], const label_type* const I[3],
+                   const GemmView& g, int device, cudaStream_t st)
+{
+    const size_t es = g.type == TYPE_FLOAT ? sizeof(float) : sizeof(double);
+    size_t bytes = 0;
+    for (int t = 0; t < 3; t++)
+    {
+        if (g.hi[t] < g.lo[t] || g.lo[t] != 0 || !T[t]->data || is_device_ptr(T[t]->data)) return NOT_PIPELINED;
+        for (unsigned d = 0; d < T[t]->ndim; d++)
+            for (unsigned e = d + 1; e < T[t]->ndim; e++)
+                if (I[t][d] == I[t][e]) return NOT_PIPELINED;            // diagonal labels
+        bytes += (size_t)(g.hi[t] + 1) * es;
+    }
+    if (bytes < PIPELINE_MIN_BYTES) return NOT_PIPELINED;
+
+    // The split label: in C and in exactly one of A, B; largest C stride first.
+    auto find = [](const tblis_tensor* X, const label_type* ix, label_type c) {
+        for (unsigned d = 0; d < X->ndim; d++)
+            if (ix[d] == c) return (int)d;
+        return -1;
+    };
+    std::vector<int> cand;
+    for (unsigned d = 0; d < T[2]->ndim; d++)
+    {
+        const int pa = find(T[0], I[0], I[2][d]), pb = find(T[1], I[1], I[2][d]);
+        if ((pa < 0) != (pb < 0) && T[2]->len[d] >= 2) cand.push_back((int)d);
+    }
+    std::sort(cand.begin(), cand.end(), [&](int x, int y) { return T[2]->stride[x] > T[2]->stride[y]; });
+    int pc = -1, op = -1, px = -1;
+    int64_t sc = 0, hc = 0, pitc = 0, sx = 0, hx = 0, pitx = 0;
+    for (int d : cand)
+    {
+        const int pa = find(T[0], I[0], I[2][d]);
+        const int o = pa >= 0 ? 0 : 1;
+        const int p = pa >= 0 ? pa : find(T[1], I[1], I[2][d]);
+        if (slice_geometry(T[2], d, sc, hc, pitc) && slice_geometry(T[o], p, sx, hx, pitx))
+        {
+            pc = d; op = o; px = p;
+            break;
+        }
+    }
+    if (pc < 0) return NOT_PIPELINED;
+    const int whole = 1 - op;                 // the operand copied in one piece
+    const int64_t extent = T[2]->len[pc];
+    const int chunks = (int)std::min<int64_t>(PIPELINE_CHUNKS, extent);
+
+    CopyStreams cs;
+    int s = copy_streams(device, cs);
+    if (s) return s;
+    Scratch stage[3], errbuf;
+    for (int t = 0; t < 3; t++)
+        if ((s = stage[t].alloc((size_t)(g.hi[t] + 1) * es, st))) return s;
+    if ((s = errbuf.alloc(sizeof(int), st))) return s;
+    TSB_CUDA(cudaMemsetAsync(errbuf.p, 0, sizeof(int), st));
+    int* err = static_cast<int*>(errbuf.p);
+
+    std::vector<cudaEvent_t> ev;
+    auto event = [&]() {
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess) ev.push_back(e);
+        else cudaGetLastError();
+        return e;
+    };
+    struct EvGuard
+    {
+        std::vector<cudaEvent_t>& v;
+        ~EvGuard() { for (cudaEvent_t e : v) cudaEventDestroy(e); }
+    } guard{ev};
+
+    auto copy2d = [&](int t, int64_t sigma, int64_t height, int64_t pitch, int64_t a, int64_t b,
+                      cudaMemcpyKind kind, cudaStream_t cst) -> int {
+        const size_t off = (size_t)(a * sigma) * es, width = (size_t)((b - a) * sigma) * es;
+        const size_t pb = std::max((size_t)pitch * es, width);
+        char* host = static_cast<char*>(T[t]->data) + off;
+        char* dev = static_cast<char*>(stage[t].p) + off;
+        if (kind == cudaMemcpyHostToDevice)
+            TSB_CUDA(cudaMemcpy2DAsync(dev, pb, host, pb, width, (size_t)height, kind, cst));
+        else
+            TSB_CUDA(cudaMemcpy2DAsync(host, pb, dev, pb, width, (size_t)height, kind, cst));
+        return TBLIS_STRA_SUCCESS;
+    };
+
+    cudaEvent_t e0 = event(), e_whole = event(), e_out = event();
+    if (!e0 || !e_whole || !e_out) return TBLIS_STRA_ERR_CUDA;
+    TSB_CUDA(cudaEventRecord(e0, st));                    // staging buffers allocated
+    TSB_CUDA(cudaStreamWaitEvent(cs.in, e0, 0));
+    TSB_CUDA(cudaStreamWaitEvent(cs.out, e0, 0));
+    TSB_CUDA(cudaMemcpyAsync(stage[whole].p, T[whole]->data, (size_t)(g.hi[whole] + 1) * es,
+                             cudaMemcpyHostToDevice, cs.in));
+    TSB_CUDA(cudaEventRecord(e_whole, cs.in));
+    std::vector<cudaEvent_t> e_in(chunks), e_done(chunks);
+    std::vector<int64_t> lo(chunks + 1);
+    for (int j = 0; j <= chunks; j++) lo[j] = extent * j / chunks;
+    for (int j = 0; j < chunks; j++)
+    {
+        e_in[j] = event();
+        e_done[j] = event();
+        if (!e_in[j] || !e_done[j]) return TBLIS_STRA_ERR_CUDA;
+        if ((s = copy2d(op, sx, hx, pitx, lo[j], lo[j + 1], cudaMemcpyHostToDevice, cs.in))) return s;
+        if ((s = copy2d(2, sc, hc, pitc, lo[j], lo[j + 1], cudaMemcpyHostToDevice, cs.in))) return s;
+        TSB_CUDA(cudaEventRecord(e_in[j], cs.in));
+    }
+    TSB_CUDA(cudaStreamWaitEvent(st, e_whole, 0));
+    for (int j = 0; j < chunks; j++)
+    {
+        // sub-views: the split label restricted to [lo[j], lo[j+1])
+        tblis_tensor sub[3];
+        std::vector<len_type> len[3];
+        void* dptr[3];
+        for (int t = 0; t < 3; t++)
+        {
+            sub[t] = *T[t];
+            len[t].assign(T[t]->len, T[t]->len + T[t]->ndim);
+            dptr[t] = stage[t].p;
+        }
+        len[op][px] = lo[j + 1] - lo[j];
+        len[2][pc] = lo[j + 1] - lo[j];
+        dptr[op] = static_cast<char*>(stage[op].p) + (size_t)(lo[j] * sx) * es;
+        dptr[2] = static_cast<char*>(stage[2].p) + (size_t)(lo[j] * sc) * es;
+        for (int t = 0; t < 3; t++) { sub[t].len = len[t].data(); sub[t].data = dptr[t]; }
+        const tblis_tensor* ST[3] = {&sub[0], &sub[1], &sub[2]};
+        GemmView gj;
+        std::shared_ptr<DevPlan> dpj;
+        if ((s = get_plan(ST, I, device, gj, dpj))) return s;
+        TSB_CUDA(cudaStreamWaitEvent(st, e_in[j], 0));
+        if ((s = run_plan(level, impl, gj, *dpj, dptr, st, device, err))) return s;
+        TSB_CUDA(cudaEventRecord(e_done[j], st));
+        TSB_CUDA(cudaStreamWaitEvent(cs.out, e_done[j], 0));
+        if ((s = copy2d(2, sc, hc, pitc, lo[j], lo[j + 1], cudaMemcpyDeviceToHost, cs.out))) return s;
+    }
+    TSB_CUDA(cudaEventRecord(e_out, cs.out));
+    TSB_CUDA(cudaStreamWaitEvent(st, e_out, 0));
+    int flag = 0;
+    TSB_CUDA(cudaMemcpyAsync(&flag, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TSB_CUDA(cudaStreamSynchronize(st));
+    return flag ? TBLIS_STRA_ERR_TIMEOUT : TBLIS_STRA_SUCCESS;
 }
 
 int mult(int level, const tblis_tensor* A, const label_type* idx_A,
@@ -837,6 +1075,20 @@ int mult(int level, const tblis_tensor* A, const label_type* idx_A,
     // Every element access is an aligned load or store of the element size.
     for (int t = 0; t < 3; t++)
         if (reinterpret_cast<uintptr_t>(T[t]->data) % es) return TBLIS_STRA_ERR_ARG;
+
+    // All operands on the host and large enough: pipelined staging.
+    if (g.m > 0 && g.n > 0 && g.batch > 0 && g.alpha != 0.0 && g.k > 0)
+    {
+        s = mult_pipelined(level, impl, T, I, g, device, st);
+        if (s != NOT_PIPELINED)
+        {
+            if (s) return s;
+            if (fp32) { float one = 1.0f; std::memcpy(C->scalar, &one, sizeof one); }
+            else { double one = 1.0; std::memcpy(C->scalar, &one, sizeof one); }
+            C->conj = 0;
+            return TBLIS_STRA_SUCCESS;
+        }
+    }
 
     // Stage host operands through device memory.
     void* dptr[3] = {A->data, B->data, C->data};

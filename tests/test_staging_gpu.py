@@ -1,0 +1,80 @@
+"""Host-resident operands: the drop-in calls stage them through device memory.
+When all three are on the host and large (>= 64 MiB together), the call
+splits C's slowest label that belongs to exactly one of A and B into 4 chunks
+and overlaps the copies of one chunk with the computation of another.  Each
+chunk is the same contraction on sub-views, so the result matches the
+all-device call within the Strassen bound (both are within it of the exact
+contraction)."""
+import numpy as np
+import pytest
+
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def bound(level, k, beta=1.0):
+    return 2 * oracle.error_bound(level, k, 1.0, 1.0) + 8 * 2.0 ** -53 * abs(beta)
+
+
+def run_pair(tsb, cuda, level, A, ia, B, ib, C0, ic, pinned):
+    import torch
+    hA, hB, hC = (torch.from_numpy(X) for X in (A, B, C0.copy(order="K")))
+    if pinned:
+        hA, hB, hC = hA.pin_memory(), hB.pin_memory(), hC.pin_memory()
+    before = tsb.launch_count()
+    tsb.contract(level, 1.0, hA, ia, hB, ib, 1.0, hC, ic, drop_in=True)
+    launches = tsb.launch_count() - before
+    dA, dB, dC = hA.to(cuda), hB.to(cuda), torch.from_numpy(C0.copy(order="K")).to(cuda)
+    tsb.contract(level, 1.0, dA, ia, dB, ib, 1.0, dC, ic)
+    torch.cuda.synchronize()
+    return hC.numpy(), dC.cpu().numpy(), launches
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+@pytest.mark.parametrize("level", [0, 1])
+def test_pipelined_split_of_b_and_c(tsb, cuda, level, pinned):
+    """Column-major config-1 pattern: C's slowest label d is in B and C."""
+    e = 42                                   # 3 x 24.9 MB
+    A = oracle.uniform((e,) * 4, 1)
+    B = oracle.uniform((e,) * 4, 2)
+    C0 = oracle.uniform((e,) * 4, 3)
+    got, want, launches = run_pair(tsb, cuda, level, A, "efac", B, "fbde", C0, "abcd", pinned)
+    assert np.abs(got - want).max() <= bound(level, e * e)
+    per_call = 3 if level == 0 else 9        # L=0: 2 packs + GEMM; L=1: 2 group packs + 7 GEMMs
+    assert launches == 4 * per_call          # four chunks
+
+
+def test_pipelined_split_of_a_and_c_row_major(tsb, cuda):
+    """Row-major operands: C's slowest label a is in A and C."""
+    e = 42
+    A = np.ascontiguousarray(oracle.uniform((e,) * 4, 4))
+    B = np.ascontiguousarray(oracle.uniform((e,) * 4, 5))
+    C0 = np.ascontiguousarray(oracle.uniform((e,) * 4, 6))
+    got, want, launches = run_pair(tsb, cuda, 1, A, "aefc", B, "fbde", C0, "abcd", True)
+    assert np.abs(got - want).max() <= bound(1, e * e)
+    assert launches == 4 * 9
+
+
+def test_pipelined_fp32(tsb, cuda):
+    import torch
+    e = 52                                   # 3 x 29 MB of FP32
+    A = oracle.uniform((e,) * 4, 7, dtype=np.float32)
+    B = oracle.uniform((e,) * 4, 8, dtype=np.float32)
+    C0 = oracle.uniform((e,) * 4, 9, dtype=np.float32)
+    got, want, launches = run_pair(tsb, cuda, 0, A, "efac", B, "fbde", C0, "abcd", True)
+    d = np.linalg.norm((got.astype(np.float64) - want).ravel()) / np.linalg.norm(want.ravel())
+    assert d <= 2e-6
+    assert launches == 4 * 5                 # 2 scales, 2 packs, GEMM per chunk
+
+
+def test_small_or_unsliceable_operands_stage_whole(tsb, cuda):
+    """Below 64 MiB (or when no label slices into plain rows) the operands are
+    staged whole: one contraction's launches."""
+    e = 20
+    A = oracle.uniform((e,) * 4, 10)
+    B = oracle.uniform((e,) * 4, 11)
+    C0 = oracle.uniform((e,) * 4, 12)
+    got, want, launches = run_pair(tsb, cuda, 1, A, "efac", B, "fbde", C0, "abcd", True)
+    assert np.abs(got - want).max() <= bound(1, e * e)
+    assert launches == 9
