@@ -188,7 +188,7 @@ def cpu_reference(ext_sample: int, min_seconds: float, level: int, impl: int):
     return flops / best / 1e12, threads, sample, "reference"
 
 
-def batched_form(torch, tsb, device, stream, count, barrier_sync, max_over_ranks):
+def batched_form(torch, tsb, device, stream, count, barrier_sync, max_over_ranks, dtypes=None):
     """The batched uneven workload: `count` contractions with 2-4 indices per
     bundle, extents uniform in 8..96, bundle products in [512, 8192], random
     index orders per operand (seed 0), U[-1,1]; one batch plan (grouped
@@ -207,6 +207,8 @@ def batched_form(torch, tsb, device, stream, count, barrier_sync, max_over_ranks
     out = {"problems": count, "tflop_per_batch": flops / 1e12,
            "workload": "2-4 indices per bundle, extents U{8..96}, bundle products in [512, 8192], random orders"}
     for dtype, name in ((torch.float64, "fp64"), (torch.float32, "fp32_split6")):
+        if dtypes is not None and dtype not in dtypes:
+            continue
         g = torch.Generator(device=device).manual_seed(1)
         tens = []
         for ext, ia, ib, ic in shapes:
@@ -281,6 +283,16 @@ def kernel_probe(args):
     if args.dtype == "f32":
         A, B, C = A.float(), B.float(), C.float()
         tsb.set_fp32_terms(args.terms)
+    if args.workspace is not None:
+        tsb.set_workspace_limit(args.workspace)      # 0: the fully fused kernel
+    if args.kernels == "batch":
+        # a 64-problem batched form (FP64, or FP32 with --dtype f32), executed twice
+        del A, B, C
+        torch.cuda.empty_cache()
+        out = batched_form(torch, tsb, dev, torch.cuda.current_stream(), 64, torch.cuda.synchronize,
+                           lambda x: x, [torch.float32 if args.dtype == "f32" else torch.float64])
+        print(json.dumps(out))
+        return
     if args.kernels == "dgemm":
         # cuBLAS DGEMM at the same m = n = k, for side-by-side profiles
         n = e * e
@@ -336,6 +348,8 @@ def main():
     ap.add_argument("--dtype", choices=["f64", "f32"], default="f64",
                     help="operand type of the --kernels probe (f32 = split-BF16 tcgen05 path)")
     ap.add_argument("--terms", type=int, default=6, help="split-BF16 product terms for f32 (3 or 6)")
+    ap.add_argument("--workspace", type=int, default=None,
+                    help="--kernels probe: device workspace limit in bytes (0 = fully fused kernel)")
     ap.add_argument("--kernels", default=None,
                     help="comma-separated levels: run one warm-up and one timed call per level "
                          "and print per-level times (profiling driver; no JSON line)")

@@ -387,6 +387,11 @@ template <int P, class Src>
 __device__ __forceinline__ void split_gemm_body(const Src& src, int* err, unsigned char* smem_raw)
 {
     using K = SG<P>;
+    // Plane pairs of the product terms (0 = hi, 1 = mid, 2 = lo): hh, hm, mh,
+    // then hl, mm, lh with three planes; compile-time so the single issuing
+    // thread builds every descriptor from constants.
+    constexpr int NTERMS = P == 3 ? 6 : 3;
+    constexpr int TERM_A[6] = {0, 0, 1, 0, 1, 2}, TERM_B[6] = {0, 1, 0, 2, 1, 0};
     constexpr int STAGES = K::STAGES;
     unsigned char* smem = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -500,11 +505,10 @@ __device__ __forceinline__ void split_gemm_body(const Src& src, int* err, unsign
                     fence_after();
                     const uint32_t base = smem_u32(stages + s * K::STAGE_BYTES);
 #pragma unroll
-                    for (int t = 0; t < 2 * P; t++)
+                    for (int t = 0; t < NTERMS; t++)
                     {
-                        if (t >= a.nterms) break;
-                        const uint64_t ad = sdesc(base + a.ta[t] * BLK);
-                        const uint64_t bd = sdesc(base + (P + a.tb[t]) * BLK);
+                        const uint64_t ad = sdesc(base + TERM_A[t] * BLK);
+                        const uint64_t bd = sdesc(base + (P + TERM_B[t]) * BLK);
                         // hi*hi accumulates in its own TMEM columns; the
                         // smaller correction terms share the next 128.
                         const uint32_t d = tmem + dcol + (t == 0 ? 0 : ST);
@@ -707,10 +711,21 @@ cudaError_t launch_split_pack_multi(const SplitPackMultiArgs& a, cudaStream_t st
     return err;
 }
 
+// The kernels run the terms hh, hm, mh (+ hl, mm, lh with three planes) in
+// this order; a descriptor asking for anything else is rejected.
+bool standard_terms(const SplitGemmArgs& a)
+{
+    static const int8_t TA[6] = {0, 0, 1, 0, 1, 2}, TB[6] = {0, 1, 0, 2, 1, 0};
+    if (a.nterms != (a.planes == 3 ? 6 : 3)) return false;
+    for (int t = 0; t < a.nterms; t++)
+        if (a.ta[t] != TA[t] || a.tb[t] != TB[t]) return false;
+    return true;
+}
+
 cudaError_t launch_split_gemm(const SplitGemmArgs& a, cudaStream_t stream, int num_sms)
 {
     if (a.batch <= 0 || a.tiles_m <= 0 || a.tiles_n <= 0 || a.nk <= 0) return cudaSuccess;
-    if (a.nc < 1 || a.nc > 4 || a.nterms < 1 || a.nterms > 2 * a.planes) return cudaErrorInvalidValue;
+    if (a.nc < 1 || a.nc > 4 || !standard_terms(a)) return cudaErrorInvalidValue;
     cudaError_t err = a.planes == 3 ? launch_split_gemm_p<3>(a, stream, num_sms)
                     : a.planes == 2 ? launch_split_gemm_p<2>(a, stream, num_sms)
                                     : cudaErrorInvalidValue;
