@@ -426,7 +426,8 @@ PackGeom pack_geom(int level, const GemmView& g)
     p.tm = cdiv(p.ms, PACK_TILE); p.tn = cdiv(p.ns, PACK_TILE);
     p.s_elems = (size_t)(g.batch * p.tm * p.k_pad * PACK_TILE);
     p.t_elems = (size_t)(g.batch * p.tn * p.k_pad * PACK_TILE);
-    p.fits = p.tm <= 65535 && p.tn <= 65535 && g.batch <= 65535 && g.batch * p.tm <= 65535 &&
+    // pack grids: (k_pad / 32, 2 * tiles, batch)
+    p.fits = 2 * p.tm <= 65535 && 2 * p.tn <= 65535 && g.batch <= 65535 && g.batch * p.tm <= 65535 &&
              g.batch * p.tn <= 65535;
     return p;
 }

@@ -34,24 +34,58 @@ namespace {
 
 constexpr int PK_K = 32;          // k values per pack CTA
 constexpr int PK_THREADS = 256;
+constexpr int PK_ROWS = PACK_TILE / 2;   // rows per pack CTA: half a tile
+
+// Pack CTAs cover 64 rows x 32 k (half of a 128-row tile: blockIdx.y = 2 *
+// tile + half), so their shared memory and registers stay small and several
+// CTAs per SM overlap one CTA's gathers with another's writes.  Element e of a
+// thread: with kfast the 32 lanes of a warp walk 32 consecutive k of one row,
+// else 32 consecutive rows of one k.
+constexpr int PK_E = PK_ROWS * PK_K / PK_THREADS;
+__device__ __forceinline__ int pk_row(bool kfast, int warp, int lane, int e)
+{
+    return kfast ? warp + 8 * e : lane + 32 * (e & 1);
+}
+__device__ __forceinline__ int pk_k(bool kfast, int warp, int lane, int e)
+{
+    return kfast ? lane : warp + 8 * (e >> 1);
+}
+
+// Write buf (rows [64 half, 64 half + 64) of the tile, PK_K k) in the tile's
+// swizzled order: per k a row of 128 consecutive doubles, so warp stores are
+// contiguous.
+__device__ __forceinline__ void pk_write(const double (*buf)[PK_K + 1], double* out, int64_t k0, int64_t k_pad,
+                                         int half, int warp, int lane)
+{
+#pragma unroll
+    for (int e = 0; e < PK_E; e++)
+    {
+        const int r = lane + 32 * (e & 1);
+        const int kk = warp + 8 * (e >> 1);
+        if (k0 + kk < k_pad)
+            out[(int64_t)kk * PACK_TILE + tile_pos((int)((k0 + kk) & 7), half * PK_ROWS + r, 0)] = buf[r][kk];
+    }
+}
 
 __global__ void __launch_bounds__(PK_THREADS)
 pack_kernel(const __grid_constant__ PackArgs a)
 {
-    __shared__ double buf[PACK_TILE][PK_K + 1];
-    __shared__ int64_t rowoff[4][PACK_TILE];     // per term: batch + row offset (or invalid)
+    __shared__ double buf[PK_ROWS][PK_K + 1];
+    __shared__ int64_t rowoff[4][PK_ROWS];       // per term: batch + row offset (or invalid)
     __shared__ int64_t koff[4][PK_K];            // per term: k offset (or invalid)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int64_t k0 = (int64_t)blockIdx.x * PK_K;
-    const int64_t t = blockIdx.y;
+    const int64_t t = blockIdx.y >> 1;
+    const int half = blockIdx.y & 1;
     const int64_t b = blockIdx.z;
-    const int64_t r0 = t * PACK_TILE;
+    const int64_t r0 = t * PACK_TILE + half * PK_ROWS;
     const int nt = a.nt;
+    const bool kfast = a.kfast != 0;
 
     // Offset tables of this CTA's rows and k values, once per term.
-    for (int i = tid; i < nt * PACK_TILE; i += PK_THREADS)
+    for (int i = tid; i < nt * PK_ROWS; i += PK_THREADS)
     {
-        const int q = i / PACK_TILE, r = i % PACK_TILE;
+        const int q = i / PK_ROWS, r = i % PK_ROWS;
         const int64_t lr = r0 + r, gr = a.t_r[q] * a.rows_blk + lr;
         rowoff[q][r] = (lr < a.rows_blk && gr < a.rows_full) ? a.bX[b] + a.rs[gr] : OFF_INVALID;
     }
@@ -63,78 +97,59 @@ pack_kernel(const __grid_constant__ PackArgs a)
     }
     __syncthreads();
 
-    // Gather and sum: with kfast the 32 lanes of a warp walk 32 consecutive k
-    // of one row, else 32 consecutive rows of one k.  Terms outermost, so all
-    // loads of one term are independent and in flight together.
-    constexpr int E = PACK_TILE * PK_K / PK_THREADS;
-    double v[E];
+    // Gather and sum, terms outermost, so all loads of one term are
+    // independent and in flight together.
+    double v[PK_E];
 #pragma unroll
-    for (int x = 0; x < E; x++) v[x] = 0.0;
+    for (int e = 0; e < PK_E; e++) v[e] = 0.0;
     for (int q = 0; q < nt; q++)
     {
         const bool neg = a.t_s[q] < 0;
 #pragma unroll
-        for (int x = 0; x < E; x++)
+        for (int e = 0; e < PK_E; e++)
         {
-            const int r = a.kfast ? warp + 8 * x : lane + 32 * (x & 3);
-            const int kk = a.kfast ? lane : warp + 8 * (x >> 2);
-            const int64_t ro = rowoff[q][r], ko = koff[q][kk];
+            const int64_t ro = rowoff[q][pk_row(kfast, warp, lane, e)], ko = koff[q][pk_k(kfast, warp, lane, e)];
             if (ro != OFF_INVALID && ko != OFF_INVALID)
             {
-                const double e = a.X[ro + ko];
-                v[x] += neg ? -e : e;
+                const double x = a.X[ro + ko];
+                v[e] += neg ? -x : x;
             }
         }
     }
 #pragma unroll
-    for (int x = 0; x < E; x++)
-    {
-        const int r = a.kfast ? warp + 8 * x : lane + 32 * (x & 3);
-        const int kk = a.kfast ? lane : warp + 8 * (x >> 2);
-        buf[r][kk] = v[x];
-    }
+    for (int e = 0; e < PK_E; e++) buf[pk_row(kfast, warp, lane, e)][pk_k(kfast, warp, lane, e)] = v[e];
     __syncthreads();
-    // Write tile rows (one k each) in the swizzled order: 128 consecutive
-    // doubles per k, so every warp store is contiguous.
-    double* out = a.out + ((b * a.tiles + t) * a.k_pad + k0) * PACK_TILE;
-#pragma unroll 4
-    for (int x = 0; x < PACK_TILE * PK_K / PK_THREADS; x++)
-    {
-        const int r = lane + 32 * (x & 3);
-        const int kk = warp + 8 * (x >> 2);
-        if (k0 + kk < a.k_pad)
-            out[(int64_t)kk * PACK_TILE + tile_pos((int)((k0 + kk) & 7), r, 0)] = buf[r][kk];
-    }
+    pk_write(buf, a.out + ((b * a.tiles + t) * a.k_pad + k0) * PACK_TILE, k0, a.k_pad, half, warp, lane);
 }
 
 // Seven sums of one product group per pass (L >= 1): each CTA reads its
-// 128-row x 32-k window of every block of the group's coarse sum once, forms
+// 64-row x 32-k window of every block of the group's coarse sum once, forms
 // the four sub-block sums X_j in registers, then writes each output's signed
 // combination through the shared-memory transpose of pack_kernel.  At L=2 this
 // reads each block of A (and B) once per group instead of once per product
 // that uses it: 48 instead of 144 block reads per operand.
-constexpr int PM_THREADS = 512;
-
-__global__ void __launch_bounds__(PM_THREADS)
+__global__ void __launch_bounds__(PK_THREADS)
 pack_multi_kernel(const __grid_constant__ PackMultiArgs a)
 {
-    __shared__ double buf[PACK_TILE][PK_K + 1];
-    __shared__ int64_t rowoff[8][PACK_TILE];     // per block (t, j): batch + row offset (or invalid)
+    __shared__ double buf[PK_ROWS][PK_K + 1];
+    __shared__ int64_t rowoff[8][PK_ROWS];       // per block (t, j): batch + row offset (or invalid)
     __shared__ int64_t koff[8][PK_K];            // per block (t, j): k offset (or invalid)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int64_t k0 = (int64_t)blockIdx.x * PK_K;
-    const int64_t t = blockIdx.y;
+    const int64_t t = blockIdx.y >> 1;
+    const int half = blockIdx.y & 1;
     const int64_t b = blockIdx.z;
-    const int64_t r0 = t * PACK_TILE;
+    const int64_t r0 = t * PACK_TILE + half * PK_ROWS;
     const int nblk = a.nt * 4;
+    const bool kfast = a.kfast != 0;
 
-    for (int i = tid; i < nblk * PACK_TILE; i += PM_THREADS)
+    for (int i = tid; i < nblk * PK_ROWS; i += PK_THREADS)
     {
-        const int q = i / PACK_TILE, r = i % PACK_TILE;
+        const int q = i / PK_ROWS, r = i % PK_ROWS;
         const int64_t lr = r0 + r, gr = a.prow[q >> 2][q & 3] * a.rows_blk + lr;
         rowoff[q][r] = (lr < a.rows_blk && gr < a.rows_full) ? a.bX[b] + a.rs[gr] : OFF_INVALID;
     }
-    for (int i = tid; i < nblk * PK_K; i += PM_THREADS)
+    for (int i = tid; i < nblk * PK_K; i += PK_THREADS)
     {
         const int q = i / PK_K, kk = i % PK_K;
         const int64_t lk = k0 + kk, gk = a.pk[q >> 2][q & 3] * a.k_blk + lk;
@@ -142,25 +157,21 @@ pack_multi_kernel(const __grid_constant__ PackMultiArgs a)
     }
     __syncthreads();
 
-    // Element e of this thread: with kfast the 32 lanes of a warp walk 32
-    // consecutive k of one row, else 32 consecutive rows of one k.
-    constexpr int E = PACK_TILE * PK_K / PM_THREADS;
-    double x[4][E];
+    double x[4][PK_E];
 #pragma unroll
     for (int j = 0; j < 4; j++)
 #pragma unroll
-        for (int e = 0; e < E; e++) x[j][e] = 0.0;
+        for (int e = 0; e < PK_E; e++) x[j][e] = 0.0;
     for (int c = 0; c < a.nt; c++)
     {
         const bool neg = a.t_s[c] < 0;
 #pragma unroll
         for (int j = 0; j < 4; j++)
 #pragma unroll
-            for (int e = 0; e < E; e++)
+            for (int e = 0; e < PK_E; e++)
             {
-                const int r = a.kfast ? warp + 16 * e : lane + 32 * (e & 3);
-                const int kk = a.kfast ? lane : warp + 16 * (e >> 2);
-                const int64_t ro = rowoff[c * 4 + j][r], ko = koff[c * 4 + j][kk];
+                const int64_t ro = rowoff[c * 4 + j][pk_row(kfast, warp, lane, e)];
+                const int64_t ko = koff[c * 4 + j][pk_k(kfast, warp, lane, e)];
                 if (ro != OFF_INVALID && ko != OFF_INVALID)
                 {
                     const double v = a.X[ro + ko];
@@ -177,26 +188,16 @@ pack_multi_kernel(const __grid_constant__ PackMultiArgs a)
                     (a.o_n[o] > 1 && a.o_j[o][1] == j ? a.o_s[o][1] : 0);
         __syncthreads();   // the previous output's tile has left buf
 #pragma unroll
-        for (int e = 0; e < E; e++)
+        for (int e = 0; e < PK_E; e++)
         {
             double v = 0.0;
 #pragma unroll
             for (int j = 0; j < 4; j++)
                 if (cf[j]) v += cf[j] > 0 ? x[j][e] : -x[j][e];
-            const int r = a.kfast ? warp + 16 * e : lane + 32 * (e & 3);
-            const int kk = a.kfast ? lane : warp + 16 * (e >> 2);
-            buf[r][kk] = v;
+            buf[pk_row(kfast, warp, lane, e)][pk_k(kfast, warp, lane, e)] = v;
         }
         __syncthreads();
-        double* out = a.out[o] + ((b * a.tiles + t) * a.k_pad + k0) * PACK_TILE;
-#pragma unroll
-        for (int e = 0; e < E; e++)
-        {
-            const int r = lane + 32 * (e & 3);
-            const int kk = warp + 16 * (e >> 2);
-            if (k0 + kk < a.k_pad)
-                out[(int64_t)kk * PACK_TILE + tile_pos((int)((k0 + kk) & 7), r, 0)] = buf[r][kk];
-        }
+        pk_write(buf, a.out[o] + ((b * a.tiles + t) * a.k_pad + k0) * PACK_TILE, k0, a.k_pad, half, warp, lane);
     }
 }
 
@@ -789,8 +790,8 @@ cudaError_t launch_pack(const PackArgs& a, cudaStream_t stream)
 {
     if (a.batch <= 0 || a.tiles <= 0 || a.k_pad <= 0) return cudaSuccess;
     if (a.k_pad % PK_K && a.k_pad % PACK_KSTEP) return cudaErrorInvalidValue;
-    dim3 grid((unsigned)((a.k_pad + PK_K - 1) / PK_K), (unsigned)a.tiles, (unsigned)a.batch);
-    if (a.tiles > 65535 || a.batch > 65535) return cudaErrorInvalidValue;
+    dim3 grid((unsigned)((a.k_pad + PK_K - 1) / PK_K), (unsigned)(2 * a.tiles), (unsigned)a.batch);
+    if (2 * a.tiles > 65535 || a.batch > 65535) return cudaErrorInvalidValue;
     timing_begin(KK_PACK, stream);
     pack_kernel<<<grid, PK_THREADS, 0, stream>>>(a);
     timing_end(KK_PACK, stream);
@@ -803,10 +804,10 @@ cudaError_t launch_pack_multi(const PackMultiArgs& a, cudaStream_t stream)
 {
     if (a.batch <= 0 || a.tiles <= 0 || a.k_pad <= 0 || a.nout <= 0) return cudaSuccess;
     if (a.k_pad % PK_K || a.nt < 1 || a.nt > 2 || a.nout > 7) return cudaErrorInvalidValue;
-    if (a.tiles > 65535 || a.batch > 65535) return cudaErrorInvalidValue;
-    dim3 grid((unsigned)(a.k_pad / PK_K), (unsigned)a.tiles, (unsigned)a.batch);
+    if (2 * a.tiles > 65535 || a.batch > 65535) return cudaErrorInvalidValue;
+    dim3 grid((unsigned)(a.k_pad / PK_K), (unsigned)(2 * a.tiles), (unsigned)a.batch);
     timing_begin(KK_PACK, stream);
-    pack_multi_kernel<<<grid, PM_THREADS, 0, stream>>>(a);
+    pack_multi_kernel<<<grid, PK_THREADS, 0, stream>>>(a);
     timing_end(KK_PACK, stream);
     cudaError_t err = cudaGetLastError();
     if (err == cudaSuccess) g_launches++;
