@@ -268,6 +268,56 @@ def time_steps(torch, fn, steps, stream):
     return start.elapsed_time(end) / 1e3
 
 
+# The FP64 square and rank-k sweep: (NIm, NJn, NPk) as extent pairs of the
+# bundles I = (a, c), J = (b, d), P = (e, f) of C(abcd) += A(efac) B(fbde).
+SWEEP = [((32, 64), (32, 64), (32, 64)), ((64, 64), (64, 64), (64, 64)),
+         ((64, 128), (64, 128), (64, 128)), ((128, 128), (128, 128), (128, 128)),
+         ((128, 128), (128, 128), (16, 16)), ((128, 128), (128, 128), (16, 32)),
+         ((128, 128), (128, 128), (32, 32)), ((128, 128), (128, 128), (32, 64))]
+
+
+def sweep(args):
+    """Effective TFLOP/s of every sweep shape at L = 0, 1, 2 and variants ABC,
+    AB and Naive (one warm-up, then the median of 3 CUDA-event timed calls),
+    and the largest error against L = 0 relative to the FP64 bound; one JSON
+    line per shape."""
+    import torch
+    tsb = load_package()
+    dev = torch.device("cuda:0")
+    gen = torch.Generator(device=dev).manual_seed(0)
+    for (a, c), (b, d), (e, f) in SWEEP:
+        ext = dict(a=a, b=b, c=c, d=d, e=e, f=f)
+        A = colmajor(torch, [ext[x] for x in IDX_A], dev, gen)
+        B = colmajor(torch, [ext[x] for x in IDX_B], dev, gen)
+        C0 = colmajor(torch, [ext[x] for x in IDX_C], dev, fill=0.0)
+        m, n, k = a * c, b * d, e * f
+        flops = 2.0 * m * n * k
+        R = C0.clone()
+        tsb.contract(0, 1.0, A, IDX_A, B, IDX_B, 0.0, R, IDX_C)
+        line = {"NIm": m, "NJn": n, "NPk": k, "tflops": {}, "err_over_bound": {}}
+        for impl, name in ((1, "ABC"), (2, "AB"), (3, "Naive")):
+            for lv in (0, 1, 2):
+                if lv == 0 and impl != 1:
+                    continue
+                C = C0.clone()
+                tsb.contract(lv, 1.0, A, IDX_A, B, IDX_B, 0.0, C, IDX_C, impl=impl)
+                ts = []
+                for _ in range(3):
+                    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    s0.record()
+                    tsb.contract(lv, 1.0, A, IDX_A, B, IDX_B, 0.0, C, IDX_C, impl=impl)
+                    s1.record()
+                    s1.synchronize()
+                    ts.append(s0.elapsed_time(s1))
+                key = f"L{lv}" if lv == 0 else f"L{lv}_{name}"
+                line["tflops"][key] = flops / statistics.median(ts) / 1e9
+                err = float((C - R).abs().max())
+                line["err_over_bound"][key] = err / (4.0 * 12.0 ** lv * k * 2.0 ** -53)
+        print(json.dumps(line), flush=True)
+        del A, B, C0, R, C
+        torch.cuda.empty_cache()
+
+
 def kernel_probe(args):
     """One warm-up and one timed contraction per requested level (the
     command the ncu captures under profiles/ run)."""
@@ -348,6 +398,8 @@ def main():
     ap.add_argument("--dtype", choices=["f64", "f32"], default="f64",
                     help="operand type of the --kernels probe (f32 = split-BF16 tcgen05 path)")
     ap.add_argument("--terms", type=int, default=6, help="split-BF16 product terms for f32 (3 or 6)")
+    ap.add_argument("--sweep", action="store_true",
+                    help="FP64 square and rank-k sweep over L = 0/1/2 and ABC/AB/Naive (one JSON line per shape)")
     ap.add_argument("--workspace", type=int, default=None,
                     help="--kernels probe: device workspace limit in bytes (0 = fully fused kernel)")
     ap.add_argument("--kernels", default=None,
@@ -355,6 +407,8 @@ def main():
                          "and print per-level times (profiling driver; no JSON line)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.sweep:
+        return sweep(args)
     if args.kernels is not None:
         return kernel_probe(args)
 
