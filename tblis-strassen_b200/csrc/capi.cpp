@@ -337,6 +337,11 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
     }
 
     // AB / Naive: one M buffer (ms x ns per batch entry), products in order.
+    // The product M = S T runs on the packed GEMM: AB packs the operand sums
+    // straight from A and B (as ABC does); Naive first forms them as dense
+    // temporaries S and T (sum_gather) and packs those.  The GEMM writes M
+    // (beta = 0), then scatter_add adds +-alpha*M into the product's C blocks.
+    // Sizes beyond the pack grids use the gather-based kernel for M.
     Scratch Mbuf;
     int s = Mbuf.alloc((size_t)(g.batch * ms * ns) * sizeof(double), st);
     if (s) return s;
@@ -353,22 +358,28 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
         if ((s = St.build(ms, ks, g.batch, st))) return s;
         if ((s = Tt.build(ks, ns, g.batch, st))) return s;
     }
+    const PackGeom pg = pack_geom(level, g);
+    Scratch Pbuf, errbuf;
+    double* PS = nullptr;
+    double* PT = nullptr;
+    int* err = shared_err;
+    if (pg.fits)
+    {
+        if ((s = Pbuf.alloc((pg.s_elems + pg.t_elems) * sizeof(double), st))) return s;
+        PS = static_cast<double*>(Pbuf.p);
+        PT = PS + pg.s_elems;
+        if (!err)
+        {
+            if ((s = errbuf.alloc(sizeof(int), st))) return s;
+            TSB_CUDA(cudaMemsetAsync(errbuf.p, 0, sizeof(int), st));
+            err = static_cast<int*>(errbuf.p);
+        }
+    }
+    const int64_t* tb[9] = {t.rsA, t.rsC, t.csB, t.csC, t.ksA, t.ksB, t.bA, t.bB, t.bC};
 
     for (const Product& pr : tab.prod)
     {
-        DmmaArgs a;
-        int terms = 1;
-        if (impl == 2)
-        {
-            a = base_args(g, t, A, B, M);
-            set_grid(a, ms, ns, ks);
-            a.H = H;
-            DevProduct d = to_dev(pr);
-            terms = std::max<int>(pr.na, pr.nb);
-            d.nc = 1; d.c_r[0] = 0; d.c_c[0] = 0; d.c_s[0] = 1; d.c_first[0] = 1;
-            a.prod[0] = d;
-        }
-        else
+        if (impl == 3)
         {
             SumGatherArgs sa{};
             sa.X = A; sa.rsX = t.rsA; sa.csX = t.ksA; sa.bX = t.bA;
@@ -382,24 +393,73 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
             sb.batch = g.batch; sb.nt = pr.nb; sb.out = static_cast<double*>(Tbuf.p);
             for (int i = 0; i < pr.nb; i++) { sb.t_r[i] = pr.b[i].r; sb.t_c[i] = pr.b[i].c; sb.t_s[i] = pr.b[i].sign; }
             TSB_CUDA(launch_sum_gather(sb, st));
-
-            std::memset(&a, 0, sizeof a);
-            a.A = static_cast<const double*>(Sbuf.p); a.B = static_cast<const double*>(Tbuf.p); a.C = M;
-            a.rsA = St.rows; a.ksA = St.cols; a.bA = St.bat;
-            a.ksB = Tt.rows; a.csB = Tt.cols; a.bB = Tt.bat;
-            a.m = ms; a.n = ns; a.k = ks; a.batch = g.batch;
-            a.a_kfast = 1; a.b_kfast = 0;
-            set_grid(a, ms, ns, ks);
-            a.H = 1;
-            DevProduct d{};
-            d.na = d.nb = d.nc = 1; d.a_s[0] = d.b_s[0] = d.c_s[0] = 1; d.c_first[0] = 1;
-            a.prod[0] = d;
         }
-        a.rsC = Mt.rows; a.csC = Mt.cols; a.bC = Mt.bat;
-        a.mC = ms; a.nC = ns; a.Hc = 1;
-        a.alpha = 1.0; a.beta = 0.0;
-        a.nprod = 1;
-        TSB_CUDA(launch_dmma(a, terms, st, sms));
+        if (pg.fits)
+        {
+            if (impl == 2)
+            {
+                if ((s = enqueue_pack_product(pr, g, pg, tb, A, B, PS, PT, st))) return s;
+            }
+            else
+            {
+                // the dense temporaries in tile order: S (ms x ks, k fastest), T (ks x ns, n fastest)
+                PackArgs pa{};
+                pa.X = static_cast<const double*>(Sbuf.p); pa.rs = St.rows; pa.ks = St.cols; pa.bX = St.bat;
+                pa.rows_full = ms; pa.k_full = ks; pa.rows_blk = ms; pa.k_blk = ks;
+                pa.nt = 1; pa.t_s[0] = 1;
+                pa.tiles = pg.tm; pa.k_pad = pg.k_pad; pa.batch = g.batch; pa.kfast = 1; pa.out = PS;
+                TSB_CUDA(launch_pack(pa, st));
+                PackArgs pb{};
+                pb.X = static_cast<const double*>(Tbuf.p); pb.rs = Tt.cols; pb.ks = Tt.rows; pb.bX = Tt.bat;
+                pb.rows_full = ns; pb.k_full = ks; pb.rows_blk = ns; pb.k_blk = ks;
+                pb.nt = 1; pb.t_s[0] = 1;
+                pb.tiles = pg.tn; pb.k_pad = pg.k_pad; pb.batch = g.batch; pb.kfast = 0; pb.out = PT;
+                TSB_CUDA(launch_pack(pb, st));
+            }
+            PackedGemmArgs ga{};
+            ga.S = PS; ga.T = PT; ga.C = M;
+            ga.rsC = Mt.rows; ga.csC = Mt.cols; ga.bC = Mt.bat;
+            ga.m = ms; ga.n = ns; ga.ms = ms; ga.ns = ns; ga.k_pad = pg.k_pad;
+            ga.tiles_m = pg.tm; ga.tiles_n = pg.tn; ga.batch = g.batch;
+            ga.alpha = 1.0; ga.beta = 0.0;
+            ga.nc = 1; ga.c_s[0] = 1; ga.c_first[0] = 1;
+            ga.err = err;
+            TSB_CUDA(launch_packed_gemm(ga, st, sms));
+        }
+        else
+        {
+            DmmaArgs a;
+            int terms = 1;
+            if (impl == 2)
+            {
+                a = base_args(g, t, A, B, M);
+                set_grid(a, ms, ns, ks);
+                a.H = H;
+                DevProduct d = to_dev(pr);
+                terms = std::max<int>(pr.na, pr.nb);
+                d.nc = 1; d.c_r[0] = 0; d.c_c[0] = 0; d.c_s[0] = 1; d.c_first[0] = 1;
+                a.prod[0] = d;
+            }
+            else
+            {
+                std::memset(&a, 0, sizeof a);
+                a.A = static_cast<const double*>(Sbuf.p); a.B = static_cast<const double*>(Tbuf.p); a.C = M;
+                a.rsA = St.rows; a.ksA = St.cols; a.bA = St.bat;
+                a.ksB = Tt.rows; a.csB = Tt.cols; a.bB = Tt.bat;
+                a.m = ms; a.n = ns; a.k = ks; a.batch = g.batch;
+                a.a_kfast = 1; a.b_kfast = 0;
+                set_grid(a, ms, ns, ks);
+                a.H = 1;
+                DevProduct d{};
+                d.na = d.nb = d.nc = 1; d.a_s[0] = d.b_s[0] = d.c_s[0] = 1; d.c_first[0] = 1;
+                a.prod[0] = d;
+            }
+            a.rsC = Mt.rows; a.csC = Mt.cols; a.bC = Mt.bat;
+            a.mC = ms; a.nC = ns; a.Hc = 1;
+            a.alpha = 1.0; a.beta = 0.0;
+            a.nprod = 1;
+            TSB_CUDA(launch_dmma(a, terms, st, sms));
+        }
 
         ScatterAddArgs sc{};
         sc.C = C; sc.rsC = t.rsC; sc.csC = t.csC; sc.bC = t.bC;
@@ -411,6 +471,13 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
             sc.c_first[q] = pr.c_first[q];
         }
         TSB_CUDA(launch_scatter_add(sc, st));
+    }
+    if (errbuf.p && blocking)
+    {
+        int flag = 0;
+        TSB_CUDA(cudaMemcpyAsync(&flag, errbuf.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        TSB_CUDA(cudaStreamSynchronize(st));
+        if (flag) return TBLIS_STRA_ERR_TIMEOUT;
     }
     return TBLIS_STRA_SUCCESS;
 }
