@@ -3,15 +3,24 @@
 //   tblis_tensor_mult              replaces src/iface/3t/mult.cxx:15
 //   stra_tblis_tensor_mult         replaces src/stra_iface/3t/stra_mult.cxx:26
 //   stra_tblis_tensor_mult_2level  replaces src/stra_iface/3t/stra_mult_2level.cxx:26
+//   tblis_matrix_mult, stra_tblis_matrix_mult[_naive|_ab][_2level]
+//                                  replace src/iface/3m and src/stra_iface/3m
 //
 // Each call: plan the contraction (plan.cpp), fetch or build the device copy of
 // its scatter vectors (cached per shape/stride/label signature), stage host
-// operands through device memory when needed, and enqueue the kernels of the
-// requested level and variant on the caller's stream:
-//   ABC   one persistent DMMA launch running every product (no workspace);
-//   AB    per product: DMMA launch with fused operand sums into one M buffer,
-//         then a scatter-add of M into its C blocks;
-//   Naive per product: sum-gather S and T, DMMA launch M = S*T, scatter-add.
+// operands through device memory when needed (pipelined in chunks when all
+// three are on the host and large), and enqueue the kernels of the requested
+// level and variant on the caller's stream:
+//   ABC   packed schedule: per group of 7 products (L >= 1) one pass packs
+//         the operand sums into tile order, then per product the packed DMMA
+//         GEMM adds +-alpha*S*T into its C blocks; with too little workspace
+//         one product at a time, and with none the fully fused kernel (one
+//         persistent launch running every product);
+//   AB    per product: pack the sums, packed GEMM into one M buffer, then a
+//         scatter-add of M into its C blocks;
+//   Naive per product: sum-gather dense S and T, pack them, packed GEMM
+//         M = S*T, scatter-add;
+//   FP32  the split-BF16 schedule on tcgen05 (bf16_split.cu).
 // After the call C->scalar is 1 and C->conj 0, as the reference leaves them
 // (src/stra_iface/3t/stra_mult.cxx:251-252).
 #include "tblis_stra_b200.h"

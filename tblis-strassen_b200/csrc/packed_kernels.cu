@@ -9,8 +9,14 @@
 //
 //   pack_kernel          S = sum_i u_i A_i and T = sum_j v_j B_j gathered
 //                        through the scatter vectors into tile order (HBM bound);
-//   packed_gemm_kernel   DMMA GEMM on S and T whose epilogue adds +-alpha*S*T
-//                        into the product's C blocks (beta on first touch).
+//   pack_multi_kernel    the 7 sums of a product group in one pass (L >= 1);
+//   packed_gemm_ws_kernel DMMA GEMM on S and T (bulk-copy operand ring on
+//                        mbarriers, no block barrier in the k loop) whose
+//                        epilogue adds +-alpha*S*T into the product's C blocks
+//                        (beta on first touch); packed_gemm_grouped_kernel the
+//                        same over many problems' tiles; packed_gemm_kernel the
+//                        earlier cp.async ring with a block barrier per k-step
+//                        (TBLIS_STRA_PACKED_CONFIG=1..4).
 //
 // Forming each sum once per element in HBM costs about 1 % of the GEMM time at
 // NIm = NJn = NPk = 16384, while summing inside the GEMM costs shared-memory
