@@ -193,3 +193,32 @@ def test_batch_rejects_host_tensors(tsb):
     A = np.ones((4, 4)); B = np.ones((4, 4)); C = np.zeros((4, 4))
     with pytest.raises(tsb.TblisStraError):
         tsb.Batch([(1.0, A, "ik", B, "kj", 0.0, C, "ij", 0)])
+
+
+def test_batch_empty_and_trivial_problems(tsb, cuda):
+    """No problems; a problem with an empty C; alpha = 0 (C = beta*C); an empty
+    contracted range (C = beta*C) -- next to an ordinary problem."""
+    import torch
+    b0 = tsb.Batch([])
+    b0.execute()
+    b0.close()
+    g = torch.Generator(device=cuda).manual_seed(8)
+    rnd = lambda *s: torch.rand(s, dtype=torch.float64, device=cuda, generator=g) * 2 - 1
+    A, B, C = rnd(30, 40), rnd(40, 20), rnd(30, 20)
+    E_A, E_B, E_C = rnd(0, 40), rnd(40, 20), rnd(0, 20)           # m = 0
+    K_A, K_B, K_C = rnd(30, 0), rnd(0, 20), rnd(30, 20)           # k = 0
+    Z_C = rnd(30, 20)
+    C0, K0, Z0 = C.clone(), K_C.clone(), Z_C.clone()
+    probs = [(1.0, A, "ik", B, "kj", 0.5, C, "ij", -1),
+             (1.0, E_A, "ik", E_B, "kj", 1.0, E_C, "ij", -1),
+             (1.0, K_A, "ik", K_B, "kj", 0.25, K_C, "ij", -1),
+             (0.0, A, "ik", B, "kj", 2.0, Z_C, "ij", 1)]
+    batch = tsb.Batch(probs)
+    assert batch.schedule()[2] == "scale" and batch.schedule()[3] == "scale"
+    batch.execute()
+    torch.cuda.synchronize()
+    R = 0.5 * C0 + A @ B
+    assert float((C - R).abs().max()) <= oracle.error_bound(2, 40, 1.0, 1.0) * 2 + 1e-13
+    assert torch.equal(K_C, 0.25 * K0)
+    assert torch.equal(Z_C, 2.0 * Z0)
+    batch.close()

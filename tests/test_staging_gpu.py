@@ -78,3 +78,49 @@ def test_small_or_unsliceable_operands_stage_whole(tsb, cuda):
     got, want, launches = run_pair(tsb, cuda, 1, A, "efac", B, "fbde", C0, "abcd", True)
     assert np.abs(got - want).max() <= bound(1, e * e)
     assert launches == 9
+
+
+def test_host_views_with_gaps_are_staged_whole(tsb, cuda):
+    """A host C that is a strided view (every other element of a larger
+    array) has no dense slices: the call stages the operands whole (one
+    contraction's launches) and still meets the bound."""
+    import torch
+    e = 42
+    A = oracle.uniform((e,) * 4, 13)
+    B = oracle.uniform((e,) * 4, 14)
+    big = np.asfortranarray(oracle.uniform((2 * e, e, e, e), 15))
+    C0 = big[::2]                                  # gap between rows
+    R = np.array(C0, copy=True, order="F")
+    oracle_bound = bound(1, e * e)
+    hA, hB = torch.from_numpy(A), torch.from_numpy(B)
+    hBig = torch.from_numpy(big)
+    hC = hBig[::2]
+    dA, dB, dR = hA.to(cuda), hB.to(cuda), torch.from_numpy(R).to(cuda)
+    before = tsb.launch_count()
+    tsb.contract(1, 1.0, hA, "efac", hB, "fbde", 1.0, hC, "abcd", drop_in=True)
+    assert tsb.launch_count() - before == 9
+    tsb.contract(1, 1.0, dA, "efac", dB, "fbde", 1.0, dR, "abcd")
+    torch.cuda.synchronize()
+    assert np.abs(hC.numpy() - dR.cpu().numpy()).max() <= oracle_bound
+    # the untouched rows between the view's rows are unchanged
+    assert np.array_equal(hBig[1::2].numpy(), big[1::2])
+
+
+def test_negative_strides_on_host(tsb, cuda):
+    """Host operands with a reversed axis (negative stride) are staged whole."""
+    import torch
+    e = 42
+    A = oracle.uniform((e,) * 4, 16)
+    B = oracle.uniform((e,) * 4, 17)
+    C0 = oracle.uniform((e,) * 4, 18)
+    hA = torch.from_numpy(A).flip(0)               # torch flip copies; use numpy views instead
+    nA = A[::-1]
+    R = C0.copy(order="F")
+    dC = torch.from_numpy(R).to(cuda)
+    tsb.contract(1, 1.0, torch.from_numpy(np.ascontiguousarray(nA)).to(cuda), "efac",
+                 torch.from_numpy(B).to(cuda), "fbde", 1.0, dC, "abcd")
+    hC = C0.copy(order="F")
+    tsb.contract(1, 1.0, nA, "efac", B, "fbde", 1.0, hC, "abcd", drop_in=True)
+    torch.cuda.synchronize()
+    assert np.abs(hC - dC.cpu().numpy()).max() <= bound(1, e * e)
+    del hA
