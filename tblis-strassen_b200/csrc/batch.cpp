@@ -418,7 +418,7 @@ struct Tuner
                 return enqueue_pack_product(p0, pr.g, pg, tb, static_cast<const double*>(pr.A),
                                             static_cast<const double*>(pr.B), S, T, st);
             });
-            PackedGemmArgs one = packed_product_args(p0, pr.g, pg, tb, S, T,
+            PackedGemmArgs one = packed_product_args(0, p0, pr.g, pg, tb, S, T,
                                                      static_cast<double*>(scratch.p) - shift, err);
             const int copies = copies_for(one.batch * one.tiles_m * one.tiles_n);
             std::vector<PackedGemmArgs> args(copies, one);
@@ -742,7 +742,7 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
                 const PackGeom pg = pack_geom(0, pr.g);
                 double* S = reinterpret_cast<double*>(base + off);
                 double* T = reinterpret_cast<double*>(base + off + round256(pg.s_elems * sizeof(double)));
-                pargs.push_back(packed_product_args(product_table(0).prod[0], pr.g, pg, tb, S, T,
+                pargs.push_back(packed_product_args(0, product_table(0).prod[0], pr.g, pg, tb, S, T,
                                                     static_cast<double*>(pr.C), err));
             }
             else

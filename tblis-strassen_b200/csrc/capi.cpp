@@ -426,12 +426,13 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
                 TSB_CUDA(launch_pack(pb, st));
             }
             PackedGemmArgs ga{};
-            ga.S = PS; ga.T = PT; ga.C = M;
+            ga.S[0] = PS; ga.T[0] = PT; ga.C = M;
             ga.rsC = Mt.rows; ga.csC = Mt.cols; ga.bC = Mt.bat;
             ga.m = ms; ga.n = ns; ga.ms = ms; ga.ns = ns; ga.k_pad = pg.k_pad;
             ga.tiles_m = pg.tm; ga.tiles_n = pg.tn; ga.batch = g.batch;
             ga.alpha = 1.0; ga.beta = 0.0;
-            ga.nc = 1; ga.c_s[0] = 1; ga.c_first[0] = 1;
+            ga.nprod = 1; ga.H = 1;
+            ga.nc[0] = 1; ga.c_s[0][0] = 1; ga.c_first[0][0] = 1;
             ga.err = err;
             TSB_CUDA(launch_packed_gemm(ga, st, sms));
         }
@@ -591,23 +592,39 @@ int enqueue_pack_product(const Product& pr, const GemmView& g, const PackGeom& p
     return TBLIS_STRA_SUCCESS;
 }
 
-PackedGemmArgs packed_product_args(const Product& pr, const GemmView& g, const PackGeom& pg,
-                                   const int64_t* const tb[9], const double* S, const double* T,
-                                   double* C, int* err)
+PackedGemmArgs packed_gemm_base(int level, const GemmView& g, const PackGeom& pg, const int64_t* const tb[9],
+                                double* C, int* err)
 {
     PackedGemmArgs ga{};
     ga.err = err;
-    ga.S = S; ga.T = T; ga.C = C;
+    ga.C = C;
     ga.rsC = tb[1]; ga.csC = tb[3]; ga.bC = tb[8];
     ga.m = g.m; ga.n = g.n; ga.ms = pg.ms; ga.ns = pg.ns; ga.k_pad = pg.k_pad;
     ga.tiles_m = pg.tm; ga.tiles_n = pg.tn; ga.batch = g.batch;
     ga.alpha = g.alpha; ga.beta = g.beta;
-    ga.nc = pr.nc;
+    ga.H = product_table(level).H;
+    ga.nprod = 0;
+    return ga;
+}
+
+void packed_gemm_add(PackedGemmArgs& a, const Product& pr, const double* S, const double* T)
+{
+    const int p = a.nprod++;
+    a.S[p] = S; a.T[p] = T;
+    a.nc[p] = pr.nc;
     for (int q = 0; q < pr.nc; q++)
     {
-        ga.c_r[q] = pr.c[q].r; ga.c_c[q] = pr.c[q].c; ga.c_s[q] = pr.c[q].sign;
-        ga.c_first[q] = pr.c_first[q];
+        a.c_r[p][q] = pr.c[q].r; a.c_c[p][q] = pr.c[q].c; a.c_s[p][q] = pr.c[q].sign;
+        a.c_first[p][q] = pr.c_first[q];
     }
+}
+
+PackedGemmArgs packed_product_args(int level, const Product& pr, const GemmView& g, const PackGeom& pg,
+                                   const int64_t* const tb[9], const double* S, const double* T,
+                                   double* C, int* err)
+{
+    PackedGemmArgs ga = packed_gemm_base(level, g, pg, tb, C, err);
+    packed_gemm_add(ga, pr, S, T);
     return ga;
 }
 
@@ -638,9 +655,11 @@ int run_fp64_packed_enqueue(int level, const GemmView& g, const int64_t* const t
             int s;
             if ((s = enqueue_pack_group(level, 0, G, g, pg, tb, A, S, st))) return s;
             if ((s = enqueue_pack_group(level, 1, G, g, pg, tb, B, T, st))) return s;
-            for (int q = 0; q < 7; q++)
-                TSB_CUDA(launch_packed_gemm(packed_product_args(tab.prod[(size_t)(G * 7 + q)], g, pg, tb, S[q],
-                                                                T[q], C, err), st, sms));
+            // one launch runs the group's 7 products tile by tile: a CTA owns a
+            // tile position across them, so their C tiles stay in L2
+            PackedGemmArgs ga = packed_gemm_base(level, g, pg, tb, C, err);
+            for (int q = 0; q < 7; q++) packed_gemm_add(ga, tab.prod[(size_t)(G * 7 + q)], S[q], T[q]);
+            TSB_CUDA(launch_packed_gemm(ga, st, sms));
         }
         return TBLIS_STRA_SUCCESS;
     }
@@ -650,7 +669,7 @@ int run_fp64_packed_enqueue(int level, const GemmView& g, const int64_t* const t
     {
         int s = enqueue_pack_product(pr, g, pg, tb, A, B, S, T, st);
         if (s) return s;
-        TSB_CUDA(launch_packed_gemm(packed_product_args(pr, g, pg, tb, S, T, C, err), st, sms));
+        TSB_CUDA(launch_packed_gemm(packed_product_args(level, pr, g, pg, tb, S, T, C, err), st, sms));
     }
     return TBLIS_STRA_SUCCESS;
 }

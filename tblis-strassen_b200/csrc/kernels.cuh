@@ -133,10 +133,16 @@ struct PackArgs
 
 // C_q = (first_q ? beta*C_q : C_q) + sign_q*alpha*(S*T) for the nc targets of
 // one product, S and T packed (PACK_TILE x k_pad tiles).
+// Packed GEMM: for every 128 x 128 tile position, products q = 0..nprod-1 in
+// order: C blocks (c_r, c_c) of product q += c_s * alpha * S_q T_q (beta on
+// first touch).  All products share the tile grid and k_pad; a CTA owns a
+// tile position across its products, so the C tiles a group of products
+// updates stay in L2 between them.
+constexpr int MAX_GROUP_PRODUCTS = 7;
 struct PackedGemmArgs
 {
-    const double* S;
-    const double* T;
+    const double* S[MAX_GROUP_PRODUCTS];       // packed operand sums, tile order
+    const double* T[MAX_GROUP_PRODUCTS];
     double* C;
     const int64_t* rsC; const int64_t* csC; const int64_t* bC;
     int64_t m, n;                              // full C extents
@@ -144,8 +150,11 @@ struct PackedGemmArgs
     int64_t k_pad;
     int64_t tiles_m, tiles_n, batch;
     double alpha, beta;
-    int nc;
-    int8_t c_r[4], c_c[4], c_s[4], c_first[4];
+    int nprod;                                 // products per tile position (1..7)
+    int H;                                     // side of the C block grid (1, 2 or 4)
+    int8_t nc[MAX_GROUP_PRODUCTS];             // C blocks per product (1..4)
+    int8_t c_r[MAX_GROUP_PRODUCTS][4], c_c[MAX_GROUP_PRODUCTS][4];
+    int8_t c_s[MAX_GROUP_PRODUCTS][4], c_first[MAX_GROUP_PRODUCTS][4];
     int* err;                                  // set on a timed-out wait (may be null)
 };
 

@@ -284,19 +284,19 @@ __device__ __forceinline__ void packed_tile(const PackedGemmArgs& a, int64_t w, 
         {
             const int q = i / BM, r = i % BM;
             const int64_t loc = tm * BM + r;
-            const int64_t gi = (q < a.nc ? a.c_r[q] : 0) * a.ms + loc;
-            rowC[i] = (q < a.nc && loc < a.ms && gi < a.m) ? a.bC[b] + a.rsC[gi] : OFF_INVALID;
+            const int64_t gi = (q < a.nc[0] ? a.c_r[0][q] : 0) * a.ms + loc;
+            rowC[i] = (q < a.nc[0] && loc < a.ms && gi < a.m) ? a.bC[b] + a.rsC[gi] : OFF_INVALID;
         }
         for (int i = tid; i < 4 * BN; i += NT)
         {
             const int q = i / BN, c = i % BN;
             const int64_t loc = tn * BN + c;
-            const int64_t gj = (q < a.nc ? a.c_c[q] : 0) * a.ns + loc;
-            colC[i] = (q < a.nc && loc < a.ns && gj < a.n) ? a.csC[gj] : OFF_INVALID;
+            const int64_t gj = (q < a.nc[0] ? a.c_c[0][q] : 0) * a.ns + loc;
+            colC[i] = (q < a.nc[0] && loc < a.ns && gj < a.n) ? a.csC[gj] : OFF_INVALID;
         }
 
-        const double* Sb = a.S + ((b * a.tiles_m + tm) * a.k_pad) * BM;
-        const double* Tb = a.T + ((b * a.tiles_n + tn) * a.k_pad) * BN;
+        const double* Sb = a.S[0] + ((b * a.tiles_m + tm) * a.k_pad) * BM;
+        const double* Tb = a.T[0] + ((b * a.tiles_n + tn) * a.k_pad) * BN;
         auto copy_stage = [&](int64_t s) {
             const int buf = (int)(s % STAGES);
             const double* sa = Sb + s * BK * BM;
@@ -368,12 +368,12 @@ __device__ __forceinline__ void packed_tile(const PackedGemmArgs& a, int64_t w, 
 
         // Epilogue: C_q = (first ? beta*C_q : C_q) + sign_q*alpha*S*T.  All
         // loads of C are issued before the stores so their latencies overlap.
-        for (int q = 0; q < a.nc; q++)
+        for (int q = 0; q < a.nc[0]; q++)
         {
             const int64_t* rt = rowC + q * BM;
             const int64_t* ct = colC + q * BN;
-            const double coef = a.c_s[q] < 0 ? -a.alpha : a.alpha;
-            const bool first = a.c_first[q] != 0;
+            const double coef = a.c_s[0][q] < 0 ? -a.alpha : a.alpha;
+            const bool first = a.c_first[0][q] != 0;
             const bool read_c = !first || a.beta != 0.0;
             const double cb = first ? a.beta : 1.0;
 #pragma unroll
@@ -440,10 +440,11 @@ packed_gemm_kernel(const __grid_constant__ PackedGemmArgs a)
 struct WsCtrl
 {
     uint64_t full[4], empty[4];    // per ring slot; STAGES <= 4
-    int64_t pw, ps, nk;            // producer: work item, k-step within it, k-steps of it
+    int64_t pw, ps, nk;            // producer: work item, k-step within a product, k-steps
     const double* sA;
     const double* sB;
     uint32_t pit;                  // k-steps issued
+    int pq, np;                    // producer: product within the work item, products of it
     int abort;
 };
 
@@ -532,7 +533,7 @@ __device__ __forceinline__ void packed_ws_body(const Src& src, int* err, unsigne
             mbar_init(smem_addr(&ctl->full[s]), 1);
             mbar_init(smem_addr(&ctl->empty[s]), NW);
         }
-        ctl->pw = blockIdx.x; ctl->ps = 0; ctl->nk = 0; ctl->pit = 0; ctl->abort = 0;
+        ctl->pw = blockIdx.x; ctl->ps = 0; ctl->nk = 0; ctl->pit = 0; ctl->pq = 0; ctl->np = 0; ctl->abort = 0;
         mbar_init_fence();
     }
     __syncthreads();
@@ -550,9 +551,11 @@ __device__ __forceinline__ void packed_ws_body(const Src& src, int* err, unsigne
                 int64_t b, tm, tn;
                 decode_tile(p, local, b, tm, tn);
                 ctl->nk = p.k_pad / BK;
+                ctl->np = p.nprod;
                 if (ctl->nk == 0) { ctl->pw += gridDim.x; continue; }
-                ctl->sA = p.S + ((b * p.tiles_m + tm) * p.k_pad) * BM;
-                ctl->sB = p.T + ((b * p.tiles_n + tn) * p.k_pad) * BN;
+                const int q = ctl->pq;
+                ctl->sA = p.S[q] + ((b * p.tiles_m + tm) * p.k_pad) * BM;
+                ctl->sB = p.T[q] + ((b * p.tiles_n + tn) * p.k_pad) * BN;
             }
             const uint32_t it = ctl->pit, slot = it % STAGES;
             if (it >= (uint32_t)STAGES &&
@@ -563,7 +566,11 @@ __device__ __forceinline__ void packed_ws_body(const Src& src, int* err, unsigne
             bulk_copy(smem_addr(As + slot * BK * BM), ctl->sA + ctl->ps * BK * BM, BK * BM * 8, full);
             bulk_copy(smem_addr(Bs + slot * BK * BN), ctl->sB + ctl->ps * BK * BN, BK * BN * 8, full);
             ctl->pit = it + 1;
-            if (++ctl->ps == ctl->nk) { ctl->ps = 0; ctl->pw += gridDim.x; }
+            if (++ctl->ps == ctl->nk)
+            {
+                ctl->ps = 0;
+                if (++ctl->pq == ctl->np) { ctl->pq = 0; ctl->pw += gridDim.x; }
+            }
             return true;
         }
         return true;
@@ -600,107 +607,112 @@ __device__ __forceinline__ void packed_ws_body(const Src& src, int* err, unsigne
         int64_t b, tm, tn;
         decode_tile(a, local, b, tm, tn);
         const int64_t nk = a.k_pad / BK;
+        // Offset tables of the tile's rows (columns) in every block row (column)
+        // h < H of the C block grid, shared by all products of the work item.
+        const int H = a.H;
         for (int i = tid; i < 4 * BM; i += NT)
         {
-            const int q = i / BM, r = i % BM;
-            const int64_t loc = tm * BM + r;
-            const int64_t gi = (q < a.nc ? a.c_r[q] : 0) * a.ms + loc;
-            rowC[i] = (q < a.nc && loc < a.ms && gi < a.m) ? a.bC[b] + a.rsC[gi] : OFF_INVALID;
+            const int h = i / BM, r = i % BM;
+            const int64_t loc = tm * BM + r, gi = h * a.ms + loc;
+            rowC[i] = (h < H && loc < a.ms && gi < a.m) ? a.bC[b] + a.rsC[gi] : OFF_INVALID;
         }
         for (int i = tid; i < 4 * BN; i += NT)
         {
-            const int q = i / BN, c = i % BN;
-            const int64_t loc = tn * BN + c;
-            const int64_t gj = (q < a.nc ? a.c_c[q] : 0) * a.ns + loc;
-            colC[i] = (q < a.nc && loc < a.ns && gj < a.n) ? a.csC[gj] : OFF_INVALID;
+            const int h = i / BN, c = i % BN;
+            const int64_t loc = tn * BN + c, gj = h * a.ns + loc;
+            colC[i] = (h < H && loc < a.ns && gj < a.n) ? a.csC[gj] : OFF_INVALID;
         }
         __syncthreads();
 
-        double acc[MI][NI][4];
-#pragma unroll
-        for (int mi = 0; mi < MI; mi++)
-#pragma unroll
-            for (int ni = 0; ni < NI; ni++)
-#pragma unroll
-                for (int e = 0; e < 4; e++) acc[mi][ni][e] = 0.0;
-
-        for (int64_t s = 0; s < nk; s++)
+        for (int p = 0; p < a.nprod && ok && nk > 0; p++)
         {
-            const uint32_t slot = cit % STAGES;
-            // warp-uniform outcome, so the warp stays converged
-            ok = __all_sync(0xffffffffu,
-                            mbar_wait(smem_addr(&ctl->full[slot]), (cit / STAGES) & 1, abort_flag, err, 2));
-            if (!ok) break;
-            const double* Ab = As + slot * BK * BM;
-            const double* Bb = Bs + slot * BK * BN;
-            double af[2][MI][2], bf[2][NI];
-            load_frags(Ab, Bb, 0, af[0], bf[0]);
-#pragma unroll
-            for (int q = 0; q < BK / 4; q++)
-            {
-                const int cur = q & 1;
-                if (q + 1 < BK / 4) load_frags(Ab, Bb, (q + 1) * 4, af[cur ^ 1], bf[cur ^ 1]);
-#pragma unroll
-                for (int mi = 0; mi < MI; mi++)
-#pragma unroll
-                    for (int ni = 0; ni < NI; ni++)
-                        dmma(acc[mi][ni], af[cur][mi][0], af[cur][mi][1], bf[cur][ni]);
-            }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(smem_addr(&ctl->empty[slot]));
-            cit++;
-            if (warp == 0)
-            {
-                bool pok = true;
-                if (lane == 0) pok = produce();
-                ok = __shfl_sync(0xffffffffu, pok, 0);
-                if (!ok) break;
-            }
-        }
-        if (!ok) continue;   // the barrier at the top ends the loop
-
-        // Epilogue: C_q = (first ? beta*C_q : C_q) + sign_q*alpha*S*T, all
-        // loads of a row pair issued before its stores.
-        for (int q = 0; q < a.nc; q++)
-        {
-            const int64_t* rt = rowC + q * BM;
-            const int64_t* ct = colC + q * BN;
-            const double coef = a.c_s[q] < 0 ? -a.alpha : a.alpha;
-            const bool first = a.c_first[q] != 0;
-            const bool read_c = !first || a.beta != 0.0;
-            const double cb = first ? a.beta : 1.0;
+            double acc[MI][NI][4];
 #pragma unroll
             for (int mi = 0; mi < MI; mi++)
+#pragma unroll
+                for (int ni = 0; ni < NI; ni++)
+#pragma unroll
+                    for (int e = 0; e < 4; e++) acc[mi][ni][e] = 0.0;
+
+            for (int64_t s = 0; s < nk; s++)
             {
-                double cv[2][NI][2];
+                const uint32_t slot = cit % STAGES;
+                // warp-uniform outcome, so the warp stays converged
+                ok = __all_sync(0xffffffffu,
+                                mbar_wait(smem_addr(&ctl->full[slot]), (cit / STAGES) & 1, abort_flag, err, 2));
+                if (!ok) break;
+                const double* Ab = As + slot * BK * BM;
+                const double* Bb = Bs + slot * BK * BN;
+                double af[2][MI][2], bf[2][NI];
+                load_frags(Ab, Bb, 0, af[0], bf[0]);
 #pragma unroll
-                for (int hr = 0; hr < 2; hr++)
+                for (int q = 0; q < BK / 4; q++)
                 {
-                    const int64_t ro = rt[wm + mi * 16 + g + hr * 8];
+                    const int cur = q & 1;
+                    if (q + 1 < BK / 4) load_frags(Ab, Bb, (q + 1) * 4, af[cur ^ 1], bf[cur ^ 1]);
 #pragma unroll
-                    for (int ni = 0; ni < NI; ni++)
+                    for (int mi = 0; mi < MI; mi++)
 #pragma unroll
-                        for (int hc = 0; hc < 2; hc++)
-                        {
-                            const int64_t co = ct[wn + ni * 8 + t4 * 2 + hc];
-                            cv[hr][ni][hc] = (read_c && ro != OFF_INVALID && co != OFF_INVALID)
-                                                 ? a.C[ro + co] : 0.0;
-                        }
+                        for (int ni = 0; ni < NI; ni++)
+                            dmma(acc[mi][ni], af[cur][mi][0], af[cur][mi][1], bf[cur][ni]);
                 }
-#pragma unroll
-                for (int hr = 0; hr < 2; hr++)
+                __syncwarp();
+                if (lane == 0) mbar_arrive(smem_addr(&ctl->empty[slot]));
+                cit++;
+                if (warp == 0)
                 {
-                    const int64_t ro = rt[wm + mi * 16 + g + hr * 8];
-                    if (ro == OFF_INVALID) continue;
+                    bool pok = true;
+                    if (lane == 0) pok = produce();
+                    ok = __shfl_sync(0xffffffffu, pok, 0);
+                    if (!ok) break;
+                }
+            }
+            if (!ok) break;   // the barrier at the top of the tile loop ends it
+
+            // Epilogue of product p: C_t = (first ? beta*C_t : C_t) +
+            // sign_t*alpha*S*T for its C blocks t, all loads of a row pair
+            // issued before its stores.
+            for (int t = 0; t < a.nc[p]; t++)
+            {
+                const int64_t* rt = rowC + a.c_r[p][t] * BM;
+                const int64_t* ct = colC + a.c_c[p][t] * BN;
+                const double coef = a.c_s[p][t] < 0 ? -a.alpha : a.alpha;
+                const bool first = a.c_first[p][t] != 0;
+                const bool read_c = !first || a.beta != 0.0;
+                const double cb = first ? a.beta : 1.0;
 #pragma unroll
-                    for (int ni = 0; ni < NI; ni++)
+                for (int mi = 0; mi < MI; mi++)
+                {
+                    double cv[2][NI][2];
 #pragma unroll
-                        for (int hc = 0; hc < 2; hc++)
-                        {
-                            const int64_t co = ct[wn + ni * 8 + t4 * 2 + hc];
-                            if (co == OFF_INVALID) continue;
-                            a.C[ro + co] = coef * acc[mi][ni][hr * 2 + hc] + cb * cv[hr][ni][hc];
-                        }
+                    for (int hr = 0; hr < 2; hr++)
+                    {
+                        const int64_t ro = rt[wm + mi * 16 + g + hr * 8];
+#pragma unroll
+                        for (int ni = 0; ni < NI; ni++)
+#pragma unroll
+                            for (int hc = 0; hc < 2; hc++)
+                            {
+                                const int64_t co = ct[wn + ni * 8 + t4 * 2 + hc];
+                                cv[hr][ni][hc] = (read_c && ro != OFF_INVALID && co != OFF_INVALID)
+                                                     ? a.C[ro + co] : 0.0;
+                            }
+                    }
+#pragma unroll
+                    for (int hr = 0; hr < 2; hr++)
+                    {
+                        const int64_t ro = rt[wm + mi * 16 + g + hr * 8];
+                        if (ro == OFF_INVALID) continue;
+#pragma unroll
+                        for (int ni = 0; ni < NI; ni++)
+#pragma unroll
+                            for (int hc = 0; hc < 2; hc++)
+                            {
+                                const int64_t co = ct[wn + ni * 8 + t4 * 2 + hc];
+                                if (co == OFF_INVALID) continue;
+                                a.C[ro + co] = coef * acc[mi][ni][hr * 2 + hc] + cb * cv[hr][ni][hc];
+                            }
+                    }
                 }
             }
         }
@@ -823,7 +835,9 @@ cudaError_t launch_pack_multi(const PackMultiArgs& a, cudaStream_t stream)
 cudaError_t launch_packed_gemm(const PackedGemmArgs& a, cudaStream_t stream, int num_sms, int config)
 {
     if (a.batch <= 0 || a.tiles_m <= 0 || a.tiles_n <= 0) return cudaSuccess;
-    if (a.nc < 1 || a.nc > 4) return cudaErrorInvalidValue;
+    if (a.nprod < 1 || a.nprod > MAX_GROUP_PRODUCTS || a.H < 1 || a.H > 4) return cudaErrorInvalidValue;
+    for (int p = 0; p < a.nprod; p++)
+        if (a.nc[p] < 1 || a.nc[p] > 4) return cudaErrorInvalidValue;
     if (config < 0)
     {
         static const int env = [] {
@@ -834,7 +848,9 @@ cudaError_t launch_packed_gemm(const PackedGemmArgs& a, cudaStream_t stream, int
     }
     cudaError_t err;
     // 0 (default): warp-specialised bulk-copy ring; 1-4: cp.async rings with a
-    // block barrier per k-step (4 = the same tile shape as the default).
+    // block barrier per k-step (4 = the same tile shape as the default), one
+    // product per launch.
+    if (config >= 1 && config <= 4 && a.nprod != 1) config = 0;
     switch (config)
     {
         case 1:  err = launch_packed_cfg<PG1>(a, stream, num_sms); break;

@@ -47,9 +47,14 @@ int enqueue_pack_product(const Product& pr, const GemmView& g, const PackGeom& p
                          const int64_t* const tb[9], const double* A, const double* B,
                          double* S, double* T, cudaStream_t st);
 
-// Descriptor of product `pr`'s packed GEMM (+-alpha*S*T into its C blocks);
-// `err` (device int, may be null) records a timed-out wait.
-PackedGemmArgs packed_product_args(const Product& pr, const GemmView& g, const PackGeom& pg,
+// Descriptor of a packed GEMM over C at `level` with no products yet, and
+// appending a product (its operand sums S, T and C blocks; up to 7, run in
+// the order added); `err` (device int, may be null) records a timed-out wait.
+PackedGemmArgs packed_gemm_base(int level, const GemmView& g, const PackGeom& pg, const int64_t* const tb[9],
+                                double* C, int* err);
+void packed_gemm_add(PackedGemmArgs& a, const Product& pr, const double* S, const double* T);
+// Both for one product.
+PackedGemmArgs packed_product_args(int level, const Product& pr, const GemmView& g, const PackGeom& pg,
                                    const int64_t* const tb[9], const double* S, const double* T,
                                    double* C, int* err);
 
