@@ -41,11 +41,11 @@ METRIC = "effective TFLOPS (2mnk/t) Strassen L1/L2 vs plain L=0 TC on 1 B200 at 
 # DRAM traffic (read + write bytes) per launch of the dominant kernel at the
 # default workload, from one full-size ncu capture (one pass of
 # dram__bytes_read.sum + dram__bytes_write.sum; summary in
-# profiles/packed_gemm_kernel_fp64_L1_e128_dram.md): packed_gemm_kernel,
-# Strassen product M1 of the L=1 contraction at extents 128 (an 8192^3 GEMM
-# on packed S, T plus the +-M update of two C blocks): 7.85 GB read,
-# 1.08 GB written.
-NCU_TRAFFIC_BYTES = 7.85e9 + 1.08e9
+# profiles/packed_gemm_ws_kernel_fp64_L1_e128_dram.md): packed_gemm_ws_kernel,
+# the launch of the L=1 product group at extents 128 (7 GEMMs of 8192^3 on
+# packed S_q, T_q, run tile position by tile position): 263.06 GB read,
+# 6.45 GB written.
+NCU_TRAFFIC_BYTES = 263.06e9 + 6.45e9
 
 
 def load_package():
