@@ -21,6 +21,12 @@
 //                    write C_q = (first ? beta*C_q : C_q) + sign*alpha*acc
 //                    / (row scale * column scale).
 //
+// With workspace for a group's planes (L >= 1), split_pack_multi_kernel forms
+// the 7 split sums of a product group from one pass over each operand, and
+// one split_gemm_kernel launch runs the group's 7 products in product order
+// for each tile position, so the C tiles they update stay in L2 between
+// products.
+//
 // Warp roles in split_gemm_kernel (192 threads, one CTA per SM):
 //   warp 0      one lane issues the bulk copies (cp.async.bulk, 1-D TMA) of
 //               each stage's plane tiles into shared memory;
@@ -453,9 +459,11 @@ __device__ __forceinline__ void split_gemm_body(const Src& src, int* err, unsign
                 const int64_t nk = a.nk;
                 const size_t planeA = (size_t)a.batch * a.tiles_m * nk * BLK;
                 const size_t planeB = (size_t)a.batch * a.tiles_n * nk * BLK;
-                const unsigned char* srcA = reinterpret_cast<const unsigned char*>(a.A) +
+                for (int q = 0; q < a.nprod && ok; q++)
+                {
+                const unsigned char* srcA = reinterpret_cast<const unsigned char*>(a.A[q]) +
                                             ((size_t)(b * a.tiles_m + tm) * nk) * BLK;
-                const unsigned char* srcB = reinterpret_cast<const unsigned char*>(a.B) +
+                const unsigned char* srcB = reinterpret_cast<const unsigned char*>(a.B[q]) +
                                             ((size_t)(b * a.tiles_n + tn) * nk) * BLK;
                 for (int64_t c = 0; c < nk; c++, it++)
                 {
@@ -470,6 +478,7 @@ __device__ __forceinline__ void split_gemm_body(const Src& src, int* err, unsign
                         bulk_copy(dst + p * BLK, srcA + p * planeA + c * BLK, BLK, bar(BAR_FULL + s));
                         bulk_copy(dst + (P + p) * BLK, srcB + p * planeB + c * BLK, BLK, bar(BAR_FULL + s));
                     }
+                }
                 }
             }
             // Copies still in flight land before the CTA leaves (bounded wait on
@@ -490,6 +499,8 @@ __device__ __forceinline__ void split_gemm_body(const Src& src, int* err, unsign
                 int64_t local;
                 const SplitGemmArgs& a = src.at(w, local);
                 const int64_t nk = a.nk;
+                for (int q = 0; q < a.nprod && ok; q++)
+                {
                 uint32_t dcol = 0;
                 for (int64_t c = 0; c < nk; c++, it++)
                 {
@@ -524,6 +535,7 @@ __device__ __forceinline__ void split_gemm_body(const Src& src, int* err, unsign
                         u++;
                     }
                 }
+                }
             }
             // Every MMA issued completes before TMEM is freed.
             mma_commit(bar(BAR_DRAIN));
@@ -546,13 +558,15 @@ __device__ __forceinline__ void split_gemm_body(const Src& src, int* err, unsign
             decode(a, local, b, tm, tn);
             const int64_t nk = a.nk;
             asm volatile("bar.sync 1, 128;\n" ::: "memory");
-            for (int qq = 0; qq < 4; qq++)
+            // Offsets of this tile's rows and columns in each block position
+            // of C; every product of the group writes into these.
+            for (int h = 0; h < 4; h++)
             {
                 const int64_t li = tm * ST + dt, lj = tn * ST + dt;
-                const int64_t gi = (qq < a.nc ? a.c_r[qq] : 0) * a.ms + li;
-                const int64_t gj = (qq < a.nc ? a.c_c[qq] : 0) * a.ns + lj;
-                rowC[qq * ST + dt] = (qq < a.nc && li < a.ms && gi < a.m) ? a.bC[b] + a.rsC[gi] : OFF_INVALID;
-                colC[qq * ST + dt] = (qq < a.nc && lj < a.ns && gj < a.n) ? a.csC[gj] : OFF_INVALID;
+                const int64_t gi = (int64_t)h * a.ms + li;
+                const int64_t gj = (int64_t)h * a.ns + lj;
+                rowC[h * ST + dt] = (h < a.H && li < a.ms && gi < a.m) ? a.bC[b] + a.rsC[gi] : OFF_INVALID;
+                colC[h * ST + dt] = (h < a.H && lj < a.ns && gj < a.n) ? a.csC[gj] : OFF_INVALID;
             }
             {
                 const int64_t li = tm * ST + dt, lj = tn * ST + dt;
@@ -561,55 +575,59 @@ __device__ __forceinline__ void split_gemm_body(const Src& src, int* err, unsign
             }
             asm volatile("bar.sync 1, 128;\n" ::: "memory");
 
-            float acc[ST];
-#pragma unroll
-            for (int j = 0; j < ST; j++) acc[j] = 0.f;
             const int64_t nch = (nk + KCH - 1) / KCH;
-            for (int64_t ch = 0; ch < nch; ch++, u++)
+            for (int p = 0; p < a.nprod && ok; p++)
             {
-                const int bacc = u & 1;
-                if (!mbar_wait(bar(BAR_ACCF + bacc), (u >> 1) & 1, abort_flag, err, 4)) { ok = false; break; }
-                fence_after();
+                float acc[ST];
 #pragma unroll
-                for (int j = 0; j < ST / 32; j++)
+                for (int j = 0; j < ST; j++) acc[j] = 0.f;
+                for (int64_t ch = 0; ch < nch; ch++, u++)
                 {
-                    float hh[32], cr[32];
-                    const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + bacc * 2 * ST + j * 32;
-                    tmem_ld32(ta, hh);
-                    tmem_ld32(ta + ST, cr);
+                    const int bacc = u & 1;
+                    if (!mbar_wait(bar(BAR_ACCF + bacc), (u >> 1) & 1, abort_flag, err, 4)) { ok = false; break; }
+                    fence_after();
 #pragma unroll
-                    for (int i = 0; i < 32; i++) acc[j * 32 + i] += hh[i] + cr[i];
-                }
-                fence_before();
-                mbar_arrive(bar(BAR_ACCE + bacc));
-            }
-            if (!ok) break;
-            // C update in batches of 32 columns: all loads of a batch are
-            // issued before any store, so their latencies overlap.
-            for (int qq = 0; qq < a.nc; qq++)
-            {
-                const int64_t ro = rowC[qq * ST + row];
-                if (ro == OFF_INVALID) continue;
-                const float coef = (a.c_s[qq] < 0 ? -a.alpha : a.alpha) * invr[row];
-                const bool first = a.c_first[qq] != 0;
-                const bool read_c = !first || a.beta != 0.f;
-                const float cb = first ? a.beta : 1.f;
-                float* crow = a.C + ro;
-#pragma unroll
-                for (int j0 = 0; j0 < ST; j0 += 32)
-                {
-                    float cv[32];
-#pragma unroll
-                    for (int i = 0; i < 32; i++)
+                    for (int j = 0; j < ST / 32; j++)
                     {
-                        const int64_t co = colC[qq * ST + j0 + i];
-                        cv[i] = (read_c && co != OFF_INVALID) ? crow[co] : 0.f;
+                        float hh[32], cr[32];
+                        const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + bacc * 2 * ST + j * 32;
+                        tmem_ld32(ta, hh);
+                        tmem_ld32(ta + ST, cr);
+#pragma unroll
+                        for (int i = 0; i < 32; i++) acc[j * 32 + i] += hh[i] + cr[i];
                     }
+                    fence_before();
+                    mbar_arrive(bar(BAR_ACCE + bacc));
+                }
+                if (!ok) break;
+                // C update in batches of 32 columns: all loads of a batch are
+                // issued before any store, so their latencies overlap.
+                for (int t = 0; t < a.nc[p]; t++)
+                {
+                    const int64_t ro = rowC[a.c_r[p][t] * ST + row];
+                    if (ro == OFF_INVALID) continue;
+                    const int64_t* cc = colC + a.c_c[p][t] * ST;
+                    const float coef = (a.c_s[p][t] < 0 ? -a.alpha : a.alpha) * invr[row];
+                    const bool first = a.c_first[p][t] != 0;
+                    const bool read_c = !first || a.beta != 0.f;
+                    const float cb = first ? a.beta : 1.f;
+                    float* crow = a.C + ro;
 #pragma unroll
-                    for (int i = 0; i < 32; i++)
+                    for (int j0 = 0; j0 < ST; j0 += 32)
                     {
-                        const int64_t co = colC[qq * ST + j0 + i];
-                        if (co != OFF_INVALID) crow[co] = coef * acc[j0 + i] * invc[j0 + i] + cb * cv[i];
+                        float cv[32];
+#pragma unroll
+                        for (int i = 0; i < 32; i++)
+                        {
+                            const int64_t co = cc[j0 + i];
+                            cv[i] = (read_c && co != OFF_INVALID) ? crow[co] : 0.f;
+                        }
+#pragma unroll
+                        for (int i = 0; i < 32; i++)
+                        {
+                            const int64_t co = cc[j0 + i];
+                            if (co != OFF_INVALID) crow[co] = coef * acc[j0 + i] * invc[j0 + i] + cb * cv[i];
+                        }
                     }
                 }
             }
@@ -722,10 +740,24 @@ bool standard_terms(const SplitGemmArgs& a)
     return true;
 }
 
+// Products 1..7, block positions 1..4 per dimension, 1..4 targets per
+// product, each inside the block grid.
+bool split_targets_valid(const SplitGemmArgs& a)
+{
+    if (a.nprod < 1 || a.nprod > MAX_GROUP_PRODUCTS || a.H < 1 || a.H > 4) return false;
+    for (int p = 0; p < a.nprod; p++)
+    {
+        if (a.nc[p] < 1 || a.nc[p] > 4 || !a.A[p] || !a.B[p]) return false;
+        for (int t = 0; t < a.nc[p]; t++)
+            if (a.c_r[p][t] < 0 || a.c_r[p][t] >= a.H || a.c_c[p][t] < 0 || a.c_c[p][t] >= a.H) return false;
+    }
+    return true;
+}
+
 cudaError_t launch_split_gemm(const SplitGemmArgs& a, cudaStream_t stream, int num_sms)
 {
     if (a.batch <= 0 || a.tiles_m <= 0 || a.tiles_n <= 0 || a.nk <= 0) return cudaSuccess;
-    if (a.nc < 1 || a.nc > 4 || !standard_terms(a)) return cudaErrorInvalidValue;
+    if (!split_targets_valid(a) || !standard_terms(a)) return cudaErrorInvalidValue;
     cudaError_t err = a.planes == 3 ? launch_split_gemm_p<3>(a, stream, num_sms)
                     : a.planes == 2 ? launch_split_gemm_p<2>(a, stream, num_sms)
                                     : cudaErrorInvalidValue;

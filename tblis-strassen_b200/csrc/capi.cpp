@@ -778,19 +778,27 @@ int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], c
     const bool a_kfast = g.unit_ksA != 0 && (g.unit_rsA == 0 || g.unit_ksA < g.unit_rsA);
     const bool b_kfast = g.unit_ksB != 0 && (g.unit_csB == 0 || g.unit_ksB < g.unit_csB);
     static const int8_t TA6[6] = {0, 0, 1, 0, 1, 2}, TB6[6] = {0, 1, 0, 2, 1, 0};
-    auto gemm = [&](const Product& pr, const void* pA, const void* pB) -> int {
+    // One GEMM launch over `n` products that share the tile grid: each CTA
+    // runs all of them for its tile position, in the order given.
+    auto gemm = [&](const Product* const* prs, const void* const* pA, const void* const* pB, int n) -> int {
         SplitGemmArgs ga{};
-        ga.A = pA; ga.B = pB; ga.C = C;
+        ga.C = C;
         ga.rsC = tb[1]; ga.csC = tb[3]; ga.bC = tb[8];
         ga.invA = invA; ga.invB = invB;
         ga.m = g.m; ga.n = g.n; ga.ms = ms; ga.ns = ns; ga.nk = nk;
         ga.tiles_m = tm; ga.tiles_n = tn; ga.batch = g.batch;
         ga.alpha = (float)g.alpha; ga.beta = (float)g.beta;
-        ga.nc = pr.nc;
-        for (int q = 0; q < pr.nc; q++)
+        ga.nprod = n; ga.H = H;
+        for (int p = 0; p < n; p++)
         {
-            ga.c_r[q] = pr.c[q].r; ga.c_c[q] = pr.c[q].c; ga.c_s[q] = pr.c[q].sign;
-            ga.c_first[q] = pr.c_first[q];
+            const Product& pr = *prs[p];
+            ga.A[p] = pA[p]; ga.B[p] = pB[p];
+            ga.nc[p] = (int8_t)pr.nc;
+            for (int q = 0; q < pr.nc; q++)
+            {
+                ga.c_r[p][q] = pr.c[q].r; ga.c_c[p][q] = pr.c[q].c; ga.c_s[p][q] = pr.c[q].sign;
+                ga.c_first[p][q] = pr.c_first[q];
+            }
         }
         ga.planes = P;
         ga.nterms = P == 3 ? 6 : 3;
@@ -803,7 +811,8 @@ int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], c
     if (grouped)
     {
         // Per group of 7 products: one pass over A and one over B form the 14
-        // split sums (7 plane sets each), then the 7 GEMMs in product order.
+        // split sums (7 plane sets each), then one GEMM launch runs the 7
+        // products in product order for each tile position.
         const size_t bytesA = (size_t)P * g.batch * tm * nk * blk, bytesB = (size_t)P * g.batch * tn * nk * blk;
         char* base = static_cast<char*>(ws) + sc;
         void* outA[7];
@@ -852,11 +861,10 @@ int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], c
                 }
                 TSB_CUDA(launch_split_pack_multi(m, st));
             }
-            for (int q = 0; q < 7; q++)
-            {
-                const int s = gemm(tab.prod[(size_t)(G * 7 + q)], outA[q], outB[q]);
-                if (s) return s;
-            }
+            const Product* prs[7];
+            for (int q = 0; q < 7; q++) prs[q] = &tab.prod[(size_t)(G * 7 + q)];
+            const int s = gemm(prs, outA, outB, 7);
+            if (s) return s;
         }
         return TBLIS_STRA_SUCCESS;
     }
@@ -878,7 +886,10 @@ int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], c
         pb.scale = scaleB; pb.tiles = tn; pb.nk = nk; pb.batch = g.batch; pb.planes = P;
         pb.kfast = b_kfast; pb.out = planesB;
         if (enqueue) TSB_CUDA(launch_split_pack(pb, st));
-        const int s = gemm(pr, planesA, planesB);
+        const Product* one = &pr;
+        const void* pA1 = planesA;
+        const void* pB1 = planesB;
+        const int s = gemm(&one, &pA1, &pB1, 1);
         if (s) return s;
     }
     return TBLIS_STRA_SUCCESS;

@@ -243,18 +243,24 @@ struct SplitPackMultiArgs
     void* out[7];
 };
 
+// Split GEMM: for every 128 x 128 tile position, products q = 0..nprod-1 in
+// order (as PackedGemmArgs): C blocks (c_r, c_c) of product q +=
+// c_s * alpha * (A_q B_q) / scales, beta on first touch.
 struct SplitGemmArgs
 {
-    const void* A;                             // bf16 planes, A side
-    const void* B;                             // bf16 planes, B side
+    const void* A[MAX_GROUP_PRODUCTS];         // bf16 planes of each product's A-side sum
+    const void* B[MAX_GROUP_PRODUCTS];         // and B-side sum
     float* C;
     const int64_t* rsC; const int64_t* csC; const int64_t* bC;
     const float* invA;                         // [batch][ms] inverse row scales
     const float* invB;                         // [batch][ns] inverse column scales
     int64_t m, n, ms, ns, nk, tiles_m, tiles_n, batch;
     float alpha, beta;
-    int nc;
-    int8_t c_r[4], c_c[4], c_s[4], c_first[4];
+    int nprod;                                 // products per tile position (1..7)
+    int H;                                     // side of the C block grid (1, 2 or 4)
+    int8_t nc[MAX_GROUP_PRODUCTS];
+    int8_t c_r[MAX_GROUP_PRODUCTS][4], c_c[MAX_GROUP_PRODUCTS][4];
+    int8_t c_s[MAX_GROUP_PRODUCTS][4], c_first[MAX_GROUP_PRODUCTS][4];
     int planes, nterms;
     int8_t ta[6], tb[6];                       // plane pair of each product term
     int* err;                                  // set on a timed-out wait (may be null)

@@ -145,3 +145,26 @@ def test_fp32_per_product_packing(tsb, cuda, terms, level):
         tsb.set_workspace_limit(None)
     err = normwise(dC.cpu().numpy(), R)
     assert err <= TOL[terms], err
+
+
+@pytest.mark.parametrize("level", [1, 2])
+def test_fp32_group_launches(tsb, cuda, terms, level):
+    """With room for a group's planes, each group of 7 products takes one
+    pass over A, one over B and one GEMM launch that runs the 7 products for
+    each tile position; the result keeps the bound."""
+    import torch
+    ext = dict(a=24, b=20, c=10, d=12, e=18, f=16)
+    ia, ib, ic = "efac", "fbde", "abcd"
+    A = draw([ext[c] for c in ia], 14, "loguniform")
+    B = draw([ext[c] for c in ib], 15, "loguniform")
+    C0 = draw([ext[c] for c in ic], 16, "uniform")
+    R = C0.astype(np.float64, order="F")
+    oracle.contract(0.75, A.astype(np.float64, order="F"), ia, B.astype(np.float64, order="F"), ib, -0.5, R, ic)
+    dA, dB, dC = to_dev(A, cuda), to_dev(B, cuda), to_dev(C0, cuda)
+    before = tsb.launch_count()
+    tsb.contract(level, 0.75, dA, ia, dB, ib, -0.5, dC, ic)
+    torch.cuda.synchronize()
+    # 2 scale launches, then per group: pack 7 S, pack 7 T, GEMM
+    assert tsb.launch_count() - before == 2 + 3 * 7 ** (level - 1)
+    err = normwise(dC.cpu().numpy(), R)
+    assert err <= TOL[terms], err
