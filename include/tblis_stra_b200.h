@@ -190,6 +190,18 @@ int tblis_stra_get_impl(void);
 int tblis_stra_set_workspace_limit(size_t bytes);
 size_t tblis_stra_get_workspace_limit(void);
 
+/* Product-parallel ABC schedule for small grids (no counterpart in the
+ * reference, whose threads split each product's loops instead): when one
+ * product has fewer 128 x 128 tiles than two per SM, the ABC variant at
+ * L >= 1 packs every product's sums, runs all 7^L products side by side in
+ * one GEMM launch into their own M_p, and forms each C block as
+ * alpha * sum_p W[h][p] M_p + beta * C in one pass.  It needs
+ * 7^L * (packed S and T + 8*batch*ms*ns) bytes within the workspace limit.
+ * mode: -1 automatic (the default), 0 never, 1 whenever the workspace fits.
+ * Per calling thread.  Returns 0 or TBLIS_STRA_ERR_ARG. */
+int tblis_stra_set_product_parallel(int mode);
+int tblis_stra_get_product_parallel(void);
+
 /* FP32 (TYPE_FLOAT) contractions run on the BF16 tensor cores with each
  * operand split into bf16 planes (no counterpart in the reference, whose FP32
  * path is its CPU micro-kernel): terms = 6 splits into hi+mid+lo and keeps the

@@ -11,8 +11,12 @@
 //                       C blocks of one product: the M -> C update of the AB and
 //                       Naive variants (src/stra_internal/3t/straprim_common.hpp:
 //                       156, 187-203, tensor2matrix.hpp:390-830).
+//   combine_kernel      C_h = alpha * sum_p W[h][p] M_p + beta * C_h for every C
+//                       block h at once, after the products have run side by
+//                       side into their own M_p (small grids, where one product
+//                       has too few tiles for the SMs).
 //
-// All three are grid-stride loops over (batch, row, col) with the column index
+// All four are grid-stride loops over (batch, row, col) with the column index
 // fastest; the scatter vectors make the access pattern coalesced whenever the
 // fastest C (or X) mode is the column bundle's first mode.
 #include "kernels.cuh"
@@ -118,7 +122,52 @@ __global__ void scatter_add_kernel(const ScatterAddArgs a)
     }
 }
 
+// One thread per C element: the terms of its block position, read from the
+// products' M at the same local (i, j), fastest index that of M's layout.
+__global__ void combine_kernel(const __grid_constant__ CombineArgs a)
+{
+    const int H2 = a.H * a.H;
+    const int64_t per = a.ms * a.ns;
+    const int64_t total = (int64_t)H2 * a.batch * per;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x)
+    {
+        const int64_t loc = e % per;
+        const int64_t rest = e / per;
+        const int64_t b = rest % a.batch;
+        const int h = (int)(rest / a.batch);
+        const int64_t i = a.col_major ? loc % a.ms : loc / a.ns;
+        const int64_t j = a.col_major ? loc / a.ms : loc % a.ns;
+        const int64_t gi = (h / a.H) * a.ms + i, gj = (h % a.H) * a.ns + j;
+        if (gi >= a.m || gj >= a.n) continue;
+        const double* Mb = a.M + b * per + loc;
+        double v = 0.0;
+        for (int t = 0; t < a.cnt[h]; t++)
+        {
+            const double x = Mb[a.prod[h][t] * a.m_pstride];
+            v += a.sign[h][t] < 0 ? -x : x;
+        }
+        double* p = a.C + a.bC[b] + a.rsC[gi] + a.csC[gj];
+        *p = a.beta != 0.0 ? a.alpha * v + a.beta * *p : a.alpha * v;
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_combine(const CombineArgs& a, cudaStream_t stream)
+{
+    const int64_t total = (int64_t)a.H * a.H * a.batch * a.ms * a.ns;
+    if (total <= 0) return cudaSuccess;
+    if (a.H < 1 || a.H > 4) return cudaErrorInvalidValue;
+    for (int h = 0; h < a.H * a.H; h++)
+        if (a.cnt[h] < 0 || a.cnt[h] > 16) return cudaErrorInvalidValue;
+    timing_begin(KK_AUX, stream);
+    combine_kernel<<<grid_for(total), THREADS, 0, stream>>>(a);
+    timing_end(KK_AUX, stream);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) g_launches++;
+    return err;
+}
 
 cudaError_t launch_scale(const ScaleArgs& a, cudaStream_t stream)
 {

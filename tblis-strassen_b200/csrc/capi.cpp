@@ -53,6 +53,7 @@ thread_local cudaStream_t t_stream = nullptr;
 thread_local int t_status = TBLIS_STRA_SUCCESS;
 thread_local size_t t_ws_limit = SIZE_MAX;   // device workspace the ABC schedule may use
 thread_local int t_fp32_terms = 6;           // split-BF16 product terms for FP32 (3 or 6)
+thread_local int t_product_parallel = -1;    // product-parallel ABC: -1 auto, 0 never, 1 when it fits
 unsigned g_num_threads = 1;
 thread_local std::string t_detail;           // what the last failing CUDA call was
 
@@ -64,7 +65,15 @@ struct DevPlan
     void* mem = nullptr;
     size_t bytes = 0;
     const int64_t *rsA, *rsC, *csB, *csC, *ksA, *ksB, *bA, *bB, *bC;
-    ~DevPlan() { if (mem) cudaFree(mem); }
+    // M_p tables of the product-parallel schedule per level, made on first use
+    mutable std::mutex mt_mu;
+    mutable void* mtab[3] = {nullptr, nullptr, nullptr};
+    ~DevPlan()
+    {
+        if (mem) cudaFree(mem);
+        for (void* p : mtab)
+            if (p) cudaFree(p);
+    }
 };
 
 std::mutex g_cache_mu;
@@ -140,6 +149,26 @@ int get_plan(const tblis_tensor* const T[3], const label_type* const I[3], int d
     std::lock_guard<std::mutex> lk(g_cache_mu);
     g_cache.emplace_front(key, dp);
     while (g_cache.size() > CACHE_MAX) g_cache.pop_back();
+    return TBLIS_STRA_SUCCESS;
+}
+
+// Device copy of the M_p tables of plan t at `level` (made once per plan and
+// level; the layout follows C's faster bundle, fixed by the plan).
+int plan_m_tables(const DevPlan& t, int level, int64_t ms, int64_t ns, int64_t nb, bool col_major,
+                  const int64_t*& out)
+{
+    std::lock_guard<std::mutex> lk(t.mt_mu);
+    if (!t.mtab[level])
+    {
+        std::vector<int64_t> h((size_t)(ms + ns + nb));
+        dense_m_tables(ms, ns, nb, col_major, h.data());
+        void* d = nullptr;
+        if (cudaMalloc(&d, h.size() * sizeof(int64_t)) != cudaSuccess) { cudaGetLastError(); return TBLIS_STRA_ERR_ALLOC; }
+        const int s = upload_complete(d, h.data(), h.size() * sizeof(int64_t));
+        if (s) { cudaFree(d); return s; }
+        t.mtab[level] = d;
+    }
+    out = static_cast<const int64_t*>(t.mtab[level]);
     return TBLIS_STRA_SUCCESS;
 }
 
@@ -285,10 +314,21 @@ void set_grid(DmmaArgs& a, int64_t ms, int64_t ns, int64_t ks)
 int run_fp64_packed(int level, const GemmView& g, const DevPlan& t, const double* A, const double* B,
                     double* C, cudaStream_t st, int sms, bool blocking, int* shared_err)
 {
-    const size_t ws_group = fp64_packed_group_workspace_bytes(level, g);
-    const size_t ws = ws_group <= t_ws_limit ? ws_group : fp64_packed_workspace_bytes(level, g);
-    Scratch buf, errbuf;
+    // Product-parallel when one product's tiles would leave SMs idle (fewer
+    // than two per SM) and its workspace is allowed.
+    const PackGeom pg = pack_geom(level, g);
+    const size_t ws_par = level >= 1 ? fp64_parallel_workspace_bytes(level, g) : 0;
+    const bool parallel = level >= 1 && t_product_parallel != 0 && ws_par <= t_ws_limit &&
+                          (t_product_parallel == 1 || g.batch * pg.tm * pg.tn < 2 * (int64_t)sms);
+    const bool m_col_major = g.unit_rsC != 0 && (g.unit_csC == 0 || g.unit_rsC <= g.unit_csC);
+    const int64_t* mtab = nullptr;
     int s;
+    if (parallel && (s = plan_m_tables(t, level, pg.ms, pg.ns, (int64_t)product_table(level).prod.size() * g.batch,
+                                       m_col_major, mtab)))
+        return s;
+    const size_t ws_group = fp64_packed_group_workspace_bytes(level, g);
+    const size_t ws = parallel ? ws_par : ws_group <= t_ws_limit ? ws_group : fp64_packed_workspace_bytes(level, g);
+    Scratch buf, errbuf;
     if ((s = buf.alloc(ws, st))) return s;
     int* err = shared_err;
     if (!err)
@@ -298,7 +338,8 @@ int run_fp64_packed(int level, const GemmView& g, const DevPlan& t, const double
         err = static_cast<int*>(errbuf.p);
     }
     const int64_t* tb[9] = {t.rsA, t.rsC, t.csB, t.csC, t.ksA, t.ksB, t.bA, t.bB, t.bC};
-    s = run_fp64_packed_enqueue(level, g, tb, A, B, C, st, sms, buf.p, ws, err);
+    s = parallel ? run_fp64_parallel_enqueue(level, g, tb, A, B, C, st, sms, buf.p, ws, mtab, m_col_major, err)
+                 : run_fp64_packed_enqueue(level, g, tb, A, B, C, st, sms, buf.p, ws, err);
     if (s) return s;
     if (blocking && !shared_err)
     {
@@ -671,6 +712,96 @@ int run_fp64_packed_enqueue(int level, const GemmView& g, const int64_t* const t
         if (s) return s;
         TSB_CUDA(launch_packed_gemm(packed_product_args(level, pr, g, pg, tb, S, T, C, err), st, sms));
     }
+    return TBLIS_STRA_SUCCESS;
+}
+
+size_t fp64_parallel_workspace_bytes(int level, const GemmView& g)
+{
+    const PackGeom pg = pack_geom(level, g);
+    const size_t np = product_table(level).prod.size();
+    const size_t st = (np * (pg.s_elems + pg.t_elems) * sizeof(double) + 255) / 256 * 256;
+    return st + np * (size_t)(g.batch * pg.ms * pg.ns) * sizeof(double);
+}
+
+void dense_m_tables(int64_t ms, int64_t ns, int64_t nb, bool col_major, int64_t* out)
+{
+    for (int64_t i = 0; i < ms; i++) out[i] = col_major ? i : i * ns;
+    for (int64_t j = 0; j < ns; j++) out[ms + j] = col_major ? j * ms : j;
+    for (int64_t b = 0; b < nb; b++) out[ms + ns + b] = b * ms * ns;
+}
+
+// The products' sums are packed back to back (S_p = S + p * s_elems), so the
+// GEMM sees product p, batch entry b as batch entry p * batch + b of one
+// problem of 7^L * batch entries writing M_p = M + p * batch * ms * ns.
+int run_fp64_parallel_enqueue(int level, const GemmView& g, const int64_t* const tb[9],
+                              const double* A, const double* B, double* C, cudaStream_t st, int sms,
+                              void* ws, size_t ws_bytes, const int64_t* mtab, bool col_major, int* err)
+{
+    if (level < 1) return TBLIS_STRA_ERR_ARG;
+    const PackGeom pg = pack_geom(level, g);
+    if (!pg.fits) return TBLIS_STRA_ERR_TOO_LARGE;
+    if (ws_bytes < fp64_parallel_workspace_bytes(level, g)) return TBLIS_STRA_ERR_ALLOC;
+    const ProductTable& tab = product_table(level);
+    const int np = (int)tab.prod.size();
+    double* S = static_cast<double*>(ws);
+    double* T = S + (size_t)np * pg.s_elems;
+    double* M = reinterpret_cast<double*>(static_cast<char*>(ws) +
+                                          ((size_t)np * (pg.s_elems + pg.t_elems) * sizeof(double) + 255) / 256 * 256);
+    int s;
+    if (pack_group(level, 0, 0))
+    {
+        for (int G = 0; G < np / 7; G++)
+        {
+            double* outS[7];
+            double* outT[7];
+            for (int q = 0; q < 7; q++)
+            {
+                outS[q] = S + (size_t)(G * 7 + q) * pg.s_elems;
+                outT[q] = T + (size_t)(G * 7 + q) * pg.t_elems;
+            }
+            if ((s = enqueue_pack_group(level, 0, G, g, pg, tb, A, outS, st))) return s;
+            if ((s = enqueue_pack_group(level, 1, G, g, pg, tb, B, outT, st))) return s;
+        }
+    }
+    else
+    {
+        for (int p = 0; p < np; p++)
+            if ((s = enqueue_pack_product(tab.prod[(size_t)p], g, pg, tb, A, B, S + (size_t)p * pg.s_elems,
+                                          T + (size_t)p * pg.t_elems, st)))
+                return s;
+    }
+
+    PackedGemmArgs ga{};
+    ga.err = err;
+    ga.C = M;
+    ga.rsC = mtab; ga.csC = mtab + pg.ms; ga.bC = mtab + pg.ms + pg.ns;
+    ga.m = pg.ms; ga.n = pg.ns; ga.ms = pg.ms; ga.ns = pg.ns; ga.k_pad = pg.k_pad;
+    ga.tiles_m = pg.tm; ga.tiles_n = pg.tn; ga.batch = (int64_t)np * g.batch;
+    ga.alpha = 1.0; ga.beta = 0.0;
+    ga.H = 1; ga.nprod = 1;
+    ga.S[0] = S; ga.T[0] = T;
+    ga.nc[0] = 1; ga.c_s[0][0] = 1; ga.c_first[0][0] = 1;
+    TSB_CUDA(launch_packed_gemm(ga, st, sms));
+
+    CombineArgs c{};
+    c.C = C; c.rsC = tb[1]; c.csC = tb[3]; c.bC = tb[8];
+    c.m = g.m; c.n = g.n; c.ms = pg.ms; c.ns = pg.ns; c.batch = g.batch;
+    c.M = M; c.m_pstride = g.batch * pg.ms * pg.ns;
+    c.alpha = g.alpha; c.beta = g.beta;
+    c.H = tab.H; c.col_major = col_major ? 1 : 0;
+    for (int p = 0; p < np; p++)
+    {
+        const Product& pr = tab.prod[(size_t)p];
+        for (int q = 0; q < pr.nc; q++)
+        {
+            const int h = pr.c[q].r * tab.H + pr.c[q].c;
+            if (h < 0 || h >= 16 || c.cnt[h] >= 16) return TBLIS_STRA_ERR_UNSUPPORTED;
+            c.prod[h][c.cnt[h]] = (int8_t)p;
+            c.sign[h][c.cnt[h]] = pr.c[q].sign;
+            c.cnt[h]++;
+        }
+    }
+    TSB_CUDA(launch_combine(c, st));
     return TBLIS_STRA_SUCCESS;
 }
 
@@ -1392,6 +1523,15 @@ int tblis_stra_set_fp32_terms(int terms)
 }
 
 int tblis_stra_get_fp32_terms(void) { return tsb::t_fp32_terms; }
+
+int tblis_stra_set_product_parallel(int mode)
+{
+    if (mode < -1 || mode > 1) return TBLIS_STRA_ERR_ARG;
+    tsb::t_product_parallel = mode;
+    return TBLIS_STRA_SUCCESS;
+}
+
+int tblis_stra_get_product_parallel(void) { return tsb::t_product_parallel; }
 
 int tblis_stra_last_status(void) { return tsb::t_status; }
 

@@ -106,6 +106,25 @@ struct ScatterAddArgs
     int8_t c_r[4], c_c[4], c_s[4], c_first[4];
 };
 
+// Products run side by side into their own M_p (dense ms x ns per batch entry,
+// M_p at M + p * m_pstride, column-major when col_major, else row-major), then
+// for every C block position h = hr * H + hc:
+//   C[h] = alpha * sum_{i < cnt[h]} sign[h][i] * M_{prod[h][i]} + beta * C[h]
+// (beta * C read only when beta != 0).  Up to 16 positions of 16 terms: the
+// 4 x 4 grid of a level-2 Strassen.
+struct CombineArgs
+{
+    double* C;
+    const int64_t* rsC; const int64_t* csC; const int64_t* bC;
+    int64_t m, n, ms, ns, batch;
+    const double* M;
+    int64_t m_pstride;
+    double alpha, beta;
+    int H, col_major;
+    int8_t cnt[16];
+    int8_t prod[16][16], sign[16][16];
+};
+
 // ---- packed operands -------------------------------------------------------
 //
 // A Strassen operand sum (or a plain operand) packed into tile order: for
@@ -303,6 +322,7 @@ cudaError_t launch_scale(const ScaleArgs& args, cudaStream_t stream);
 cudaError_t launch_scale_f32(const ScaleF32Args& args, cudaStream_t stream);
 cudaError_t launch_sum_gather(const SumGatherArgs& args, cudaStream_t stream);
 cudaError_t launch_scatter_add(const ScatterAddArgs& args, cudaStream_t stream);
+cudaError_t launch_combine(const CombineArgs& args, cudaStream_t stream);
 
 // Number of kernels this library has launched (all launchers count).
 unsigned long long launches();

@@ -63,6 +63,18 @@ int run_fp64_packed_enqueue(int level, const GemmView& g, const int64_t* const t
                             const double* A, const double* B, double* C, cudaStream_t st, int sms,
                             void* ws, size_t ws_bytes, int* err);
 
+// Product-parallel ABC schedule (L >= 1) on caller workspace: every
+// product's sums packed (S_p, T_p), one GEMM launch over all 7^L products
+// into M_p (dense ms x ns per batch entry), then one combine launch forming
+// each C block from the M_p.  mtab: the M_p row, column and batch tables
+// (dense_m_tables); col_major: M's layout.
+size_t fp64_parallel_workspace_bytes(int level, const GemmView& g);
+int run_fp64_parallel_enqueue(int level, const GemmView& g, const int64_t* const tb[9],
+                              const double* A, const double* B, double* C, cudaStream_t st, int sms,
+                              void* ws, size_t ws_bytes, const int64_t* mtab, bool col_major, int* err);
+// Host copy of those tables: rows[ms], cols[ns], batch[nb].
+void dense_m_tables(int64_t ms, int64_t ns, int64_t nb, bool col_major, int64_t* out);
+
 // Split-BF16 schedule of one FP32 contraction on caller workspace.
 size_t fp32_workspace_bytes(int level, const GemmView& g, int terms);
 // The same with the 7 split sums of a product group held at once (L >= 1);

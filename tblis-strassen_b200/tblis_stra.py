@@ -124,6 +124,9 @@ def _load() -> ctypes.CDLL:
     lib.tblis_stra_kernel_timing.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong),
                                              ctypes.POINTER(ctypes.c_double)]
     lib.tblis_stra_kernel_timing.restype = ctypes.c_int
+    lib.tblis_stra_set_product_parallel.argtypes = [ctypes.c_int]
+    lib.tblis_stra_set_product_parallel.restype = ctypes.c_int
+    lib.tblis_stra_get_product_parallel.restype = ctypes.c_int
     lib.tblis_stra_set_fp32_terms.argtypes = [ctypes.c_int]
     lib.tblis_stra_set_fp32_terms.restype = ctypes.c_int
     lib.tblis_stra_get_fp32_terms.restype = ctypes.c_int
@@ -364,6 +367,16 @@ class Batch:
 
 
 KERNEL_KINDS = {"fused": 0, "pack": 1, "packed_gemm": 2, "aux": 3, "split_gemm": 4}
+
+
+def set_product_parallel(mode: int) -> None:
+    """Product-parallel ABC schedule for small grids: -1 automatic (default),
+    0 never, 1 whenever its workspace fits."""
+    _check(lib.tblis_stra_set_product_parallel(mode))
+
+
+def get_product_parallel() -> int:
+    return int(lib.tblis_stra_get_product_parallel())
 
 
 def set_fp32_terms(terms: int) -> None:

@@ -55,6 +55,17 @@ def test_impl_knob(tsb):
     assert tsb.get_impl() == 1
 
 
+def test_product_parallel_knob(tsb):
+    assert tsb.get_product_parallel() == -1
+    for mode in (0, 1, -1):
+        tsb.set_product_parallel(mode)
+        assert tsb.get_product_parallel() == mode
+    for bad in (2, -2):
+        with pytest.raises(tsb.TblisStraError):
+            tsb.set_product_parallel(bad)
+    assert tsb.get_product_parallel() == -1
+
+
 def test_status_strings(tsb):
     for s in range(12):
         assert tsb.status_string(s) != "unknown status"

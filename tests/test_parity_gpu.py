@@ -35,12 +35,15 @@ def to_dev(x, cuda):
     return out
 
 
-@pytest.fixture(params=["packed", "packed_single", "fused"])
+@pytest.fixture(params=["packed", "packed_single", "packed_parallel", "fused"])
 def schedule(request, tsb, monkeypatch):
-    """ABC runs packed operand sums (default: at L >= 1 the 7 sums of a product
-    group formed in one pass), packed sums one product at a time (workspace
-    limited to one product's S and T), or, with no workspace, the fully fused
-    kernel; all must meet the same bound."""
+    """ABC runs packed operand sums (at L >= 1 the 7 sums of a product group
+    formed in one pass, the group's products run tile by tile in one GEMM),
+    packed sums one product at a time (workspace limited to one product's S
+    and T), all products side by side into M_p and one combine pass
+    (product-parallel, the automatic choice for small grids), or, with no
+    workspace, the fully fused kernel; all must meet the same bound."""
+    tsb.set_product_parallel(1 if request.param == "packed_parallel" else 0)
     if request.param == "packed_single":
         orig = tsb.contract
 
@@ -56,6 +59,7 @@ def schedule(request, tsb, monkeypatch):
         tsb.set_workspace_limit(None if request.param == "packed" else 0)
     yield request.param
     tsb.set_workspace_limit(None)
+    tsb.set_product_parallel(-1)
 
 
 def single_product_bytes(tsb, level, A, ia, B, ib, C, ic):
@@ -198,6 +202,27 @@ def test_async_stream_entry_point(tsb, cuda):
     assert torch.allclose(C, A @ B, atol=1e-12)
 
 
+@pytest.mark.parametrize("order", ["F", "C"])
+@pytest.mark.parametrize("level", [1, 2])
+def test_product_parallel_batch_and_beta0(tsb, cuda, level, order):
+    """Product-parallel ABC with a batch label, ragged blocks, both M layouts
+    (C column- or row-major) and beta = 0 over a NaN-filled C: C is written,
+    never read."""
+    ext = dict(i=131, j=67, k=150, z=3)
+    A = oracle.uniform((ext["i"], ext["k"], ext["z"]), 4, order)
+    B = oracle.uniform((ext["k"], ext["j"], ext["z"]), 5, order)
+    C0 = np.full((ext["i"], ext["j"], ext["z"]), np.nan, order=order)
+    R = np.zeros(C0.shape, order=order)
+    oracle.contract(-1.5, A, "ikz", B, "kjz", 0.0, R, "ijz")
+    tsb.set_product_parallel(1)
+    try:
+        C = run_gpu(tsb, cuda, level, 1, -1.5, A, "ikz", B, "kjz", 0.0, C0, "ijz")
+    finally:
+        tsb.set_product_parallel(-1)
+    assert np.isfinite(C).all()
+    assert np.abs(C - R).max() <= tol(level, ext["k"], A, B, -1.5)
+
+
 def test_launch_counter_moves(tsb, cuda):
     A = oracle.uniform((16, 16), 1)
     tsb.set_workspace_limit(0)
@@ -209,14 +234,22 @@ def test_launch_counter_moves(tsb, cuda):
         tsb.set_workspace_limit(None)
     before = tsb.launch_count()
     run_gpu(tsb, cuda, 1, 1, 1.0, A, "ik", A, "kj", 0.0, A, "ij")
-    assert tsb.launch_count() == before + 3         # packed ABC: pack 7 S, pack 7 T, one GEMM for the group
-    tsb.set_workspace_limit(single_product_bytes(tsb, 1, A, "ik", A, "kj", A, "ij"))
+    assert tsb.launch_count() == before + 4         # small grid: pack 7 S, pack 7 T, GEMM of all 7, combine
+    before = tsb.launch_count()
+    run_gpu(tsb, cuda, 2, 1, 1.0, A, "ik", A, "kj", 0.0, A, "ij")
+    assert tsb.launch_count() == before + 16        # L=2: 7 groups x 2 packs, GEMM of all 49, combine
+    tsb.set_product_parallel(0)
     try:
+        before = tsb.launch_count()
+        run_gpu(tsb, cuda, 1, 1, 1.0, A, "ik", A, "kj", 0.0, A, "ij")
+        assert tsb.launch_count() == before + 3     # grouped: pack 7 S, pack 7 T, one GEMM for the group
+        tsb.set_workspace_limit(single_product_bytes(tsb, 1, A, "ik", A, "kj", A, "ij"))
         before = tsb.launch_count()
         run_gpu(tsb, cuda, 1, 1, 1.0, A, "ik", A, "kj", 0.0, A, "ij")
         assert tsb.launch_count() == before + 21    # one product at a time: 7 x (pack S, pack T, GEMM)
     finally:
         tsb.set_workspace_limit(None)
+        tsb.set_product_parallel(-1)
 
 
 @pytest.mark.parametrize("level", [1, 2])
