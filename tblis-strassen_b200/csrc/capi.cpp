@@ -351,6 +351,50 @@ int run_fp64_packed(int level, const GemmView& g, const DevPlan& t, const double
     return TBLIS_STRA_SUCCESS;
 }
 
+// Naive's explicit operand sums of product pr as dense temporaries
+// S (ms x ks, k fastest) and T (ks x ns, n fastest) per batch entry
+// (straprim_naive2, src/stra_internal/3t/straprim_common.hpp:70-157).
+int enqueue_sum_gather(const Product& pr, const GemmView& g, const DevPlan& t, int64_t ms, int64_t ns,
+                       int64_t ks, const double* A, const double* B, double* S, double* T, cudaStream_t st)
+{
+    SumGatherArgs sa{};
+    sa.X = A; sa.rsX = t.rsA; sa.csX = t.ksA; sa.bX = t.bA;
+    sa.rows_full = g.m; sa.cols_full = g.k; sa.rows = ms; sa.cols = ks;
+    sa.batch = g.batch; sa.nt = pr.na; sa.out = S;
+    for (int i = 0; i < pr.na; i++) { sa.t_r[i] = pr.a[i].r; sa.t_c[i] = pr.a[i].c; sa.t_s[i] = pr.a[i].sign; }
+    TSB_CUDA(launch_sum_gather(sa, st));
+    SumGatherArgs sb{};
+    sb.X = B; sb.rsX = t.ksB; sb.csX = t.csB; sb.bX = t.bB;
+    sb.rows_full = g.k; sb.cols_full = g.n; sb.rows = ks; sb.cols = ns;
+    sb.batch = g.batch; sb.nt = pr.nb; sb.out = T;
+    for (int i = 0; i < pr.nb; i++) { sb.t_r[i] = pr.b[i].r; sb.t_c[i] = pr.b[i].c; sb.t_s[i] = pr.b[i].sign; }
+    TSB_CUDA(launch_sum_gather(sb, st));
+    return TBLIS_STRA_SUCCESS;
+}
+
+// Naive product pr on the packed GEMM: its dense sums S and T (tables St,
+// Tt), then those packed in tile order into PS and PT.
+int enqueue_naive_product(const Product& pr, const GemmView& g, const DevPlan& t, const PackGeom& pg,
+                          const double* A, const double* B, double* S, double* T, const DenseTables& St,
+                          const DenseTables& Tt, double* PS, double* PT, cudaStream_t st)
+{
+    int s = enqueue_sum_gather(pr, g, t, pg.ms, pg.ns, pg.ks, A, B, S, T, st);
+    if (s) return s;
+    PackArgs pa{};
+    pa.X = S; pa.rs = St.rows; pa.ks = St.cols; pa.bX = St.bat;
+    pa.rows_full = pg.ms; pa.k_full = pg.ks; pa.rows_blk = pg.ms; pa.k_blk = pg.ks;
+    pa.nt = 1; pa.t_s[0] = 1;
+    pa.tiles = pg.tm; pa.k_pad = pg.k_pad; pa.batch = g.batch; pa.kfast = 1; pa.out = PS;
+    TSB_CUDA(launch_pack(pa, st));
+    PackArgs pb{};
+    pb.X = T; pb.rs = Tt.cols; pb.ks = Tt.rows; pb.bX = Tt.bat;
+    pb.rows_full = pg.ns; pb.k_full = pg.ks; pb.rows_blk = pg.ns; pb.k_blk = pg.ks;
+    pb.nt = 1; pb.t_s[0] = 1;
+    pb.tiles = pg.tn; pb.k_pad = pg.k_pad; pb.batch = g.batch; pb.kfast = 0; pb.out = PT;
+    TSB_CUDA(launch_pack(pb, st));
+    return TBLIS_STRA_SUCCESS;
+}
+
 // shared_err (may be null): a device flag of the caller's that the kernels'
 // timed-out waits set; the caller then reads it, and `blocking` checks none.
 int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
@@ -383,6 +427,67 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
         a.H = a.Hc = H;
         for (int p = 0; p < a.nprod; p++) a.prod[p] = to_dev(tab.prod[p]);
         TSB_CUDA(launch_dmma(a, max_terms(tab), st, sms));
+        return TBLIS_STRA_SUCCESS;
+    }
+
+    // AB / Naive with room for every product's M: the sums of all products
+    // packed (AB straight from A and B; Naive from its dense temporaries S and
+    // T, formed product by product), one GEMM launch over all products into
+    // their M_p, then one pass adds sum_p W[h][p] M_p into every C block.
+    const PackGeom pgp = pack_geom(level, g);
+    if (pgp.fits && t_product_parallel != 0 &&
+        fp64_parallel_workspace_bytes(level, g) + (impl == 3 ? (size_t)(g.batch * (ms + ns) * ks) * 8 : 0) <=
+            t_ws_limit)
+    {
+        const bool col_major = g.unit_rsC != 0 && (g.unit_csC == 0 || g.unit_rsC <= g.unit_csC);
+        const int np = (int)tab.prod.size();
+        const int64_t* mtab = nullptr;
+        int s;
+        if ((s = plan_m_tables(t, level, pgp.ms, pgp.ns, (int64_t)np * g.batch, col_major, mtab))) return s;
+        Scratch wsbuf, errbuf;
+        const size_t ws = fp64_parallel_workspace_bytes(level, g);
+        if ((s = wsbuf.alloc(ws, st))) return s;
+        int* err = shared_err;
+        if (!err)
+        {
+            if ((s = errbuf.alloc(sizeof(int), st))) return s;
+            TSB_CUDA(cudaMemsetAsync(errbuf.p, 0, sizeof(int), st));
+            err = static_cast<int*>(errbuf.p);
+        }
+        const int64_t* tb[9] = {t.rsA, t.rsC, t.csB, t.csC, t.ksA, t.ksB, t.bA, t.bB, t.bC};
+        if (impl == 2)
+        {
+            if ((s = run_fp64_parallel_enqueue(level, g, tb, A, B, C, st, sms, wsbuf.p, ws, mtab, col_major, err)))
+                return s;
+        }
+        else
+        {
+            Scratch Sd, Td;
+            DenseTables St, Tt;
+            if ((s = Sd.alloc((size_t)(g.batch * ms * ks) * sizeof(double), st))) return s;
+            if ((s = Td.alloc((size_t)(g.batch * ks * ns) * sizeof(double), st))) return s;
+            if ((s = St.build(ms, ks, g.batch, st))) return s;
+            if ((s = Tt.build(ks, ns, g.batch, st))) return s;
+            double* PS = static_cast<double*>(wsbuf.p);
+            double* PT = PS + (size_t)np * pgp.s_elems;
+            for (int p = 0; p < np; p++)
+            {
+                const Product& pr = tab.prod[(size_t)p];
+                if ((s = enqueue_naive_product(pr, g, t, pgp, A, B, static_cast<double*>(Sd.p),
+                                               static_cast<double*>(Td.p), St, Tt,
+                                               PS + (size_t)p * pgp.s_elems, PT + (size_t)p * pgp.t_elems, st)))
+                    return s;
+            }
+            if ((s = enqueue_products_and_combine(level, g, tb, C, st, sms, wsbuf.p, mtab, col_major, err)))
+                return s;
+        }
+        if (blocking && !shared_err)
+        {
+            int flag = 0;
+            TSB_CUDA(cudaMemcpyAsync(&flag, errbuf.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            TSB_CUDA(cudaStreamSynchronize(st));
+            if (flag) return TBLIS_STRA_ERR_TIMEOUT;
+        }
         return TBLIS_STRA_SUCCESS;
     }
 
@@ -429,20 +534,11 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
 
     for (const Product& pr : tab.prod)
     {
-        if (impl == 3)
+        if (impl == 3 && !pg.fits)
         {
-            SumGatherArgs sa{};
-            sa.X = A; sa.rsX = t.rsA; sa.csX = t.ksA; sa.bX = t.bA;
-            sa.rows_full = g.m; sa.cols_full = g.k; sa.rows = ms; sa.cols = ks;
-            sa.batch = g.batch; sa.nt = pr.na; sa.out = static_cast<double*>(Sbuf.p);
-            for (int i = 0; i < pr.na; i++) { sa.t_r[i] = pr.a[i].r; sa.t_c[i] = pr.a[i].c; sa.t_s[i] = pr.a[i].sign; }
-            TSB_CUDA(launch_sum_gather(sa, st));
-            SumGatherArgs sb{};
-            sb.X = B; sb.rsX = t.ksB; sb.csX = t.csB; sb.bX = t.bB;
-            sb.rows_full = g.k; sb.cols_full = g.n; sb.rows = ks; sb.cols = ns;
-            sb.batch = g.batch; sb.nt = pr.nb; sb.out = static_cast<double*>(Tbuf.p);
-            for (int i = 0; i < pr.nb; i++) { sb.t_r[i] = pr.b[i].r; sb.t_c[i] = pr.b[i].c; sb.t_s[i] = pr.b[i].sign; }
-            TSB_CUDA(launch_sum_gather(sb, st));
+            if ((s = enqueue_sum_gather(pr, g, t, ms, ns, ks, A, B, static_cast<double*>(Sbuf.p),
+                                        static_cast<double*>(Tbuf.p), st)))
+                return s;
         }
         if (pg.fits)
         {
@@ -452,19 +548,9 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
             }
             else
             {
-                // the dense temporaries in tile order: S (ms x ks, k fastest), T (ks x ns, n fastest)
-                PackArgs pa{};
-                pa.X = static_cast<const double*>(Sbuf.p); pa.rs = St.rows; pa.ks = St.cols; pa.bX = St.bat;
-                pa.rows_full = ms; pa.k_full = ks; pa.rows_blk = ms; pa.k_blk = ks;
-                pa.nt = 1; pa.t_s[0] = 1;
-                pa.tiles = pg.tm; pa.k_pad = pg.k_pad; pa.batch = g.batch; pa.kfast = 1; pa.out = PS;
-                TSB_CUDA(launch_pack(pa, st));
-                PackArgs pb{};
-                pb.X = static_cast<const double*>(Tbuf.p); pb.rs = Tt.cols; pb.ks = Tt.rows; pb.bX = Tt.bat;
-                pb.rows_full = ns; pb.k_full = ks; pb.rows_blk = ns; pb.k_blk = ks;
-                pb.nt = 1; pb.t_s[0] = 1;
-                pb.tiles = pg.tn; pb.k_pad = pg.k_pad; pb.batch = g.batch; pb.kfast = 0; pb.out = PT;
-                TSB_CUDA(launch_pack(pb, st));
+                if ((s = enqueue_naive_product(pr, g, t, pg, A, B, static_cast<double*>(Sbuf.p),
+                                               static_cast<double*>(Tbuf.p), St, Tt, PS, PT, st)))
+                    return s;
             }
             PackedGemmArgs ga{};
             ga.S[0] = PS; ga.T[0] = PT; ga.C = M;
@@ -745,8 +831,6 @@ int run_fp64_parallel_enqueue(int level, const GemmView& g, const int64_t* const
     const int np = (int)tab.prod.size();
     double* S = static_cast<double*>(ws);
     double* T = S + (size_t)np * pg.s_elems;
-    double* M = reinterpret_cast<double*>(static_cast<char*>(ws) +
-                                          ((size_t)np * (pg.s_elems + pg.t_elems) * sizeof(double) + 255) / 256 * 256);
     int s;
     if (pack_group(level, 0, 0))
     {
@@ -770,7 +854,22 @@ int run_fp64_parallel_enqueue(int level, const GemmView& g, const int64_t* const
                                           T + (size_t)p * pg.t_elems, st)))
                 return s;
     }
+    return enqueue_products_and_combine(level, g, tb, C, st, sms, ws, mtab, col_major, err);
+}
 
+// The GEMM over all products (their sums packed back to back at the start
+// of ws) into M_p, then the combine launch.
+int enqueue_products_and_combine(int level, const GemmView& g, const int64_t* const tb[9], double* C,
+                                 cudaStream_t st, int sms, void* ws, const int64_t* mtab, bool col_major,
+                                 int* err)
+{
+    const PackGeom pg = pack_geom(level, g);
+    const ProductTable& tab = product_table(level);
+    const int np = (int)tab.prod.size();
+    double* S = static_cast<double*>(ws);
+    double* T = S + (size_t)np * pg.s_elems;
+    double* M = reinterpret_cast<double*>(static_cast<char*>(ws) +
+                                          ((size_t)np * (pg.s_elems + pg.t_elems) * sizeof(double) + 255) / 256 * 256);
     PackedGemmArgs ga{};
     ga.err = err;
     ga.C = M;

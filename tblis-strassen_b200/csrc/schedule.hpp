@@ -72,6 +72,11 @@ size_t fp64_parallel_workspace_bytes(int level, const GemmView& g);
 int run_fp64_parallel_enqueue(int level, const GemmView& g, const int64_t* const tb[9],
                               const double* A, const double* B, double* C, cudaStream_t st, int sms,
                               void* ws, size_t ws_bytes, const int64_t* mtab, bool col_major, int* err);
+// Its second half alone, once the products' sums are packed in ws (S_p at
+// ws + p * s_elems doubles, then T_p).
+int enqueue_products_and_combine(int level, const GemmView& g, const int64_t* const tb[9], double* C,
+                                 cudaStream_t st, int sms, void* ws, const int64_t* mtab, bool col_major,
+                                 int* err);
 // Host copy of those tables: rows[ms], cols[ns], batch[nb].
 void dense_m_tables(int64_t ms, int64_t ns, int64_t nb, bool col_major, int64_t* out);
 
