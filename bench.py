@@ -335,6 +335,7 @@ def kernel_probe(args):
         tsb.set_fp32_terms(args.terms)
     if args.workspace is not None:
         tsb.set_workspace_limit(args.workspace)      # 0: the fully fused kernel
+    tsb.set_product_parallel(args.product_parallel)
     if args.kernels == "batch":
         # a 64-problem batched form (FP64, or FP32 with --dtype f32), executed twice
         del A, B, C
@@ -402,6 +403,8 @@ def main():
                     help="FP64 square and rank-k sweep over L = 0/1/2 and ABC/AB/Naive (one JSON line per shape)")
     ap.add_argument("--workspace", type=int, default=None,
                     help="--kernels probe: device workspace limit in bytes (0 = fully fused kernel)")
+    ap.add_argument("--product-parallel", type=int, default=-1, choices=[-1, 0, 1],
+                    help="--kernels probe: product-parallel schedule (-1 automatic, 0 never, 1 when it fits)")
     ap.add_argument("--kernels", default=None,
                     help="comma-separated levels: run one warm-up and one timed call per level "
                          "and print per-level times (profiling driver; no JSON line)")

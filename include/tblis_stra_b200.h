@@ -190,15 +190,17 @@ int tblis_stra_get_impl(void);
 int tblis_stra_set_workspace_limit(size_t bytes);
 size_t tblis_stra_get_workspace_limit(void);
 
-/* Product-parallel ABC schedule for small grids (no counterpart in the
- * reference, whose threads split each product's loops instead): when one
- * product has fewer 128 x 128 tiles than two per SM, the ABC variant at
- * L >= 1 packs every product's sums, runs all 7^L products side by side in
- * one GEMM launch into their own M_p, and forms each C block as
- * alpha * sum_p W[h][p] M_p + beta * C in one pass.  It needs
- * 7^L * (packed S and T + 8*batch*ms*ns) bytes within the workspace limit.
- * mode: -1 automatic (the default), 0 never, 1 whenever the workspace fits.
- * Per calling thread.  Returns 0 or TBLIS_STRA_ERR_ARG. */
+/* Product-parallel schedule (no counterpart in the reference, whose threads
+ * split each product's loops instead).  At L >= 1, when the last wave of one
+ * product's 128 x 128 tiles would leave more than a tenth of the SMs' time
+ * idle (fewer tiles than SMs included), ABC packs every product's sums, runs
+ * all 7^L products side by side in one GEMM launch into their own M_p, and
+ * forms each C block as alpha * sum_p W[h][p] M_p + beta * C in one pass;
+ * FP32 does the same on its split-BF16 path.  It needs 7^L * (packed sums +
+ * batch*ms*ns elements of M) bytes within the workspace limit.  AB and Naive
+ * (which hold M temporaries by design) always take this form when mode is
+ * not 0.  mode: -1 automatic (the default), 0 never, 1 whenever the
+ * workspace fits.  Per calling thread.  Returns 0 or TBLIS_STRA_ERR_ARG. */
 int tblis_stra_set_product_parallel(int mode);
 int tblis_stra_get_product_parallel(void);
 

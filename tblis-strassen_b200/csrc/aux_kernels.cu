@@ -13,15 +13,16 @@
 //                       156, 187-203, tensor2matrix.hpp:390-830).
 //   combine_kernel      C_h = alpha * sum_p W[h][p] M_p + beta * C_h for every C
 //                       block h at once, after the products have run side by
-//                       side into their own M_p (small grids, where one product
-//                       has too few tiles for the SMs).
+//                       side into their own M_p (the product-parallel schedule):
+//                       each M_p is read once, C written once.
 //
-// All four are grid-stride loops over (batch, row, col) with the column index
-// fastest; the scatter vectors make the access pattern coalesced whenever the
-// fastest C (or X) mode is the column bundle's first mode.
+// The first three are grid-stride loops over (batch, row, col) with the column
+// index fastest; the scatter vectors make the access pattern coalesced
+// whenever the fastest C (or X) mode is the column bundle's first mode.
 #include "kernels.cuh"
 #include "timing.hpp"
 
+#include <algorithm>
 #include <atomic>
 
 namespace tsb {
@@ -122,52 +123,85 @@ __global__ void scatter_add_kernel(const ScatterAddArgs a)
     }
 }
 
-// One thread per C element: the terms of its block position, read from the
-// products' M at the same local (i, j), fastest index that of M's layout.
-__global__ void combine_kernel(const __grid_constant__ CombineArgs a)
+// One thread per local position (i, j) of every C block: it reads each
+// product's M_p there once, adds it (with sign) into the accumulators of the
+// product's block positions, kept in shared memory (column threadIdx.x of
+// acc[h]), then writes the H * H C elements.  M is read once in total.
+// Grid: x over the ms * ns local positions (fastest index that of M's
+// layout), y over batch entries.
+constexpr int COMBINE_THREADS = 256;
+
+template <class T>
+__global__ void __launch_bounds__(COMBINE_THREADS)
+combine_kernel(const __grid_constant__ CombineArgsT<T> a)
 {
-    const int H2 = a.H * a.H;
-    const int64_t per = a.ms * a.ns;
-    const int64_t total = (int64_t)H2 * a.batch * per;
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
-         e += (int64_t)gridDim.x * blockDim.x)
+    __shared__ double acc[16][COMBINE_THREADS];
+    const int tid = threadIdx.x;
+    const int H = a.H, H2 = H * H;
+    const uint32_t per = (uint32_t)(a.ms * a.ns);
+    const uint32_t fast = (uint32_t)(a.col_major ? a.ms : a.ns);
+    for (int64_t b = blockIdx.y; b < a.batch; b += gridDim.y)
     {
-        const int64_t loc = e % per;
-        const int64_t rest = e / per;
-        const int64_t b = rest % a.batch;
-        const int h = (int)(rest / a.batch);
-        const int64_t i = a.col_major ? loc % a.ms : loc / a.ns;
-        const int64_t j = a.col_major ? loc / a.ms : loc % a.ns;
-        const int64_t gi = (h / a.H) * a.ms + i, gj = (h % a.H) * a.ns + j;
-        if (gi >= a.m || gj >= a.n) continue;
-        const double* Mb = a.M + b * per + loc;
-        double v = 0.0;
-        for (int t = 0; t < a.cnt[h]; t++)
+        const T* __restrict__ Mb = a.M + b * (int64_t)per;
+        const int64_t cb = a.bC[b];
+        for (uint32_t loc = blockIdx.x * COMBINE_THREADS + tid; loc < per; loc += gridDim.x * COMBINE_THREADS)
         {
-            const double x = Mb[a.prod[h][t] * a.m_pstride];
-            v += a.sign[h][t] < 0 ? -x : x;
+            for (int h = 0; h < H2; h++) acc[h][tid] = 0.0;
+#pragma unroll 7
+            for (int p = 0; p < a.np; p++)
+            {
+                const double x = (double)Mb[p * a.m_pstride + loc];
+                for (int t = 0; t < a.nt[p]; t++)
+                    acc[a.th[p][t]][tid] += a.ts[p][t] < 0 ? -x : x;
+            }
+            const uint32_t q = loc / fast, r = loc - q * fast;
+            const int64_t i = a.col_major ? r : q, j = a.col_major ? q : r;
+            for (int hr = 0; hr < H; hr++)
+            {
+                const int64_t gi = hr * a.ms + i;
+                if (gi >= a.m) break;
+                const int64_t ro = cb + a.rsC[gi];
+                for (int hc = 0; hc < H; hc++)
+                {
+                    const int64_t gj = hc * a.ns + j;
+                    if (gj >= a.n) break;
+                    T* p = a.C + ro + a.csC[gj];
+                    const double v = acc[hr * H + hc][tid];
+                    *p = (T)(a.beta != 0.0 ? a.alpha * v + a.beta * (double)*p : a.alpha * v);
+                }
+            }
         }
-        double* p = a.C + a.bC[b] + a.rsC[gi] + a.csC[gj];
-        *p = a.beta != 0.0 ? a.alpha * v + a.beta * *p : a.alpha * v;
     }
 }
 
 }  // namespace
 
-cudaError_t launch_combine(const CombineArgs& a, cudaStream_t stream)
+template <class T>
+cudaError_t launch_combine_t(const CombineArgsT<T>& a, cudaStream_t stream)
 {
-    const int64_t total = (int64_t)a.H * a.H * a.batch * a.ms * a.ns;
-    if (total <= 0) return cudaSuccess;
-    if (a.H < 1 || a.H > 4) return cudaErrorInvalidValue;
-    for (int h = 0; h < a.H * a.H; h++)
-        if (a.cnt[h] < 0 || a.cnt[h] > 16) return cudaErrorInvalidValue;
+    const int64_t per = a.ms * a.ns;
+    if (per <= 0 || a.batch <= 0) return cudaSuccess;
+    if (a.H < 1 || a.H > 4 || a.np < 1 || a.np > MAX_COMBINE_PRODUCTS ||
+        per >= ((int64_t)1 << 32) - COMBINE_THREADS * (int64_t)65535)
+        return cudaErrorInvalidValue;
+    for (int p = 0; p < a.np; p++)
+    {
+        if (a.nt[p] < 0 || a.nt[p] > 4) return cudaErrorInvalidValue;
+        for (int t = 0; t < a.nt[p]; t++)
+            if (a.th[p][t] < 0 || a.th[p][t] >= a.H * a.H) return cudaErrorInvalidValue;
+    }
+    const dim3 grid((unsigned)std::min<int64_t>((per + COMBINE_THREADS - 1) / COMBINE_THREADS, 65535),
+                    (unsigned)std::min<int64_t>(a.batch, 65535));
     timing_begin(KK_AUX, stream);
-    combine_kernel<<<grid_for(total), THREADS, 0, stream>>>(a);
+    combine_kernel<T><<<grid, COMBINE_THREADS, 0, stream>>>(a);
     timing_end(KK_AUX, stream);
     cudaError_t err = cudaGetLastError();
     if (err == cudaSuccess) g_launches++;
     return err;
 }
+
+cudaError_t launch_combine(const CombineArgs& a, cudaStream_t stream) { return launch_combine_t(a, stream); }
+cudaError_t launch_combine(const CombineF32Args& a, cudaStream_t stream) { return launch_combine_t(a, stream); }
 
 cudaError_t launch_scale(const ScaleArgs& a, cudaStream_t stream)
 {

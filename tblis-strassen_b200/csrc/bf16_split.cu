@@ -457,14 +457,17 @@ __device__ __forceinline__ void split_gemm_body(const Src& src, int* err, unsign
                 const SplitGemmArgs& a = src.at(w, local);
                 decode(a, local, b, tm, tn);
                 const int64_t nk = a.nk;
-                const size_t planeA = (size_t)a.batch * a.tiles_m * nk * BLK;
-                const size_t planeB = (size_t)a.batch * a.tiles_n * nk * BLK;
+                // batch entry b = pp * pbatch + bl: entry bl of the pp-th plane set
+                const int64_t pb = a.pbatch > 0 ? a.pbatch : a.batch;
+                const int64_t pp = b / pb, bl = b - pp * pb;
+                const size_t planeA = (size_t)pb * a.tiles_m * nk * BLK;
+                const size_t planeB = (size_t)pb * a.tiles_n * nk * BLK;
                 for (int q = 0; q < a.nprod && ok; q++)
                 {
-                const unsigned char* srcA = reinterpret_cast<const unsigned char*>(a.A[q]) +
-                                            ((size_t)(b * a.tiles_m + tm) * nk) * BLK;
-                const unsigned char* srcB = reinterpret_cast<const unsigned char*>(a.B[q]) +
-                                            ((size_t)(b * a.tiles_n + tn) * nk) * BLK;
+                const unsigned char* srcA = reinterpret_cast<const unsigned char*>(a.A[q]) + pp * P * planeA +
+                                            ((size_t)(bl * a.tiles_m + tm) * nk) * BLK;
+                const unsigned char* srcB = reinterpret_cast<const unsigned char*>(a.B[q]) + pp * P * planeB +
+                                            ((size_t)(bl * a.tiles_n + tn) * nk) * BLK;
                 for (int64_t c = 0; c < nk; c++, it++)
                 {
                     const int s = it % STAGES;
@@ -569,9 +572,11 @@ __device__ __forceinline__ void split_gemm_body(const Src& src, int* err, unsign
                 colC[h * ST + dt] = (h < a.H && lj < a.ns && gj < a.n) ? a.csC[gj] : OFF_INVALID;
             }
             {
+                const int64_t pb = a.pbatch > 0 ? a.pbatch : a.batch;
+                const int64_t bl = b % pb;
                 const int64_t li = tm * ST + dt, lj = tn * ST + dt;
-                invr[dt] = li < a.ms ? a.invA[b * a.ms + li] : 0.f;
-                invc[dt] = lj < a.ns ? a.invB[b * a.ns + lj] : 0.f;
+                invr[dt] = li < a.ms ? a.invA[bl * a.ms + li] : 0.f;
+                invc[dt] = lj < a.ns ? a.invB[bl * a.ns + lj] : 0.f;
             }
             asm volatile("bar.sync 1, 128;\n" ::: "memory");
 

@@ -172,6 +172,21 @@ int plan_m_tables(const DevPlan& t, int level, int64_t ms, int64_t ns, int64_t n
     return TBLIS_STRA_SUCCESS;
 }
 
+// Whether the product-parallel form beats running each group's products
+// tile by tile (M's local index must fit 32 bits).  At L = 2 it does at every
+// size measured: a product's C tiles spread over up to 4 blocks, and with
+// products side by side each is written once (as M) and combined in one
+// pass.  At L = 1 it does when the last wave of one product's `tiles` on `sms`
+// SMs leaves more than a tenth of the launch idle (fewer tiles than SMs
+// included).
+bool parallel_pays(int level, int64_t tiles, int sms, int64_t ms, int64_t ns)
+{
+    if (ms * ns >= ((int64_t)1 << 31)) return false;
+    if (level >= 2) return true;
+    const int64_t rounds = (tiles + sms - 1) / sms;
+    return rounds * sms * 10 > tiles * 11;
+}
+
 int num_sms(int device)
 {
     static std::mutex mu;
@@ -314,12 +329,13 @@ void set_grid(DmmaArgs& a, int64_t ms, int64_t ns, int64_t ks)
 int run_fp64_packed(int level, const GemmView& g, const DevPlan& t, const double* A, const double* B,
                     double* C, cudaStream_t st, int sms, bool blocking, int* shared_err)
 {
-    // Product-parallel when one product's tiles would leave SMs idle (fewer
-    // than two per SM) and its workspace is allowed.
+    // Product-parallel when one product's tiles would leave SMs idle and its
+    // workspace is allowed.
     const PackGeom pg = pack_geom(level, g);
     const size_t ws_par = level >= 1 ? fp64_parallel_workspace_bytes(level, g) : 0;
     const bool parallel = level >= 1 && t_product_parallel != 0 && ws_par <= t_ws_limit &&
-                          (t_product_parallel == 1 || g.batch * pg.tm * pg.tn < 2 * (int64_t)sms);
+                          pg.ms * pg.ns < ((int64_t)1 << 31) &&
+                          (t_product_parallel == 1 || parallel_pays(level, g.batch * pg.tm * pg.tn, sms, pg.ms, pg.ns));
     const bool m_col_major = g.unit_rsC != 0 && (g.unit_csC == 0 || g.unit_rsC <= g.unit_csC);
     const int64_t* mtab = nullptr;
     int s;
@@ -435,7 +451,7 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
     // T, formed product by product), one GEMM launch over all products into
     // their M_p, then one pass adds sum_p W[h][p] M_p into every C block.
     const PackGeom pgp = pack_geom(level, g);
-    if (pgp.fits && t_product_parallel != 0 &&
+    if (pgp.fits && t_product_parallel != 0 && pgp.ms * pgp.ns < ((int64_t)1 << 31) &&
         fp64_parallel_workspace_bytes(level, g) + (impl == 3 ? (size_t)(g.batch * (ms + ns) * ks) * 8 : 0) <=
             t_ws_limit)
     {
@@ -888,16 +904,16 @@ int enqueue_products_and_combine(int level, const GemmView& g, const int64_t* co
     c.M = M; c.m_pstride = g.batch * pg.ms * pg.ns;
     c.alpha = g.alpha; c.beta = g.beta;
     c.H = tab.H; c.col_major = col_major ? 1 : 0;
+    if (np > MAX_COMBINE_PRODUCTS) return TBLIS_STRA_ERR_UNSUPPORTED;
+    c.np = np;
     for (int p = 0; p < np; p++)
     {
         const Product& pr = tab.prod[(size_t)p];
+        c.nt[p] = (int8_t)pr.nc;
         for (int q = 0; q < pr.nc; q++)
         {
-            const int h = pr.c[q].r * tab.H + pr.c[q].c;
-            if (h < 0 || h >= 16 || c.cnt[h] >= 16) return TBLIS_STRA_ERR_UNSUPPORTED;
-            c.prod[h][c.cnt[h]] = (int8_t)p;
-            c.sign[h][c.cnt[h]] = pr.c[q].sign;
-            c.cnt[h]++;
+            c.th[p][q] = (int8_t)(pr.c[q].r * tab.H + pr.c[q].c);
+            c.ts[p][q] = pr.c[q].sign;
         }
     }
     TSB_CUDA(launch_combine(c, st));
@@ -971,6 +987,58 @@ size_t fp32_group_workspace_bytes(int level, const GemmView& g, int terms)
     const size_t sc = ((size_t)g.batch * (ms + ns) * 2 * sizeof(float) + 255) / 256 * 256;
     return sc + 7 * (one - sc);
 }
+
+namespace {
+
+// The split sums of product group G of one operand (0 = A, 1 = B) from one
+// pass over it, scaled by `scale` and split into P bf16 planes at out[q].
+int enqueue_split_pack_group(int level, int operand, int G, const GemmView& g, const int64_t* const tb[9],
+                             const float* X, const float* scale, int P, void* const out[7], cudaStream_t st)
+{
+    const PackGroup* grp = pack_group(level, operand, G);
+    if (!grp) return TBLIS_STRA_ERR_UNSUPPORTED;
+    const int H = product_table(level).H;
+    const int64_t ms = cdiv(g.m, H), ns = cdiv(g.n, H), ks = cdiv(g.k, H);
+    SplitPackMultiArgs m{};
+    m.X = X;
+    if (operand == 0)
+    {
+        m.rs = tb[0]; m.ks = tb[4]; m.bX = tb[6];
+        m.rows_full = g.m; m.rows_blk = ms; m.tiles = cdiv(ms, SPLIT_TILE);
+        m.kfast = g.unit_ksA != 0 && (g.unit_rsA == 0 || g.unit_ksA < g.unit_rsA);
+    }
+    else
+    {
+        m.rs = tb[2]; m.ks = tb[5]; m.bX = tb[7];
+        m.rows_full = g.n; m.rows_blk = ns; m.tiles = cdiv(ns, SPLIT_TILE);
+        m.kfast = g.unit_ksB != 0 && (g.unit_csB == 0 || g.unit_ksB < g.unit_csB);
+    }
+    m.scale = scale;
+    m.k_full = g.k; m.k_blk = ks; m.nk = cdiv(ks, SPLIT_K); m.batch = g.batch; m.planes = P;
+    m.nt = grp->nt;
+    for (int c = 0; c < grp->nt; c++)
+    {
+        m.t_s[c] = grp->t_s[c];
+        for (int j = 0; j < 4; j++)
+        {
+            // block (row[j/2], col[j%2]) of the operand; B is packed n-major
+            const int br = grp->row[c][j / 2], bc = grp->col[c][j % 2];
+            m.prow[c][j] = (int8_t)(operand == 0 ? br : bc);
+            m.pk[c][j] = (int8_t)(operand == 0 ? bc : br);
+        }
+    }
+    m.nout = 7;
+    for (int q = 0; q < 7; q++)
+    {
+        m.o_n[q] = grp->o_n[q];
+        for (int i = 0; i < grp->o_n[q]; i++) { m.o_j[q][i] = grp->o_j[q][i]; m.o_s[q][i] = grp->o_s[q][i]; }
+        m.out[q] = out[q];
+    }
+    TSB_CUDA(launch_split_pack_multi(m, st));
+    return TBLIS_STRA_SUCCESS;
+}
+
+}  // namespace
 
 int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], const float* A,
                      const float* B, float* C, cudaStream_t st, int sms, void* ws, size_t ws_bytes,
@@ -1056,40 +1124,10 @@ int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], c
         {
             for (int operand = 0; operand < 2; operand++)
             {
-                const PackGroup* grp = pack_group(level, operand, G);
-                if (!grp) return TBLIS_STRA_ERR_UNSUPPORTED;
-                SplitPackMultiArgs m{};
-                if (operand == 0)
-                {
-                    m.X = A; m.rs = tb[0]; m.ks = tb[4]; m.bX = tb[6];
-                    m.rows_full = g.m; m.rows_blk = ms; m.scale = scaleA; m.tiles = tm; m.kfast = a_kfast;
-                }
-                else
-                {
-                    m.X = B; m.rs = tb[2]; m.ks = tb[5]; m.bX = tb[7];
-                    m.rows_full = g.n; m.rows_blk = ns; m.scale = scaleB; m.tiles = tn; m.kfast = b_kfast;
-                }
-                m.k_full = g.k; m.k_blk = ks; m.nk = nk; m.batch = g.batch; m.planes = P;
-                m.nt = grp->nt;
-                for (int c = 0; c < grp->nt; c++)
-                {
-                    m.t_s[c] = grp->t_s[c];
-                    for (int j = 0; j < 4; j++)
-                    {
-                        // block (row[j/2], col[j%2]) of the operand; B is packed n-major
-                        const int br = grp->row[c][j / 2], bc = grp->col[c][j % 2];
-                        m.prow[c][j] = (int8_t)(operand == 0 ? br : bc);
-                        m.pk[c][j] = (int8_t)(operand == 0 ? bc : br);
-                    }
-                }
-                m.nout = 7;
-                for (int q = 0; q < 7; q++)
-                {
-                    m.o_n[q] = grp->o_n[q];
-                    for (int i = 0; i < grp->o_n[q]; i++) { m.o_j[q][i] = grp->o_j[q][i]; m.o_s[q][i] = grp->o_s[q][i]; }
-                    m.out[q] = operand == 0 ? outA[q] : outB[q];
-                }
-                TSB_CUDA(launch_split_pack_multi(m, st));
+                const int s = enqueue_split_pack_group(level, operand, G, g, tb, operand == 0 ? A : B,
+                                                       operand == 0 ? scaleA : scaleB, P,
+                                                       operand == 0 ? outA : outB, st);
+                if (s) return s;
             }
             const Product* prs[7];
             for (int q = 0; q < 7; q++) prs[q] = &tab.prod[(size_t)(G * 7 + q)];
@@ -1125,6 +1163,106 @@ int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], c
     return TBLIS_STRA_SUCCESS;
 }
 
+size_t fp32_parallel_workspace_bytes(int level, const GemmView& g, int terms)
+{
+    const int H = product_table(level).H;
+    const size_t np = product_table(level).prod.size();
+    const int64_t ms = cdiv(g.m, H), ns = cdiv(g.n, H), ks = cdiv(g.k, H);
+    const int64_t nk = cdiv(ks, SPLIT_K);
+    const size_t blk = (size_t)SPLIT_TILE * SPLIT_K * 2;
+    const int P = terms == 3 ? 2 : 3;
+    const size_t sc = ((size_t)g.batch * (ms + ns) * 2 * sizeof(float) + 255) / 256 * 256;
+    const size_t planes = np * P * (size_t)g.batch * (cdiv(ms, SPLIT_TILE) + cdiv(ns, SPLIT_TILE)) * nk * blk;
+    return sc + planes + np * (size_t)(g.batch * ms * ns) * sizeof(float);
+}
+
+// Product-parallel split-BF16 schedule (L >= 1): row and column scales, the
+// split sums of every product (plane set p of A at planesA + p * bytesA, of B
+// likewise), one GEMM launch over all products (batch entry p * batch + b
+// reads plane set p) into M_p, then one combine launch into C.
+int run_fp32_parallel_enqueue(int level, const GemmView& g, const int64_t* const tb[9], const float* A,
+                              const float* B, float* C, cudaStream_t st, int sms, void* ws, size_t ws_bytes,
+                              int terms, const int64_t* mtab, bool col_major, int* err)
+{
+    if (level < 1) return TBLIS_STRA_ERR_ARG;
+    const ProductTable& tab = product_table(level);
+    const int H = tab.H;
+    const int np = (int)tab.prod.size();
+    const int64_t ms = cdiv(g.m, H), ns = cdiv(g.n, H), ks = cdiv(g.k, H);
+    const int64_t nk = cdiv(ks, SPLIT_K);
+    const int64_t tm = cdiv(ms, SPLIT_TILE), tn = cdiv(ns, SPLIT_TILE);
+    if (g.batch * tm > 65535 || g.batch * tn > 65535 || nk > 2147483647) return TBLIS_STRA_ERR_TOO_LARGE;
+    if (ws_bytes < fp32_parallel_workspace_bytes(level, g, terms)) return TBLIS_STRA_ERR_ALLOC;
+    const int P = terms == 3 ? 2 : 3;
+    const size_t blk = (size_t)SPLIT_TILE * SPLIT_K * 2;
+    const size_t sc = ((size_t)g.batch * (ms + ns) * 2 * sizeof(float) + 255) / 256 * 256;
+    float* scaleA = static_cast<float*>(ws);
+    float* invA = scaleA + g.batch * ms;
+    float* scaleB = invA + g.batch * ms;
+    float* invB = scaleB + g.batch * ns;
+    const size_t bytesA = (size_t)P * g.batch * tm * nk * blk, bytesB = (size_t)P * g.batch * tn * nk * blk;
+    char* planesA = static_cast<char*>(ws) + sc;
+    char* planesB = planesA + np * bytesA;
+    float* M = reinterpret_cast<float*>(planesB + np * bytesB);
+
+    SplitScaleArgs sa{A, tb[0], tb[4], tb[6], g.m, g.k, ms, H, g.batch, scaleA, invA};
+    TSB_CUDA(launch_split_scale(sa, st));
+    SplitScaleArgs sb{B, tb[2], tb[5], tb[7], g.n, g.k, ns, H, g.batch, scaleB, invB};
+    TSB_CUDA(launch_split_scale(sb, st));
+
+    if (!pack_group(level, 0, 0)) return TBLIS_STRA_ERR_UNSUPPORTED;
+    for (int G = 0; G < np / 7; G++)
+    {
+        void* outA[7];
+        void* outB[7];
+        for (int q = 0; q < 7; q++)
+        {
+            outA[q] = planesA + (size_t)(G * 7 + q) * bytesA;
+            outB[q] = planesB + (size_t)(G * 7 + q) * bytesB;
+        }
+        int s;
+        if ((s = enqueue_split_pack_group(level, 0, G, g, tb, A, scaleA, P, outA, st))) return s;
+        if ((s = enqueue_split_pack_group(level, 1, G, g, tb, B, scaleB, P, outB, st))) return s;
+    }
+
+    static const int8_t TA6[6] = {0, 0, 1, 0, 1, 2}, TB6[6] = {0, 1, 0, 2, 1, 0};
+    SplitGemmArgs ga{};
+    ga.A[0] = planesA; ga.B[0] = planesB; ga.C = M;
+    ga.rsC = mtab; ga.csC = mtab + ms; ga.bC = mtab + ms + ns;
+    ga.invA = invA; ga.invB = invB;
+    ga.m = ms; ga.n = ns; ga.ms = ms; ga.ns = ns; ga.nk = nk;
+    ga.tiles_m = tm; ga.tiles_n = tn; ga.batch = (int64_t)np * g.batch; ga.pbatch = g.batch;
+    ga.alpha = 1.f; ga.beta = 0.f;
+    ga.nprod = 1; ga.H = 1;
+    ga.nc[0] = 1; ga.c_s[0][0] = 1; ga.c_first[0][0] = 1;
+    ga.planes = P;
+    ga.nterms = P == 3 ? 6 : 3;
+    for (int i = 0; i < 6; i++) { ga.ta[i] = TA6[i]; ga.tb[i] = TB6[i]; }
+    ga.err = err;
+    TSB_CUDA(launch_split_gemm(ga, st, sms));
+
+    CombineF32Args c{};
+    c.C = C; c.rsC = tb[1]; c.csC = tb[3]; c.bC = tb[8];
+    c.m = g.m; c.n = g.n; c.ms = ms; c.ns = ns; c.batch = g.batch;
+    c.M = M; c.m_pstride = g.batch * ms * ns;
+    c.alpha = g.alpha; c.beta = g.beta;
+    c.H = H; c.col_major = col_major ? 1 : 0;
+    if (np > MAX_COMBINE_PRODUCTS) return TBLIS_STRA_ERR_UNSUPPORTED;
+    c.np = np;
+    for (int p = 0; p < np; p++)
+    {
+        const Product& pr = tab.prod[(size_t)p];
+        c.nt[p] = (int8_t)pr.nc;
+        for (int q = 0; q < pr.nc; q++)
+        {
+            c.th[p][q] = (int8_t)(pr.c[q].r * H + pr.c[q].c);
+            c.ts[p][q] = pr.c[q].sign;
+        }
+    }
+    TSB_CUDA(launch_combine(c, st));
+    return TBLIS_STRA_SUCCESS;
+}
+
 namespace {
 
 int run_fp32(int level, const GemmView& g, const DevPlan& t, const float* A, const float* B,
@@ -1140,8 +1278,23 @@ int run_fp32(int level, const GemmView& g, const DevPlan& t, const float* A, con
     const int terms = t_fp32_terms;
     Scratch wsbuf, errbuf;
     int s;
+    // Product-parallel when one product's 128 x 128 tiles would leave SMs
+    // idle and its workspace is allowed (as for FP64).
+    const int sms = num_sms(device);
+    const int H = product_table(level).H;
+    const int64_t tiles = g.batch * cdiv(cdiv(g.m, H), SPLIT_TILE) * cdiv(cdiv(g.n, H), SPLIT_TILE);
+    const size_t wsb_par = level >= 1 ? fp32_parallel_workspace_bytes(level, g, terms) : 0;
+    const bool parallel = level >= 1 && t_product_parallel != 0 && wsb_par <= t_ws_limit &&
+                          pack_group(level, 0, 0) && cdiv(g.m, H) * cdiv(g.n, H) < ((int64_t)1 << 31) &&
+                          (t_product_parallel == 1 || parallel_pays(level, tiles, sms, cdiv(g.m, H), cdiv(g.n, H)));
+    const bool m_col_major = g.unit_rsC != 0 && (g.unit_csC == 0 || g.unit_rsC <= g.unit_csC);
+    const int64_t* mtab = nullptr;
+    if (parallel && (s = plan_m_tables(t, level, cdiv(g.m, H), cdiv(g.n, H),
+                                       (int64_t)product_table(level).prod.size() * g.batch, m_col_major, mtab)))
+        return s;
     const size_t wsb_group = fp32_group_workspace_bytes(level, g, terms);
-    const size_t wsb = wsb_group <= t_ws_limit ? wsb_group : fp32_workspace_bytes(level, g, terms);
+    const size_t wsb = parallel ? wsb_par
+                       : wsb_group <= t_ws_limit ? wsb_group : fp32_workspace_bytes(level, g, terms);
     if ((s = wsbuf.alloc(wsb, st))) return s;
     int* err = shared_err;
     if (!err)
@@ -1151,7 +1304,9 @@ int run_fp32(int level, const GemmView& g, const DevPlan& t, const float* A, con
         err = static_cast<int*>(errbuf.p);
     }
     const int64_t* tb[9] = {t.rsA, t.rsC, t.csB, t.csC, t.ksA, t.ksB, t.bA, t.bB, t.bC};
-    s = run_fp32_enqueue(level, g, tb, A, B, C, st, num_sms(device), wsbuf.p, wsb, terms, err);
+    s = parallel ? run_fp32_parallel_enqueue(level, g, tb, A, B, C, st, sms, wsbuf.p, wsb, terms, mtab,
+                                             m_col_major, err)
+                 : run_fp32_enqueue(level, g, tb, A, B, C, st, sms, wsbuf.p, wsb, terms, err);
     if (s) return s;
     if (blocking && !shared_err)
     {

@@ -109,21 +109,26 @@ struct ScatterAddArgs
 // Products run side by side into their own M_p (dense ms x ns per batch entry,
 // M_p at M + p * m_pstride, column-major when col_major, else row-major), then
 // for every C block position h = hr * H + hc:
-//   C[h] = alpha * sum_{i < cnt[h]} sign[h][i] * M_{prod[h][i]} + beta * C[h]
-// (beta * C read only when beta != 0).  Up to 16 positions of 16 terms: the
-// 4 x 4 grid of a level-2 Strassen.
-struct CombineArgs
+//   C[h] = alpha * sum_p W[h][p] M_p + beta * C[h]
+// where product p adds sign ts[p][t] * M_p into position th[p][t], t < nt[p]
+// (sums in FP64, beta * C read only when beta != 0).  Up to 49 products on a
+// grid of up to 4 x 4 positions: a level-2 Strassen.  T = double or float.
+constexpr int MAX_COMBINE_PRODUCTS = 49;
+template <class T>
+struct CombineArgsT
 {
-    double* C;
+    T* C;
     const int64_t* rsC; const int64_t* csC; const int64_t* bC;
     int64_t m, n, ms, ns, batch;
-    const double* M;
+    const T* M;
     int64_t m_pstride;
     double alpha, beta;
-    int H, col_major;
-    int8_t cnt[16];
-    int8_t prod[16][16], sign[16][16];
+    int H, col_major, np;
+    int8_t nt[MAX_COMBINE_PRODUCTS];
+    int8_t th[MAX_COMBINE_PRODUCTS][4], ts[MAX_COMBINE_PRODUCTS][4];
 };
+using CombineArgs = CombineArgsT<double>;
+using CombineF32Args = CombineArgsT<float>;
 
 // ---- packed operands -------------------------------------------------------
 //
@@ -150,9 +155,7 @@ struct PackArgs
     double* out;
 };
 
-// C_q = (first_q ? beta*C_q : C_q) + sign_q*alpha*(S*T) for the nc targets of
-// one product, S and T packed (PACK_TILE x k_pad tiles).
-// Packed GEMM: for every 128 x 128 tile position, products q = 0..nprod-1 in
+// Packed GEMM (S and T packed, PACK_TILE x k_pad tiles): for every 128 x 128 tile position, products q = 0..nprod-1 in
 // order: C blocks (c_r, c_c) of product q += c_s * alpha * S_q T_q (beta on
 // first touch).  All products share the tile grid and k_pad; a CTA owns a
 // tile position across its products, so the C tiles a group of products
@@ -274,6 +277,12 @@ struct SplitGemmArgs
     const float* invA;                         // [batch][ms] inverse row scales
     const float* invB;                         // [batch][ns] inverse column scales
     int64_t m, n, ms, ns, nk, tiles_m, tiles_n, batch;
+    // Batch entries per plane set (0: batch).  With pbatch < batch, entry
+    // b = pp * pbatch + bl reads entry bl of plane set pp, which starts
+    // pp * planes * pbatch * tiles * nk blocks after A[q] (B[q]); the row and
+    // column scales are those of bl, the C tables those of b.  Products run
+    // side by side this way, one plane set each.
+    int64_t pbatch;
     float alpha, beta;
     int nprod;                                 // products per tile position (1..7)
     int H;                                     // side of the C block grid (1, 2 or 4)
@@ -323,6 +332,7 @@ cudaError_t launch_scale_f32(const ScaleF32Args& args, cudaStream_t stream);
 cudaError_t launch_sum_gather(const SumGatherArgs& args, cudaStream_t stream);
 cudaError_t launch_scatter_add(const ScatterAddArgs& args, cudaStream_t stream);
 cudaError_t launch_combine(const CombineArgs& args, cudaStream_t stream);
+cudaError_t launch_combine(const CombineF32Args& args, cudaStream_t stream);
 
 // Number of kernels this library has launched (all launchers count).
 unsigned long long launches();

@@ -85,6 +85,11 @@ size_t fp32_workspace_bytes(int level, const GemmView& g, int terms);
 // The same with the 7 split sums of a product group held at once (L >= 1);
 // run_fp32_enqueue forms them in one pass whenever ws_bytes allows it.
 size_t fp32_group_workspace_bytes(int level, const GemmView& g, int terms);
+// Product-parallel split-BF16 schedule (L >= 1; M tables as for FP64).
+size_t fp32_parallel_workspace_bytes(int level, const GemmView& g, int terms);
+int run_fp32_parallel_enqueue(int level, const GemmView& g, const int64_t* const tb[9], const float* A,
+                              const float* B, float* C, cudaStream_t st, int sms, void* ws, size_t ws_bytes,
+                              int terms, const int64_t* mtab, bool col_major, int* err);
 // With `defer` (L = 0 only) the GEMM is not launched: its descriptor is
 // returned for a grouped launch; with enqueue == false nothing is launched at
 // all (the descriptor alone, for a plan built before capture).

@@ -47,9 +47,19 @@ def terms(request, tsb):
     tsb.set_fp32_terms(6)
 
 
+@pytest.fixture(params=["grouped", "parallel"])
+def fp32_schedule(request, tsb):
+    """L >= 1 runs each group of 7 products tile by tile in one GEMM launch
+    (grouped), or every product side by side into M_p and one combine pass
+    (parallel, the automatic choice for small grids)."""
+    tsb.set_product_parallel(1 if request.param == "parallel" else 0)
+    yield request.param
+    tsb.set_product_parallel(-1)
+
+
 @pytest.mark.parametrize("dist", ["uniform", "loguniform"])
 @pytest.mark.parametrize("level", [0, 1, 2])
-def test_fp32_4d_vs_fp64_oracle(tsb, cuda, terms, level, dist):
+def test_fp32_4d_vs_fp64_oracle(tsb, cuda, terms, level, dist, fp32_schedule):
     import torch
     ext = dict(a=24, b=20, c=10, d=12, e=18, f=16)
     ia, ib, ic = "efac", "fbde", "abcd"
@@ -66,7 +76,7 @@ def test_fp32_4d_vs_fp64_oracle(tsb, cuda, terms, level, dist):
 
 
 @pytest.mark.parametrize("level", [0, 1, 2])
-def test_fp32_ragged_batch_and_beta0(tsb, cuda, terms, level):
+def test_fp32_ragged_batch_and_beta0(tsb, cuda, terms, level, fp32_schedule):
     import torch
     ext = dict(i=131, j=67, k=150, z=3)
     A = draw((ext["i"], ext["k"], ext["z"]), 4, "uniform")
@@ -83,7 +93,7 @@ def test_fp32_ragged_batch_and_beta0(tsb, cuda, terms, level):
 
 
 @pytest.mark.parametrize("level", [0, 1, 2])
-def test_fp32_config1_size_vs_fp64_gpu(tsb, cuda, terms, level):
+def test_fp32_config1_size_vs_fp64_gpu(tsb, cuda, terms, level, fp32_schedule):
     """NIm = NJn = NPk = 4096 (extents 64): the FP64 GPU path (itself checked
     against the oracle bound) is the reference; log-uniform magnitudes."""
     import torch
@@ -160,11 +170,18 @@ def test_fp32_group_launches(tsb, cuda, terms, level):
     C0 = draw([ext[c] for c in ic], 16, "uniform")
     R = C0.astype(np.float64, order="F")
     oracle.contract(0.75, A.astype(np.float64, order="F"), ia, B.astype(np.float64, order="F"), ib, -0.5, R, ic)
-    dA, dB, dC = to_dev(A, cuda), to_dev(B, cuda), to_dev(C0, cuda)
-    before = tsb.launch_count()
-    tsb.contract(level, 0.75, dA, ia, dB, ib, -0.5, dC, ic)
-    torch.cuda.synchronize()
-    # 2 scale launches, then per group: pack 7 S, pack 7 T, GEMM
-    assert tsb.launch_count() - before == 2 + 3 * 7 ** (level - 1)
-    err = normwise(dC.cpu().numpy(), R)
-    assert err <= TOL[terms], err
+    for mode, launches in ((0, 2 + 3 * 7 ** (level - 1)), (-1, 2 + 2 * 7 ** (level - 1) + 2)):
+        # grouped: 2 scale launches, then per group pack 7 S, pack 7 T, GEMM;
+        # automatic on this small grid (product-parallel): 2 scales, the
+        # group packs, one GEMM over all products, the combine
+        dA, dB, dC = to_dev(A, cuda), to_dev(B, cuda), to_dev(C0, cuda)
+        tsb.set_product_parallel(mode)
+        try:
+            before = tsb.launch_count()
+            tsb.contract(level, 0.75, dA, ia, dB, ib, -0.5, dC, ic)
+            torch.cuda.synchronize()
+            assert tsb.launch_count() - before == launches, mode
+        finally:
+            tsb.set_product_parallel(-1)
+        err = normwise(dC.cpu().numpy(), R)
+        assert err <= TOL[terms], (mode, err)
