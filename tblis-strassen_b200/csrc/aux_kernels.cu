@@ -126,7 +126,8 @@ __global__ void scatter_add_kernel(const ScatterAddArgs a)
 // One thread per local position (i, j) of every C block: it reads each
 // product's M_p there once, adds it (with sign) into the accumulators of the
 // product's block positions, kept in shared memory (column threadIdx.x of
-// acc[h]), then writes the H * H C elements.  M is read once in total.
+// acc[h], H * H rows of dynamic shared memory), then writes the H * H C
+// elements.  M is read once in total.
 // Grid: x over the ms * ns local positions (fastest index that of M's
 // layout), y over batch entries.
 constexpr int COMBINE_THREADS = 256;
@@ -135,7 +136,8 @@ template <class T>
 __global__ void __launch_bounds__(COMBINE_THREADS)
 combine_kernel(const __grid_constant__ CombineArgsT<T> a)
 {
-    __shared__ double acc[16][COMBINE_THREADS];
+    extern __shared__ double combine_acc[];
+    double (*acc)[COMBINE_THREADS] = reinterpret_cast<double (*)[COMBINE_THREADS]>(combine_acc);
     const int tid = threadIdx.x;
     const int H = a.H, H2 = H * H;
     const uint32_t per = (uint32_t)(a.ms * a.ns);
@@ -147,12 +149,21 @@ combine_kernel(const __grid_constant__ CombineArgsT<T> a)
         for (uint32_t loc = blockIdx.x * COMBINE_THREADS + tid; loc < per; loc += gridDim.x * COMBINE_THREADS)
         {
             for (int h = 0; h < H2; h++) acc[h][tid] = 0.0;
-#pragma unroll 7
-            for (int p = 0; p < a.np; p++)
+            // seven products' loads in flight before their accumulator updates
+            for (int p0 = 0; p0 < a.np; p0 += 7)
             {
-                const double x = (double)Mb[p * a.m_pstride + loc];
-                for (int t = 0; t < a.nt[p]; t++)
-                    acc[a.th[p][t]][tid] += a.ts[p][t] < 0 ? -x : x;
+                double x[7];
+#pragma unroll
+                for (int u = 0; u < 7; u++)
+                    x[u] = p0 + u < a.np ? (double)__ldg(Mb + (p0 + u) * a.m_pstride + loc) : 0.0;
+#pragma unroll
+                for (int u = 0; u < 7; u++)
+                {
+                    const int p = p0 + u;
+                    if (p >= a.np) break;
+                    for (int t = 0; t < a.nt[p]; t++)
+                        acc[a.th[p][t]][tid] += a.ts[p][t] < 0 ? -x[u] : x[u];
+                }
             }
             const uint32_t q = loc / fast, r = loc - q * fast;
             const int64_t i = a.col_major ? r : q, j = a.col_major ? q : r;
@@ -192,10 +203,15 @@ cudaError_t launch_combine_t(const CombineArgsT<T>& a, cudaStream_t stream)
     }
     const dim3 grid((unsigned)std::min<int64_t>((per + COMBINE_THREADS - 1) / COMBINE_THREADS, 65535),
                     (unsigned)std::min<int64_t>(a.batch, 65535));
+    const size_t smem = (size_t)a.H * a.H * COMBINE_THREADS * sizeof(double);
+    // as much shared memory as the SM gives: occupancy is bound by it
+    cudaError_t err = cudaFuncSetAttribute(combine_kernel<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                           (int)cudaSharedmemCarveoutMaxShared);
+    if (err != cudaSuccess) return err;
     timing_begin(KK_AUX, stream);
-    combine_kernel<T><<<grid, COMBINE_THREADS, 0, stream>>>(a);
+    combine_kernel<T><<<grid, COMBINE_THREADS, smem, stream>>>(a);
     timing_end(KK_AUX, stream);
-    cudaError_t err = cudaGetLastError();
+    err = cudaGetLastError();
     if (err == cudaSuccess) g_launches++;
     return err;
 }
