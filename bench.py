@@ -598,7 +598,7 @@ def main():
         nbytes = npk * npk * 8
         e2e = {"value": world * flops * n2 / te / 1e12, "unit": "TFLOP/s",
                "h2d_bytes_per_step": 3 * nbytes, "d2h_bytes_per_step": nbytes,
-               "path": "stra_tblis_tensor_mult with pinned host tensors (copies inside the call, pipelined in 4 chunks of C's slowest B/C label)"}
+               "path": "stra_tblis_tensor_mult with pinned host tensors (copies inside the call, pipelined in 8 chunks: C's slowest B/C label in 4 x its A/C label c in 2)"}
         del hA, hB, hC
 
     batched = None

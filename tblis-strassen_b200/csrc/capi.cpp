@@ -1322,11 +1322,13 @@ int run_fp32(int level, const GemmView& g, const DevPlan& t, const float* A, con
 //
 // When A, B and C all live in host memory, the call splits the slowest label
 // of C that is also in exactly one of A and B into chunks: the other operand is
-// copied whole first, then chunk j of C and of the split operand is copied
-// in while chunk j-1 computes, and chunk j of C is copied back while chunk j+1
-// computes.  Each chunk is the same contraction on sub-views (the split label
-// restricted to the chunk's range), so every chunk is exact and C's chunks are
-// disjoint; beta applies once per element.
+// copied first, then chunk j of C and of the split operand is copied in while
+// chunk j-1 computes, and chunk j of C is copied back while chunk j+1
+// computes.  When C's geometry allows it, the other operand is cut in two
+// along one of its own C labels as well (chunks (i, j), i outer), so the first
+// chunk waits for half of it only.  Each chunk is the same contraction on
+// sub-views (the split labels restricted to the chunk's ranges), so every
+// chunk is exact and C's chunks are disjoint; beta applies once per element.
 
 struct CopyStreams { cudaStream_t in = nullptr, out = nullptr; };
 
@@ -1448,9 +1450,31 @@ int mult_pipelined(int level, int impl, const tblis_tensor* const T[3], const la
         }
     }
     if (pc < 0) return NOT_PIPELINED;
-    const int whole = 1 - op;                 // the operand copied in one piece
+    const int whole = 1 - op;                 // the operand not cut along pc
     const int64_t extent = T[2]->len[pc];
     const int chunks = (int)std::min<int64_t>(PIPELINE_CHUNKS, extent);
+
+    // Second cut, of the other operand: a C label qc of that operand only whose
+    // C stride sits next to pc's (inner * extent == outer, the outer one C's
+    // last), so block (i, j) of C is one 2-D copy: rows of (inner range) *
+    // inner stride elements, one per outer index.
+    int qc = -1, pw = -1;
+    int64_t sw = 0, hw = 0, pitw = 0;
+    for (unsigned d = 0; d < T[2]->ndim && qc < 0; d++)
+    {
+        const int pa = find(T[0], I[0], I[2][d]), pb = find(T[1], I[1], I[2][d]);
+        const int pwhole = whole == 0 ? pa : pb, pother = whole == 0 ? pb : pa;
+        if ((int)d == pc || pwhole < 0 || pother >= 0 || T[2]->len[d] < 2) continue;
+        const int inner = T[2]->stride[d] < T[2]->stride[pc] ? (int)d : pc;
+        const int outer = inner == pc ? (int)d : pc;
+        int64_t si, hi, pi, so, ho, po;
+        if (!slice_geometry(T[2], inner, si, hi, pi) || !slice_geometry(T[2], outer, so, ho, po)) continue;
+        if (T[2]->stride[inner] * T[2]->len[inner] != T[2]->stride[outer] || ho != 1) continue;
+        if (!slice_geometry(T[whole], pwhole, sw, hw, pitw)) continue;
+        qc = (int)d;
+        pw = pwhole;
+    }
+    const int halves = qc >= 0 ? 2 : 1;
 
     CopyStreams cs;
     int s = copy_streams(device, cs);
@@ -1488,54 +1512,98 @@ int mult_pipelined(int level, int impl, const tblis_tensor* const T[3], const la
         return TBLIS_STRA_SUCCESS;
     };
 
-    cudaEvent_t e0 = event(), e_whole = event(), e_out = event();
-    if (!e0 || !e_whole || !e_out) return TBLIS_STRA_ERR_CUDA;
+    // C block (i, j): the pc range of chunk j and, with a second cut, the qc
+    // range of half i, as one 2-D copy.
+    auto copy_c = [&](const int64_t* rq, const int64_t* rp, cudaMemcpyKind kind, cudaStream_t cst) -> int {
+        if (qc < 0) return copy2d(2, sc, hc, pitc, rp[0], rp[1], kind, cst);
+        const bool q_inner = T[2]->stride[qc] < T[2]->stride[pc];
+        const int64_t* ri = q_inner ? rq : rp;
+        const int64_t* ro = q_inner ? rp : rq;
+        const int inner = q_inner ? qc : pc, outer = q_inner ? pc : qc;
+        const int64_t si = T[2]->stride[inner], so = T[2]->stride[outer];
+        const size_t off = (size_t)(ri[0] * si + ro[0] * so) * es;
+        const size_t width = (size_t)((ri[1] - ri[0]) * si) * es;
+        char* host = static_cast<char*>(T[2]->data) + off;
+        char* dev = static_cast<char*>(stage[2].p) + off;
+        const size_t pb = (size_t)so * es;
+        if (kind == cudaMemcpyHostToDevice)
+            TSB_CUDA(cudaMemcpy2DAsync(dev, pb, host, pb, width, (size_t)(ro[1] - ro[0]), kind, cst));
+        else
+            TSB_CUDA(cudaMemcpy2DAsync(host, pb, dev, pb, width, (size_t)(ro[1] - ro[0]), kind, cst));
+        return TBLIS_STRA_SUCCESS;
+    };
+
+    cudaEvent_t e0 = event(), e_out = event();
+    if (!e0 || !e_out) return TBLIS_STRA_ERR_CUDA;
     TSB_CUDA(cudaEventRecord(e0, st));                    // staging buffers allocated
     TSB_CUDA(cudaStreamWaitEvent(cs.in, e0, 0));
     TSB_CUDA(cudaStreamWaitEvent(cs.out, e0, 0));
-    TSB_CUDA(cudaMemcpyAsync(stage[whole].p, T[whole]->data, (size_t)(g.hi[whole] + 1) * es,
-                             cudaMemcpyHostToDevice, cs.in));
-    TSB_CUDA(cudaEventRecord(e_whole, cs.in));
-    std::vector<cudaEvent_t> e_in(chunks), e_done(chunks);
-    std::vector<int64_t> lo(chunks + 1);
+    std::vector<int64_t> lo(chunks + 1), lw(halves + 1);
     for (int j = 0; j <= chunks; j++) lo[j] = extent * j / chunks;
-    for (int j = 0; j < chunks; j++)
-    {
-        e_in[j] = event();
-        e_done[j] = event();
-        if (!e_in[j] || !e_done[j]) return TBLIS_STRA_ERR_CUDA;
-        if ((s = copy2d(op, sx, hx, pitx, lo[j], lo[j + 1], cudaMemcpyHostToDevice, cs.in))) return s;
-        if ((s = copy2d(2, sc, hc, pitc, lo[j], lo[j + 1], cudaMemcpyHostToDevice, cs.in))) return s;
-        TSB_CUDA(cudaEventRecord(e_in[j], cs.in));
-    }
-    TSB_CUDA(cudaStreamWaitEvent(st, e_whole, 0));
-    for (int j = 0; j < chunks; j++)
-    {
-        // sub-views: the split label restricted to [lo[j], lo[j+1])
-        tblis_tensor sub[3];
-        std::vector<len_type> len[3];
-        void* dptr[3];
-        for (int t = 0; t < 3; t++)
+    const int64_t ext_w = qc >= 0 ? T[2]->len[qc] : 1;
+    for (int i = 0; i <= halves; i++) lw[i] = ext_w * i / halves;
+    // Copies in the order the chunks need them: half i of the other operand
+    // (all of it without a second cut) before its first chunk, slice j of the
+    // split operand with chunk (0, j), C block (i, j) with its chunk.
+    const int nck = halves * chunks;
+    std::vector<cudaEvent_t> e_in(nck), e_done(nck);
+    for (int i = 0; i < halves; i++)
+        for (int j = 0; j < chunks; j++)
         {
-            sub[t] = *T[t];
-            len[t].assign(T[t]->len, T[t]->len + T[t]->ndim);
-            dptr[t] = stage[t].p;
+            const int c = i * chunks + j;
+            e_in[c] = event();
+            e_done[c] = event();
+            if (!e_in[c] || !e_done[c]) return TBLIS_STRA_ERR_CUDA;
+            if (j == 0)
+            {
+                if (qc < 0)
+                    TSB_CUDA(cudaMemcpyAsync(stage[whole].p, T[whole]->data, (size_t)(g.hi[whole] + 1) * es,
+                                             cudaMemcpyHostToDevice, cs.in));
+                else if ((s = copy2d(whole, sw, hw, pitw, lw[i], lw[i + 1], cudaMemcpyHostToDevice, cs.in)))
+                    return s;
+            }
+            if (i == 0 && (s = copy2d(op, sx, hx, pitx, lo[j], lo[j + 1], cudaMemcpyHostToDevice, cs.in)))
+                return s;
+            if ((s = copy_c(&lw[i], &lo[j], cudaMemcpyHostToDevice, cs.in))) return s;
+            TSB_CUDA(cudaEventRecord(e_in[c], cs.in));
         }
-        len[op][px] = lo[j + 1] - lo[j];
-        len[2][pc] = lo[j + 1] - lo[j];
-        dptr[op] = static_cast<char*>(stage[op].p) + (size_t)(lo[j] * sx) * es;
-        dptr[2] = static_cast<char*>(stage[2].p) + (size_t)(lo[j] * sc) * es;
-        for (int t = 0; t < 3; t++) { sub[t].len = len[t].data(); sub[t].data = dptr[t]; }
-        const tblis_tensor* ST[3] = {&sub[0], &sub[1], &sub[2]};
-        GemmView gj;
-        std::shared_ptr<DevPlan> dpj;
-        if ((s = get_plan(ST, I, device, gj, dpj))) return s;
-        TSB_CUDA(cudaStreamWaitEvent(st, e_in[j], 0));
-        if ((s = run_plan(level, impl, gj, *dpj, dptr, st, device, err))) return s;
-        TSB_CUDA(cudaEventRecord(e_done[j], st));
-        TSB_CUDA(cudaStreamWaitEvent(cs.out, e_done[j], 0));
-        if ((s = copy2d(2, sc, hc, pitc, lo[j], lo[j + 1], cudaMemcpyDeviceToHost, cs.out))) return s;
-    }
+    for (int i = 0; i < halves; i++)
+        for (int j = 0; j < chunks; j++)
+        {
+            const int c = i * chunks + j;
+            // sub-views: the split labels restricted to the chunk's ranges
+            tblis_tensor sub[3];
+            std::vector<len_type> len[3];
+            void* dptr[3];
+            for (int t = 0; t < 3; t++)
+            {
+                sub[t] = *T[t];
+                len[t].assign(T[t]->len, T[t]->len + T[t]->ndim);
+                dptr[t] = stage[t].p;
+            }
+            len[op][px] = lo[j + 1] - lo[j];
+            len[2][pc] = lo[j + 1] - lo[j];
+            dptr[op] = static_cast<char*>(stage[op].p) + (size_t)(lo[j] * sx) * es;
+            size_t coff = (size_t)(lo[j] * T[2]->stride[pc]) * es;
+            if (qc >= 0)
+            {
+                len[whole][pw] = lw[i + 1] - lw[i];
+                len[2][qc] = lw[i + 1] - lw[i];
+                dptr[whole] = static_cast<char*>(stage[whole].p) + (size_t)(lw[i] * sw) * es;
+                coff += (size_t)(lw[i] * T[2]->stride[qc]) * es;
+            }
+            dptr[2] = static_cast<char*>(stage[2].p) + coff;
+            for (int t = 0; t < 3; t++) { sub[t].len = len[t].data(); sub[t].data = dptr[t]; }
+            const tblis_tensor* ST[3] = {&sub[0], &sub[1], &sub[2]};
+            GemmView gj;
+            std::shared_ptr<DevPlan> dpj;
+            if ((s = get_plan(ST, I, device, gj, dpj))) return s;
+            TSB_CUDA(cudaStreamWaitEvent(st, e_in[c], 0));
+            if ((s = run_plan(level, impl, gj, *dpj, dptr, st, device, err))) return s;
+            TSB_CUDA(cudaEventRecord(e_done[c], st));
+            TSB_CUDA(cudaStreamWaitEvent(cs.out, e_done[c], 0));
+            if ((s = copy_c(&lw[i], &lo[j], cudaMemcpyDeviceToHost, cs.out))) return s;
+        }
     TSB_CUDA(cudaEventRecord(e_out, cs.out));
     TSB_CUDA(cudaStreamWaitEvent(st, e_out, 0));
     int flag = 0;

@@ -1,10 +1,11 @@
 """Host-resident operands: the drop-in calls stage them through device memory.
 When all three are on the host and large (>= 64 MiB together), the call
 splits C's slowest label that belongs to exactly one of A and B into 4 chunks
-and overlaps the copies of one chunk with the computation of another.  Each
-chunk is the same contraction on sub-views, so the result matches the
-all-device call within the Strassen bound (both are within it of the exact
-contraction)."""
+and, when C's layout allows a second cut, the other operand in 2 along one of
+its C labels (8 chunks), and overlaps the copies of one chunk with the
+computation of another.  Each chunk is the same contraction on sub-views, so
+the result matches the all-device call within the Strassen bound (both are
+within it of the exact contraction)."""
 import numpy as np
 import pytest
 
@@ -44,7 +45,7 @@ def test_pipelined_split_of_b_and_c(tsb, cuda, level, pinned):
     # L=0: 2 packs + GEMM; L=1 (14 tiles per product, product-parallel):
     # 2 group packs + the GEMM over the 7 products + the combine
     per_call = 3 if level == 0 else 4
-    assert launches == 4 * per_call          # four chunks
+    assert launches == 8 * per_call          # d in 4 chunks x c in 2
 
 
 def test_pipelined_split_of_a_and_c_row_major(tsb, cuda):
@@ -55,7 +56,7 @@ def test_pipelined_split_of_a_and_c_row_major(tsb, cuda):
     C0 = np.ascontiguousarray(oracle.uniform((e,) * 4, 6))
     got, want, launches = run_pair(tsb, cuda, 1, A, "aefc", B, "fbde", C0, "abcd", True)
     assert np.abs(got - want).max() <= bound(1, e * e)
-    assert launches == 4 * 4                 # product-parallel L=1 per chunk
+    assert launches == 8 * 4                 # a in 4 x b in 2; product-parallel L=1 per chunk
 
 
 def test_pipelined_fp32(tsb, cuda):
@@ -67,7 +68,19 @@ def test_pipelined_fp32(tsb, cuda):
     got, want, launches = run_pair(tsb, cuda, 0, A, "efac", B, "fbde", C0, "abcd", True)
     d = np.linalg.norm((got.astype(np.float64) - want).ravel()) / np.linalg.norm(want.ravel())
     assert d <= 2e-6
-    assert launches == 4 * 5                 # 2 scales, 2 packs, GEMM per chunk
+    assert launches == 8 * 5                 # 8 chunks of 2 scales, 2 packs, GEMM
+
+
+def test_pipelined_one_cut_with_batch_label(tsb, cuda):
+    """A batch label z outermost in C leaves no 2-D block of C for a second
+    cut: d alone is cut in 4 chunks, A copied whole."""
+    e, z = 32, 3                             # 3 x 25 MB
+    A = np.asfortranarray(oracle.uniform((e, e, e, e, z), 19))
+    B = np.asfortranarray(oracle.uniform((e, e, e, e, z), 20))
+    C0 = np.asfortranarray(oracle.uniform((e, e, e, e, z), 21))
+    got, want, launches = run_pair(tsb, cuda, 1, A, "efacz", B, "fbdez", C0, "abcdz", True)
+    assert np.abs(got - want).max() <= bound(1, e * e)
+    assert launches == 4 * 4                 # 4 chunks; product-parallel L=1 per chunk
 
 
 def test_small_or_unsliceable_operands_stage_whole(tsb, cuda):
