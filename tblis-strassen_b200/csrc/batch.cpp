@@ -89,6 +89,8 @@ struct Prob
     GemmView g;
     const void* A; const void* B; void* C;
     size_t tab_off[9];        // element offsets of the 9 scatter vectors in the table buffer
+    size_t mtab_off[3] = {0, 0, 0};   // M_p tables of the product-parallel form at L = 1, 2
+    bool mcol = false;        // M_p layout (column-major)
     int level_req;            // -1 or 0..2
     int level = 0, variant = V_SCALE;
     bool empty = false;       // nothing to write (m, n or batch zero)
@@ -319,6 +321,19 @@ std::vector<Choice> candidates(const Prob& pr, bool prune = true)
     return c;
 }
 
+// Workspace of one problem's schedule: the product-parallel form where it
+// applies (packed FP64 and split FP32 at L >= 1), else the grouped sums.
+size_t schedule_workspace_bytes(const Prob& pr, const Choice& x, int sms)
+{
+    if (x.variant == V_SPLIT || x.variant == V_SGROUP)
+        return use_product_parallel(x.level, pr.g, sms, true, FP32_TERMS)
+                   ? fp32_parallel_workspace_bytes(x.level, pr.g, FP32_TERMS)
+                   : fp32_group_workspace_bytes(x.level, pr.g, FP32_TERMS);
+    if (x.variant == V_PACKED && use_product_parallel(x.level, pr.g, sms, false, 0))
+        return fp64_parallel_workspace_bytes(x.level, pr.g);
+    return fp64_packed_group_workspace_bytes(x.level, pr.g);
+}
+
 constexpr int MAX_COPIES = 64;
 
 struct Tuner
@@ -430,6 +445,13 @@ struct Tuner
             });
             return pack_ms + gemm_ms / copies;
         }
+        if (c.variant == V_PACKED && use_product_parallel(c.level, pr.g, sms, false, 0))
+            return time([&] {
+                return run_fp64_parallel_enqueue(c.level, pr.g, tb, static_cast<const double*>(pr.A),
+                                                 static_cast<const double*>(pr.B),
+                                                 static_cast<double*>(scratch.p) - shift, st, sms, ws.p, ws_bytes,
+                                                 tab + pr.mtab_off[c.level], pr.mcol, err);
+            });
         if (c.variant == V_PACKED)
             return time([&] {
                 return run_fp64_packed_enqueue(c.level, pr.g, tb, static_cast<const double*>(pr.A),
@@ -454,6 +476,13 @@ struct Tuner
             });
             return prep_ms + gemm_ms / (double)args.size();
         }
+        if (c.variant == V_SPLIT && use_product_parallel(c.level, pr.g, sms, true, FP32_TERMS))
+            return time([&] {
+                return run_fp32_parallel_enqueue(c.level, pr.g, tb, static_cast<const float*>(pr.A),
+                                                 static_cast<const float*>(pr.B),
+                                                 static_cast<float*>(scratch.p) - shift, st, sms, ws.p, ws_bytes,
+                                                 FP32_TERMS, tab + pr.mtab_off[c.level], pr.mcol, err);
+            });
         if (c.variant == V_SPLIT)
             return time([&] {
                 return run_fp32_enqueue(c.level, pr.g, tb, static_cast<const float*>(pr.A),
@@ -592,6 +621,14 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
         const std::vector<int64_t>* v[9] = {&pr.g.rsA, &pr.g.rsC, &pr.g.csB, &pr.g.csC, &pr.g.ksA,
                                             &pr.g.ksB, &pr.g.bA, &pr.g.bB, &pr.g.bC};
         for (int j = 0; j < 9; j++) { pr.tab_off[j] = total_tab; total_tab += std::max<size_t>(v[j]->size(), 1); }
+        pr.mcol = m_tables_col_major(pr.g);
+        for (int L = 1; L <= 2; L++)
+        {
+            const int H = product_table(L).H;
+            const int64_t nb = (int64_t)product_table(L).prod.size() * pr.g.batch;
+            pr.mtab_off[L] = total_tab;
+            total_tab += (size_t)std::max<int64_t>((pr.g.m + H - 1) / H + (pr.g.n + H - 1) / H + nb, 1);
+        }
         pr.level_req = q.level;
         pr.empty = pr.g.m == 0 || pr.g.n == 0 || pr.g.batch == 0;
         pr.scale = !pr.empty && (pr.g.alpha == 0.0 || pr.g.k == 0);
@@ -604,6 +641,13 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
         const std::vector<int64_t>* v[9] = {&pr.g.rsA, &pr.g.rsC, &pr.g.csB, &pr.g.csC, &pr.g.ksA,
                                             &pr.g.ksB, &pr.g.bA, &pr.g.bB, &pr.g.bC};
         for (int j = 0; j < 9; j++) std::copy(v[j]->begin(), v[j]->end(), host.begin() + (ptrdiff_t)pr.tab_off[j]);
+        for (int L = 1; L <= 2; L++)
+        {
+            const int H = product_table(L).H;
+            const int64_t nb = (int64_t)product_table(L).prod.size() * pr.g.batch;
+            dense_m_tables((pr.g.m + H - 1) / H, (pr.g.n + H - 1) / H, nb, pr.mcol,
+                           host.data() + pr.mtab_off[L]);
+        }
     }
     TSB_TRY(plan->tables.alloc(host.size() * 8));
     TSB_TRY(upload_complete(plan->tables.p, host.data(), host.size() * 8));
@@ -625,9 +669,7 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
             if (c.size() < 2) continue;
             need = true;
             for (const Choice& x : c)
-                tune_ws = std::max(tune_ws, (x.variant == V_SPLIT || x.variant == V_SGROUP)
-                                                ? fp32_group_workspace_bytes(x.level, pr.g, FP32_TERMS)
-                                                                 : fp64_packed_group_workspace_bytes(x.level, pr.g));
+                tune_ws = std::max(tune_ws, schedule_workspace_bytes(pr, x, sms));
         }
         Tuner tuner;
         if (need) TSB_TRY(tuner.init((size_t)max_c_span * sizeof(double), tune_ws, err, sms));
@@ -681,7 +723,7 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
     // 4b. problem-by-problem packed schedules share one workspace
     size_t seq_bytes = 0;
     for (auto& pr : probs)
-        if (pr.variant == V_PACKED) seq_bytes = std::max(seq_bytes, fp64_packed_group_workspace_bytes(pr.level, pr.g));
+        if (pr.variant == V_PACKED) seq_bytes = std::max(seq_bytes, schedule_workspace_bytes(pr, {pr.level, pr.variant}, sms));
     if (seq_bytes) TSB_TRY(plan->seq_ws.alloc(seq_bytes));
     // 4c. chunks of grouped problems: FP64 packed (V_PGROUP) and FP32 split
     // (V_SGROUP) problems, each kind in consecutive chunks of at most
@@ -778,7 +820,7 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
             const int b = load[0] <= load[1] ? 0 : 1;
             f32_list[b].push_back(i);
             load[b] += probs[i].flops();
-            need[b] = std::max(need[b], fp32_group_workspace_bytes(probs[i].level, probs[i].g, FP32_TERMS));
+            need[b] = std::max(need[b], schedule_workspace_bytes(probs[i], {probs[i].level, V_SPLIT}, sms));
         }
         for (int b = 0; b < 2; b++)
             if (need[b]) TSB_TRY(plan->f32_ws[b].alloc(need[b]));
@@ -858,10 +900,18 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
                 const Prob& pr = probs[i];
                 const int64_t* tb[9];
                 pr.tables(tab, tb);
-                TSB_TRY(run_fp32_enqueue(pr.level, pr.g, tb, static_cast<const float*>(pr.A),
-                                         static_cast<const float*>(pr.B), static_cast<float*>(pr.C),
-                                         cs.f32[b], sms, plan->f32_ws[b].p,
-                                         fp32_group_workspace_bytes(pr.level, pr.g, FP32_TERMS), FP32_TERMS, err));
+                if (use_product_parallel(pr.level, pr.g, sms, true, FP32_TERMS))
+                    TSB_TRY(run_fp32_parallel_enqueue(pr.level, pr.g, tb, static_cast<const float*>(pr.A),
+                                                      static_cast<const float*>(pr.B), static_cast<float*>(pr.C),
+                                                      cs.f32[b], sms, plan->f32_ws[b].p,
+                                                      fp32_parallel_workspace_bytes(pr.level, pr.g, FP32_TERMS),
+                                                      FP32_TERMS, tab + pr.mtab_off[pr.level], pr.mcol, err));
+                else
+                    TSB_TRY(run_fp32_enqueue(pr.level, pr.g, tb, static_cast<const float*>(pr.A),
+                                             static_cast<const float*>(pr.B), static_cast<float*>(pr.C),
+                                             cs.f32[b], sms, plan->f32_ws[b].p,
+                                             fp32_group_workspace_bytes(pr.level, pr.g, FP32_TERMS), FP32_TERMS,
+                                             err));
             }
             if (use_f32[b]) TSB_CU(cudaEventRecord(ev_f32[b], cs.f32[b]));
         }
@@ -891,10 +941,17 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
             if (pr.variant != V_PACKED) continue;
             const int64_t* tb[9];
             pr.tables(tab, tb);
-            TSB_TRY(run_fp64_packed_enqueue(pr.level, pr.g, tb, static_cast<const double*>(pr.A),
-                                            static_cast<const double*>(pr.B), static_cast<double*>(pr.C),
-                                            cs.main, sms, plan->seq_ws.p,
-                                            fp64_packed_group_workspace_bytes(pr.level, pr.g), err));
+            if (use_product_parallel(pr.level, pr.g, sms, false, 0))
+                TSB_TRY(run_fp64_parallel_enqueue(pr.level, pr.g, tb, static_cast<const double*>(pr.A),
+                                                  static_cast<const double*>(pr.B), static_cast<double*>(pr.C),
+                                                  cs.main, sms, plan->seq_ws.p,
+                                                  fp64_parallel_workspace_bytes(pr.level, pr.g),
+                                                  tab + pr.mtab_off[pr.level], pr.mcol, err));
+            else
+                TSB_TRY(run_fp64_packed_enqueue(pr.level, pr.g, tb, static_cast<const double*>(pr.A),
+                                                static_cast<const double*>(pr.B), static_cast<double*>(pr.C),
+                                                cs.main, sms, plan->seq_ws.p,
+                                                fp64_packed_group_workspace_bytes(pr.level, pr.g), err));
         }
         for (size_t c = 0; c < chunks.size(); c++)
         {

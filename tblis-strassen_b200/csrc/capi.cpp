@@ -332,11 +332,9 @@ int run_fp64_packed(int level, const GemmView& g, const DevPlan& t, const double
     // Product-parallel when one product's tiles would leave SMs idle and its
     // workspace is allowed.
     const PackGeom pg = pack_geom(level, g);
-    const size_t ws_par = level >= 1 ? fp64_parallel_workspace_bytes(level, g) : 0;
-    const bool parallel = level >= 1 && t_product_parallel != 0 && ws_par <= t_ws_limit &&
-                          pg.ms * pg.ns < ((int64_t)1 << 31) &&
-                          (t_product_parallel == 1 || parallel_pays(level, g.batch * pg.tm * pg.tn, sms, pg.ms, pg.ns));
-    const bool m_col_major = g.unit_rsC != 0 && (g.unit_csC == 0 || g.unit_rsC <= g.unit_csC);
+    const bool parallel = use_product_parallel(level, g, sms, false, 0);
+    const size_t ws_par = parallel ? fp64_parallel_workspace_bytes(level, g) : 0;
+    const bool m_col_major = m_tables_col_major(g);
     const int64_t* mtab = nullptr;
     int s;
     if (parallel && (s = plan_m_tables(t, level, pg.ms, pg.ns, (int64_t)product_table(level).prod.size() * g.batch,
@@ -455,7 +453,7 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
         fp64_parallel_workspace_bytes(level, g) + (impl == 3 ? (size_t)(g.batch * (ms + ns) * ks) * 8 : 0) <=
             t_ws_limit)
     {
-        const bool col_major = g.unit_rsC != 0 && (g.unit_csC == 0 || g.unit_rsC <= g.unit_csC);
+        const bool col_major = m_tables_col_major(g);
         const int np = (int)tab.prod.size();
         const int64_t* mtab = nullptr;
         int s;
@@ -1176,6 +1174,32 @@ size_t fp32_parallel_workspace_bytes(int level, const GemmView& g, int terms)
     return sc + planes + np * (size_t)(g.batch * ms * ns) * sizeof(float);
 }
 
+bool use_product_parallel(int level, const GemmView& g, int sms, bool fp32, int terms)
+{
+    if (level < 1 || t_product_parallel == 0) return false;
+    const int H = product_table(level).H;
+    const int64_t ms = cdiv(g.m, H), ns = cdiv(g.n, H);
+    if (ms * ns >= ((int64_t)1 << 31)) return false;
+    int64_t tiles;
+    if (fp32)
+    {
+        if (!pack_group(level, 0, 0) || fp32_parallel_workspace_bytes(level, g, terms) > t_ws_limit) return false;
+        tiles = g.batch * cdiv(ms, SPLIT_TILE) * cdiv(ns, SPLIT_TILE);
+    }
+    else
+    {
+        const PackGeom pg = pack_geom(level, g);
+        if (!pg.fits || fp64_parallel_workspace_bytes(level, g) > t_ws_limit) return false;
+        tiles = g.batch * pg.tm * pg.tn;
+    }
+    return t_product_parallel == 1 || parallel_pays(level, tiles, sms, ms, ns);
+}
+
+bool m_tables_col_major(const GemmView& g)
+{
+    return g.unit_rsC != 0 && (g.unit_csC == 0 || g.unit_rsC <= g.unit_csC);
+}
+
 // Product-parallel split-BF16 schedule (L >= 1): row and column scales, the
 // split sums of every product (plane set p of A at planesA + p * bytesA, of B
 // likewise), one GEMM launch over all products (batch entry p * batch + b
@@ -1282,12 +1306,9 @@ int run_fp32(int level, const GemmView& g, const DevPlan& t, const float* A, con
     // idle and its workspace is allowed (as for FP64).
     const int sms = num_sms(device);
     const int H = product_table(level).H;
-    const int64_t tiles = g.batch * cdiv(cdiv(g.m, H), SPLIT_TILE) * cdiv(cdiv(g.n, H), SPLIT_TILE);
-    const size_t wsb_par = level >= 1 ? fp32_parallel_workspace_bytes(level, g, terms) : 0;
-    const bool parallel = level >= 1 && t_product_parallel != 0 && wsb_par <= t_ws_limit &&
-                          pack_group(level, 0, 0) && cdiv(g.m, H) * cdiv(g.n, H) < ((int64_t)1 << 31) &&
-                          (t_product_parallel == 1 || parallel_pays(level, tiles, sms, cdiv(g.m, H), cdiv(g.n, H)));
-    const bool m_col_major = g.unit_rsC != 0 && (g.unit_csC == 0 || g.unit_rsC <= g.unit_csC);
+    const bool parallel = use_product_parallel(level, g, sms, true, terms);
+    const size_t wsb_par = parallel ? fp32_parallel_workspace_bytes(level, g, terms) : 0;
+    const bool m_col_major = m_tables_col_major(g);
     const int64_t* mtab = nullptr;
     if (parallel && (s = plan_m_tables(t, level, cdiv(g.m, H), cdiv(g.n, H),
                                        (int64_t)product_table(level).prod.size() * g.batch, m_col_major, mtab)))

@@ -79,6 +79,13 @@ int enqueue_products_and_combine(int level, const GemmView& g, const int64_t* co
                                  int* err);
 // Host copy of those tables: rows[ms], cols[ns], batch[nb].
 void dense_m_tables(int64_t ms, int64_t ns, int64_t nb, bool col_major, int64_t* out);
+// M's layout for C's layout: column-major when C's row bundle is the faster.
+bool m_tables_col_major(const GemmView& g);
+// Whether a contraction at `level` runs product-parallel: the automatic rule
+// (L = 2 always; L = 1 when one product's last wave of tiles leaves more than
+// a tenth of the SMs idle), the calling thread's setting
+// (tblis_stra_set_product_parallel) and its workspace limit.
+bool use_product_parallel(int level, const GemmView& g, int sms, bool fp32, int terms);
 
 // Split-BF16 schedule of one FP32 contraction on caller workspace.
 size_t fp32_workspace_bytes(int level, const GemmView& g, int terms);
