@@ -199,7 +199,9 @@ size_t tblis_stra_get_workspace_limit(void);
  * FP32 does the same on its split-BF16 path.  It needs 7^L * (packed sums +
  * batch*ms*ns elements of M) bytes within the workspace limit.  AB and Naive
  * (which hold M temporaries by design) always take this form when mode is
- * not 0.  mode: -1 automatic (the default), 0 never, 1 whenever the
+ * not 0.  At L = 0 with fewer C tiles than SMs and at least 1024 summed
+ * indices, the same machinery cuts the summed range into up to 49 pieces
+ * (k-split) run side by side and summed by the combine pass.  mode: -1 automatic (the default), 0 never, 1 whenever the
  * workspace fits.  Per calling thread.  Returns 0 or TBLIS_STRA_ERR_ARG. */
 int tblis_stra_set_product_parallel(int mode);
 int tblis_stra_get_product_parallel(void);

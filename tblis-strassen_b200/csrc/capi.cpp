@@ -335,6 +335,34 @@ int run_fp64_packed(int level, const GemmView& g, const DevPlan& t, const double
     const bool parallel = use_product_parallel(level, g, sms, false, 0);
     const size_t ws_par = parallel ? fp64_parallel_workspace_bytes(level, g) : 0;
     const bool m_col_major = m_tables_col_major(g);
+    // A plain contraction with fewer C tiles than SMs: k-split.
+    const int P = level == 0 && t_product_parallel != 0 ? ksplit_pieces(g, sms) : 1;
+    if (P >= 2 && fp64_ksplit_workspace_bytes(g, P) <= t_ws_limit)
+    {
+        const int64_t* ktab = nullptr;
+        int s;
+        if ((s = plan_m_tables(t, 0, g.m, g.n, (int64_t)P * g.batch, m_col_major, ktab))) return s;
+        Scratch kbuf, kerr;
+        const size_t wsk = fp64_ksplit_workspace_bytes(g, P);
+        if ((s = kbuf.alloc(wsk, st))) return s;
+        int* err = shared_err;
+        if (!err)
+        {
+            if ((s = kerr.alloc(sizeof(int), st))) return s;
+            TSB_CUDA(cudaMemsetAsync(kerr.p, 0, sizeof(int), st));
+            err = static_cast<int*>(kerr.p);
+        }
+        const int64_t* tb[9] = {t.rsA, t.rsC, t.csB, t.csC, t.ksA, t.ksB, t.bA, t.bB, t.bC};
+        if ((s = run_fp64_ksplit_enqueue(g, tb, A, B, C, st, sms, kbuf.p, wsk, P, ktab, m_col_major, err))) return s;
+        if (blocking && !shared_err)
+        {
+            int flag = 0;
+            TSB_CUDA(cudaMemcpyAsync(&flag, kerr.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            TSB_CUDA(cudaStreamSynchronize(st));
+            if (flag) return TBLIS_STRA_ERR_TIMEOUT;
+        }
+        return TBLIS_STRA_SUCCESS;
+    }
     const int64_t* mtab = nullptr;
     int s;
     if (parallel && (s = plan_m_tables(t, level, pg.ms, pg.ns, (int64_t)product_table(level).prod.size() * g.batch,
@@ -914,6 +942,95 @@ int enqueue_products_and_combine(int level, const GemmView& g, const int64_t* co
             c.ts[p][q] = pr.c[q].sign;
         }
     }
+    TSB_CUDA(launch_combine(c, st));
+    return TBLIS_STRA_SUCCESS;
+}
+
+// ---- k-split plain contraction (L = 0, few tiles) ----------------------------
+//
+// When the C tiles of a plain contraction are fewer than the SMs, the summed
+// range is cut into P pieces of kq (a multiple of the pack k-step): piece p is
+// packed as the "product" A(:, piece p) B(piece p, :), the P pieces run side by
+// side in one GEMM launch into their own M_p (batch entry p * batch + b), and
+// the combine pass forms C = alpha * sum_p M_p + beta * C in FP64 in piece
+// order.  No counterpart in the reference, whose threads split the loops of
+// the one GEMM instead.
+
+PackGeom ksplit_geom(const GemmView& g, int P)
+{
+    PackGeom p;
+    p.ms = g.m; p.ns = g.n;
+    p.ks = cdiv(cdiv(g.k, P), PACK_KSTEP) * PACK_KSTEP;
+    p.k_pad = p.ks;
+    p.tm = cdiv(p.ms, PACK_TILE); p.tn = cdiv(p.ns, PACK_TILE);
+    p.s_elems = (size_t)(g.batch * p.tm * p.k_pad * PACK_TILE);
+    p.t_elems = (size_t)(g.batch * p.tn * p.k_pad * PACK_TILE);
+    p.fits = 2 * p.tm <= 65535 && 2 * p.tn <= 65535 && g.batch <= 65535 && g.batch * p.tm <= 65535 &&
+             g.batch * p.tn <= 65535;
+    return p;
+}
+
+int ksplit_pieces(const GemmView& g, int sms)
+{
+    const int64_t tiles = g.batch * cdiv(g.m, PACK_TILE) * cdiv(g.n, PACK_TILE);
+    if (tiles >= sms || g.k < 1024 || g.m * g.n >= ((int64_t)1 << 31)) return 1;
+    int64_t P = cdiv(2 * (int64_t)sms, tiles);
+    P = std::min<int64_t>(P, g.k / 512);
+    P = std::min<int64_t>(P, MAX_COMBINE_PRODUCTS);
+    return (int)std::max<int64_t>(P, 1);
+}
+
+size_t fp64_ksplit_workspace_bytes(const GemmView& g, int P)
+{
+    const PackGeom pg = ksplit_geom(g, P);
+    const size_t st = ((size_t)P * (pg.s_elems + pg.t_elems) * sizeof(double) + 255) / 256 * 256;
+    return st + (size_t)P * (size_t)(g.batch * g.m * g.n) * sizeof(double);
+}
+
+int run_fp64_ksplit_enqueue(const GemmView& g, const int64_t* const tb[9], const double* A, const double* B,
+                            double* C, cudaStream_t st, int sms, void* ws, size_t ws_bytes, int P,
+                            const int64_t* mtab, bool col_major, int* err)
+{
+    if (P < 2 || P > MAX_COMBINE_PRODUCTS) return TBLIS_STRA_ERR_ARG;
+    const PackGeom pg = ksplit_geom(g, P);
+    if (!pg.fits) return TBLIS_STRA_ERR_TOO_LARGE;
+    if (ws_bytes < fp64_ksplit_workspace_bytes(g, P)) return TBLIS_STRA_ERR_ALLOC;
+    double* S = static_cast<double*>(ws);
+    double* T = S + (size_t)P * pg.s_elems;
+    double* M = reinterpret_cast<double*>(static_cast<char*>(ws) +
+                                          ((size_t)P * (pg.s_elems + pg.t_elems) * sizeof(double) + 255) / 256 * 256);
+    int s;
+    for (int p = 0; p < P; p++)
+    {
+        Product piece;
+        piece.na = piece.nb = piece.nc = 1;
+        piece.a[0] = {0, (int8_t)p, 1};     // rows 0.., k piece p
+        piece.b[0] = {(int8_t)p, 0, 1};     // k piece p, columns 0..
+        piece.c[0] = {0, 0, 1};
+        if ((s = enqueue_pack_product(piece, g, pg, tb, A, B, S + (size_t)p * pg.s_elems,
+                                      T + (size_t)p * pg.t_elems, st)))
+            return s;
+    }
+    PackedGemmArgs ga{};
+    ga.err = err;
+    ga.C = M;
+    ga.rsC = mtab; ga.csC = mtab + g.m; ga.bC = mtab + g.m + g.n;
+    ga.m = g.m; ga.n = g.n; ga.ms = g.m; ga.ns = g.n; ga.k_pad = pg.k_pad;
+    ga.tiles_m = pg.tm; ga.tiles_n = pg.tn; ga.batch = (int64_t)P * g.batch;
+    ga.alpha = 1.0; ga.beta = 0.0;
+    ga.H = 1; ga.nprod = 1;
+    ga.S[0] = S; ga.T[0] = T;
+    ga.nc[0] = 1; ga.c_s[0][0] = 1; ga.c_first[0][0] = 1;
+    TSB_CUDA(launch_packed_gemm(ga, st, sms));
+
+    CombineArgs c{};
+    c.C = C; c.rsC = tb[1]; c.csC = tb[3]; c.bC = tb[8];
+    c.m = g.m; c.n = g.n; c.ms = g.m; c.ns = g.n; c.batch = g.batch;
+    c.M = M; c.m_pstride = g.batch * g.m * g.n;
+    c.alpha = g.alpha; c.beta = g.beta;
+    c.H = 1; c.col_major = col_major ? 1 : 0;
+    c.np = P;
+    for (int p = 0; p < P; p++) { c.nt[p] = 1; c.th[p][0] = 0; c.ts[p][0] = 1; }
     TSB_CUDA(launch_combine(c, st));
     return TBLIS_STRA_SUCCESS;
 }

@@ -77,6 +77,15 @@ int run_fp64_parallel_enqueue(int level, const GemmView& g, const int64_t* const
 int enqueue_products_and_combine(int level, const GemmView& g, const int64_t* const tb[9], double* C,
                                  cudaStream_t st, int sms, void* ws, const int64_t* mtab, bool col_major,
                                  int* err);
+// k-split plain contraction (L = 0): the number of pieces for a grid of
+// fewer C tiles than SMs (1: no split), its workspace, and the schedule (P
+// packed piece pairs, one GEMM over them into M_p, one combine launch; M
+// tables for m x n with P * batch entries).
+int ksplit_pieces(const GemmView& g, int sms);
+size_t fp64_ksplit_workspace_bytes(const GemmView& g, int P);
+int run_fp64_ksplit_enqueue(const GemmView& g, const int64_t* const tb[9], const double* A, const double* B,
+                            double* C, cudaStream_t st, int sms, void* ws, size_t ws_bytes, int P,
+                            const int64_t* mtab, bool col_major, int* err);
 // Host copy of those tables: rows[ms], cols[ns], batch[nb].
 void dense_m_tables(int64_t ms, int64_t ns, int64_t nb, bool col_major, int64_t* out);
 // M's layout for C's layout: column-major when C's row bundle is the faster.

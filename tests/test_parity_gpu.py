@@ -223,6 +223,34 @@ def test_product_parallel_batch_and_beta0(tsb, cuda, level, order):
     assert np.abs(C - R).max() <= tol(level, ext["k"], A, B, -1.5)
 
 
+@pytest.mark.parametrize("order", ["F", "C"])
+def test_ksplit_small_grid_large_k(tsb, cuda, order):
+    """L=0 with fewer C tiles than SMs and a long summed range: k is cut into
+    pieces run side by side and summed by the combine pass (9 pieces here:
+    4 tiles, k = 5000), with a batch label and beta = 0 over a NaN-filled C."""
+    import torch
+    ext = dict(i=200, j=190, k=5000, z=2)
+    A = oracle.uniform((ext["i"], ext["k"], ext["z"]), 31, order)
+    B = oracle.uniform((ext["k"], ext["j"], ext["z"]), 32, order)
+    C0 = np.full((ext["i"], ext["j"], ext["z"]), np.nan, order=order)
+    R = np.zeros(C0.shape, order=order)
+    oracle.contract(0.5, A, "ikz", B, "kjz", 0.0, R, "ijz")
+    before = tsb.launch_count()
+    C = run_gpu(tsb, cuda, 0, 1, 0.5, A, "ikz", B, "kjz", 0.0, C0, "ijz")
+    # tiles: 2 x 2 x batch 2 = 8; pieces min(ceil(296 / 8), 5000 // 512) = 9
+    assert tsb.launch_count() - before == 2 * 9 + 2
+    assert np.isfinite(C).all()
+    assert np.abs(C - R).max() <= tol(0, ext["k"], A, B, 0.5)
+    tsb.set_product_parallel(0)
+    try:
+        before = tsb.launch_count()
+        C = run_gpu(tsb, cuda, 0, 1, 0.5, A, "ikz", B, "kjz", 0.0, C0, "ijz")
+        assert tsb.launch_count() - before == 3        # no split: 2 packs + GEMM
+    finally:
+        tsb.set_product_parallel(-1)
+    assert np.abs(C - R).max() <= tol(0, ext["k"], A, B, 0.5)
+
+
 def test_launch_counter_moves(tsb, cuda):
     A = oracle.uniform((16, 16), 1)
     tsb.set_workspace_limit(0)

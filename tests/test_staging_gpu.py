@@ -42,9 +42,10 @@ def test_pipelined_split_of_b_and_c(tsb, cuda, level, pinned):
     C0 = oracle.uniform((e,) * 4, 3)
     got, want, launches = run_pair(tsb, cuda, level, A, "efac", B, "fbde", C0, "abcd", pinned)
     assert np.abs(got - want).max() <= bound(level, e * e)
-    # L=0: 2 packs + GEMM; L=1 (14 tiles per product, product-parallel):
+    # L=0 (28 tiles, k 1764: k-split in 3 pieces): 6 packs + the GEMM over the
+    # pieces + the combine; L=1 (14 tiles per product, product-parallel):
     # 2 group packs + the GEMM over the 7 products + the combine
-    per_call = 3 if level == 0 else 4
+    per_call = 8 if level == 0 else 4
     assert launches == 8 * per_call          # d in 4 chunks x c in 2
 
 
