@@ -203,8 +203,16 @@ split_pack_kernel(const __grid_constant__ SplitPackArgs a)
         buf[r][k_of(x)] = v[x] * rscale[r];
     }
     __syncthreads();
-    write_planes(buf, a.out, (size_t)a.batch * a.tiles * a.nk * BLK,
-                 ((size_t)(b * a.tiles + t) * a.nk + c) * BLK, half, a.planes, tid);
+    if (a.nkpiece > 0)
+    {
+        const int64_t p = c / a.nkpiece;
+        const size_t plane = (size_t)a.batch * a.tiles * a.nkpiece * BLK;
+        write_planes(buf, reinterpret_cast<unsigned char*>(a.out) + p * a.planes * plane, plane,
+                     ((size_t)(b * a.tiles + t) * a.nkpiece + (c - p * a.nkpiece)) * BLK, half, a.planes, tid);
+    }
+    else
+        write_planes(buf, a.out, (size_t)a.batch * a.tiles * a.nk * BLK,
+                     ((size_t)(b * a.tiles + t) * a.nk + c) * BLK, half, a.planes, tid);
 }
 
 // Seven split sums of one product group per pass (L >= 1), the FP32 form of
@@ -711,6 +719,7 @@ cudaError_t launch_split_pack(const SplitPackArgs& a, cudaStream_t stream)
 {
     if (a.batch <= 0 || a.tiles <= 0 || a.nk <= 0) return cudaSuccess;
     if (2 * a.tiles > 65535 || a.batch > 65535 || (a.planes != 2 && a.planes != 3)) return cudaErrorInvalidValue;
+    if (a.nkpiece < 0 || (a.nkpiece > 0 && a.nk % a.nkpiece)) return cudaErrorInvalidValue;
     dim3 grid((unsigned)a.nk, (unsigned)(2 * a.tiles), (unsigned)a.batch);
     timing_begin(KK_PACK, stream);
     split_pack_kernel<<<grid, 256, 0, stream>>>(a);

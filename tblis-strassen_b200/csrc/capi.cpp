@@ -999,17 +999,27 @@ int run_fp64_ksplit_enqueue(const GemmView& g, const int64_t* const tb[9], const
     double* T = S + (size_t)P * pg.s_elems;
     double* M = reinterpret_cast<double*>(static_cast<char*>(ws) +
                                           ((size_t)P * (pg.s_elems + pg.t_elems) * sizeof(double) + 255) / 256 * 256);
-    int s;
-    for (int p = 0; p < P; p++)
+    // One pack launch per operand over all P * kq summed indices, each piece
+    // written as its own batch entries (kpiece).
+    for (int operand = 0; operand < 2; operand++)
     {
-        Product piece;
-        piece.na = piece.nb = piece.nc = 1;
-        piece.a[0] = {0, (int8_t)p, 1};     // rows 0.., k piece p
-        piece.b[0] = {(int8_t)p, 0, 1};     // k piece p, columns 0..
-        piece.c[0] = {0, 0, 1};
-        if ((s = enqueue_pack_product(piece, g, pg, tb, A, B, S + (size_t)p * pg.s_elems,
-                                      T + (size_t)p * pg.t_elems, st)))
-            return s;
+        PackArgs pa{};
+        if (operand == 0)
+        {
+            pa.X = A; pa.rs = tb[0]; pa.ks = tb[4]; pa.bX = tb[6];
+            pa.rows_full = g.m; pa.rows_blk = g.m; pa.tiles = pg.tm; pa.out = S;
+            pa.kfast = g.unit_ksA != 0 && (g.unit_rsA == 0 || g.unit_ksA < g.unit_rsA);
+        }
+        else
+        {
+            pa.X = B; pa.rs = tb[2]; pa.ks = tb[5]; pa.bX = tb[7];
+            pa.rows_full = g.n; pa.rows_blk = g.n; pa.tiles = pg.tn; pa.out = T;
+            pa.kfast = g.unit_ksB != 0 && (g.unit_csB == 0 || g.unit_ksB < g.unit_csB);
+        }
+        pa.k_full = g.k; pa.k_blk = (int64_t)P * pg.ks;
+        pa.nt = 1; pa.t_r[0] = 0; pa.t_c[0] = 0; pa.t_s[0] = 1;
+        pa.k_pad = (int64_t)P * pg.k_pad; pa.batch = g.batch; pa.kpiece = pg.k_pad;
+        TSB_CUDA(launch_pack(pa, st));
     }
     PackedGemmArgs ga{};
     ga.err = err;
@@ -1404,6 +1414,94 @@ int run_fp32_parallel_enqueue(int level, const GemmView& g, const int64_t* const
     return TBLIS_STRA_SUCCESS;
 }
 
+// k-split of a plain FP32 contraction (as run_fp64_ksplit_enqueue): the row
+// and column scales over the whole summed range, the split planes of each
+// piece (plane set p), one split GEMM over P * batch entries into M_p (FP32),
+// and the combine pass summing the pieces in FP64.
+size_t fp32_ksplit_workspace_bytes(const GemmView& g, int P, int terms)
+{
+    const int64_t kq = cdiv(cdiv(g.k, P), SPLIT_K) * SPLIT_K;
+    const int64_t nk = kq / SPLIT_K;
+    const size_t blk = (size_t)SPLIT_TILE * SPLIT_K * 2;
+    const int planes = terms == 3 ? 2 : 3;
+    const size_t sc = ((size_t)g.batch * (g.m + g.n) * 2 * sizeof(float) + 255) / 256 * 256;
+    const size_t pl = (size_t)P * planes * g.batch * (cdiv(g.m, SPLIT_TILE) + cdiv(g.n, SPLIT_TILE)) * nk * blk;
+    return sc + pl + (size_t)P * (size_t)(g.batch * g.m * g.n) * sizeof(float);
+}
+
+int run_fp32_ksplit_enqueue(const GemmView& g, const int64_t* const tb[9], const float* A, const float* B,
+                            float* C, cudaStream_t st, int sms, void* ws, size_t ws_bytes, int terms, int P,
+                            const int64_t* mtab, bool col_major, int* err)
+{
+    if (P < 2 || P > MAX_COMBINE_PRODUCTS) return TBLIS_STRA_ERR_ARG;
+    const int64_t kq = cdiv(cdiv(g.k, P), SPLIT_K) * SPLIT_K;
+    const int64_t nk = kq / SPLIT_K;
+    const int64_t tm = cdiv(g.m, SPLIT_TILE), tn = cdiv(g.n, SPLIT_TILE);
+    if (g.batch * tm > 65535 || g.batch * tn > 65535) return TBLIS_STRA_ERR_TOO_LARGE;
+    if (ws_bytes < fp32_ksplit_workspace_bytes(g, P, terms)) return TBLIS_STRA_ERR_ALLOC;
+    const int planes = terms == 3 ? 2 : 3;
+    const size_t blk = (size_t)SPLIT_TILE * SPLIT_K * 2;
+    const size_t sc = ((size_t)g.batch * (g.m + g.n) * 2 * sizeof(float) + 255) / 256 * 256;
+    float* scaleA = static_cast<float*>(ws);
+    float* invA = scaleA + g.batch * g.m;
+    float* scaleB = invA + g.batch * g.m;
+    float* invB = scaleB + g.batch * g.n;
+    const size_t bytesA = (size_t)planes * g.batch * tm * nk * blk, bytesB = (size_t)planes * g.batch * tn * nk * blk;
+    char* planesA = static_cast<char*>(ws) + sc;
+    char* planesB = planesA + P * bytesA;
+    float* M = reinterpret_cast<float*>(planesB + P * bytesB);
+
+    SplitScaleArgs sa{A, tb[0], tb[4], tb[6], g.m, g.k, g.m, 1, g.batch, scaleA, invA};
+    TSB_CUDA(launch_split_scale(sa, st));
+    SplitScaleArgs sb{B, tb[2], tb[5], tb[7], g.n, g.k, g.n, 1, g.batch, scaleB, invB};
+    TSB_CUDA(launch_split_scale(sb, st));
+    // One split-pack launch per operand over all P * kq summed indices, each
+    // piece written as its own plane set (nkpiece).
+    SplitPackArgs pa{};
+    pa.X = A; pa.rs = tb[0]; pa.ks = tb[4]; pa.bX = tb[6];
+    pa.rows_full = g.m; pa.k_full = g.k; pa.rows_blk = g.m; pa.k_blk = (int64_t)P * kq;
+    pa.nt = 1; pa.t_r[0] = 0; pa.t_c[0] = 0; pa.t_s[0] = 1;
+    pa.scale = scaleA; pa.tiles = tm; pa.nk = (int64_t)P * nk; pa.nkpiece = nk; pa.batch = g.batch;
+    pa.planes = planes; pa.out = planesA;
+    pa.kfast = g.unit_ksA != 0 && (g.unit_rsA == 0 || g.unit_ksA < g.unit_rsA);
+    TSB_CUDA(launch_split_pack(pa, st));
+    SplitPackArgs pb{};
+    pb.X = B; pb.rs = tb[2]; pb.ks = tb[5]; pb.bX = tb[7];
+    pb.rows_full = g.n; pb.k_full = g.k; pb.rows_blk = g.n; pb.k_blk = (int64_t)P * kq;
+    pb.nt = 1; pb.t_r[0] = 0; pb.t_c[0] = 0; pb.t_s[0] = 1;
+    pb.scale = scaleB; pb.tiles = tn; pb.nk = (int64_t)P * nk; pb.nkpiece = nk; pb.batch = g.batch;
+    pb.planes = planes; pb.out = planesB;
+    pb.kfast = g.unit_ksB != 0 && (g.unit_csB == 0 || g.unit_ksB < g.unit_csB);
+    TSB_CUDA(launch_split_pack(pb, st));
+
+    static const int8_t TA6[6] = {0, 0, 1, 0, 1, 2}, TB6[6] = {0, 1, 0, 2, 1, 0};
+    SplitGemmArgs ga{};
+    ga.A[0] = planesA; ga.B[0] = planesB; ga.C = M;
+    ga.rsC = mtab; ga.csC = mtab + g.m; ga.bC = mtab + g.m + g.n;
+    ga.invA = invA; ga.invB = invB;
+    ga.m = g.m; ga.n = g.n; ga.ms = g.m; ga.ns = g.n; ga.nk = nk;
+    ga.tiles_m = tm; ga.tiles_n = tn; ga.batch = (int64_t)P * g.batch; ga.pbatch = g.batch;
+    ga.alpha = 1.f; ga.beta = 0.f;
+    ga.nprod = 1; ga.H = 1;
+    ga.nc[0] = 1; ga.c_s[0][0] = 1; ga.c_first[0][0] = 1;
+    ga.planes = planes;
+    ga.nterms = planes == 3 ? 6 : 3;
+    for (int i = 0; i < 6; i++) { ga.ta[i] = TA6[i]; ga.tb[i] = TB6[i]; }
+    ga.err = err;
+    TSB_CUDA(launch_split_gemm(ga, st, sms));
+
+    CombineF32Args c{};
+    c.C = C; c.rsC = tb[1]; c.csC = tb[3]; c.bC = tb[8];
+    c.m = g.m; c.n = g.n; c.ms = g.m; c.ns = g.n; c.batch = g.batch;
+    c.M = M; c.m_pstride = g.batch * g.m * g.n;
+    c.alpha = g.alpha; c.beta = g.beta;
+    c.H = 1; c.col_major = col_major ? 1 : 0;
+    c.np = P;
+    for (int p = 0; p < P; p++) { c.nt[p] = 1; c.th[p][0] = 0; c.ts[p][0] = 1; }
+    TSB_CUDA(launch_combine(c, st));
+    return TBLIS_STRA_SUCCESS;
+}
+
 namespace {
 
 int run_fp32(int level, const GemmView& g, const DevPlan& t, const float* A, const float* B,
@@ -1423,6 +1521,34 @@ int run_fp32(int level, const GemmView& g, const DevPlan& t, const float* A, con
     // idle and its workspace is allowed (as for FP64).
     const int sms = num_sms(device);
     const int H = product_table(level).H;
+    const int64_t* tb[9] = {t.rsA, t.rsC, t.csB, t.csC, t.ksA, t.ksB, t.bA, t.bB, t.bC};
+    // A plain contraction with fewer C tiles than SMs: k-split.
+    const int P = level == 0 && t_product_parallel != 0 ? ksplit_pieces(g, sms) : 1;
+    if (P >= 2 && fp32_ksplit_workspace_bytes(g, P, terms) <= t_ws_limit)
+    {
+        const int64_t* ktab = nullptr;
+        if ((s = plan_m_tables(t, 0, g.m, g.n, (int64_t)P * g.batch, m_tables_col_major(g), ktab))) return s;
+        const size_t wsk = fp32_ksplit_workspace_bytes(g, P, terms);
+        if ((s = wsbuf.alloc(wsk, st))) return s;
+        int* err = shared_err;
+        if (!err)
+        {
+            if ((s = errbuf.alloc(sizeof(int), st))) return s;
+            TSB_CUDA(cudaMemsetAsync(errbuf.p, 0, sizeof(int), st));
+            err = static_cast<int*>(errbuf.p);
+        }
+        if ((s = run_fp32_ksplit_enqueue(g, tb, A, B, C, st, sms, wsbuf.p, wsk, terms, P, ktab,
+                                         m_tables_col_major(g), err)))
+            return s;
+        if (blocking && !shared_err)
+        {
+            int flag = 0;
+            TSB_CUDA(cudaMemcpyAsync(&flag, errbuf.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            TSB_CUDA(cudaStreamSynchronize(st));
+            if (flag) return TBLIS_STRA_ERR_TIMEOUT;
+        }
+        return TBLIS_STRA_SUCCESS;
+    }
     const bool parallel = use_product_parallel(level, g, sms, true, terms);
     const size_t wsb_par = parallel ? fp32_parallel_workspace_bytes(level, g, terms) : 0;
     const bool m_col_major = m_tables_col_major(g);
@@ -1441,7 +1567,6 @@ int run_fp32(int level, const GemmView& g, const DevPlan& t, const float* A, con
         TSB_CUDA(cudaMemsetAsync(errbuf.p, 0, sizeof(int), st));
         err = static_cast<int*>(errbuf.p);
     }
-    const int64_t* tb[9] = {t.rsA, t.rsC, t.csB, t.csC, t.ksA, t.ksB, t.bA, t.bB, t.bC};
     s = parallel ? run_fp32_parallel_enqueue(level, g, tb, A, B, C, st, sms, wsbuf.p, wsb, terms, mtab,
                                              m_col_major, err)
                  : run_fp32_enqueue(level, g, tb, A, B, C, st, sms, wsbuf.p, wsb, terms, err);

@@ -153,6 +153,10 @@ struct PackArgs
     int64_t tiles, k_pad, batch;
     int kfast;                                 // 1: X is contiguous along k
     double* out;
+    // 0, or the k length of the pieces of a k-split (a multiple of the pack
+    // k-step dividing k_pad): piece p = k / kpiece is written as batch entry
+    // p * batch + b of a problem whose k_pad is kpiece.
+    int64_t kpiece;
 };
 
 // Packed GEMM (S and T packed, PACK_TILE x k_pad tiles): for every 128 x 128 tile position, products q = 0..nprod-1 in
@@ -242,6 +246,10 @@ struct SplitPackArgs
     int planes;                                // 2 (3-term) or 3 (6-term)
     int kfast;
     void* out;                                 // bf16 planes
+    // 0, or the k blocks per piece of a k-split (dividing nk): k block c of
+    // piece p = c / nkpiece is written as batch entry b of plane set p (plane
+    // sets of planes * batch * tiles * nkpiece blocks, one after another).
+    int64_t nkpiece;
 };
 
 // Seven split sums of one product group in one pass (split_pack_multi_kernel;

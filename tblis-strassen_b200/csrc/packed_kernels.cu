@@ -125,7 +125,15 @@ pack_kernel(const __grid_constant__ PackArgs a)
 #pragma unroll
     for (int e = 0; e < PK_E; e++) buf[pk_row(kfast, warp, lane, e)][pk_k(kfast, warp, lane, e)] = v[e];
     __syncthreads();
-    pk_write(buf, a.out + ((b * a.tiles + t) * a.k_pad + k0) * PACK_TILE, k0, a.k_pad, half, warp, lane);
+    double* dst;
+    if (a.kpiece > 0)
+    {
+        const int64_t p = k0 / a.kpiece;
+        dst = a.out + (((p * a.batch + b) * a.tiles + t) * a.kpiece + (k0 - p * a.kpiece)) * PACK_TILE;
+    }
+    else
+        dst = a.out + ((b * a.tiles + t) * a.k_pad + k0) * PACK_TILE;
+    pk_write(buf, dst, k0, a.k_pad, half, warp, lane);
 }
 
 // Seven sums of one product group per pass (L >= 1): each CTA reads its
@@ -808,6 +816,7 @@ cudaError_t launch_pack(const PackArgs& a, cudaStream_t stream)
 {
     if (a.batch <= 0 || a.tiles <= 0 || a.k_pad <= 0) return cudaSuccess;
     if (a.k_pad % PK_K && a.k_pad % PACK_KSTEP) return cudaErrorInvalidValue;
+    if (a.kpiece < 0 || (a.kpiece > 0 && (a.kpiece % PK_K || a.k_pad % a.kpiece))) return cudaErrorInvalidValue;
     dim3 grid((unsigned)((a.k_pad + PK_K - 1) / PK_K), (unsigned)(2 * a.tiles), (unsigned)a.batch);
     if (2 * a.tiles > 65535 || a.batch > 65535) return cudaErrorInvalidValue;
     timing_begin(KK_PACK, stream);

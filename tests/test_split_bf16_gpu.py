@@ -185,3 +185,27 @@ def test_fp32_group_launches(tsb, cuda, terms, level):
             tsb.set_product_parallel(-1)
         err = normwise(dC.cpu().numpy(), R)
         assert err <= TOL[terms], (mode, err)
+
+
+def test_fp32_ksplit_small_grid_large_k(tsb, cuda, terms):
+    """L=0 with fewer C tiles than SMs and a long summed range: the split
+    planes of 9 k pieces run side by side and the combine pass sums them in
+    FP64 (batch label, beta = 0 over a NaN-filled C)."""
+    import torch
+    ext = dict(i=200, j=190, k=5000, z=2)
+    A = draw((ext["i"], ext["k"], ext["z"]), 41, "loguniform")
+    B = draw((ext["k"], ext["j"], ext["z"]), 42, "loguniform")
+    C0 = np.full((ext["i"], ext["j"], ext["z"]), np.nan, dtype=np.float32, order="F")
+    R = np.zeros(C0.shape, order="F")
+    oracle.contract(1.0, A.astype(np.float64, order="F"), "ikz", B.astype(np.float64, order="F"), "kjz",
+                    0.0, R, "ijz")
+    dC = to_dev(C0, cuda)
+    before = tsb.launch_count()
+    tsb.contract(0, 1.0, to_dev(A, cuda), "ikz", to_dev(B, cuda), "kjz", 0.0, dC, "ijz")
+    torch.cuda.synchronize()
+    # 2 scales, one pack per operand (9 pieces), the GEMM over the pieces,
+    # the combine
+    assert tsb.launch_count() - before == 6
+    out = dC.cpu().numpy()
+    assert np.isfinite(out).all()
+    assert normwise(out, R) <= TOL[terms]

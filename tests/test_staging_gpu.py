@@ -42,10 +42,10 @@ def test_pipelined_split_of_b_and_c(tsb, cuda, level, pinned):
     C0 = oracle.uniform((e,) * 4, 3)
     got, want, launches = run_pair(tsb, cuda, level, A, "efac", B, "fbde", C0, "abcd", pinned)
     assert np.abs(got - want).max() <= bound(level, e * e)
-    # L=0 (28 tiles, k 1764: k-split in 3 pieces): 6 packs + the GEMM over the
+    # L=0 (28 tiles, k 1764: k-split in 3 pieces): 2 packs + the GEMM over the
     # pieces + the combine; L=1 (14 tiles per product, product-parallel):
     # 2 group packs + the GEMM over the 7 products + the combine
-    per_call = 8 if level == 0 else 4
+    per_call = 4
     assert launches == 8 * per_call          # d in 4 chunks x c in 2
 
 
@@ -69,7 +69,9 @@ def test_pipelined_fp32(tsb, cuda):
     got, want, launches = run_pair(tsb, cuda, 0, A, "efac", B, "fbde", C0, "abcd", True)
     d = np.linalg.norm((got.astype(np.float64) - want).ravel()) / np.linalg.norm(want.ravel())
     assert d <= 2e-6
-    assert launches == 8 * 5                 # 8 chunks of 2 scales, 2 packs, GEMM
+    # 8 chunks of 1352 x 676 x 2704 (66 tiles: k-split in 5 pieces): 2 scales,
+    # 2 packs, the GEMM over the pieces, the combine
+    assert launches == 8 * 6
 
 
 def test_pipelined_one_cut_with_batch_label(tsb, cuda):
