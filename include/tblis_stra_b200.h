@@ -196,7 +196,7 @@ size_t tblis_stra_get_workspace_limit(void);
  * idle (fewer tiles than SMs included), ABC packs every product's sums, runs
  * all 7^L products side by side in one GEMM launch into their own M_p, and
  * forms each C block as alpha * sum_p W[h][p] M_p + beta * C in one pass;
- * FP32 does the same on its split-BF16 path.  It needs 7^L * (packed sums +
+ * FP32 takes this form on its split-BF16 path at every L >= 1.  It needs 7^L * (packed sums +
  * batch*ms*ns elements of M) bytes within the workspace limit.  AB and Naive
  * (which hold M temporaries by design) always take this form when mode is
  * not 0.  At L = 0 with fewer C tiles than SMs and at least 1024 summed

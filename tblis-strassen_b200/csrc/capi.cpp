@@ -176,13 +176,15 @@ int plan_m_tables(const DevPlan& t, int level, int64_t ms, int64_t ns, int64_t n
 // tile by tile (M's local index must fit 32 bits).  At L = 2 it does at every
 // size measured: a product's C tiles spread over up to 4 blocks, and with
 // products side by side each is written once (as M) and combined in one
-// pass.  At L = 1 it does when the last wave of one product's `tiles` on `sms`
-// SMs leaves more than a tenth of the launch idle (fewer tiles than SMs
-// included).
-bool parallel_pays(int level, int64_t tiles, int sms, int64_t ms, int64_t ns)
+// pass.  So it does for the split-BF16 GEMM at L = 1 (16384^3, 6 terms: 200 ->
+// 234 TFLOP/s), whose drain epilogue of up to 2 C tiles per product competes
+// with the MMAs of the next.  For FP64 at L = 1 it does when the last wave of
+// one product's `tiles` on `sms` SMs leaves more than a tenth of the launch
+// idle (fewer tiles than SMs included).
+bool parallel_pays(int level, bool fp32, int64_t tiles, int sms, int64_t ms, int64_t ns)
 {
     if (ms * ns >= ((int64_t)1 << 31)) return false;
-    if (level >= 2) return true;
+    if (level >= 2 || fp32) return true;
     const int64_t rounds = (tiles + sms - 1) / sms;
     return rounds * sms * 10 > tiles * 11;
 }
@@ -1192,9 +1194,11 @@ int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], c
 
     if (enqueue)
     {
-        SplitScaleArgs sa{A, tb[0], tb[4], tb[6], g.m, g.k, ms, H, g.batch, scaleA, invA};
+        SplitScaleArgs sa{A, tb[0], tb[4], tb[6], g.m, g.k, ms, H, g.batch, scaleA, invA,
+                       g.unit_ksA != 0 && (g.unit_rsA == 0 || g.unit_ksA < g.unit_rsA) ? 1 : 0};
         TSB_CUDA(launch_split_scale(sa, st));
-        SplitScaleArgs sb{B, tb[2], tb[5], tb[7], g.n, g.k, ns, H, g.batch, scaleB, invB};
+        SplitScaleArgs sb{B, tb[2], tb[5], tb[7], g.n, g.k, ns, H, g.batch, scaleB, invB,
+                       g.unit_ksB != 0 && (g.unit_csB == 0 || g.unit_ksB < g.unit_csB) ? 1 : 0};
         TSB_CUDA(launch_split_scale(sb, st));
     }
 
@@ -1319,7 +1323,7 @@ bool use_product_parallel(int level, const GemmView& g, int sms, bool fp32, int 
         if (!pg.fits || fp64_parallel_workspace_bytes(level, g) > t_ws_limit) return false;
         tiles = g.batch * pg.tm * pg.tn;
     }
-    return t_product_parallel == 1 || parallel_pays(level, tiles, sms, ms, ns);
+    return t_product_parallel == 1 || parallel_pays(level, fp32, tiles, sms, ms, ns);
 }
 
 bool m_tables_col_major(const GemmView& g)
@@ -1356,9 +1360,11 @@ int run_fp32_parallel_enqueue(int level, const GemmView& g, const int64_t* const
     char* planesB = planesA + np * bytesA;
     float* M = reinterpret_cast<float*>(planesB + np * bytesB);
 
-    SplitScaleArgs sa{A, tb[0], tb[4], tb[6], g.m, g.k, ms, H, g.batch, scaleA, invA};
+    SplitScaleArgs sa{A, tb[0], tb[4], tb[6], g.m, g.k, ms, H, g.batch, scaleA, invA,
+                       g.unit_ksA != 0 && (g.unit_rsA == 0 || g.unit_ksA < g.unit_rsA) ? 1 : 0};
     TSB_CUDA(launch_split_scale(sa, st));
-    SplitScaleArgs sb{B, tb[2], tb[5], tb[7], g.n, g.k, ns, H, g.batch, scaleB, invB};
+    SplitScaleArgs sb{B, tb[2], tb[5], tb[7], g.n, g.k, ns, H, g.batch, scaleB, invB,
+                       g.unit_ksB != 0 && (g.unit_csB == 0 || g.unit_ksB < g.unit_csB) ? 1 : 0};
     TSB_CUDA(launch_split_scale(sb, st));
 
     if (!pack_group(level, 0, 0)) return TBLIS_STRA_ERR_UNSUPPORTED;
@@ -1451,9 +1457,11 @@ int run_fp32_ksplit_enqueue(const GemmView& g, const int64_t* const tb[9], const
     char* planesB = planesA + P * bytesA;
     float* M = reinterpret_cast<float*>(planesB + P * bytesB);
 
-    SplitScaleArgs sa{A, tb[0], tb[4], tb[6], g.m, g.k, g.m, 1, g.batch, scaleA, invA};
+    SplitScaleArgs sa{A, tb[0], tb[4], tb[6], g.m, g.k, g.m, 1, g.batch, scaleA, invA,
+                       g.unit_ksA != 0 && (g.unit_rsA == 0 || g.unit_ksA < g.unit_rsA) ? 1 : 0};
     TSB_CUDA(launch_split_scale(sa, st));
-    SplitScaleArgs sb{B, tb[2], tb[5], tb[7], g.n, g.k, g.n, 1, g.batch, scaleB, invB};
+    SplitScaleArgs sb{B, tb[2], tb[5], tb[7], g.n, g.k, g.n, 1, g.batch, scaleB, invB,
+                       g.unit_ksB != 0 && (g.unit_csB == 0 || g.unit_ksB < g.unit_csB) ? 1 : 0};
     TSB_CUDA(launch_split_scale(sb, st));
     // One split-pack launch per operand over all P * kq summed indices, each
     // piece written as its own plane set (nkpiece).
