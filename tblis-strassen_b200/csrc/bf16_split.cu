@@ -72,75 +72,30 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p)
 
 // ---- row scales -------------------------------------------------------------------
 
-// Power of two 2^-e with 2^-e * m in [0.5, 1) for the row maximum m.
-__device__ __forceinline__ void write_scale(const SplitScaleArgs& a, int64_t i, float m)
-{
-    int e = 0;
-    if (m > 0.f && isfinite(m)) frexpf(m, &e);
-    e = max(-120, min(120, e));
-    a.scale[i] = ldexpf(1.f, -e);
-    a.inv[i] = ldexpf(1.f, e);
-}
-
-// Row maxima over every block of the row index.  kfast: one warp per row, its
-// lanes on consecutive k, eight loads in flight per lane; else one thread per
-// row (consecutive threads on consecutive rows), eight k in flight.
-constexpr int SC_U = 8;
-
 __global__ void scale_kernel(const __grid_constant__ SplitScaleArgs a)
 {
+    const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    if (a.kfast)
-    {
-        const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-        if (wid >= a.batch * a.rows_blk) return;
-        const int64_t b = wid / a.rows_blk, r = wid % a.rows_blk;
-        float m = 0.f;
-        for (int h = 0; h < a.parts; h++)
-        {
-            const int64_t gr = h * a.rows_blk + r;
-            if (gr >= a.rows_full) continue;
-            const float* row = a.X + a.bX[b] + a.rs[gr];
-            for (int64_t k0 = lane; k0 < a.k_full; k0 += 32 * SC_U)
-            {
-                int64_t off[SC_U];
-#pragma unroll
-                for (int u = 0; u < SC_U; u++)
-                {
-                    const int64_t k = k0 + 32 * u;
-                    off[u] = k < a.k_full ? a.ks[k] : OFF_INVALID;
-                }
-                float x[SC_U];
-#pragma unroll
-                for (int u = 0; u < SC_U; u++) x[u] = off[u] != OFF_INVALID ? fabsf(row[off[u]]) : 0.f;
-#pragma unroll
-                for (int u = 0; u < SC_U; u++) m = fmaxf(m, x[u]);
-            }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-        if (lane == 0) write_scale(a, wid, m);
-        return;
-    }
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.batch * a.rows_blk) return;
-    const int64_t b = i / a.rows_blk, r = i % a.rows_blk;
+    if (wid >= a.batch * a.rows_blk) return;
+    const int64_t b = wid / a.rows_blk, r = wid % a.rows_blk;
     float m = 0.f;
     for (int h = 0; h < a.parts; h++)
     {
         const int64_t gr = h * a.rows_blk + r;
         if (gr >= a.rows_full) continue;
-        const float* row = a.X + a.bX[b] + a.rs[gr];
-        for (int64_t k0 = 0; k0 < a.k_full; k0 += SC_U)
-        {
-            float x[SC_U];
-#pragma unroll
-            for (int u = 0; u < SC_U; u++) x[u] = k0 + u < a.k_full ? fabsf(row[a.ks[k0 + u]]) : 0.f;
-#pragma unroll
-            for (int u = 0; u < SC_U; u++) m = fmaxf(m, x[u]);
-        }
+        const int64_t base = a.bX[b] + a.rs[gr];
+        for (int64_t k = lane; k < a.k_full; k += 32) m = fmaxf(m, fabsf(a.X[base + a.ks[k]]));
     }
-    write_scale(a, i, m);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0)
+    {
+        int e = 0;
+        if (m > 0.f && isfinite(m)) frexpf(m, &e);
+        e = max(-120, min(120, e));
+        a.scale[wid] = ldexpf(1.f, -e);
+        a.inv[wid] = ldexpf(1.f, e);
+    }
 }
 
 // ---- split pack -------------------------------------------------------------------
@@ -749,9 +704,9 @@ cudaError_t launch_split_grouped_p(const SplitGroupArgs& g, cudaStream_t stream,
 
 cudaError_t launch_split_scale(const SplitScaleArgs& a, cudaStream_t stream)
 {
-    const int64_t rows = a.batch * a.rows_blk;
-    if (rows <= 0) return cudaSuccess;
-    const int64_t blocks = ((a.kfast ? rows * 32 : rows) + 255) / 256;
+    const int64_t warps = a.batch * a.rows_blk;
+    if (warps <= 0) return cudaSuccess;
+    const int64_t blocks = (warps * 32 + 255) / 256;
     timing_begin(KK_AUX, stream);
     scale_kernel<<<(unsigned)blocks, 256, 0, stream>>>(a);
     timing_end(KK_AUX, stream);

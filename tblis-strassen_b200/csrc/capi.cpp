@@ -1194,11 +1194,9 @@ int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], c
 
     if (enqueue)
     {
-        SplitScaleArgs sa{A, tb[0], tb[4], tb[6], g.m, g.k, ms, H, g.batch, scaleA, invA,
-                       g.unit_ksA != 0 && (g.unit_rsA == 0 || g.unit_ksA < g.unit_rsA) ? 1 : 0};
+        SplitScaleArgs sa{A, tb[0], tb[4], tb[6], g.m, g.k, ms, H, g.batch, scaleA, invA};
         TSB_CUDA(launch_split_scale(sa, st));
-        SplitScaleArgs sb{B, tb[2], tb[5], tb[7], g.n, g.k, ns, H, g.batch, scaleB, invB,
-                       g.unit_ksB != 0 && (g.unit_csB == 0 || g.unit_ksB < g.unit_csB) ? 1 : 0};
+        SplitScaleArgs sb{B, tb[2], tb[5], tb[7], g.n, g.k, ns, H, g.batch, scaleB, invB};
         TSB_CUDA(launch_split_scale(sb, st));
     }
 
@@ -1360,11 +1358,9 @@ int run_fp32_parallel_enqueue(int level, const GemmView& g, const int64_t* const
     char* planesB = planesA + np * bytesA;
     float* M = reinterpret_cast<float*>(planesB + np * bytesB);
 
-    SplitScaleArgs sa{A, tb[0], tb[4], tb[6], g.m, g.k, ms, H, g.batch, scaleA, invA,
-                       g.unit_ksA != 0 && (g.unit_rsA == 0 || g.unit_ksA < g.unit_rsA) ? 1 : 0};
+    SplitScaleArgs sa{A, tb[0], tb[4], tb[6], g.m, g.k, ms, H, g.batch, scaleA, invA};
     TSB_CUDA(launch_split_scale(sa, st));
-    SplitScaleArgs sb{B, tb[2], tb[5], tb[7], g.n, g.k, ns, H, g.batch, scaleB, invB,
-                       g.unit_ksB != 0 && (g.unit_csB == 0 || g.unit_ksB < g.unit_csB) ? 1 : 0};
+    SplitScaleArgs sb{B, tb[2], tb[5], tb[7], g.n, g.k, ns, H, g.batch, scaleB, invB};
     TSB_CUDA(launch_split_scale(sb, st));
 
     if (!pack_group(level, 0, 0)) return TBLIS_STRA_ERR_UNSUPPORTED;
@@ -1457,11 +1453,9 @@ int run_fp32_ksplit_enqueue(const GemmView& g, const int64_t* const tb[9], const
     char* planesB = planesA + P * bytesA;
     float* M = reinterpret_cast<float*>(planesB + P * bytesB);
 
-    SplitScaleArgs sa{A, tb[0], tb[4], tb[6], g.m, g.k, g.m, 1, g.batch, scaleA, invA,
-                       g.unit_ksA != 0 && (g.unit_rsA == 0 || g.unit_ksA < g.unit_rsA) ? 1 : 0};
+    SplitScaleArgs sa{A, tb[0], tb[4], tb[6], g.m, g.k, g.m, 1, g.batch, scaleA, invA};
     TSB_CUDA(launch_split_scale(sa, st));
-    SplitScaleArgs sb{B, tb[2], tb[5], tb[7], g.n, g.k, g.n, 1, g.batch, scaleB, invB,
-                       g.unit_ksB != 0 && (g.unit_csB == 0 || g.unit_ksB < g.unit_csB) ? 1 : 0};
+    SplitScaleArgs sb{B, tb[2], tb[5], tb[7], g.n, g.k, g.n, 1, g.batch, scaleB, invB};
     TSB_CUDA(launch_split_scale(sb, st));
     // One split-pack launch per operand over all P * kq summed indices, each
     // piece written as its own plane set (nkpiece).

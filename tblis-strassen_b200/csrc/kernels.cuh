@@ -232,8 +232,6 @@ struct SplitScaleArgs
     int64_t batch;
     float* scale;                              // [batch][rows_blk] power-of-two multipliers
     float* inv;                                // their inverses
-    int kfast;                                 // 1: X is contiguous along k (a warp walks k),
-                                               // 0: along rows (a thread owns a row)
 };
 
 struct SplitPackArgs
