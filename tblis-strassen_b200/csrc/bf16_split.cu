@@ -21,11 +21,15 @@
 //                    write C_q = (first ? beta*C_q : C_q) + sign*alpha*acc
 //                    / (row scale * column scale).
 //
-// With workspace for a group's planes (L >= 1), split_pack_multi_kernel forms
-// the 7 split sums of a product group from one pass over each operand, and
-// one split_gemm_kernel launch runs the group's 7 products in product order
-// for each tile position, so the C tiles they update stay in L2 between
-// products.
+// At L >= 1, split_pack_multi_kernel forms the 7 split sums of a product group
+// from one pass over each operand.  By default one split_gemm_kernel launch
+// then runs every product side by side (batch entry p * batch + b reads plane
+// set p, `pbatch`) into its own M_p, which the combine pass of aux_kernels.cu
+// sums into C; with that form off, one launch per group runs the group's 7
+// products in product order for each tile position (nprod, per-product C
+// targets), so the C tiles they update stay in L2 between products.  A plain
+// contraction on a small grid splits its summed range the same way
+// (split_pack_kernel's `nkpiece`).
 //
 // Warp roles in split_gemm_kernel (192 threads, one CTA per SM):
 //   warp 0      one lane issues the bulk copies (cp.async.bulk, 1-D TMA) of

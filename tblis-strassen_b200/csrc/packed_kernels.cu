@@ -8,12 +8,17 @@
 // (src/stra_nodes/stra_gemm_ukr.hpp:622-940).  Here, per Strassen product:
 //
 //   pack_kernel          S = sum_i u_i A_i and T = sum_j v_j B_j gathered
-//                        through the scatter vectors into tile order (HBM bound);
+//                        through the scatter vectors into tile order (HBM bound;
+//                        `kpiece` writes the pieces of a k-split as batch
+//                        entries);
 //   pack_multi_kernel    the 7 sums of a product group in one pass (L >= 1);
 //   packed_gemm_ws_kernel DMMA GEMM on S and T (bulk-copy operand ring on
 //                        mbarriers, no block barrier in the k loop) whose
 //                        epilogue adds +-alpha*S*T into the product's C blocks
-//                        (beta on first touch); packed_gemm_grouped_kernel the
+//                        (beta on first touch), for up to 7 products per tile
+//                        position; in the product-parallel and k-split forms
+//                        it sees every product (piece) as a batch entry and
+//                        writes its own M; packed_gemm_grouped_kernel the
 //                        same over many problems' tiles; packed_gemm_kernel the
 //                        earlier cp.async ring with a block barrier per k-step
 //                        (TBLIS_STRA_PACKED_CONFIG=1..4).
