@@ -380,6 +380,36 @@ def kernel_probe(args):
               f"extent {e}: {ms:.3f} ms  {flops / ms / 1e9:.2f} TFLOP/s effective")
 
 
+def rank_sync(torch, dist, device):
+    """(barrier_sync, max_over_ranks) for this process: a barrier bracketed by
+    device synchronisation (CPU ranks, device None, skip it), and the maximum
+    of a per-rank float over all ranks (itself with one process)."""
+    def sync():
+        if device is not None:
+            torch.cuda.synchronize(device)
+
+    def barrier_sync():
+        sync()
+        if dist is not None:
+            dist.barrier()
+        sync()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    return barrier_sync, max_over_ranks
+
+
+def aggregate_tflops(world, flops_per_step, steps, seconds):
+    """Whole-job throughput: every rank runs its own replica of the step, so
+    the job does world * steps steps in the slowest rank's time."""
+    return world * flops_per_step * steps / seconds / 1e12
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -457,18 +487,7 @@ def main():
     torch.cuda.set_device(device)
     stream = torch.cuda.current_stream(device)
 
-    def barrier_sync():
-        torch.cuda.synchronize(device)
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize(device)
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier_sync, max_over_ranks = rank_sync(torch, dist, device)
 
     gen = torch.Generator(device=device).manual_seed(0 + rank)
     shape = (e,) * 4
@@ -495,7 +514,7 @@ def main():
     clocks = sampler.stop() if sampler else None
     t = max_over_ranks(t)
     ms_per_step = t / args.steps * 1e3
-    value = world * flops * args.steps / t / 1e12
+    value = aggregate_tflops(world, flops, args.steps, t)
 
     kinds_snapshot = {k: tsb.kernel_timing(k) for k in ("fused", "pack", "packed_gemm", "aux")}
     tsb.set_kernel_timing(False)
