@@ -14,8 +14,10 @@ the 126 MB L2, so no flush is needed between steps.  The same line also reports
 the plain L=0 kernel on the same GPU, the end-to-end figure through the C ABI
 with pinned host buffers (host<->device copies inside the timed region), the
 roofline of the dominant kernel against a cuBLAS DGEMM measured in the same
-run, clocks sampled during the timed region, and the reference's own CPU
-implementation timed on a bounded sample (rank 0, N=1).
+run, clocks sampled during the timed region, the error of sampled entries
+against exact (long-double) dot products of the same inputs, and the
+reference's own CPU implementation timed on the same workload (one full-size
+call on all host cores; rank 0, N=1).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -155,21 +157,21 @@ def dgemm_peak(torch, device, n=8192, reps=5):
     return 2.0 * n ** 3 / best / 1e12
 
 
-def cpu_reference(ext_sample: int, min_seconds: float, level: int, impl: int):
+def cpu_reference(ext: int, min_seconds: float, level: int, impl: int):
     """The reference's own CPU implementation (oracle/_ref, compiled from its
-    sources) on a bounded sample: the same contraction pattern at extent
-    `ext_sample` per index, all host threads, min over repetitions (the
-    reference's run_kernel, test/test_strassen.cxx:74-95) until min_seconds of
-    CPU work.  Returns (TFLOP/s, threads, sample description, kind)."""
+    sources) on the benchmark workload itself: the same contraction at extent
+    `ext` per index (NIm = NJn = NPk = ext^2), all host threads, the minimum
+    over repetitions (the reference's run_kernel, test/test_strassen.cxx:74-95)
+    run until `min_seconds` of CPU work have been spent (at least one).
+    Returns (TFLOP/s, threads, sample description, kind)."""
     from oracle import oracle
     import numpy as np
     if not oracle.ref_available():
         return None
     threads = os.cpu_count() or 1
     oracle.ref_set_threads(threads)
-    e = ext_sample
-    A = oracle.uniform((e,) * 4, 0)
-    B = oracle.uniform((e,) * 4, 1)
+    e = ext
+    A, B = oracle.uniform_pair((e,) * 4, (e,) * 4, seed=0)
     C = np.zeros((e,) * 4, order="F")
     flops = 2.0 * float(e ** 2) ** 3
     best, spent, reps = float("inf"), 0.0, 0
@@ -181,11 +183,38 @@ def cpu_reference(ext_sample: int, min_seconds: float, level: int, impl: int):
         if reps >= 20:
             break
     sample = (f"reference stra_tblis_tensor_mult{'_2level' if level == 2 else ''} "
-              f"(L={level}, impl={impl}) on the same pattern at extent {e} "
-              f"(NIm=NJn=NPk={e * e}), min of {reps} reps ({spent:.1f} s CPU wall)")
+              f"(L={level}, impl={impl}) on the benchmark workload itself, extent {e} "
+              f"(NIm=NJn=NPk={e * e}), seed-0 U[-1,1] column-major, min of {reps} rep(s) "
+              f"({spent:.1f} s CPU wall, {threads} threads)")
     if level == 0:
         sample = sample.replace("stra_tblis_tensor_mult", "tblis_tensor_mult")
     return flops / best / 1e12, threads, sample, "reference"
+
+
+def sampled_exact_error(torch, A, B, C, nsamples=4096, seed=7):
+    """Error of C(abcd) = A(efac) B(fbde) at `nsamples` random entries against
+    exact dot products of the same inputs (long double on the host, the
+    oracle's exact_dots): (max |C - exact|, sampled normwise error
+    ||C_s - exact_s|| / ||exact_s||).  A, B, C are device tensors with every
+    extent equal; FP32 values are promoted exactly."""
+    from oracle import oracle
+    import numpy as np
+    e = A.shape[0]
+    rng = np.random.default_rng(seed)
+    idx = rng.integers(0, e, size=(nsamples, 4))
+    worst, num, den = 0.0, 0.0, 0.0
+    for lo in range(0, nsamples, 512):
+        part = torch.as_tensor(idx[lo:lo + 512], device=A.device)
+        a, b, c, d = part[:, 0], part[:, 1], part[:, 2], part[:, 3]
+        Ar = A[:, :, a, c].permute(2, 0, 1).reshape(len(a), -1).double().cpu().numpy()
+        Bc = B[:, b, d, :].permute(1, 2, 0).reshape(len(a), -1).double().cpu().numpy()
+        got = C[a, b, c, d].double().cpu().numpy().astype(np.longdouble)
+        ex = oracle.exact_dots(Ar, Bc)
+        diff = np.abs(got - ex)
+        worst = max(worst, float(diff.max()))
+        num += float(np.sum(diff * diff))
+        den += float(np.sum(ex * ex))
+    return worst, (num / den) ** 0.5 if den else 0.0
 
 
 def batched_form(torch, tsb, device, stream, count, barrier_sync, max_over_ranks, dtypes=None):
@@ -419,8 +448,8 @@ def main():
     ap.add_argument("--extent", type=int, default=128, help="extent of each of the six indices")
     ap.add_argument("--level", type=int, default=1)
     ap.add_argument("--variant", type=int, default=1, help="1 ABC, 2 AB, 3 Naive")
-    ap.add_argument("--cpu-sample-extent", type=int, default=64)
-    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--cpu-seconds", type=float, default=30.0,
+                    help="CPU time budget of the reference's timed repetitions (at least one full-size call)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP32 split-BF16 lines")
@@ -460,8 +489,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        r = cpu_reference(min(args.cpu_sample_extent, e), args.cpu_seconds * max(args.steps, 1) / 5.0,
-                          args.level, args.variant)
+        r = cpu_reference(e, args.cpu_seconds, args.level, args.variant)
         if r is None:
             print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref not built"}))
             return
@@ -531,9 +559,11 @@ def main():
         tl = max_over_ranks(time_steps(torch, lambda: step(lv, 1), max(2, args.steps // 2), stream))
         levels[f"L{lv}"] = flops * max(2, args.steps // 2) / tl / 1e12
 
-    # ---- accuracy of this run's result against the plain kernel -------------
+    # ---- accuracy of this run's result: sampled entries against exact dots --
     C.zero_()
     step()
+    torch.cuda.synchronize(device)
+    exact_err, exact_nw = sampled_exact_error(torch, A, B, C)
     C0 = colmajor(torch, shape, device, fill=0.0)
     tsb.contract(0, 1.0, A, IDX_A, B, IDX_B, 0.0, C0, IDX_C, stream=stream)
     torch.cuda.synchronize(device)
@@ -558,8 +588,7 @@ def main():
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
                 "executed_frac": achieved * (7.0 / 8.0) ** args.level / peak,
                 "kernel": {"fused": "stra_dmma_kernel", "pack": "pack_kernel",
-                           "packed_gemm": ("packed_gemm_kernel" if os.environ.get("TBLIS_STRA_PACKED_CONFIG", "0") in ("1", "2", "3", "4")
-                                           else "packed_gemm_ws_kernel"), "aux": "aux"}[dom],
+                           "packed_gemm": "packed_gemm_ws_kernel", "aux": "aux"}[dom],
                 "launches_timed": n_launch, "kernel_ms_total": dom_ms,
                 "share_of_step": dom_ms / (t * 1e3),
                 "other_kernels_ms": {k: v[1] for k, v in kinds.items() if k != dom}}
@@ -572,7 +601,9 @@ def main():
         Cref = colmajor(torch, shape, device, fill=0.0)
         tsb.contract(0, 1.0, A64r, IDX_A, B64r, IDX_B, 0.0, Cref, IDX_C, stream=stream)
         del A64r, B64r
-        precision = {"oracle": "this library's FP64 L=0 contraction of the same FP32 values",
+        precision = {"oracle": ("normwise_err: this library's FP64 L=0 contraction of the same FP32 values "
+                               "(itself checked below against exact dots); sampled_*_vs_exact: 1024 entries "
+                               "against long-double dot products of the same FP32 values"),
                      "tolerance_normwise": {"6": 1e-6, "3": 6e-5}}
         nref = float(torch.linalg.norm(Cref.flatten()))
         C32 = colmajor(torch, shape, device, fill=0.0).float()
@@ -586,7 +617,10 @@ def main():
                 barrier_sync()
                 tt = max_over_ranks(time_steps(torch, run32, 3, stream))
                 err = float(torch.linalg.norm((C32.double() - Cref).flatten())) / nref
-                precision[f"L{lv}_{terms}terms"] = {"tflops": flops * 3 / tt / 1e12, "normwise_err": err}
+                s_max, s_nw = sampled_exact_error(torch, A32, B32, C32, nsamples=1024)
+                precision[f"L{lv}_{terms}terms"] = {"tflops": flops * 3 / tt / 1e12, "normwise_err": err,
+                                                    "sampled_normwise_err_vs_exact": s_nw,
+                                                    "sampled_max_err_vs_exact": s_max}
         tsb.set_fp32_terms(6)
         best6 = max(v["tflops"] for k, v in precision.items() if k.endswith("_6terms"))
         precision["best_6terms_vs_fp64_L0"] = best6 / levels["L0"]
@@ -626,7 +660,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        r = cpu_reference(args.cpu_sample_extent, args.cpu_seconds, args.level, args.variant)
+        r = cpu_reference(e, 0.0, args.level, args.variant)
         if r is not None:
             cpu = {"value": r[0], "unit": "TFLOP/s", "cores": r[1], "kind": r[3], "sample": r[2]}
 
@@ -640,6 +674,9 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic U[-1,1] (seed 0)",
             "config": config, "levels_tflops": levels,
             "ratio_vs_L0": value / world / levels["L0"] if levels.get("L0") else None,
+            "err_vs_exact_samples": {"max_abs": exact_err, "normwise": exact_nw, "samples": 4096,
+                                     "bound": bound, "within_bound": exact_err <= bound,
+                                     "exact": "long-double dot products of the same inputs on the host"},
             "max_err_vs_L0": max_err, "error_bound": bound,
             "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
             "precision_form": precision,

@@ -252,9 +252,11 @@ int tblis_stra_plan_query(const tblis_tensor* A, const label_type* idx_A,
  * call cudaMalloc: an application whose own pool has reserved the whole
  * device, a host that forbids plug-ins from allocating device memory, or code
  * that cannot afford cudaMalloc/cudaFree's implicit device synchronisation.
- * Same arguments as tblis_stra_mult; always the ABC variant; A, B and C must
- * be device memory (TBLIS_STRA_ERR_ARG otherwise); `stream` NULL = the legacy
- * default stream.  The contraction's scatter vectors go into one static
+ * Same arguments as tblis_stra_mult, with these limits: FP64 (TYPE_DOUBLE)
+ * operands only (TBLIS_STRA_ERR_UNSUPPORTED otherwise); always the ABC
+ * variant; A, B and C must be device memory of the current device
+ * (TBLIS_STRA_ERR_ARG otherwise); `stream` NULL = the legacy default stream.
+ * The contraction's scatter vectors are generated on the GPU into one static
  * 2 MiB device array, so 2*m + 2*n + 2*k + 3*batch (the planned sizes) may not
  * exceed 262144, else TBLIS_STRA_ERR_TOO_LARGE.  The first call on a device
  * looks the array up (cudaGetSymbolAddress) and should come before any stream

@@ -18,12 +18,14 @@
 #      sandybridge AVX kernels and TCI, plus oracle/ref_harness.cxx, with g++/gcc
 #      -O3 -mavx -fPIC into one shared object.
 #
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref.sh [REFERENCE_ROOT]
+#   (default: $TBLIS_STRA_REFERENCE_ROOT, else a directory named "reference"
+#   beside this repository)
 # Outputs go only to oracle/_ref/.
 set -euo pipefail
 
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${TBLIS_STRA_REFERENCE_ROOT:-$(cd "$HERE/../.." && pwd)/reference}}"
 OUT="$HERE/_ref"
 GEN="$OUT/gen"
 SHADOW="$OUT/shadow"

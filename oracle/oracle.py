@@ -180,6 +180,28 @@ def uniform(shape, seed: int, order: str = "F", dtype=np.float64) -> np.ndarray:
     return np.asarray(x.reshape(shape, order=order), order=order)
 
 
+def uniform_pair(shape_a, shape_b, seed: int = 0, order: str = "F"):
+    """A then B drawn from ONE seeded stream (numpy MT19937), i.i.d.
+    U[-1, 1], column-major by default: the config-1 inputs ("entries
+    i.i.d. uniform[-1,1] from seed 0", A first, then B)."""
+    rng = np.random.Generator(np.random.MT19937(seed))
+    out = []
+    for shape in (shape_a, shape_b):
+        x = rng.uniform(-1.0, 1.0, size=int(np.prod(shape)))
+        out.append(np.asarray(x.reshape(shape, order=order), order=order))
+    return out[0], out[1]
+
+
+def exact_dots(Arows: np.ndarray, Bcols: np.ndarray) -> np.ndarray:
+    """Per-sample dot products sum_p Arows[s, p] * Bcols[s, p] accumulated in
+    long double (x87 80-bit on x86-64): the products of two doubles carry at
+    most 2^-64 relative error there, so for the sums checked here (p up to
+    2^14) the result is exact to far below the FP64 bound."""
+    a = np.asarray(Arows, dtype=np.longdouble)
+    b = np.asarray(Bcols, dtype=np.longdouble)
+    return np.sum(a * b, axis=1)
+
+
 def error_bound(level: int, npk: int, maxA: float, maxB: float) -> float:
     """max|C - Cref| <= 4 * 12^L * NPk * 2^-53 * max|A| * max|B| (FP64 bound)."""
     return 4.0 * (12.0 ** level) * npk * 2.0 ** -53 * maxA * maxB

@@ -46,6 +46,7 @@
 #include <vector>
 
 #include "kernels.cuh"
+#include "memkind.hpp"
 #include "plan.hpp"
 #include "schedule.hpp"
 
@@ -112,13 +113,6 @@ int fused_config(int variant, int level)
     if (variant == V_FUSED) return 2;
     if (variant == V_FUSED_SMALL) return level == 1 ? -1 : 1;
     return -1;
-}
-
-bool device_ptr(const void* p)
-{
-    cudaPointerAttributes attr;
-    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) { cudaGetLastError(); return false; }
-    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
 }
 
 DmmaArgs make_args(const Prob& pr, const int64_t* tab, int level, int config, double* C_override,
@@ -615,7 +609,7 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
             if (pr.g.hi[t] < pr.g.lo[t]) continue;
             if (!T[t]->data) return TBLIS_STRA_ERR_NULL;
             if (reinterpret_cast<uintptr_t>(T[t]->data) % es) return TBLIS_STRA_ERR_ARG;
-            if (!device_ptr(T[t]->data)) return TBLIS_STRA_ERR_ARG;   // batches take device memory only
+            if (mem_kind(T[t]->data, plan->device) != MemKind::LOCAL) return TBLIS_STRA_ERR_ARG;   // this GPU's memory only
         }
         max_c_span = std::max<int64_t>(max_c_span, pr.g.hi[2] - pr.g.lo[2] + 1);
         const std::vector<int64_t>* v[9] = {&pr.g.rsA, &pr.g.rsC, &pr.g.csB, &pr.g.csC, &pr.g.ksA,

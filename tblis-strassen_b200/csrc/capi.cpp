@@ -38,6 +38,7 @@
 #include <vector>
 
 #include "kernels.cuh"
+#include "memkind.hpp"
 #include "plan.hpp"
 #include "schedule.hpp"
 
@@ -202,13 +203,6 @@ int num_sms(int device)
     return v;
 }
 
-bool is_device_ptr(const void* p)
-{
-    if (!p) return false;
-    cudaPointerAttributes attr;
-    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) { cudaGetLastError(); return false; }
-    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
-}
 
 // The library's own stream-ordered memory pool per device.  Its release
 // threshold is unlimited, so memory freed by one call is reused by the next
@@ -1680,7 +1674,8 @@ int mult_pipelined(int level, int impl, const tblis_tensor* const T[3], const la
     size_t bytes = 0;
     for (int t = 0; t < 3; t++)
     {
-        if (g.hi[t] < g.lo[t] || g.lo[t] != 0 || !T[t]->data || is_device_ptr(T[t]->data)) return NOT_PIPELINED;
+        if (g.hi[t] < g.lo[t] || g.lo[t] != 0 || !T[t]->data || mem_kind(T[t]->data, device) != MemKind::HOST)
+            return NOT_PIPELINED;
         for (unsigned d = 0; d < T[t]->ndim; d++)
             for (unsigned e = d + 1; e < T[t]->ndim; e++)
                 if (I[t][d] == I[t][e]) return NOT_PIPELINED;            // diagonal labels
@@ -1923,7 +1918,9 @@ int mult(int level, const tblis_tensor* A, const label_type* idx_A,
     {
         if (g.hi[t] < g.lo[t]) continue;            // empty tensor
         if (!T[t]->data) return TBLIS_STRA_ERR_NULL;
-        if (is_device_ptr(T[t]->data)) continue;
+        const MemKind mk = mem_kind(T[t]->data, device);
+        if (mk == MemKind::OTHER_DEVICE) return TBLIS_STRA_ERR_ARG;   // another GPU's memory
+        if (mk == MemKind::LOCAL) continue;
         const size_t n = (size_t)(g.hi[t] - g.lo[t] + 1);
         if ((s = stage[t].alloc(n * es, st))) return s;
         const char* hsrc = static_cast<const char*>(T[t]->data) + g.lo[t] * (int64_t)es;

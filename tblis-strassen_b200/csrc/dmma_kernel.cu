@@ -28,7 +28,6 @@
 #include "timing.hpp"
 
 #include <atomic>
-#include <cstdlib>
 
 namespace tsb {
 
@@ -578,15 +577,6 @@ cudaError_t launch_dmma(const DmmaArgs& args, int terms, cudaStream_t stream, in
 {
     if (args.batch <= 0 || args.ms <= 0 || args.ns <= 0) return cudaSuccess;
     if (terms > 4 || args.H > 4 || args.Hc > 4) return cudaErrorInvalidValue;
-    if (config < 0)
-    {
-        // Development override for tile sweeps: TBLIS_STRA_DMMA_CONFIG=<id>.
-        static const int env = [] {
-            const char* s = std::getenv("TBLIS_STRA_DMMA_CONFIG");
-            return s ? std::atoi(s) : -1;
-        }();
-        config = env;
-    }
     cudaError_t err;
     if (terms <= 1 && args.H <= 1 && args.Hc <= 1)
     {

@@ -321,8 +321,7 @@ cudaError_t launch_split_gemm_grouped(const SplitGroupArgs& args, int planes, cu
 
 cudaError_t launch_pack(const PackArgs& args, cudaStream_t stream);
 cudaError_t launch_pack_multi(const PackMultiArgs& args, cudaStream_t stream);
-cudaError_t launch_packed_gemm(const PackedGemmArgs& args, cudaStream_t stream, int num_sms,
-                               int config = -1);
+cudaError_t launch_packed_gemm(const PackedGemmArgs& args, cudaStream_t stream, int num_sms);
 cudaError_t launch_packed_gemm_grouped(const PackedGroupArgs& args, cudaStream_t stream, int num_sms);
 
 // Launchers (kernels.cu).  `terms` = largest number of blocks in one sum

@@ -13,9 +13,11 @@
 // NOALLOC_MAX_ENTRIES int64 values (2 MiB, resident on every GPU that loads the
 // library until the process exits).  A contraction needs
 // 2*m + 2*n + 2*k + 3*batch entries; larger requests are rejected with
-// TBLIS_STRA_ERR_TOO_LARGE.  Only the ABC variant runs here (AB and Naive need
-// M/S/T buffers), at level 0, 1 or 2; all three operands must be device
-// memory.
+// TBLIS_STRA_ERR_TOO_LARGE.  The vectors are written into the array by a small
+// kernel from their mixed-radix form (extents and strides of the folded
+// modes, passed by value), so no host buffer is involved.  Only FP64 operands
+// and the ABC variant run here (AB and Naive need M/S/T buffers), at level 0,
+// 1 or 2; all three operands must be device memory of the current device.
 //
 // Set-up: the first call on each device (with that device current) looks up
 // the array's device address with cudaGetSymbolAddress; make that first call
@@ -28,20 +30,60 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <map>
 #include <mutex>
-#include <vector>
 
 #include "kernels.cuh"
+#include "memkind.hpp"
 #include "plan.hpp"
 
 namespace tsb {
+
+extern std::atomic<unsigned long long> g_launches;
+
 namespace {
 
 constexpr size_t NOALLOC_MAX_ENTRIES = size_t(1) << 18;   // 2 MiB of int64
 
 __device__ __align__(256) int64_t g_noalloc_scratch[NOALLOC_MAX_ENTRIES];
+
+// Modes per scatter vector: every folded mode has extent >= 2, so a vector of
+// at most NOALLOC_MAX_ENTRIES entries has at most 18 of them.
+constexpr int GEN_MAX_MODES = 18;
+
+// The nine scatter vectors in mixed-radix form: entry i of vector v (stored at
+// out + off[v] + i, i < count[v]) is sum_d digit_d(i) * stride[v][d], digits of
+// i over len[v][0..nm[v]) with the first mode fastest.
+struct ScatterGenArgs
+{
+    int64_t* out;
+    int64_t off[10];                       // off[9] = total entries
+    int nm[9];
+    int64_t len[9][GEN_MAX_MODES];
+    int64_t stride[9][GEN_MAX_MODES];
+};
+
+__global__ void scatter_gen_kernel(const __grid_constant__ ScatterGenArgs a)
+{
+    const int64_t total = a.off[9];
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x)
+    {
+        int v = 0;
+        while (v < 8 && e >= a.off[v + 1]) v++;
+        int64_t i = e - a.off[v], off = 0;
+        for (int d = 0; d < a.nm[v]; d++)
+        {
+            const int64_t l = a.len[v][d];
+            const int64_t q = i / l;
+            off += (i - q * l) * a.stride[v][d];
+            i = q;
+        }
+        a.out[e] = off;
+    }
+}
 
 std::mutex g_noalloc_mu;
 std::map<int, int64_t*> g_noalloc_ptr;   // device -> address of g_noalloc_scratch
@@ -59,31 +101,35 @@ int noalloc_scratch(int device, int64_t** out)
     return TBLIS_STRA_SUCCESS;
 }
 
-bool on_device(const void* p)
-{
-    cudaPointerAttributes attr;
-    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) { cudaGetLastError(); return false; }
-    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
-}
-
 int noalloc_mult(int level, const tblis_tensor* A, const label_type* idx_A,
                  const tblis_tensor* B, const label_type* idx_B,
                  tblis_tensor* C, const label_type* idx_C, cudaStream_t st)
 {
     if (level < 0 || level > 2) return TBLIS_STRA_ERR_ARG;
     GemmView g;
-    int s = plan_contraction(A, idx_A, B, idx_B, C, idx_C, g, true);
+    int s = plan_contraction(A, idx_A, B, idx_B, C, idx_C, g, false);
     if (s) return s;
     if (g.type != TYPE_DOUBLE) return TBLIS_STRA_ERR_UNSUPPORTED;
+    const int64_t count[9] = {g.m, g.m, g.n, g.n, g.k, g.k, g.batch, g.batch, g.batch};
     const size_t need = 2 * (size_t)g.m + 2 * (size_t)g.n + 2 * (size_t)g.k + 3 * (size_t)g.batch;
     if (need > NOALLOC_MAX_ENTRIES) return TBLIS_STRA_ERR_TOO_LARGE;
+    for (int v = 0; v < 9; v++)
+        if (g.mode_len[v].size() > (size_t)GEN_MAX_MODES) return TBLIS_STRA_ERR_TOO_LARGE;
+
+    int device = 0;
     const tblis_tensor* T[3] = {A, B, C};
+    bool device_known = false;
     for (int t = 0; t < 3; t++)
     {
         if (g.hi[t] < g.lo[t]) continue;   // empty tensor: never dereferenced
         if (!T[t]->data) return TBLIS_STRA_ERR_NULL;
         if (reinterpret_cast<uintptr_t>(T[t]->data) % sizeof(double)) return TBLIS_STRA_ERR_ARG;
-        if (!on_device(T[t]->data)) return TBLIS_STRA_ERR_ARG;
+        if (!device_known)
+        {
+            if (cudaGetDevice(&device) != cudaSuccess) { cudaGetLastError(); return TBLIS_STRA_ERR_NO_DEVICE; }
+            device_known = true;
+        }
+        if (mem_kind(T[t]->data, device) != MemKind::LOCAL) return TBLIS_STRA_ERR_ARG;
     }
     if (g.m == 0 || g.n == 0 || g.batch == 0)
     {
@@ -93,33 +139,37 @@ int noalloc_mult(int level, const tblis_tensor* A, const label_type* idx_A,
         return TBLIS_STRA_SUCCESS;
     }
 
-    int device = 0;
-    if (cudaGetDevice(&device) != cudaSuccess) { cudaGetLastError(); return TBLIS_STRA_ERR_NO_DEVICE; }
     int64_t* scratch = nullptr;
     if ((s = noalloc_scratch(device, &scratch))) return s;
 
-    // Pack the scatter vectors (host memory) and copy them into the array.
-    const std::vector<int64_t>* parts[9] = {&g.rsA, &g.rsC, &g.csB, &g.csC, &g.ksA, &g.ksB,
-                                            &g.bA, &g.bB, &g.bC};
-    std::vector<int64_t> host;
-    host.reserve(need);
-    size_t off[9];
-    for (int i = 0; i < 9; i++)
+    // Write the scatter vectors into the array on the caller's stream.
+    ScatterGenArgs gen;
+    std::memset(&gen, 0, sizeof gen);
+    gen.out = scratch;
+    gen.off[0] = 0;
+    for (int v = 0; v < 9; v++)
     {
-        off[i] = host.size();
-        host.insert(host.end(), parts[i]->begin(), parts[i]->end());
+        gen.off[v + 1] = gen.off[v] + count[v];
+        gen.nm[v] = (int)g.mode_len[v].size();
+        for (int d = 0; d < gen.nm[v]; d++)
+        {
+            gen.len[v][d] = g.mode_len[v][d];
+            gen.stride[v][d] = g.mode_stride[v][d];
+        }
     }
-    if (cudaMemcpyAsync(scratch, host.data(), host.size() * sizeof(int64_t),
-                        cudaMemcpyHostToDevice, st) != cudaSuccess)
-        return TBLIS_STRA_ERR_CUDA;
-    // (pageable source: the call returns once the data is staged, so `host`
-    // may be released afterwards)
+    {
+        const int threads = 256;
+        const int64_t blocks = std::min<int64_t>((gen.off[9] + threads - 1) / threads, 1024);
+        scatter_gen_kernel<<<(unsigned)blocks, threads, 0, st>>>(gen);
+        if (cudaGetLastError() != cudaSuccess) return TBLIS_STRA_ERR_CUDA;
+        g_launches++;
+    }
 
-    const int64_t* rsA = scratch + off[0]; const int64_t* rsC = scratch + off[1];
-    const int64_t* csB = scratch + off[2]; const int64_t* csC = scratch + off[3];
-    const int64_t* ksA = scratch + off[4]; const int64_t* ksB = scratch + off[5];
-    const int64_t* bA = scratch + off[6];  const int64_t* bB = scratch + off[7];
-    const int64_t* bC = scratch + off[8];
+    const int64_t* rsA = scratch + gen.off[0]; const int64_t* rsC = scratch + gen.off[1];
+    const int64_t* csB = scratch + gen.off[2]; const int64_t* csC = scratch + gen.off[3];
+    const int64_t* ksA = scratch + gen.off[4]; const int64_t* ksB = scratch + gen.off[5];
+    const int64_t* bA = scratch + gen.off[6];  const int64_t* bB = scratch + gen.off[7];
+    const int64_t* bC = scratch + gen.off[8];
     double* Cd = static_cast<double*>(C->data);
 
     if (g.alpha == 0.0 || g.k == 0)

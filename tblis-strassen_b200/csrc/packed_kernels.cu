@@ -19,9 +19,7 @@
 //                        position; in the product-parallel and k-split forms
 //                        it sees every product (piece) as a batch entry and
 //                        writes its own M; packed_gemm_grouped_kernel the
-//                        same over many problems' tiles; packed_gemm_kernel the
-//                        earlier cp.async ring with a block barrier per k-step
-//                        (TBLIS_STRA_PACKED_CONFIG=1..4).
+//                        same over many problems' tiles.
 //
 // Forming each sum once per element in HBM costs about 1 % of the GEMM time at
 // NIm = NJn = NPk = 16384, while summing inside the GEMM costs shared-memory
@@ -33,7 +31,6 @@
 #include "timing.hpp"
 
 #include <atomic>
-#include <cstdlib>
 
 namespace tsb {
 
@@ -222,27 +219,6 @@ pack_multi_kernel(const __grid_constant__ PackMultiArgs a)
 
 // ---- packed GEMM ------------------------------------------------------------------
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p)
-{
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src)
-{
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" :: "r"(dst), "l"(src));
-}
-
-__device__ __forceinline__ void cp_async_commit()
-{
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-
-template <int N>
-__device__ __forceinline__ void cp_async_wait()
-{
-    asm volatile("cp.async.wait_group %0;\n" :: "n"(N) : "memory");
-}
-
 __device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, double b0)
 {
     asm("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 "
@@ -264,185 +240,13 @@ struct PCfg
     static_assert((BK * BM / 2) % NT == 0, "16-byte chunks per thread");
 };
 
-// One output tile (work item w of the problem `a`) of the packed GEMM.
-template <class K>
-__device__ __forceinline__ void packed_tile(const PackedGemmArgs& a, int64_t w, unsigned char* smem)
-{
-    constexpr int BM = K::BM, BN = K::BN, BK = K::BK, NT = K::NT, STAGES = K::STAGES;
-    constexpr int MI = K::MI, NI = K::NI;
-    double* As = reinterpret_cast<double*>(smem);
-    double* Bs = As + STAGES * BK * BM;
-    int64_t* rowC = reinterpret_cast<int64_t*>(Bs + STAGES * BK * BN);
-    int64_t* colC = rowC + 4 * BM;
-
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int g = lane >> 2, t4 = lane & 3;
-    const int wm = (warp / K::WN) * K::WTM;
-    const int wn = (warp % K::WN) * K::WTN;
-    const int64_t tiles = a.tiles_m * a.tiles_n;
-    const int64_t nk = a.k_pad / BK;
-
-    {
-        const int64_t b = w / tiles;
-        const int64_t tw = w - b * tiles;
-        const int64_t GROUP = 8;
-        const int64_t group = tw / (GROUP * a.tiles_n);
-        const int64_t first_m = group * GROUP;
-        const int64_t gsize = (a.tiles_m - first_m) < GROUP ? (a.tiles_m - first_m) : GROUP;
-        const int64_t tm = first_m + (tw % gsize);
-        const int64_t tn = (tw % (GROUP * a.tiles_n)) / gsize;
-
-        __syncthreads();   // previous tile's epilogue done with the tables
-        for (int i = tid; i < 4 * BM; i += NT)
-        {
-            const int q = i / BM, r = i % BM;
-            const int64_t loc = tm * BM + r;
-            const int64_t gi = (q < a.nc[0] ? a.c_r[0][q] : 0) * a.ms + loc;
-            rowC[i] = (q < a.nc[0] && loc < a.ms && gi < a.m) ? a.bC[b] + a.rsC[gi] : OFF_INVALID;
-        }
-        for (int i = tid; i < 4 * BN; i += NT)
-        {
-            const int q = i / BN, c = i % BN;
-            const int64_t loc = tn * BN + c;
-            const int64_t gj = (q < a.nc[0] ? a.c_c[0][q] : 0) * a.ns + loc;
-            colC[i] = (q < a.nc[0] && loc < a.ns && gj < a.n) ? a.csC[gj] : OFF_INVALID;
-        }
-
-        const double* Sb = a.S[0] + ((b * a.tiles_m + tm) * a.k_pad) * BM;
-        const double* Tb = a.T[0] + ((b * a.tiles_n + tn) * a.k_pad) * BN;
-        auto copy_stage = [&](int64_t s) {
-            const int buf = (int)(s % STAGES);
-            const double* sa = Sb + s * BK * BM;
-            const double* sb = Tb + s * BK * BN;
-            const uint32_t da = smem_u32(As + buf * BK * BM);
-            const uint32_t db = smem_u32(Bs + buf * BK * BN);
-#pragma unroll
-            for (int c = tid; c < BK * BM / 2; c += NT) cp_async16(da + c * 16, sa + 2 * c);
-#pragma unroll
-            for (int c = tid; c < BK * BN / 2; c += NT) cp_async16(db + c * 16, sb + 2 * c);
-        };
-
-        for (int64_t s = 0; s < STAGES - 1; s++)
-        {
-            if (s < nk) copy_stage(s);
-            cp_async_commit();
-        }
-
-        double acc[MI][NI][4];
-#pragma unroll
-        for (int mi = 0; mi < MI; mi++)
-#pragma unroll
-            for (int ni = 0; ni < NI; ni++)
-#pragma unroll
-                for (int e = 0; e < 4; e++) acc[mi][ni][e] = 0.0;
-
-        auto load_frags = [&](const double* Ab, const double* Bb, int k4,
-                              double (&af)[MI][2], double (&bf)[NI]) {
-            const int kr = k4 + t4;
-            const int pg = 2 * ((g + swz_c(kr)) & 7);
-#pragma unroll
-            for (int mi = 0; mi < MI; mi++)
-            {
-                const double2 v = *reinterpret_cast<const double2*>(Ab + kr * BM + wm + mi * 16 + pg);
-                af[mi][0] = v.x; af[mi][1] = v.y;
-            }
-#pragma unroll
-            for (int nj = 0; nj < NI / 2; nj++)
-            {
-                const double2 v = *reinterpret_cast<const double2*>(Bb + kr * BN + wn + nj * 16 + pg);
-                bf[2 * nj] = v.x; bf[2 * nj + 1] = v.y;
-            }
-        };
-
-        for (int64_t s = 0; s < nk; s++)
-        {
-            cp_async_wait<STAGES - 2>();
-            __syncthreads();
-            if (s + STAGES - 1 < nk) copy_stage(s + STAGES - 1);
-            cp_async_commit();
-            const int buf = (int)(s % STAGES);
-            const double* Ab = As + buf * BK * BM;
-            const double* Bb = Bs + buf * BK * BN;
-            double af[2][MI][2], bf[2][NI];
-            load_frags(Ab, Bb, 0, af[0], bf[0]);
-#pragma unroll
-            for (int q = 0; q < BK / 4; q++)
-            {
-                const int cur = q & 1;
-                if (q + 1 < BK / 4) load_frags(Ab, Bb, (q + 1) * 4, af[cur ^ 1], bf[cur ^ 1]);
-#pragma unroll
-                for (int mi = 0; mi < MI; mi++)
-#pragma unroll
-                    for (int ni = 0; ni < NI; ni++)
-                        dmma(acc[mi][ni], af[cur][mi][0], af[cur][mi][1], bf[cur][ni]);
-            }
-        }
-        cp_async_wait<0>();
-
-        // Epilogue: C_q = (first ? beta*C_q : C_q) + sign_q*alpha*S*T.  All
-        // loads of C are issued before the stores so their latencies overlap.
-        for (int q = 0; q < a.nc[0]; q++)
-        {
-            const int64_t* rt = rowC + q * BM;
-            const int64_t* ct = colC + q * BN;
-            const double coef = a.c_s[0][q] < 0 ? -a.alpha : a.alpha;
-            const bool first = a.c_first[0][q] != 0;
-            const bool read_c = !first || a.beta != 0.0;
-            const double cb = first ? a.beta : 1.0;
-#pragma unroll
-            for (int mi = 0; mi < MI; mi++)
-            {
-                double cv[2][NI][2];
-#pragma unroll
-                for (int hr = 0; hr < 2; hr++)
-                {
-                    const int64_t ro = rt[wm + mi * 16 + g + hr * 8];
-#pragma unroll
-                    for (int ni = 0; ni < NI; ni++)
-#pragma unroll
-                        for (int hc = 0; hc < 2; hc++)
-                        {
-                            const int64_t co = ct[wn + ni * 8 + t4 * 2 + hc];
-                            cv[hr][ni][hc] = (read_c && ro != OFF_INVALID && co != OFF_INVALID)
-                                                 ? a.C[ro + co] : 0.0;
-                        }
-                }
-#pragma unroll
-                for (int hr = 0; hr < 2; hr++)
-                {
-                    const int64_t ro = rt[wm + mi * 16 + g + hr * 8];
-                    if (ro == OFF_INVALID) continue;
-#pragma unroll
-                    for (int ni = 0; ni < NI; ni++)
-#pragma unroll
-                        for (int hc = 0; hc < 2; hc++)
-                        {
-                            const int64_t co = ct[wn + ni * 8 + t4 * 2 + hc];
-                            if (co == OFF_INVALID) continue;
-                            a.C[ro + co] = coef * acc[mi][ni][hr * 2 + hc] + cb * cv[hr][ni][hc];
-                        }
-                }
-            }
-        }
-    }
-}
-
-template <class K>
-__global__ void __launch_bounds__(K::NT, 1)
-packed_gemm_kernel(const __grid_constant__ PackedGemmArgs a)
-{
-    extern __shared__ __align__(128) unsigned char smem[];
-    const int64_t work = a.batch * a.tiles_m * a.tiles_n;
-    for (int64_t w = blockIdx.x; w < work; w += gridDim.x) packed_tile<K>(a, w, smem);
-}
-
 // ---- warp-specialised packed GEMM ----------------------------------------------------
 //
-// The same tiles, fragments and epilogue as packed_tile, with the operand
-// ring filled by 1-D bulk copies (one 32 KB copy of S and one of T per
-// k-step: a packed tile's k-steps are contiguous) that complete on an
-// mbarrier, instead of every thread issuing 16-byte cp.async and the CTA
-// meeting at a barrier each k-step.  Thread 0 also produces: after each
+// 128 x 128 output tiles of 16 warps with 32 x 32 warp tiles of m16n8k4 DMMA
+// fragments, read as 128-bit pairs from the swizzled k-major layout.  The
+// operand ring is filled by 1-D bulk copies (one 32 KB copy of S and one of T
+// per k-step: a packed tile's k-steps are contiguous) that complete on an
+// mbarrier, so the CTA never meets at a block barrier inside the k loop.  Thread 0 also produces: after each
 // k-step it refills the slot that step used once all 16 warps have released
 // it (one arrival per warp), so warps drift apart by up to STAGES - 1 steps
 // and the DMMA pipe does not drain at a block-wide barrier.  The producer
@@ -758,27 +562,6 @@ packed_gemm_grouped_kernel(const __grid_constant__ PackedGroupArgs g)
 }
 
 template <class K>
-cudaError_t launch_packed_cfg(const PackedGemmArgs& a, cudaStream_t stream, int num_sms)
-{
-    static_assert(K::smem <= 227 * 1024, "shared memory budget");
-    if (a.k_pad % K::BK) return cudaErrorInvalidValue;
-    auto kern = packed_gemm_kernel<K>;
-    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::smem);
-    if (err != cudaSuccess) return err;
-    const int64_t work = a.batch * a.tiles_m * a.tiles_n;
-    int per_sm = 0;
-    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, K::NT, K::smem);
-    if (err != cudaSuccess) return err;
-    if (per_sm < 1) per_sm = 1;
-    int64_t grid = (int64_t)num_sms * per_sm;
-    if (work < grid) grid = work;
-    timing_begin(KK_PACKED_GEMM, stream);
-    kern<<<(unsigned)grid, K::NT, K::smem, stream>>>(a);
-    timing_end(KK_PACKED_GEMM, stream);
-    return cudaGetLastError();
-}
-
-template <class K>
 cudaError_t launch_packed_ws_cfg(const PackedGemmArgs& a, cudaStream_t stream, int num_sms)
 {
     static_assert(ws_smem<K>() <= 227 * 1024, "shared memory budget");
@@ -811,9 +594,6 @@ cudaError_t launch_packed_grouped_cfg(const PackedGroupArgs& g, cudaStream_t str
 }
 
 using PG0 = PCfg<32, 3, 4, 4>;   // 16 warps of 32 x 32, k-step 32
-using PG1 = PCfg<16, 6, 4, 4>;
-using PG2 = PCfg<16, 4, 4, 4>;
-using PG3 = PCfg<16, 4, 2, 4>;   // 8 warps of 64 x 32
 
 }  // namespace
 
@@ -846,33 +626,13 @@ cudaError_t launch_pack_multi(const PackMultiArgs& a, cudaStream_t stream)
     return err;
 }
 
-cudaError_t launch_packed_gemm(const PackedGemmArgs& a, cudaStream_t stream, int num_sms, int config)
+cudaError_t launch_packed_gemm(const PackedGemmArgs& a, cudaStream_t stream, int num_sms)
 {
     if (a.batch <= 0 || a.tiles_m <= 0 || a.tiles_n <= 0) return cudaSuccess;
     if (a.nprod < 1 || a.nprod > MAX_GROUP_PRODUCTS || a.H < 1 || a.H > 4) return cudaErrorInvalidValue;
     for (int p = 0; p < a.nprod; p++)
         if (a.nc[p] < 1 || a.nc[p] > 4) return cudaErrorInvalidValue;
-    if (config < 0)
-    {
-        static const int env = [] {
-            const char* s = std::getenv("TBLIS_STRA_PACKED_CONFIG");
-            return s ? std::atoi(s) : -1;
-        }();
-        config = env;
-    }
-    cudaError_t err;
-    // 0 (default): warp-specialised bulk-copy ring; 1-4: cp.async rings with a
-    // block barrier per k-step (4 = the same tile shape as the default), one
-    // product per launch.
-    if (config >= 1 && config <= 4 && a.nprod != 1) config = 0;
-    switch (config)
-    {
-        case 1:  err = launch_packed_cfg<PG1>(a, stream, num_sms); break;
-        case 2:  err = launch_packed_cfg<PG2>(a, stream, num_sms); break;
-        case 3:  err = launch_packed_cfg<PG3>(a, stream, num_sms); break;
-        case 4:  err = launch_packed_cfg<PG0>(a, stream, num_sms); break;
-        default: err = launch_packed_ws_cfg<PG0>(a, stream, num_sms); break;
-    }
+    const cudaError_t err = launch_packed_ws_cfg<PG0>(a, stream, num_sms);
     if (err == cudaSuccess) g_launches++;
     return err;
 }

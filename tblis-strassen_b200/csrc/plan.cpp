@@ -357,6 +357,12 @@ int plan_contraction(const tblis_tensor* A, const label_type* idx_A,
     g.unit_ksA = first_stride(k_len, k_str[0], k_blocked ? 2 : 1);
     g.unit_ksB = first_stride(k_len, k_str[1], k_blocked ? 2 : 1);
 
+    const std::vector<int64_t>* ml[9] = {&g.AC.len, &g.AC.len, &g.BC.len, &g.BC.len, &k_len, &k_len,
+                                         &b_len, &b_len, &b_len};
+    const std::vector<int64_t>* msd[9] = {&g.AC.stride[0], &g.AC.stride[1], &g.BC.stride[0], &g.BC.stride[1],
+                                          &k_str[0], &k_str[1], &b_str[0], &b_str[1], &b_str[2]};
+    for (int v = 0; v < 9; v++) { g.mode_len[v] = *ml[v]; g.mode_stride[v] = *msd[v]; }
+
     if (build_scatter)
     {
         scatter(g.AC.len, g.AC.stride[0], g.rsA);

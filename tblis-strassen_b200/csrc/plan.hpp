@@ -59,6 +59,11 @@ struct GemmView
     int64_t unit_rsA = 0, unit_ksA = 0, unit_ksB = 0, unit_csB = 0, unit_rsC = 0, unit_csC = 0;
     // Offset span touched in each tensor (elements), for host staging.
     int64_t lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    // The mixed-radix form of the nine scatter vectors, in the order rsA,
+    // rsC, csB, csC, ksA, ksB, bA, bB, bC: entry i of vector v is
+    // sum_d digit_d(i) * stride[d] with digits of i over len (first mode
+    // fastest).  Filled whether or not the vectors themselves are built.
+    std::vector<int64_t> mode_len[9], mode_stride[9];
     // Bundles after folding, kept for diagnostics and tests.
     Bundle ABC, AB, AC, BC, A_only, B_only, C_only;
 };
