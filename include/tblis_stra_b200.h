@@ -215,6 +215,28 @@ int tblis_stra_get_product_parallel(void);
 int tblis_stra_set_fp32_terms(int terms);
 int tblis_stra_get_fp32_terms(void);
 
+/* Bound, in SM clock cycles, on each wait of the warp-specialised kernels
+ * (the packed FP64 GEMM and the split-BF16 tcgen05 GEMM) for a copy, an MMA
+ * stage or a drained accumulator; 0 (the default) means about one second.
+ * When a wait runs out, the kernel stops issuing work, lets its own copies
+ * and MMAs land, frees its tensor memory and ends; blocking calls then return
+ * TBLIS_STRA_ERR_TIMEOUT and the device stays usable.  No counterpart in the
+ * reference (its CPU threads cannot stall on an asynchronous copy).  Per
+ * calling thread, read when a call (or a batch's create) enqueues its
+ * kernels.  Returns 0 or TBLIS_STRA_ERR_ARG (negative cycles). */
+int tblis_stra_set_wait_limit(long long cycles);
+long long tblis_stra_get_wait_limit(void);
+
+/* Largest single device allocation (bytes) a call of the calling thread may
+ * make for its scatter-vector tables, workspace, staging buffers and flags
+ * (default: unlimited).  A request above it fails as an out-of-memory
+ * allocation would: the call returns TBLIS_STRA_ERR_ALLOC and leaves C
+ * untouched.  Unlike tblis_stra_set_workspace_limit, which makes ABC fall
+ * back to schedules that need less, this is a hard ceiling.  No counterpart in
+ * the reference (its host pools grow on demand). */
+int tblis_stra_set_alloc_limit(size_t bytes);
+size_t tblis_stra_get_alloc_limit(void);
+
 /* Status of the calling thread's last contraction call; string form. */
 int tblis_stra_last_status(void);
 const char* tblis_stra_status_string(int status);

@@ -168,6 +168,7 @@ struct DevBuf
     ~DevBuf() { if (p) cudaFree(p); }
     int alloc(size_t bytes)
     {
+        if (std::max<size_t>(bytes, 16) > alloc_limit_bytes()) return TBLIS_STRA_ERR_ALLOC;
         if (cudaMalloc(&p, std::max<size_t>(bytes, 16)) != cudaSuccess) { cudaGetLastError(); p = nullptr; return TBLIS_STRA_ERR_ALLOC; }
         return TBLIS_STRA_SUCCESS;
     }
@@ -434,6 +435,7 @@ struct Tuner
             PackedGroupArgs g;
             if (upload_packed(args, nullptr, g, desc.p, desc_cap)) return 1e30;
             g.err = err;
+            g.wait_limit = wait_limit_cycles();
             const double gemm_ms = time([&] {
                 return launch_packed_gemm_grouped(g, st, sms) == cudaSuccess ? 0 : (int)TBLIS_STRA_ERR_CUDA;
             });
@@ -465,6 +467,7 @@ struct Tuner
             SplitGroupArgs g;
             if (upload_split(args, nullptr, g, desc.p, desc_cap)) return 1e30;
             g.err = err;
+            g.wait_limit = wait_limit_cycles();
             const double gemm_ms = time([&] {
                 return launch_split_gemm_grouped(g, one.planes, st, sms) == cudaSuccess ? 0 : (int)TBLIS_STRA_ERR_CUDA;
             });
@@ -796,11 +799,13 @@ int batch_create(int count, const tblis_stra_problem* problems, BatchPlan** out)
         {
             TSB_TRY(upload_packed(pargs, &plan->descs.back(), ch.pg));
             ch.pg.err = err;
+            ch.pg.wait_limit = wait_limit_cycles();
         }
         else
         {
             TSB_TRY(upload_split(sargs, &plan->descs.back(), ch.sg));
             ch.sg.err = err;
+            ch.sg.wait_limit = wait_limit_cycles();
         }
     }
     // 4d. FP32 problems on two branches balanced by flops

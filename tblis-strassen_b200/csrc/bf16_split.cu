@@ -401,8 +401,18 @@ struct SplitGroup
     }
 };
 
+// Named barrier 1 over the 128 drain threads with an OR over `flag`: true
+// when any of them passes a non-zero flag.
+__device__ __forceinline__ bool drain_any(bool flag)
+{
+    uint32_t out;
+    asm volatile("{\n.reg .pred q, p;\nsetp.ne.u32 q, %1, 0;\nbar.red.or.pred p, 1, 128, q;\n"
+                 "selp.u32 %0, 1, 0, p;\n}\n" : "=r"(out) : "r"((uint32_t)flag) : "memory");
+    return out != 0;
+}
+
 template <int P, class Src>
-__device__ __forceinline__ void split_gemm_body(const Src& src, int* err, unsigned char* smem_raw)
+__device__ __forceinline__ void split_gemm_body(const Src& src, int* err, long long limit, unsigned char* smem_raw)
 {
     using K = SG<P>;
     // Plane pairs of the product terms (0 = hi, 1 = mid, 2 = lo): hh, hm, mh,
@@ -484,7 +494,7 @@ __device__ __forceinline__ void split_gemm_body(const Src& src, int* err, unsign
                 {
                     const int s = it % STAGES;
                     const uint32_t ph = (it / STAGES) & 1;
-                    if (!mbar_wait(bar(BAR_EMPTY + s), ph ^ 1, abort_flag, err, 1)) { ok = false; break; }
+                    if (!mbar_wait(bar(BAR_EMPTY + s), ph ^ 1, abort_flag, err, 1, limit)) { ok = false; break; }
                     mbar_expect_tx(bar(BAR_FULL + s), 2 * P * BLK);
                     const uint32_t dst = smem_u32(stages + s * K::STAGE_BYTES);
 #pragma unroll
@@ -500,7 +510,7 @@ __device__ __forceinline__ void split_gemm_body(const Src& src, int* err, unsign
             // the full barrier of each of the last STAGES stages issued).
             volatile int never = 0;
             for (uint32_t i = (it > STAGES ? it - STAGES : 0); i < it; i++)
-                mbar_wait(bar(BAR_FULL + i % STAGES), (i / STAGES) & 1, &never, nullptr, 0);
+                mbar_wait(bar(BAR_FULL + i % STAGES), (i / STAGES) & 1, &never, nullptr, 0, MBAR_WAIT_LIMIT);
         }
     }
     else if (warp == 1)
@@ -522,12 +532,12 @@ __device__ __forceinline__ void split_gemm_body(const Src& src, int* err, unsign
                     if (c % KCH == 0)
                     {
                         const int bacc = u & 1;
-                        if (!mbar_wait(bar(BAR_ACCE + bacc), ((u >> 1) & 1) ^ 1, abort_flag, err, 2)) { ok = false; break; }
+                        if (!mbar_wait(bar(BAR_ACCE + bacc), ((u >> 1) & 1) ^ 1, abort_flag, err, 2, limit)) { ok = false; break; }
                         fence_after();
                         dcol = bacc * 2 * ST;
                     }
                     const int s = it % STAGES;
-                    if (!mbar_wait(bar(BAR_FULL + s), (it / STAGES) & 1, abort_flag, err, 3)) { ok = false; break; }
+                    if (!mbar_wait(bar(BAR_FULL + s), (it / STAGES) & 1, abort_flag, err, 3, limit)) { ok = false; break; }
                     fence_after();
                     const uint32_t base = smem_u32(stages + s * K::STAGE_BYTES);
 #pragma unroll
@@ -555,7 +565,7 @@ __device__ __forceinline__ void split_gemm_body(const Src& src, int* err, unsign
             // Every MMA issued completes before TMEM is freed.
             mma_commit(bar(BAR_DRAIN));
             volatile int never = 0;
-            mbar_wait(bar(BAR_DRAIN), 0, &never, nullptr, 0);
+            mbar_wait(bar(BAR_DRAIN), 0, &never, nullptr, 0, MBAR_WAIT_LIMIT);
         }
     }
     else
@@ -566,13 +576,16 @@ __device__ __forceinline__ void split_gemm_body(const Src& src, int* err, unsign
         const int dt = tid - 64;                 // 0..127
         uint32_t u = 0;
         bool ok = true;
-        for (int64_t w = blockIdx.x; w < work && ok; w += gridDim.x)
+        for (int64_t w = blockIdx.x; w < work; w += gridDim.x)
         {
+            // Every drain thread takes part in every tile's barrier; a failed
+            // wait in any of them ends the loop for all of them here (one
+            // that failed in the previous tile skipped the rest of it).
+            if (drain_any(!ok)) break;
             int64_t local, b, tm, tn;
             const SplitGemmArgs& a = src.at(w, local);
             decode(a, local, b, tm, tn);
             const int64_t nk = a.nk;
-            asm volatile("bar.sync 1, 128;\n" ::: "memory");
             // Offsets of this tile's rows and columns in each block position
             // of C; every product of the group writes into these.
             for (int h = 0; h < 4; h++)
@@ -601,7 +614,13 @@ __device__ __forceinline__ void split_gemm_body(const Src& src, int* err, unsign
                 for (int64_t ch = 0; ch < nch; ch++, u++)
                 {
                     const int bacc = u & 1;
-                    if (!mbar_wait(bar(BAR_ACCF + bacc), (u >> 1) & 1, abort_flag, err, 4)) { ok = false; break; }
+                    // warp-uniform outcome: the TMEM loads below are warp-collective
+                    if (!__all_sync(0xffffffffu, mbar_wait(bar(BAR_ACCF + bacc), (u >> 1) & 1, abort_flag, err, 4,
+                                                          limit)))
+                    {
+                        ok = false;
+                        break;
+                    }
                     fence_after();
 #pragma unroll
                     for (int j = 0; j < ST / 32; j++)
@@ -664,7 +683,7 @@ __global__ void __launch_bounds__(192, 1)
 split_gemm_kernel(const __grid_constant__ SplitGemmArgs a)
 {
     extern __shared__ unsigned char smem_raw[];
-    split_gemm_body<P>(OneSplit{&a}, a.err, smem_raw);
+    split_gemm_body<P>(OneSplit{&a}, a.err, wait_cycles(a.wait_limit), smem_raw);
 }
 
 template <int P>
@@ -672,7 +691,7 @@ __global__ void __launch_bounds__(192, 1)
 split_gemm_grouped_kernel(const __grid_constant__ SplitGroupArgs g)
 {
     extern __shared__ unsigned char smem_raw[];
-    split_gemm_body<P>(SplitGroup{g}, g.err, smem_raw);
+    split_gemm_body<P>(SplitGroup{g}, g.err, wait_cycles(g.wait_limit), smem_raw);
 }
 
 template <int P>

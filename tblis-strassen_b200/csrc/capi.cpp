@@ -55,6 +55,8 @@ thread_local int t_status = TBLIS_STRA_SUCCESS;
 thread_local size_t t_ws_limit = SIZE_MAX;   // device workspace the ABC schedule may use
 thread_local int t_fp32_terms = 6;           // split-BF16 product terms for FP32 (3 or 6)
 thread_local int t_product_parallel = -1;    // product-parallel ABC: -1 auto, 0 never, 1 when it fits
+thread_local long long t_wait_limit = 0;     // pipeline wait bound in SM cycles (0: the kernels' default)
+thread_local size_t t_alloc_limit = SIZE_MAX;  // largest single device allocation a call may make
 unsigned g_num_threads = 1;
 thread_local std::string t_detail;           // what the last failing CUDA call was
 
@@ -117,7 +119,8 @@ int upload_plan(const GemmView& g, int device, std::shared_ptr<DevPlan>& out)
         pos += std::max<size_t>(parts[i]->size(), 1);
     }
     dp->bytes = total * sizeof(int64_t);
-    if (cudaMalloc(&dp->mem, dp->bytes) != cudaSuccess) { dp->mem = nullptr; return TBLIS_STRA_ERR_ALLOC; }
+    if (dp->bytes > t_alloc_limit) return TBLIS_STRA_ERR_ALLOC;
+    if (cudaMalloc(&dp->mem, dp->bytes) != cudaSuccess) { cudaGetLastError(); dp->mem = nullptr; return TBLIS_STRA_ERR_ALLOC; }
     const int s = upload_complete(dp->mem, host.data(), dp->bytes);
     if (s) return s;
     const int64_t* base = static_cast<const int64_t*>(dp->mem);
@@ -164,6 +167,7 @@ int plan_m_tables(const DevPlan& t, int level, int64_t ms, int64_t ns, int64_t n
         std::vector<int64_t> h((size_t)(ms + ns + nb));
         dense_m_tables(ms, ns, nb, col_major, h.data());
         void* d = nullptr;
+        if (h.size() * sizeof(int64_t) > t_alloc_limit) return TBLIS_STRA_ERR_ALLOC;
         if (cudaMalloc(&d, h.size() * sizeof(int64_t)) != cudaSuccess) { cudaGetLastError(); return TBLIS_STRA_ERR_ALLOC; }
         const int s = upload_complete(d, h.data(), h.size() * sizeof(int64_t));
         if (s) { cudaFree(d); return s; }
@@ -237,6 +241,7 @@ struct Scratch
     {
         s = st;
         if (bytes == 0) bytes = 16;
+        if (bytes > t_alloc_limit) return TBLIS_STRA_ERR_ALLOC;
         int device = 0;
         if (cudaGetDevice(&device) != cudaSuccess) { cudaGetLastError(); return TBLIS_STRA_ERR_NO_DEVICE; }
         cudaMemPool_t pool = library_pool(device);
@@ -599,6 +604,7 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
             ga.nprod = 1; ga.H = 1;
             ga.nc[0] = 1; ga.c_s[0][0] = 1; ga.c_first[0][0] = 1;
             ga.err = err;
+            ga.wait_limit = wait_limit_cycles();
             TSB_CUDA(launch_packed_gemm(ga, st, sms));
         }
         else
@@ -762,6 +768,7 @@ PackedGemmArgs packed_gemm_base(int level, const GemmView& g, const PackGeom& pg
 {
     PackedGemmArgs ga{};
     ga.err = err;
+    ga.wait_limit = wait_limit_cycles();
     ga.C = C;
     ga.rsC = tb[1]; ga.csC = tb[3]; ga.bC = tb[8];
     ga.m = g.m; ga.n = g.n; ga.ms = pg.ms; ga.ns = pg.ns; ga.k_pad = pg.k_pad;
@@ -910,6 +917,7 @@ int enqueue_products_and_combine(int level, const GemmView& g, const int64_t* co
                                           ((size_t)np * (pg.s_elems + pg.t_elems) * sizeof(double) + 255) / 256 * 256);
     PackedGemmArgs ga{};
     ga.err = err;
+    ga.wait_limit = wait_limit_cycles();
     ga.C = M;
     ga.rsC = mtab; ga.csC = mtab + pg.ms; ga.bC = mtab + pg.ms + pg.ns;
     ga.m = pg.ms; ga.n = pg.ns; ga.ms = pg.ms; ga.ns = pg.ns; ga.k_pad = pg.k_pad;
@@ -1019,6 +1027,7 @@ int run_fp64_ksplit_enqueue(const GemmView& g, const int64_t* const tb[9], const
     }
     PackedGemmArgs ga{};
     ga.err = err;
+    ga.wait_limit = wait_limit_cycles();
     ga.C = M;
     ga.rsC = mtab; ga.csC = mtab + g.m; ga.bC = mtab + g.m + g.n;
     ga.m = g.m; ga.n = g.n; ga.ms = g.m; ga.ns = g.n; ga.k_pad = pg.k_pad;
@@ -1045,6 +1054,9 @@ int run_fp64_ksplit_enqueue(const GemmView& g, const int64_t* const tb[9], const
 // pageable memory may return before its DMA completes, and kernels on
 // non-blocking streams are not ordered after it, so tables read by such
 // kernels go through a private non-blocking stream per device, synchronised.
+long long wait_limit_cycles() { return t_wait_limit; }
+size_t alloc_limit_bytes() { return t_alloc_limit; }
+
 int upload_complete(void* dst, const void* src, size_t bytes)
 {
     static std::mutex mu;
@@ -1223,6 +1235,7 @@ int run_fp32_enqueue(int level, const GemmView& g, const int64_t* const tb[9], c
         ga.nterms = P == 3 ? 6 : 3;
         for (int i = 0; i < 6; i++) { ga.ta[i] = TA6[i]; ga.tb[i] = TB6[i]; }
         ga.err = err;
+        ga.wait_limit = wait_limit_cycles();
         if (defer) { *defer = ga; return TBLIS_STRA_SUCCESS; }
         TSB_CUDA(launch_split_gemm(ga, st, sms));
         return TBLIS_STRA_SUCCESS;
@@ -1386,6 +1399,7 @@ int run_fp32_parallel_enqueue(int level, const GemmView& g, const int64_t* const
     ga.nterms = P == 3 ? 6 : 3;
     for (int i = 0; i < 6; i++) { ga.ta[i] = TA6[i]; ga.tb[i] = TB6[i]; }
     ga.err = err;
+    ga.wait_limit = wait_limit_cycles();
     TSB_CUDA(launch_split_gemm(ga, st, sms));
 
     CombineF32Args c{};
@@ -1484,6 +1498,7 @@ int run_fp32_ksplit_enqueue(const GemmView& g, const int64_t* const tb[9], const
     ga.nterms = planes == 3 ? 6 : 3;
     for (int i = 0; i < 6; i++) { ga.ta[i] = TA6[i]; ga.tb[i] = TB6[i]; }
     ga.err = err;
+    ga.wait_limit = wait_limit_cycles();
     TSB_CUDA(launch_split_gemm(ga, st, sms));
 
     CombineF32Args c{};
@@ -2116,6 +2131,21 @@ int tblis_stra_set_product_parallel(int mode)
 }
 
 int tblis_stra_get_product_parallel(void) { return tsb::t_product_parallel; }
+
+int tblis_stra_set_wait_limit(long long cycles)
+{
+    if (cycles < 0) return TBLIS_STRA_ERR_ARG;
+    tsb::t_wait_limit = cycles;
+    return TBLIS_STRA_SUCCESS;
+}
+long long tblis_stra_get_wait_limit(void) { return tsb::t_wait_limit; }
+
+int tblis_stra_set_alloc_limit(size_t bytes)
+{
+    tsb::t_alloc_limit = bytes;
+    return TBLIS_STRA_SUCCESS;
+}
+size_t tblis_stra_get_alloc_limit(void) { return tsb::t_alloc_limit; }
 
 int tblis_stra_last_status(void) { return tsb::t_status; }
 

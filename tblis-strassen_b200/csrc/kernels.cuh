@@ -182,6 +182,7 @@ struct PackedGemmArgs
     int8_t c_r[MAX_GROUP_PRODUCTS][4], c_c[MAX_GROUP_PRODUCTS][4];
     int8_t c_s[MAX_GROUP_PRODUCTS][4], c_first[MAX_GROUP_PRODUCTS][4];
     int* err;                                  // set on a timed-out wait (may be null)
+    long long wait_limit;                      // bound on each pipeline wait, SM cycles (0: ~1 s)
 };
 
 // Seven packed operand sums in one pass (pack_multi_kernel): the blocks of
@@ -213,6 +214,7 @@ struct PackedGroupArgs
     int nprob;
     int64_t total;
     int* err;                      // set on a timed-out wait (may be null)
+    long long wait_limit;          // bound on each pipeline wait, SM cycles (0: ~1 s)
 };
 
 // ---- split-BF16 (FP32 contractions on tcgen05) --------------------------------------
@@ -300,6 +302,7 @@ struct SplitGemmArgs
     int planes, nterms;
     int8_t ta[6], tb[6];                       // plane pair of each product term
     int* err;                                  // set on a timed-out wait (may be null)
+    long long wait_limit;                      // bound on each pipeline wait, SM cycles (0: ~1 s)
 };
 
 // Grouped split GEMM: many problems' tiles in one persistent launch (all
@@ -311,6 +314,7 @@ struct SplitGroupArgs
     int nprob;
     int64_t total;
     int* err;                      // set on a timed-out wait (may be null)
+    long long wait_limit;          // bound on each pipeline wait, SM cycles (0: ~1 s)
 };
 
 cudaError_t launch_split_scale(const SplitScaleArgs& args, cudaStream_t stream);

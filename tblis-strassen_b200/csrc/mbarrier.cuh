@@ -10,6 +10,15 @@ namespace tsb {
 
 constexpr long long MBAR_WAIT_LIMIT = 2000000000LL;   // clock cycles (~1 s)
 
+// The bound a kernel applies to its pipeline waits: `requested` cycles when
+// positive (tblis_stra_set_wait_limit), else MBAR_WAIT_LIMIT.  Waits that only
+// let a CTA's own copies or MMAs land before it exits always use
+// MBAR_WAIT_LIMIT, so no CTA leaves with work in flight.
+__host__ __device__ __forceinline__ long long wait_cycles(long long requested)
+{
+    return requested > 0 ? requested : MBAR_WAIT_LIMIT;
+}
+
 __device__ __forceinline__ uint32_t smem_addr(const void* p)
 {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -36,9 +45,10 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t addr, uint32_t bytes)
                  :: "r"(addr), "r"(bytes) : "memory");
 }
 
-// Bounded wait for the phase of the given parity; false on timeout or abort.
+// Bounded wait (at most `limit` clock cycles) for the phase of the given
+// parity; false on timeout or abort.
 __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity, volatile int* abort_flag,
-                                          int* err, int code)
+                                          int* err, int code, long long limit)
 {
     const long long start = clock64();
     while (true)
@@ -48,7 +58,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity, volati
                      "selp.u32 %0, 1, 0, p;\n}\n" : "=r"(done) : "r"(addr), "r"(parity) : "memory");
         if (done) return true;
         if (*abort_flag) return false;
-        if (clock64() - start > MBAR_WAIT_LIMIT)
+        if (clock64() - start > limit)
         {
             *abort_flag = 1;
             if (err) atomicExch(err, code);

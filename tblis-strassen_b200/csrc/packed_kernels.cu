@@ -324,7 +324,7 @@ constexpr size_t ws_smem()
 }
 
 template <class K, class Src>
-__device__ __forceinline__ void packed_ws_body(const Src& src, int* err, unsigned char* smem)
+__device__ __forceinline__ void packed_ws_body(const Src& src, int* err, long long limit, unsigned char* smem)
 {
     constexpr int BM = K::BM, BN = K::BN, BK = K::BK, NT = K::NT, STAGES = K::STAGES;
     constexpr int MI = K::MI, NI = K::NI, NW = NT / 32;
@@ -376,7 +376,7 @@ __device__ __forceinline__ void packed_ws_body(const Src& src, int* err, unsigne
             }
             const uint32_t it = ctl->pit, slot = it % STAGES;
             if (it >= (uint32_t)STAGES &&
-                !mbar_wait(smem_addr(&ctl->empty[slot]), ((it / STAGES) & 1) ^ 1, abort_flag, err, 1))
+                !mbar_wait(smem_addr(&ctl->empty[slot]), ((it / STAGES) & 1) ^ 1, abort_flag, err, 1, limit))
                 return false;
             const uint32_t full = smem_addr(&ctl->full[slot]);
             mbar_expect_tx(full, (uint32_t)((BK * BM + BK * BN) * 8));
@@ -456,7 +456,8 @@ __device__ __forceinline__ void packed_ws_body(const Src& src, int* err, unsigne
                 const uint32_t slot = cit % STAGES;
                 // warp-uniform outcome, so the warp stays converged
                 ok = __all_sync(0xffffffffu,
-                                mbar_wait(smem_addr(&ctl->full[slot]), (cit / STAGES) & 1, abort_flag, err, 2));
+                                mbar_wait(smem_addr(&ctl->full[slot]), (cit / STAGES) & 1, abort_flag, err, 2,
+                                          limit));
                 if (!ok) break;
                 const double* Ab = As + slot * BK * BM;
                 const double* Bb = Bs + slot * BK * BN;
@@ -541,7 +542,7 @@ __device__ __forceinline__ void packed_ws_body(const Src& src, int* err, unsigne
         volatile int never = 0;
         const uint32_t pit = ctl->pit;
         for (uint32_t i = (pit > (uint32_t)STAGES ? pit - STAGES : 0); i < pit; i++)
-            mbar_wait(smem_addr(&ctl->full[i % STAGES]), (i / STAGES) & 1, &never, nullptr, 0);
+            mbar_wait(smem_addr(&ctl->full[i % STAGES]), (i / STAGES) & 1, &never, nullptr, 0, MBAR_WAIT_LIMIT);
     }
 }
 
@@ -550,7 +551,7 @@ __global__ void __launch_bounds__(K::NT, 1)
 packed_gemm_ws_kernel(const __grid_constant__ PackedGemmArgs a)
 {
     extern __shared__ __align__(128) unsigned char smem[];
-    packed_ws_body<K>(OneProblem{&a}, a.err, smem);
+    packed_ws_body<K>(OneProblem{&a}, a.err, wait_cycles(a.wait_limit), smem);
 }
 
 template <class K>
@@ -558,7 +559,7 @@ __global__ void __launch_bounds__(K::NT, 1)
 packed_gemm_grouped_kernel(const __grid_constant__ PackedGroupArgs g)
 {
     extern __shared__ __align__(128) unsigned char smem[];
-    packed_ws_body<K>(ProblemGroup{g}, g.err, smem);
+    packed_ws_body<K>(ProblemGroup{g}, g.err, wait_cycles(g.wait_limit), smem);
 }
 
 template <class K>

@@ -21,6 +21,12 @@ void note_cuda_error(const char* what, cudaError_t e, const char* file, int line
 void note_detail(const std::string& what);
 void clear_detail();
 
+// The calling thread's bound on the pipeline waits of the warp-specialised
+// kernels, in SM clock cycles (tblis_stra_set_wait_limit; 0 = the default).
+long long wait_limit_cycles();
+// The calling thread's ceiling on one device allocation (tblis_stra_set_alloc_limit).
+size_t alloc_limit_bytes();
+
 // Host -> device copy complete on return (see capi.cpp).
 int upload_complete(void* dst, const void* src, size_t bytes);
 

@@ -147,6 +147,12 @@ def _load() -> ctypes.CDLL:
     lib.tblis_stra_get_batch_schedules.restype = ctypes.c_uint
     lib.tblis_stra_batch_destroy.argtypes = [ctypes.c_void_p]
     lib.tblis_stra_batch_destroy.restype = None
+    lib.tblis_stra_set_wait_limit.argtypes = [ctypes.c_longlong]
+    lib.tblis_stra_set_wait_limit.restype = ctypes.c_int
+    lib.tblis_stra_get_wait_limit.restype = ctypes.c_longlong
+    lib.tblis_stra_set_alloc_limit.argtypes = [ctypes.c_size_t]
+    lib.tblis_stra_set_alloc_limit.restype = ctypes.c_int
+    lib.tblis_stra_get_alloc_limit.restype = ctypes.c_size_t
     lib.tblis_get_num_threads.restype = ctypes.c_uint
     lib.tblis_set_num_threads.argtypes = [ctypes.c_uint]
     return lib
@@ -367,6 +373,29 @@ class Batch:
 
 
 KERNEL_KINDS = {"fused": 0, "pack": 1, "packed_gemm": 2, "aux": 3, "split_gemm": 4}
+
+
+def set_wait_limit(cycles: int) -> None:
+    """Bound (SM clock cycles) on each pipeline wait of the warp-specialised
+    kernels; 0 restores the default (about one second).  A wait that runs out
+    ends the kernel cleanly and blocking calls raise status
+    TBLIS_STRA_ERR_TIMEOUT."""
+    _check(lib.tblis_stra_set_wait_limit(cycles))
+
+
+def get_wait_limit() -> int:
+    return int(lib.tblis_stra_get_wait_limit())
+
+
+def set_alloc_limit(nbytes: int | None) -> None:
+    """Ceiling on any single device allocation a call makes (None = no
+    ceiling); a call that would exceed it raises status TBLIS_STRA_ERR_ALLOC
+    and leaves C untouched."""
+    _check(lib.tblis_stra_set_alloc_limit(ctypes.c_size_t(-1).value if nbytes is None else nbytes))
+
+
+def get_alloc_limit() -> int:
+    return int(lib.tblis_stra_get_alloc_limit())
 
 
 def set_product_parallel(mode: int) -> None:

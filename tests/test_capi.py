@@ -45,6 +45,43 @@ def test_struct_layout_matches_header(tsb, tmp_path):
     assert got == want
 
 
+def test_struct_layout_matches_reference_header():
+    """include/tblis_stra_b200.h against the reference's own
+    src/util/basic_types.h, through the fixture tests/golden/make_layout.py
+    compiled from the reference header: every offset, field size, struct size
+    and alignment of tblis_tensor and tblis_matrix, the scalar typedefs and the
+    type_t values."""
+    import json
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from make_layout import layout
+    with open(os.path.join(ROOT, "tests", "golden", "struct_layout.json")) as f:
+        want = json.load(f)
+    want.pop("_source")
+    got = layout(["-I" + os.path.join(ROOT, "include")], HEADER)
+    assert got == want
+
+
+def build_c_example(tmp_path):
+    """Compile and link tests/capi_example.c the way INTEGRATION.md says a C
+    caller does: the public header and -ltblis_stra_b200, nothing else."""
+    lib_dir = os.path.join(ROOT, "tblis-strassen_b200")
+    exe = tmp_path / "capi_example"
+    subprocess.check_call(["gcc", "-std=c11", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                           os.path.join(ROOT, "tests", "capi_example.c"), "-o", str(exe),
+                           "-L", lib_dir, "-ltblis_stra_b200", "-Wl,-rpath," + lib_dir])
+    return str(exe)
+
+
+def test_c_example_links_and_runs(tsb, tmp_path):
+    """The linked C program runs; without a GPU the drop-in call reports
+    TBLIS_STRA_ERR_NO_DEVICE as its status instead of aborting."""
+    import torch
+    exe = build_c_example(tmp_path)
+    r = subprocess.run([exe, "1", "1", str(tmp_path / "C.bin"), "6"], capture_output=True)
+    assert r.returncode == (0 if torch.cuda.is_available() else 10), r.stderr
+
+
 def test_impl_knob(tsb):
     assert tsb.get_impl() == 1
     for impl in (2, 3, 1):
