@@ -286,6 +286,43 @@ def batched_form(torch, tsb, device, stream, count, barrier_sync, max_over_ranks
     return out
 
 
+def differentiation_form(torch, device, stream, barrier_sync, max_over_ranks, steps=3):
+    """Forward plus backward of the two-contraction chain C(a,b,i,j) =
+    sum_{e,f} A(a,b,e,f) B(e,f,i,j), D(a,b,k,l) = sum_{i,j} C E(i,j,k,l),
+    loss = sum D*W (a,b,e,f = 128, i,j,k,l = 48; U[-1,1]) through the
+    autograd binding: FP64 and FP32 (split-BF16, 6 terms) at L = 0 and 1.
+    One step = forward + backward (6 contractions, 4.24 TFLOP by 2mnk)."""
+    import importlib
+    ag = importlib.import_module("tblis_strassen_b200.autograd")
+    n, m = 128, 48
+    # 2mnk of: C, D (forward); dL/dC, dA, dB, dE (backward)
+    flops = 2.0 * (n * n * m * m * n * n + n * n * m * m * m * m
+                   + n * n * m * m * m * m + n * n * n * n * m * m + n * n * m * m * n * n + m * m * m * m * n * n)
+    out = {"workload": "C(abij)=A(abef)B(efij), D(abkl)=C(abij)E(ijkl), loss=sum D*W; a,b,e,f=128, i,j,k,l=48",
+           "tflop_per_step": flops / 1e12}
+    for dtype, name in ((torch.float64, "fp64"), (torch.float32, "fp32_split6")):
+        g = torch.Generator(device=device).manual_seed(2)
+        A = (torch.rand((n, n, n, n), dtype=dtype, device=device, generator=g) * 2 - 1).requires_grad_()
+        B = (torch.rand((n, n, m, m), dtype=dtype, device=device, generator=g) * 2 - 1).requires_grad_()
+        E = (torch.rand((m, m, m, m), dtype=dtype, device=device, generator=g) * 2 - 1).requires_grad_()
+        W = torch.rand((n, n, m, m), dtype=dtype, device=device, generator=g) * 2 - 1
+        for level in (0, 1):
+            def step():
+                for X in (A, B, E):
+                    X.grad = None
+                C = ag.contract(A, "abef", B, "efij", "abij", level=level)
+                D = ag.contract(C, "abij", E, "ijkl", "abkl", level=level)
+                (D * W).sum().backward()
+            for _ in range(2):
+                step()
+            barrier_sync()
+            t = max_over_ranks(time_steps(torch, step, steps, stream))
+            out[f"{name}_L{level}"] = {"tflops_effective": flops * steps / t / 1e12, "ms_per_step": t / steps * 1e3}
+        del A, B, E, W
+        torch.cuda.empty_cache()
+    return out
+
+
 def time_steps(torch, fn, steps, stream):
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
@@ -454,6 +491,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP32 split-BF16 lines")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-form lines")
+    ap.add_argument("--no-autograd", action="store_true", help="skip the differentiation-form lines")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--dtype", choices=["f64", "f32"], default="f64",
                     help="operand type of the --kernels probe (f32 = split-BF16 tcgen05 path)")
@@ -559,6 +597,28 @@ def main():
         tl = max_over_ranks(time_steps(torch, lambda: step(lv, 1), max(2, args.steps // 2), stream))
         levels[f"L{lv}"] = flops * max(2, args.steps // 2) / tl / 1e12
 
+    # ---- the no-workspace ABC kernel (all products in one persistent launch,
+    #      operand sums formed per staged tile), through the regular call with
+    #      no workspace allowed and through the allocation-free entry point
+    no_workspace = {}
+    tsb.set_workspace_limit(0)
+    try:
+        for _ in range(2):
+            step()
+        barrier_sync()
+        nw = max(2, args.steps // 4)
+        tf = max_over_ranks(time_steps(torch, step, nw, stream))
+        no_workspace[f"L{args.level}_workspace0"] = flops * nw / tf / 1e12
+    finally:
+        tsb.set_workspace_limit(None)
+    noalloc = tsb.noalloc_mult
+    for _ in range(2):
+        noalloc(args.level, 1.0, A, IDX_A, B, IDX_B, 1.0, C, IDX_C, stream=stream)
+    barrier_sync()
+    tf = max_over_ranks(time_steps(torch, lambda: noalloc(args.level, 1.0, A, IDX_A, B, IDX_B, 1.0, C, IDX_C,
+                                                            stream=stream), nw, stream))
+    no_workspace[f"L{args.level}_noalloc"] = flops * nw / tf / 1e12
+
     # ---- accuracy of this run's result: sampled entries against exact dots --
     C.zero_()
     step()
@@ -574,6 +634,13 @@ def main():
 
     # ---- roofline of the dominant kernel ------------------------------------
     peak = dgemm_peak(torch, device)
+    # the FP64 tensor-pipe ceiling itself: register-only DMMA loops, with the
+    # SM clock sampled while they run (about 0.5 s per launch)
+    psampler = ClockSampler(local_rank) if rank == 0 else None
+    if psampler:
+        psampler.start()
+    dmma_ceiling, dmma_ms = tsb.measure_dmma_peak(500000, stream)
+    pclocks = psampler.stop() if psampler else None
     kinds = kinds_snapshot
     dom = max(kinds, key=lambda k: kinds[k][1])
     n_launch, dom_ms = kinds[dom]
@@ -587,6 +654,13 @@ def main():
                 "traffic": NCU_TRAFFIC_BYTES,
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
                 "executed_frac": achieved * (7.0 / 8.0) ** args.level / peak,
+                "peak_dmma": dmma_ceiling,
+                "peak_dmma_source": ("register-only m16n8k4 DMMA loops on every SM (tblis_stra_measure_dmma_peak), "
+                                     f"one {dmma_ms:.0f} ms launch, SM clock median "
+                                     f"{(pclocks or {}).get('sm_mhz')} MHz"),
+                "frac_of_dmma_ceiling": achieved / dmma_ceiling,
+                "executed_frac_of_dmma_ceiling": achieved * (7.0 / 8.0) ** args.level / dmma_ceiling,
+                "L0_frac_of_dmma_ceiling": None,
                 "kernel": {"fused": "stra_dmma_kernel", "pack": "pack_kernel",
                            "packed_gemm": "packed_gemm_ws_kernel", "aux": "aux"}[dom],
                 "launches_timed": n_launch, "kernel_ms_total": dom_ms,
@@ -626,6 +700,11 @@ def main():
         precision["best_6terms_vs_fp64_L0"] = best6 / levels["L0"]
         del A32, B32, C32, Cref
         torch.cuda.empty_cache()
+
+    # ---- differentiation form: forward + backward through the autograd binding
+    differentiation = None
+    if not args.no_autograd:
+        differentiation = differentiation_form(torch, device, stream, barrier_sync, max_over_ranks)
 
     # ---- end to end through the C ABI with pinned host buffers --------------
     e2e = None
@@ -669,6 +748,8 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return
+    if levels.get("L0"):
+        roofline["L0_frac_of_dmma_ceiling"] = levels["L0"] / dmma_ceiling
     line = {"metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic U[-1,1] (seed 0)",
@@ -681,6 +762,8 @@ def main():
             "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
             "precision_form": precision,
             "batched_form": batched,
+            "differentiation_form": differentiation,
+            "no_workspace_tflops": no_workspace,
             "gpu_launches": launches,
             "measured_peaks_file": {k: measured_peaks().get(k) for k in ("hbm_gbs", "bf16_tflops")}}
     print(json.dumps(line))

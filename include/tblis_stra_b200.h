@@ -367,6 +367,13 @@ void tblis_stra_batch_destroy(tblis_stra_batch batch);
 int tblis_stra_set_kernel_timing(int on);
 int tblis_stra_kernel_timing(int kind, unsigned long long* launches, double* total_ms);
 
+/* The FP64 tensor-pipe ceiling of the current GPU (no counterpart in the
+ * reference): the DMMA throughput, in TFLOP/s, of register-only m16n8k4 MMA
+ * loops on every SM (`iterations` rounds of 8 MMAs per warp, 32 warps per SM),
+ * timed with CUDA events on `stream` after one warm-up launch; `ms` is the
+ * timed launch's duration.  The roofline denominator of the FP64 kernels. */
+int tblis_stra_measure_dmma_peak(int iterations, double* tflops, double* ms, void* stream);
+
 /* Library version string. */
 const char* tblis_stra_version(void);
 

@@ -469,7 +469,27 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
         a.nprod = (int)tab.prod.size();
         a.H = a.Hc = H;
         for (int p = 0; p < a.nprod; p++) a.prod[p] = to_dev(tab.prod[p]);
-        TSB_CUDA(launch_dmma(a, max_terms(tab), st, sms));
+        // The producer/consumer fused kernel; the earlier all-warps kernel
+        // where it cannot run these arguments.
+        Scratch ferr;
+        int* err = shared_err;
+        int s;
+        if (!err && blocking)
+        {
+            if ((s = ferr.alloc(sizeof(int), st))) return s;
+            TSB_CUDA(cudaMemsetAsync(ferr.p, 0, sizeof(int), st));
+            err = static_cast<int*>(ferr.p);
+        }
+        cudaError_t e = launch_fused(a, st, sms, err, wait_limit_cycles());
+        if (e == cudaErrorNotSupported) e = launch_dmma(a, max_terms(tab), st, sms);
+        TSB_CUDA(e);
+        if (blocking && !shared_err)
+        {
+            int flag = 0;
+            TSB_CUDA(cudaMemcpyAsync(&flag, ferr.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            TSB_CUDA(cudaStreamSynchronize(st));
+            if (flag) return TBLIS_STRA_ERR_TIMEOUT;
+        }
         return TBLIS_STRA_SUCCESS;
     }
 
@@ -2131,6 +2151,18 @@ int tblis_stra_set_product_parallel(int mode)
 }
 
 int tblis_stra_get_product_parallel(void) { return tsb::t_product_parallel; }
+
+int tblis_stra_measure_dmma_peak(int iterations, double* tflops, double* ms, void* stream)
+{
+    if (!tflops || !ms) return TBLIS_STRA_ERR_NULL;
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) { cudaGetLastError(); return TBLIS_STRA_ERR_NO_DEVICE; }
+    const cudaError_t e = tsb::measure_dmma_peak(iterations, tsb::num_sms(device), static_cast<cudaStream_t>(stream),
+                                                 tflops, ms);
+    if (e == cudaErrorInvalidValue) return TBLIS_STRA_ERR_ARG;
+    if (e != cudaSuccess) { tsb::note_cuda_error("measure_dmma_peak", e, __FILE__, __LINE__); return TBLIS_STRA_ERR_CUDA; }
+    return TBLIS_STRA_SUCCESS;
+}
 
 int tblis_stra_set_wait_limit(long long cycles)
 {

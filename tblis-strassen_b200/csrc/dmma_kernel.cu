@@ -86,25 +86,6 @@ struct Cfg
     static_assert((BK * BM) % NT == 0 && (BK * BN) % NT == 0, "loader covers the tile");
 };
 
-// Loader lane maps: element e (= thread + x * threads) of a BK x BM tile.
-// k-fast: half-warps take 8 consecutive k of rows (m, m+8); row-fast: 16
-// consecutive rows of one k.
-template <int BK, int BM>
-__device__ __forceinline__ void lane_map(bool kfast, int e, int& kk, int& m)
-{
-    if (kfast)
-    {
-        kk = (e & 7) + 8 * ((e >> 4) % (BK / 8));
-        const int ridx = 2 * (e / (16 * (BK / 8))) + ((e >> 3) & 1);
-        m = (ridx & ~15) | ((ridx & 1) << 3) | ((ridx >> 1) & 7);
-    }
-    else
-    {
-        m = e % BM;
-        kk = e / BM;
-    }
-}
-
 // One (batch, tile) work item of a contraction: all of its Strassen products.
 template <class K, bool KA, bool KB>
 __device__ __forceinline__ void dmma_tile(const DmmaArgs& args, int64_t w, unsigned char* smem)
@@ -528,9 +509,63 @@ int config_family(int terms, int H, int Hc)
     return 3;
 }
 
+// FP64 tensor-pipe ceiling: every warp issues `iters` rounds of 8
+// independent m16n8k4 DMMAs on register operands (no memory traffic), so the
+// pipe, not the operand feed, sets the rate.  The result is stored only if it
+// equals an impossible value (the operands are non-negative, so the sum is),
+// which keeps the loop alive.
+__device__ double g_dmma_peak_sink;
+
+__global__ void __launch_bounds__(512, 2) dmma_peak_kernel(int iters)
+{
+    double acc[8][4];
+#pragma unroll
+    for (int j = 0; j < 8; j++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) acc[j][e] = 0.0;
+    const double a0 = 1e-3 * (threadIdx.x & 31), a1 = 2e-3, b0 = 1e-3 * blockIdx.x;
+    for (int i = 0; i < iters; i++)
+    {
+#pragma unroll
+        for (int j = 0; j < 8; j++) dmma(acc[j], a0, a1, b0);
+    }
+    double t = 0.0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) t += acc[j][0] + acc[j][1] + acc[j][2] + acc[j][3];
+    if (t == -1.0) g_dmma_peak_sink = t;
+}
+
 }  // namespace
 
 std::atomic<unsigned long long> g_launches{0};
+
+cudaError_t measure_dmma_peak(int iters, int num_sms, cudaStream_t stream, double* tflops, double* ms)
+{
+    if (iters <= 0 || num_sms <= 0) return cudaErrorInvalidValue;
+    const int per_sm = 2, threads = 512;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t err = cudaEventCreate(&e0);
+    if (err == cudaSuccess) err = cudaEventCreate(&e1);
+    if (err == cudaSuccess)
+    {
+        dmma_peak_kernel<<<num_sms * per_sm, threads, 0, stream>>>(iters);   // warm-up
+        cudaEventRecord(e0, stream);
+        dmma_peak_kernel<<<num_sms * per_sm, threads, 0, stream>>>(iters);
+        cudaEventRecord(e1, stream);
+        err = cudaEventSynchronize(e1);
+    }
+    float t = 0.f;
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&t, e0, e1);
+    if (err == cudaSuccess) err = cudaGetLastError();
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (err != cudaSuccess) return err;
+    g_launches += 2;
+    const double flops = 2.0 * 16 * 8 * 4 * 8.0 * (double)iters * (threads / 32) * (double)num_sms * per_sm;
+    *ms = t;
+    *tflops = flops / (t * 1e-3) / 1e12;
+    return cudaSuccess;
+}
 
 void dmma_tile_shape(int terms, int H, int Hc, int config, int* bm, int* bn)
 {

@@ -1,0 +1,415 @@
+// Fully fused FP64 ABC Strassen kernel: all 7^L products of a contraction in
+// one persistent launch, no workspace.
+//
+// What it replaces in the reference (src/stra_internal/3t/stra_mult.cxx:308-605
+// and its 2-level form): the per-product control tree with fused packing
+// (stra_pack_{two,four}_*, src/kernels/3m/gemm.hpp:504-816, 1344-1917) and the
+// micro-kernel that adds +-M into up to 4 C blocks (stra_gemm_ukr_{two,four},
+// src/stra_nodes/stra_gemm_ukr.hpp:622-940).
+//
+// Warp roles (384 threads per CTA, one CTA per SM, persistent over
+// (batch, 128 x 128 tile) work items; every CTA runs all products of its tile
+// in order, so C blocks shared by products need no atomics and beta is
+// applied once, by the first product touching a block):
+//
+//   producer warpgroup (warps 0-3): for each k-step of 32 gathers the 2, or
+//     up to 4 at L = 2, A blocks (and B blocks) of the product's signed sums
+//     through the scatter vectors into registers, forms S = sum_i u_i A_i and
+//     T = sum_j v_j B_j, and stores them into a ring slot in the swizzled
+//     k-major layout of the DMMA fragments (tile_pos), so each operand sum is
+//     formed once per staged tile rather than per fragment read; the slot's
+//     "full" mbarrier then completes.  Its registers are cut to PROD_REGS.
+//   consumer warpgroups (warps 4-11): 2 x 4 warps of 64 x 32 (m16n8k4 DMMA
+//     fragments read as 128-bit pairs), registers raised to CONS_REGS; after a
+//     slot is read each warp arrives on its "empty" mbarrier; after the last
+//     k-step of a product the epilogue adds +-alpha*S*T into the product's C
+//     blocks.
+//
+// The producer runs up to STAGES k-steps ahead, across product and tile
+// boundaries.  Every wait is bounded; a wait that runs out makes both roles
+// leave their loops at the next tile (a collective OR over each role's named
+// barrier), and with no asynchronous copies in flight the CTA simply ends.
+#include "kernels.cuh"
+#include "mbarrier.cuh"
+#include "tile_layout.cuh"
+#include "timing.hpp"
+
+#include <atomic>
+
+namespace tsb {
+
+extern std::atomic<unsigned long long> g_launches;
+
+namespace {
+
+constexpr int FT = 128;                  // tile rows (A side) and columns (B side)
+constexpr int FBK = 32;                  // k per ring slot
+constexpr int FSTAGES = 3;
+constexpr int FHMAX = 4;                 // largest block grid side (level 2)
+constexpr int NPW = 4;                   // producer warps (one warpgroup)
+constexpr int NCW = 8;                   // consumer warps: 2 (M) x 4 (N)
+constexpr int FTHREADS = 32 * (NPW + NCW);
+constexpr int PT = 32 * NPW;             // producer threads
+constexpr int CT = 32 * NCW;             // consumer threads
+constexpr int CWM = 2, CWN = 4;
+constexpr int WTM = FT / CWM, WTN = FT / CWN;   // 64 x 32 warp tile
+constexpr int MI = WTM / 16, NI = WTN / 8;      // 4 x 4 fragments
+constexpr int PE = FBK * FT / PT;        // elements of one operand tile per producer thread (32)
+constexpr int PCH = 16;                  // producer elements per batch of loads
+
+// Register split: threads x launch registers is the CTA's pool; the producer
+// gives back what the consumers take (checked against the compiled count on
+// the host before every launch).
+constexpr int PROD_REGS = 96;
+constexpr int CONS_REGS = 200;
+
+struct FusedCtrl
+{
+    uint64_t full[FSTAGES], empty[FSTAGES];
+    int abort;
+};
+
+constexpr size_t SLOT_DOUBLES = size_t(FBK) * FT * 2;                  // S and T tiles
+constexpr size_t RING_BYTES = FSTAGES * SLOT_DOUBLES * 8;
+constexpr size_t TAB_BYTES = size_t(4) * FHMAX * FT * 8                 // rowA, colB, rowC, colC
+                             + size_t(2) * FHMAX * FBK * 8;             // k tables of A and B
+constexpr size_t FUSED_SMEM = RING_BYTES + TAB_BYTES + sizeof(FusedCtrl);
+static_assert(FUSED_SMEM <= 227 * 1024, "shared memory budget");
+static_assert(PE % PCH == 0, "producer batches cover a tile");
+
+__device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, double b0)
+{
+    asm("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 "
+        "{%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a0), "d"(a1), "d"(b0));
+}
+
+// Named barrier `id` over `count` threads with an OR over `flag`.
+template <int ID, int COUNT>
+__device__ __forceinline__ bool bar_any(bool flag)
+{
+    uint32_t out;
+    asm volatile("{\n.reg .pred q, p;\nsetp.ne.u32 q, %1, 0;\nbar.red.or.pred p, %2, %3, q;\n"
+                 "selp.u32 %0, 1, 0, p;\n}\n" : "=r"(out) : "r"((uint32_t)flag), "n"(ID), "n"(COUNT) : "memory");
+    return out != 0;
+}
+
+template <int ID, int COUNT>
+__device__ __forceinline__ void bar_sync()
+{
+    asm volatile("bar.sync %0, %1;\n" :: "n"(ID), "n"(COUNT) : "memory");
+}
+
+__device__ __forceinline__ void decode_work(const DmmaArgs& a, int64_t w, int64_t& b, int64_t& tm, int64_t& tn)
+{
+    const int64_t tiles = (int64_t)a.tiles_m * a.tiles_n;
+    b = w / tiles;
+    const int64_t tw = w - b * tiles;
+    const int64_t GROUP = 8;
+    const int64_t group = tw / (GROUP * a.tiles_n);
+    const int64_t first_m = group * GROUP;
+    const int64_t gsize = (a.tiles_m - first_m) < GROUP ? (a.tiles_m - first_m) : GROUP;
+    tm = first_m + (tw % gsize);
+    tn = (tw % (GROUP * a.tiles_n)) / gsize;
+}
+
+// One operand sum of one ring slot: X(r, k) = sum_t sign_t * X[row_t(r) + k_t(k)]
+// over the terms of the product's sum, stored at tile_pos(k, r).  `rows` is
+// the row (column) offset table [FHMAX][FT] of the tile, `ktab` this k-step's
+// k offset table [FHMAX][FBK]; invalid entries read as zero.
+template <bool KFAST>
+__device__ __forceinline__ void produce_tile(const double* __restrict__ X, const int64_t* rows, const int64_t* ktab,
+                                             int nt, const int8_t* t_row, const int8_t* t_k, const int8_t* t_s,
+                                             double* dst, int ptid)
+{
+#pragma unroll 1
+    for (int c0 = 0; c0 < PE; c0 += PCH)
+    {
+        double v[PCH];
+#pragma unroll
+        for (int e = 0; e < PCH; e++) v[e] = 0.0;
+#pragma unroll 1
+        for (int t = 0; t < nt; t++)
+        {
+            const int64_t* rt = rows + t_row[t] * FT;
+            const int64_t* kt = ktab + t_k[t] * FBK;
+            const bool neg = t_s[t] < 0;
+            double x[PCH];
+#pragma unroll
+            for (int e = 0; e < PCH; e++)
+            {
+                int kk, r;
+                lane_map<FBK, FT>(KFAST, ptid + (c0 + e) * PT, kk, r);
+                const int64_t ro = rt[r], ko = kt[kk];
+                x[e] = (ro != OFF_INVALID && ko != OFF_INVALID) ? __ldg(X + (ro + ko)) : 0.0;
+            }
+#pragma unroll
+            for (int e = 0; e < PCH; e++) v[e] += neg ? -x[e] : x[e];
+        }
+#pragma unroll
+        for (int e = 0; e < PCH; e++)
+        {
+            int kk, r;
+            lane_map<FBK, FT>(KFAST, ptid + (c0 + e) * PT, kk, r);
+            dst[tile_pos(kk, r, FT)] = v[e];
+        }
+    }
+}
+
+template <bool KA, bool KB>
+__global__ void __launch_bounds__(FTHREADS, 1)
+stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    double* ring = reinterpret_cast<double*>(smem);
+    int64_t* rowA = reinterpret_cast<int64_t*>(smem + RING_BYTES);
+    int64_t* colB = rowA + FHMAX * FT;
+    int64_t* rowC = colB + FHMAX * FT;
+    int64_t* colC = rowC + FHMAX * FT;
+    int64_t* kA = colC + FHMAX * FT;         // [FHMAX][FBK]
+    int64_t* kB = kA + FHMAX * FBK;
+    FusedCtrl* ctl = reinterpret_cast<FusedCtrl*>(kB + FHMAX * FBK);
+    volatile int* abort_flag = &ctl->abort;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0)
+    {
+        for (int s = 0; s < FSTAGES; s++)
+        {
+            mbar_init(smem_addr(&ctl->full[s]), PT);
+            mbar_init(smem_addr(&ctl->empty[s]), NCW);
+        }
+        ctl->abort = 0;
+        mbar_init_fence();
+    }
+    __syncthreads();
+
+    const int64_t tiles = (int64_t)a.tiles_m * a.tiles_n;
+    const int64_t work = a.batch * tiles;
+    const int64_t nk = (a.ks + FBK - 1) / FBK;
+    const int H = a.H;
+
+    if (warp < NPW)
+    {
+        // ---------------- producer warpgroup ----------------
+        asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" :: "n"(PROD_REGS));
+        const int ptid = tid;
+        uint32_t it = 0;
+        bool ok = true;      // this thread's waits so far
+        bool stop = false;   // set only right after a collective check, so uniform
+        // Every exit is taken right after a collective OR over the producers'
+        // named barrier; a thread whose wait ran out keeps walking the same
+        // loop (producing nothing) until the next one.
+        for (int64_t w = blockIdx.x; w < work && !stop; w += gridDim.x)
+        {
+            if (bar_any<1, PT>(!ok)) break;
+            int64_t b, tm, tn;
+            decode_work(a, w, b, tm, tn);
+            const int64_t offA = a.bA[b], offB = a.bB[b];
+            for (int i = ptid; i < FHMAX * FT; i += PT)
+            {
+                const int h = i / FT, r = i % FT;
+                const int64_t li = tm * FT + r, gi = h * a.ms + li;
+                rowA[i] = (h < H && li < a.ms && gi < a.m) ? offA + a.rsA[gi] : OFF_INVALID;
+                const int64_t lj = tn * FT + r, gj = h * a.ns + lj;
+                colB[i] = (h < H && lj < a.ns && gj < a.n) ? offB + a.csB[gj] : OFF_INVALID;
+            }
+            for (int p = 0; p < a.nprod && !stop; p++)
+            {
+                const DevProduct& P = a.prod[p];
+                for (int64_t s = 0; s < nk; s++)
+                {
+                    // All producers are done with the last k-step's tables (and
+                    // the tile's row tables are complete); a wait that ran out
+                    // in any of them ends the loops for all of them.
+                    if (bar_any<1, PT>(!ok)) { stop = true; break; }
+                    for (int i = ptid; i < 2 * FHMAX * FBK; i += PT)
+                    {
+                        const int op = i / (FHMAX * FBK), e = i % (FHMAX * FBK);
+                        const int h = e / FBK, kk = e % FBK;
+                        const int64_t kl = s * FBK + kk, gk = h * a.ks + kl;
+                        const bool in = h < H && kl < a.ks && gk < a.k;
+                        if (op == 0) kA[e] = in ? a.ksA[gk] : OFF_INVALID;
+                        else         kB[e] = in ? a.ksB[gk] : OFF_INVALID;
+                    }
+                    bar_sync<1, PT>();
+                    const uint32_t slot = it % FSTAGES;
+                    const uint32_t use = it / FSTAGES;   // earlier uses of this slot
+                    it++;
+                    if (!ok || (use > 0 && !mbar_wait(smem_addr(&ctl->empty[slot]), (use & 1) ^ 1, abort_flag, err,
+                                                      1, limit)))
+                    {
+                        ok = false;
+                        continue;
+                    }
+                    double* S = ring + slot * SLOT_DOUBLES;
+                    double* T = S + FBK * FT;
+                    produce_tile<KA>(a.A, rowA, kA, P.na, P.a_r, P.a_c, P.a_s, S, ptid);
+                    produce_tile<KB>(a.B, colB, kB, P.nb, P.b_c, P.b_r, P.b_s, T, ptid);
+                    mbar_arrive(smem_addr(&ctl->full[slot]));   // release: the stores above are visible
+                }
+            }
+        }
+    }
+    else
+    {
+        // ---------------- consumer warpgroups ----------------
+        asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" :: "n"(CONS_REGS));
+        const int ctid = tid - PT;
+        const int cw = warp - NPW;
+        const int g = lane >> 2, t4 = lane & 3;
+        const int wm = (cw / CWN) * WTM;
+        const int wn = (cw % CWN) * WTN;
+        uint32_t cit = 0;
+        bool ok = true;
+        for (int64_t w = blockIdx.x; w < work; w += gridDim.x)
+        {
+            if (bar_any<2, CT>(!ok)) break;
+            int64_t b, tm, tn;
+            decode_work(a, w, b, tm, tn);
+            const int64_t offC = a.bC[b];
+            for (int i = ctid; i < FHMAX * FT; i += CT)
+            {
+                const int h = i / FT, r = i % FT;
+                const int64_t li = tm * FT + r, gi = h * a.ms + li;
+                rowC[i] = (h < H && li < a.ms && gi < a.m) ? offC + a.rsC[gi] : OFF_INVALID;
+                const int64_t lj = tn * FT + r, gj = h * a.ns + lj;
+                colC[i] = (h < H && lj < a.ns && gj < a.n) ? a.csC[gj] : OFF_INVALID;
+            }
+            bar_sync<2, CT>();
+
+            for (int p = 0; p < a.nprod && ok; p++)
+            {
+                double acc[MI][NI][4];
+#pragma unroll
+                for (int mi = 0; mi < MI; mi++)
+#pragma unroll
+                    for (int ni = 0; ni < NI; ni++)
+#pragma unroll
+                        for (int e = 0; e < 4; e++) acc[mi][ni][e] = 0.0;
+
+                for (int64_t s = 0; s < nk; s++)
+                {
+                    const uint32_t slot = cit % FSTAGES;
+                    ok = __all_sync(0xffffffffu, mbar_wait(smem_addr(&ctl->full[slot]), (cit / FSTAGES) & 1,
+                                                           abort_flag, err, 2, limit));
+                    if (!ok) break;
+                    const double* Ab = ring + slot * SLOT_DOUBLES;
+                    const double* Bb = Ab + FBK * FT;
+#pragma unroll 2
+                    for (int k4 = 0; k4 < FBK; k4 += 4)
+                    {
+                        const int kr = k4 + t4;
+                        const int pg = 2 * ((g + swz_c(kr)) & 7);
+                        double af[MI][2], bf[NI];
+#pragma unroll
+                        for (int mi = 0; mi < MI; mi++)
+                        {
+                            const double2 v = *reinterpret_cast<const double2*>(Ab + kr * FT + wm + mi * 16 + pg);
+                            af[mi][0] = v.x; af[mi][1] = v.y;
+                        }
+#pragma unroll
+                        for (int nj = 0; nj < NI / 2; nj++)
+                        {
+                            const double2 v = *reinterpret_cast<const double2*>(Bb + kr * FT + wn + nj * 16 + pg);
+                            bf[2 * nj] = v.x; bf[2 * nj + 1] = v.y;
+                        }
+#pragma unroll
+                        for (int mi = 0; mi < MI; mi++)
+#pragma unroll
+                            for (int ni = 0; ni < NI; ni++)
+                                dmma(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
+                    }
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(smem_addr(&ctl->empty[slot]));
+                    cit++;
+                }
+                if (!ok) break;
+
+                // C_t = (first ? beta*C_t : C_t) + sign_t*alpha*S*T for the
+                // product's C blocks t; loads of a row pair before its stores.
+                const DevProduct& P = a.prod[p];
+                for (int t = 0; t < P.nc; t++)
+                {
+                    const int64_t* rt = rowC + P.c_r[t] * FT;
+                    const int64_t* ct = colC + P.c_c[t] * FT;
+                    const double coef = P.c_s[t] < 0 ? -a.alpha : a.alpha;
+                    const bool first = P.c_first[t] != 0;
+                    const bool read_c = !first || a.beta != 0.0;
+                    const double cb = first ? a.beta : 1.0;
+#pragma unroll
+                    for (int mi = 0; mi < MI; mi++)
+                    {
+                        double cv[2][NI][2];
+#pragma unroll
+                        for (int hr = 0; hr < 2; hr++)
+                        {
+                            const int64_t ro = rt[wm + mi * 16 + g + hr * 8];
+#pragma unroll
+                            for (int ni = 0; ni < NI; ni++)
+#pragma unroll
+                                for (int hc = 0; hc < 2; hc++)
+                                {
+                                    const int64_t co = ct[wn + ni * 8 + t4 * 2 + hc];
+                                    cv[hr][ni][hc] = (read_c && ro != OFF_INVALID && co != OFF_INVALID)
+                                                         ? a.C[ro + co] : 0.0;
+                                }
+                        }
+#pragma unroll
+                        for (int hr = 0; hr < 2; hr++)
+                        {
+                            const int64_t ro = rt[wm + mi * 16 + g + hr * 8];
+                            if (ro == OFF_INVALID) continue;
+#pragma unroll
+                            for (int ni = 0; ni < NI; ni++)
+#pragma unroll
+                                for (int hc = 0; hc < 2; hc++)
+                                {
+                                    const int64_t co = ct[wn + ni * 8 + t4 * 2 + hc];
+                                    if (co == OFF_INVALID) continue;
+                                    a.C[ro + co] = coef * acc[mi][ni][hr * 2 + hc] + cb * cv[hr][ni][hc];
+                                }
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+}  // namespace
+
+size_t fused_smem_bytes() { return FUSED_SMEM; }
+
+cudaError_t launch_fused(const DmmaArgs& in, cudaStream_t stream, int num_sms, int* err, long long wait_limit)
+{
+    if (in.batch <= 0 || in.ms <= 0 || in.ns <= 0) return cudaSuccess;
+    // direct C updates on an H x H grid of up to 4 x 4 blocks only
+    if (in.H < 1 || in.H > FHMAX || in.Hc != in.H || in.mC != in.m || in.nC != in.n) return cudaErrorNotSupported;
+    if (in.nprod < 1 || in.nprod > MAX_PRODUCTS) return cudaErrorInvalidValue;
+    auto kern = in.a_kfast ? (in.b_kfast ? stra_fused_kernel<true, true> : stra_fused_kernel<true, false>)
+                           : (in.b_kfast ? stra_fused_kernel<false, true> : stra_fused_kernel<false, false>);
+    // The register split must fit the pool the CTA is launched with.
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, kern);
+    if (e != cudaSuccess) return e;
+    if ((size_t)fa.numRegs * FTHREADS < (size_t)PROD_REGS * PT + (size_t)CONS_REGS * CT) return cudaErrorNotSupported;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FUSED_SMEM);
+    if (e != cudaSuccess) return e;
+    DmmaArgs args = in;
+    args.tiles_m = (int)((args.ms + FT - 1) / FT);
+    args.tiles_n = (int)((args.ns + FT - 1) / FT);
+    args.work = args.batch * (int64_t)args.tiles_m * args.tiles_n;
+    if (args.work <= 0) return cudaSuccess;
+    int64_t grid = num_sms;
+    if (args.work < grid) grid = args.work;
+    timing_begin(KK_FUSED, stream);
+    kern<<<(unsigned)grid, FTHREADS, FUSED_SMEM, stream>>>(args, err, wait_cycles(wait_limit));
+    timing_end(KK_FUSED, stream);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) g_launches++;
+    return e;
+}
+
+}  // namespace tsb

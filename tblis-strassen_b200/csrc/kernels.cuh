@@ -336,6 +336,12 @@ cudaError_t launch_dmma(const DmmaArgs& args, int terms, cudaStream_t stream, in
 // Tile shape (rows x columns per CTA) of the fused-kernel configuration that
 // launch_dmma / launch_dmma_grouped pick for these parameters.
 void dmma_tile_shape(int terms, int H, int Hc, int config, int* bm, int* bn);
+// Fully fused ABC kernel with a producer warpgroup forming the operand sums
+// once per staged tile (fused_kernel.cu): C updated directly (Hc == H,
+// mC == m, nC == n), H <= 4.  cudaErrorNotSupported when it cannot run
+// these arguments (the caller then uses launch_dmma).  `err` (may be null)
+// is set when a bounded wait runs out; wait_limit as PackedGemmArgs.
+cudaError_t launch_fused(const DmmaArgs& args, cudaStream_t stream, int num_sms, int* err, long long wait_limit);
 cudaError_t launch_dmma_grouped(const DmmaGroupArgs& g, int terms, int H, int Hc, int config,
                                 cudaStream_t stream, int num_sms);
 cudaError_t launch_scale(const ScaleArgs& args, cudaStream_t stream);
@@ -344,6 +350,11 @@ cudaError_t launch_sum_gather(const SumGatherArgs& args, cudaStream_t stream);
 cudaError_t launch_scatter_add(const ScatterAddArgs& args, cudaStream_t stream);
 cudaError_t launch_combine(const CombineArgs& args, cudaStream_t stream);
 cudaError_t launch_combine(const CombineF32Args& args, cudaStream_t stream);
+
+// The FP64 tensor-pipe ceiling of this GPU: DMMA throughput of register-only
+// m16n8k4 loops over every SM (2 CTAs of 16 warps each), `iters` rounds of 8
+// MMAs per warp, timed with CUDA events on `stream` after one warm-up launch.
+cudaError_t measure_dmma_peak(int iters, int num_sms, cudaStream_t stream, double* tflops, double* ms);
 
 // Number of kernels this library has launched (all launchers count).
 unsigned long long launches();

@@ -215,7 +215,11 @@ int noalloc_mult(int level, const tblis_tensor* A, const label_type* idx_A,
         }
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        if (launch_dmma(a, terms, st, sms) != cudaSuccess) return TBLIS_STRA_ERR_CUDA;
+        // No error flag (it would need memory): a bounded wait that runs out
+        // still ends the kernel cleanly.
+        cudaError_t e = launch_fused(a, st, sms, nullptr, 0);
+        if (e == cudaErrorNotSupported) e = launch_dmma(a, terms, st, sms);
+        if (e != cudaSuccess) { cudaGetLastError(); return TBLIS_STRA_ERR_CUDA; }
     }
     double one = 1.0;
     std::memcpy(C->scalar, &one, sizeof one);

@@ -21,4 +21,24 @@ __host__ __device__ __forceinline__ int tile_pos(int k, int m, int ld)
     return k * ld + (m & ~15) + 2 * (((m & 7) + swz_c(k)) & 7) + ((m >> 3) & 1);
 }
 
+// Loader lane maps: element e (= thread + x * threads) of a BK x BM tile.
+// k-fast: half-warps take 8 consecutive k of rows (m, m+8); row-fast: 16
+// consecutive rows of one k.  Both write 16 distinct 8-byte slots of one
+// 128-byte line per half-warp in the tile_pos layout.
+template <int BK, int BM>
+__device__ __forceinline__ void lane_map(bool kfast, int e, int& kk, int& m)
+{
+    if (kfast)
+    {
+        kk = (e & 7) + 8 * ((e >> 4) % (BK / 8));
+        const int ridx = 2 * (e / (16 * (BK / 8))) + ((e >> 3) & 1);
+        m = (ridx & ~15) | ((ridx & 1) << 3) | ((ridx >> 1) & 7);
+    }
+    else
+    {
+        m = e % BM;
+        kk = e / BM;
+    }
+}
+
 }  // namespace tsb

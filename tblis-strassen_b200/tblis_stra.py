@@ -153,6 +153,11 @@ def _load() -> ctypes.CDLL:
     lib.tblis_stra_set_alloc_limit.argtypes = [ctypes.c_size_t]
     lib.tblis_stra_set_alloc_limit.restype = ctypes.c_int
     lib.tblis_stra_get_alloc_limit.restype = ctypes.c_size_t
+    lib.tblis_stra_measure_dmma_peak.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                                 ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
+    lib.tblis_stra_measure_dmma_peak.restype = ctypes.c_int
+    lib.tblis_stra_mult_noalloc.argtypes = [ctypes.c_int, T, S, T, S, T, S, ctypes.c_void_p]
+    lib.tblis_stra_mult_noalloc.restype = ctypes.c_int
     lib.tblis_get_num_threads.restype = ctypes.c_uint
     lib.tblis_set_num_threads.argtypes = [ctypes.c_uint]
     return lib
@@ -263,6 +268,20 @@ def contract(level: int, alpha, A, idx_A: str, B, idx_B: str, beta, C, idx_C: st
     finally:
         if old_impl is not None:
             lib.tblis_stra_set_impl(old_impl)
+
+
+def noalloc_mult(level: int, alpha, A, idx_A: str, B, idx_B: str, beta, C, idx_C: str, stream=None) -> None:
+    """C = alpha*A*B + beta*C through tblis_stra_mult_noalloc: the ABC
+    variant on device tensors of the current GPU (FP64), allocating no device
+    memory (the scatter vectors go into the library's static device array);
+    asynchronous on `stream`."""
+    va = _View(A, alpha)
+    vb = _View(B, 1.0, va.code)
+    vc = _View(C, beta, va.code)
+    ia, ib, ic = _labels(idx_A, va.t.ndim), _labels(idx_B, vb.t.ndim), _labels(idx_C, vc.t.ndim)
+    handle = None if stream is None else getattr(stream, "cuda_stream", stream)
+    _check(lib.tblis_stra_mult_noalloc(level, ctypes.byref(va.t), ia, ctypes.byref(vb.t), ib,
+                                       ctypes.byref(vc.t), ic, handle))
 
 
 def mult(alpha, A, idx_A, B, idx_B, beta, C, idx_C, **kw) -> None:
@@ -428,6 +447,15 @@ def kernel_timing(kind: str):
     ms = ctypes.c_double()
     _check(lib.tblis_stra_kernel_timing(KERNEL_KINDS[kind], ctypes.byref(n), ctypes.byref(ms)))
     return int(n.value), float(ms.value)
+
+
+def measure_dmma_peak(iterations: int = 20000, stream=None):
+    """(TFLOP/s, ms): the FP64 tensor-pipe ceiling of the current GPU from
+    register-only DMMA loops (the roofline denominator of the FP64 kernels)."""
+    tf, ms = ctypes.c_double(), ctypes.c_double()
+    handle = None if stream is None else getattr(stream, "cuda_stream", stream)
+    _check(lib.tblis_stra_measure_dmma_peak(iterations, ctypes.byref(tf), ctypes.byref(ms), handle))
+    return tf.value, ms.value
 
 
 def launch_count() -> int:
