@@ -206,6 +206,39 @@ size_t tblis_stra_get_workspace_limit(void);
 int tblis_stra_set_product_parallel(int mode);
 int tblis_stra_get_product_parallel(void);
 
+/* Fast matrix-multiplication algorithm of the Strassen levels, per calling
+ * thread (default 0).  The reference generates its product code from U/V/W
+ * coefficient files for any <m,k,n> shape (src/stra_internal/3t/strassen:1-14,
+ * src/stra_internal/3m/my_stra_gen.py, my_stra_gen.sh names a <3,2,3> family);
+ * here the same coefficients drive the kernels at run time.  Built-in ids:
+ *   0  Strassen <2,2,2> with 7 products (levels 1 and 2);
+ *   1  the classical <2,2,2> with 8 products;
+ *   2  <3,2,2>, 3  <2,3,2>, 4  <2,2,3>: Strassen on the leading 2 x 2 x 2
+ *      blocks plus the 4 classical products of the third block row, summed
+ *      slice or column (11 products for 12 classical).
+ * Level L applies the algorithm's L-th Kronecker power: an mb^L x kb^L block
+ * grid of A, kb^L x nb^L of B, mb^L x nb^L of C, rank^L products (the kernels
+ * take grids up to 4 x 4 and up to 49 products; tblis_stra_algorithm_info
+ * reports the levels an algorithm runs at).  Other algorithms than 0 run
+ * FP64 contractions with the ABC variant; AB, Naive and FP32 calls return
+ * TBLIS_STRA_ERR_UNSUPPORTED, and batches always use Strassen.  Returns 0 or
+ * TBLIS_STRA_ERR_ARG (unknown id). */
+int tblis_stra_set_algorithm(int id);
+int tblis_stra_get_algorithm(void);
+/* Shape <mb, kb, nb>, rank and the highest level (0 .. 2) the kernels run
+ * algorithm `id` at. */
+int tblis_stra_algorithm_info(int id, int* mb, int* kb, int* nb, int* rank, int* levels);
+/* Adds an algorithm given by its coefficient matrices, row-major with one row
+ * per block id (row * grid columns + column) and one column per product:
+ * U is (mb*kb) x rank, V (kb*nb) x rank, W (mb*nb) x rank, entries in
+ * {-1, 0, 1} -- the layout of the reference's coefficient files.  The
+ * coefficients are checked to multiply matrices exactly (else
+ * TBLIS_STRA_ERR_ARG); TBLIS_STRA_ERR_UNSUPPORTED when the kernels cannot run
+ * even one level of it (a sum or C update of more than 4 blocks).  On
+ * success *id is the new algorithm's id (process-wide, at most 64). */
+int tblis_stra_register_algorithm(int mb, int kb, int nb, int rank, const int* U, const int* V, const int* W,
+                                  int* id);
+
 /* FP32 (TYPE_FLOAT) contractions run on the BF16 tensor cores with each
  * operand split into bf16 planes (no counterpart in the reference, whose FP32
  * path is its CPU micro-kernel): terms = 6 splits into hi+mid+lo and keeps the

@@ -173,6 +173,102 @@ def strassen_matmul(A: np.ndarray, B: np.ndarray, level: int) -> np.ndarray:
     return C
 
 
+# ---- other fast matrix-multiplication families -----------------------------
+
+def fmm_matmul(A: np.ndarray, B: np.ndarray, dims, U, V, W, level: int = 1) -> np.ndarray:
+    """A @ B by the <mb, kb, nb> algorithm with coefficient matrices U (mb*kb x
+    R), V (kb*nb x R), W (mb*nb x R) -- block id = row * cols + col, the layout
+    of the reference's coefficient files (src/stra_internal/3t/strassen:1-14)
+    -- applied recursively `level` times (outer level most significant).
+    Ragged sizes are zero-padded to multiples of the grid."""
+    mb, kb, nb = dims
+    U, V, W = (np.asarray(X) for X in (U, V, W))
+    if level == 0:
+        return A @ B
+    m, k = A.shape
+    n = B.shape[1]
+    ms, ks, ns = -(-m // mb), -(-k // kb), -(-n // nb)
+    Ap = np.zeros((ms * mb, ks * kb)); Ap[:m, :k] = A
+    Bp = np.zeros((ks * kb, ns * nb)); Bp[:k, :n] = B
+    C = np.zeros((ms * mb, ns * nb))
+    blk = lambda X, r, c, a, b: X[r * a:(r + 1) * a, c * b:(c + 1) * b]
+    for p in range(U.shape[1]):
+        S = sum(U[i, p] * blk(Ap, i // kb, i % kb, ms, ks) for i in range(mb * kb) if U[i, p])
+        T = sum(V[j, p] * blk(Bp, j // nb, j % nb, ks, ns) for j in range(kb * nb) if V[j, p])
+        if isinstance(S, int) or isinstance(T, int):
+            continue
+        M = fmm_matmul(S, T, dims, U, V, W, level - 1)
+        for q in range(mb * nb):
+            if W[q, p]:
+                r, c = divmod(q, nb)
+                C[r * ms:(r + 1) * ms, c * ns:(c + 1) * ns] += W[q, p] * M
+    return C[:m, :n]
+
+
+def parse_coefficients(text: str):
+    """U, V, W from the reference's coefficient-file format: three blocks of
+    whitespace-separated integer rows (one row per block id, one column per
+    product) separated by lines starting with '#'."""
+    blocks, cur = [], []
+    for line in text.splitlines():
+        if line.strip().startswith("#"):
+            if cur:
+                blocks.append(cur)
+            cur = []
+            continue
+        if line.strip():
+            cur.append([int(x) for x in line.split()])
+    if cur:
+        blocks.append(cur)
+    if len(blocks) != 3:
+        raise ValueError(f"expected U, V and W blocks, found {len(blocks)}")
+    return tuple(np.array(b, dtype=np.int64) for b in blocks)
+
+
+def classical_coeffs(mb: int, kb: int, nb: int):
+    """U, V, W of the classical <mb, kb, nb> product: one product per (row,
+    summed slice, column)."""
+    R = mb * kb * nb
+    U = np.zeros((mb * kb, R), dtype=np.int64); V = np.zeros((kb * nb, R), dtype=np.int64)
+    W = np.zeros((mb * nb, R), dtype=np.int64)
+    r = 0
+    for i in range(mb):
+        for t in range(kb):
+            for j in range(nb):
+                U[i * kb + t, r] = V[t * nb + j, r] = W[i * nb + j, r] = 1
+                r += 1
+    return U, V, W
+
+
+def strassen_plus_classical(axis: int):
+    """<3,2,2> (axis 0), <2,3,2> (axis 1) or <2,2,3> (axis 2) with 11
+    products: Strassen on the leading 2 x 2 x 2 blocks and the 4 classical
+    products of the extra block row, summed slice or column."""
+    mb, kb, nb = (3 if axis == 0 else 2), (3 if axis == 1 else 2), (3 if axis == 2 else 2)
+    U = np.zeros((mb * kb, 11), dtype=np.int64); V = np.zeros((kb * nb, 11), dtype=np.int64)
+    W = np.zeros((mb * nb, 11), dtype=np.int64)
+    for r in range(7):
+        for i in range(4):
+            br, bc = divmod(i, 2)
+            U[br * kb + bc, r] = globals()["U"][i, r]
+            V[br * nb + bc, r] = globals()["V"][i, r]
+            W[br * nb + bc, r] = globals()["W"][i, r]
+    r = 7
+    for x in range(2):
+        for y in range(2):
+            if axis == 0:
+                a, b, c = (2, x), (x, y), (2, y)
+            elif axis == 1:
+                a, b, c = (x, 2), (2, y), (x, y)
+            else:
+                a, b, c = (x, y), (y, 2), (x, 2)
+            U[a[0] * kb + a[1], r] = 1
+            V[b[0] * nb + b[1], r] = 1
+            W[c[0] * nb + c[1], r] = 1
+            r += 1
+    return U, V, W
+
+
 def uniform(shape, seed: int, order: str = "F", dtype=np.float64) -> np.ndarray:
     """Seeded i.i.d. U[-1, 1] entries (numpy MT19937), column-major by default."""
     rng = np.random.Generator(np.random.MT19937(seed))

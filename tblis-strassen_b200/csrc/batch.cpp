@@ -1009,7 +1009,11 @@ int tblis_stra_batch_create(int count, const tblis_stra_problem* problems, tblis
 {
     if (!batch) return TBLIS_STRA_ERR_NULL;
     tsb::BatchPlan* p = nullptr;
+    // batches plan with Strassen whatever algorithm the thread has selected
+    const int alg = tsb::thread_algorithm();
+    tsb::set_thread_algorithm(0);
     const int s = tsb::batch_create(count, problems, &p);
+    tsb::set_thread_algorithm(alg);
     *batch = reinterpret_cast<tblis_stra_batch>(p);
     return s;
 }

@@ -453,7 +453,7 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
     }
     const ProductTable& tab = product_table(level);
     const int H = tab.H;
-    const int64_t ms = cdiv(g.m, H), ns = cdiv(g.n, H), ks = cdiv(g.k, H);
+    const int64_t ms = cdiv(g.m, H), ns = cdiv(g.n, tab.Hn), ks = cdiv(g.k, tab.Hk);
     const int sms = num_sms(device);
 
     if (level == 0 || impl == 1)
@@ -468,6 +468,7 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
         set_grid(a, ms, ns, ks);
         a.nprod = (int)tab.prod.size();
         a.H = a.Hc = H;
+        a.Hk = tab.Hk; a.Hn = tab.Hn;
         for (int p = 0; p < a.nprod; p++) a.prod[p] = to_dev(tab.prod[p]);
         // The producer/consumer fused kernel; the earlier all-warps kernel
         // where it cannot run these arguments.
@@ -481,7 +482,11 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
             err = static_cast<int*>(ferr.p);
         }
         cudaError_t e = launch_fused(a, st, sms, err, wait_limit_cycles());
-        if (e == cudaErrorNotSupported) e = launch_dmma(a, max_terms(tab), st, sms);
+        if (e == cudaErrorNotSupported)
+        {
+            if (tab.Hk != H || tab.Hn != H) return TBLIS_STRA_ERR_UNSUPPORTED;   // square grids only there
+            e = launch_dmma(a, max_terms(tab), st, sms);
+        }
         TSB_CUDA(e);
         if (blocking && !shared_err)
         {
@@ -687,9 +692,9 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
 
 PackGeom pack_geom(int level, const GemmView& g)
 {
-    const int H = product_table(level).H;
+    const ProductTable& tab = product_table(level);
     PackGeom p;
-    p.ms = cdiv(g.m, H); p.ns = cdiv(g.n, H); p.ks = cdiv(g.k, H);
+    p.ms = cdiv(g.m, tab.H); p.ns = cdiv(g.n, tab.Hn); p.ks = cdiv(g.k, tab.Hk);
     p.k_pad = cdiv(p.ks, PACK_KSTEP) * PACK_KSTEP;
     p.tm = cdiv(p.ms, PACK_TILE); p.tn = cdiv(p.ns, PACK_TILE);
     p.s_elems = (size_t)(g.batch * p.tm * p.k_pad * PACK_TILE);
@@ -795,6 +800,7 @@ PackedGemmArgs packed_gemm_base(int level, const GemmView& g, const PackGeom& pg
     ga.tiles_m = pg.tm; ga.tiles_n = pg.tn; ga.batch = g.batch;
     ga.alpha = g.alpha; ga.beta = g.beta;
     ga.H = product_table(level).H;
+    ga.Hn = product_table(level).Hn;
     ga.nprod = 0;
     return ga;
 }
@@ -1332,7 +1338,7 @@ size_t fp32_parallel_workspace_bytes(int level, const GemmView& g, int terms)
 
 bool use_product_parallel(int level, const GemmView& g, int sms, bool fp32, int terms)
 {
-    if (level < 1 || t_product_parallel == 0) return false;
+    if (level < 1 || t_product_parallel == 0 || thread_algorithm() != 0) return false;
     const int H = product_table(level).H;
     const int64_t ms = cdiv(g.m, H), ns = cdiv(g.n, H);
     if (ms * ns >= ((int64_t)1 << 31)) return false;
@@ -1925,6 +1931,11 @@ int mult(int level, const tblis_tensor* A, const label_type* idx_A,
     int s = get_plan(T, I, device, g, dp);
     if (s) return s;
     const bool fp32 = g.type == TYPE_FLOAT;
+    // Fast-multiplication algorithms other than Strassen run the FP64 ABC
+    // variant (packed product by product, or the fused kernel).
+    if (level >= 1 && thread_algorithm() != 0 &&
+        (fp32 || impl != 1 || !fmm_table(thread_algorithm(), level)))
+        return TBLIS_STRA_ERR_UNSUPPORTED;
     const size_t es = fp32 ? sizeof(float) : sizeof(double);
 
     // Every element access is an aligned load or store of the element size.
@@ -2161,6 +2172,44 @@ int tblis_stra_measure_dmma_peak(int iterations, double* tflops, double* ms, voi
                                                  tflops, ms);
     if (e == cudaErrorInvalidValue) return TBLIS_STRA_ERR_ARG;
     if (e != cudaSuccess) { tsb::note_cuda_error("measure_dmma_peak", e, __FILE__, __LINE__); return TBLIS_STRA_ERR_CUDA; }
+    return TBLIS_STRA_SUCCESS;
+}
+
+int tblis_stra_set_algorithm(int id)
+{
+    if (!tsb::algorithm_by_id(id) || !tsb::fmm_table(id, 1)) return TBLIS_STRA_ERR_ARG;
+    tsb::set_thread_algorithm(id);
+    return TBLIS_STRA_SUCCESS;
+}
+int tblis_stra_get_algorithm(void) { return tsb::thread_algorithm(); }
+
+int tblis_stra_algorithm_info(int id, int* mb, int* kb, int* nb, int* rank, int* levels)
+{
+    const tsb::FmmAlgorithm* a = tsb::algorithm_by_id(id);
+    if (!a) return TBLIS_STRA_ERR_ARG;
+    if (mb) *mb = a->mb;
+    if (kb) *kb = a->kb;
+    if (nb) *nb = a->nb;
+    if (rank) *rank = a->rank;
+    if (levels) *levels = tsb::fmm_table(id, 2) ? 2 : tsb::fmm_table(id, 1) ? 1 : 0;
+    return TBLIS_STRA_SUCCESS;
+}
+
+int tblis_stra_register_algorithm(int mb, int kb, int nb, int rank, const int* U, const int* V, const int* W,
+                                  int* id)
+{
+    if (!U || !V || !W || !id) return TBLIS_STRA_ERR_NULL;
+    if (mb < 1 || kb < 1 || nb < 1 || rank < 1 || mb > 4 || kb > 4 || nb > 4 || rank > 49)
+        return TBLIS_STRA_ERR_ARG;
+    tsb::FmmAlgorithm a;
+    a.name = "registered";
+    a.mb = mb; a.kb = kb; a.nb = nb; a.rank = rank;
+    a.U.assign(U, U + mb * kb * rank);
+    a.V.assign(V, V + kb * nb * rank);
+    a.W.assign(W, W + mb * nb * rank);
+    const int r = tsb::register_algorithm(a);
+    if (r < 0) return -r;
+    *id = r;
     return TBLIS_STRA_SUCCESS;
 }
 

@@ -188,7 +188,9 @@ stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
     const int64_t tiles = (int64_t)a.tiles_m * a.tiles_n;
     const int64_t work = a.batch * tiles;
     const int64_t nk = (a.ks + FBK - 1) / FBK;
-    const int H = a.H;
+    const int H = a.H;                           // block rows of A and C
+    const int Hk = a.Hk > 0 ? a.Hk : a.H;        // block columns of A, rows of B
+    const int Hn = a.Hn > 0 ? a.Hn : a.H;        // block columns of B and C
 
     if (warp < NPW)
     {
@@ -213,7 +215,7 @@ stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
                 const int64_t li = tm * FT + r, gi = h * a.ms + li;
                 rowA[i] = (h < H && li < a.ms && gi < a.m) ? offA + a.rsA[gi] : OFF_INVALID;
                 const int64_t lj = tn * FT + r, gj = h * a.ns + lj;
-                colB[i] = (h < H && lj < a.ns && gj < a.n) ? offB + a.csB[gj] : OFF_INVALID;
+                colB[i] = (h < Hn && lj < a.ns && gj < a.n) ? offB + a.csB[gj] : OFF_INVALID;
             }
             for (int p = 0; p < a.nprod && !stop; p++)
             {
@@ -229,7 +231,7 @@ stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
                         const int op = i / (FHMAX * FBK), e = i % (FHMAX * FBK);
                         const int h = e / FBK, kk = e % FBK;
                         const int64_t kl = s * FBK + kk, gk = h * a.ks + kl;
-                        const bool in = h < H && kl < a.ks && gk < a.k;
+                        const bool in = h < Hk && kl < a.ks && gk < a.k;
                         if (op == 0) kA[e] = in ? a.ksA[gk] : OFF_INVALID;
                         else         kB[e] = in ? a.ksB[gk] : OFF_INVALID;
                     }
@@ -275,7 +277,7 @@ stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
                 const int64_t li = tm * FT + r, gi = h * a.ms + li;
                 rowC[i] = (h < H && li < a.ms && gi < a.m) ? offC + a.rsC[gi] : OFF_INVALID;
                 const int64_t lj = tn * FT + r, gj = h * a.ns + lj;
-                colC[i] = (h < H && lj < a.ns && gj < a.n) ? a.csC[gj] : OFF_INVALID;
+                colC[i] = (h < Hn && lj < a.ns && gj < a.n) ? a.csC[gj] : OFF_INVALID;
             }
             bar_sync<2, CT>();
 
@@ -387,6 +389,7 @@ cudaError_t launch_fused(const DmmaArgs& in, cudaStream_t stream, int num_sms, i
     if (in.batch <= 0 || in.ms <= 0 || in.ns <= 0) return cudaSuccess;
     // direct C updates on an H x H grid of up to 4 x 4 blocks only
     if (in.H < 1 || in.H > FHMAX || in.Hc != in.H || in.mC != in.m || in.nC != in.n) return cudaErrorNotSupported;
+    if (in.Hk < 0 || in.Hk > FHMAX || in.Hn < 0 || in.Hn > FHMAX) return cudaErrorNotSupported;
     if (in.nprod < 1 || in.nprod > MAX_PRODUCTS) return cudaErrorInvalidValue;
     auto kern = in.a_kfast ? (in.b_kfast ? stra_fused_kernel<true, true> : stra_fused_kernel<true, false>)
                            : (in.b_kfast ? stra_fused_kernel<false, true> : stra_fused_kernel<false, false>);

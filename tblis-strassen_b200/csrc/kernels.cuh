@@ -47,6 +47,9 @@ struct DmmaArgs
     double alpha, beta;
     int a_kfast, b_kfast;   // loader thread mapping: 1 = consecutive threads walk k
     int nprod, H, Hc;       // products; grid parts on the A/B side and the C side
+    // Rectangular grids of other fast-multiplication algorithms (fused kernel
+    // only): A is H x Hk blocks, B Hk x Hn, C H x Hn; 0 means H.
+    int Hk, Hn;
     DevProduct prod[MAX_PRODUCTS];
 };
 
@@ -177,7 +180,8 @@ struct PackedGemmArgs
     int64_t tiles_m, tiles_n, batch;
     double alpha, beta;
     int nprod;                                 // products per tile position (1..7)
-    int H;                                     // side of the C block grid (1, 2 or 4)
+    int H;                                     // block rows of the C grid (1 .. 4)
+    int Hn;                                    // block columns of the C grid (0: H)
     int8_t nc[MAX_GROUP_PRODUCTS];             // C blocks per product (1..4)
     int8_t c_r[MAX_GROUP_PRODUCTS][4], c_c[MAX_GROUP_PRODUCTS][4];
     int8_t c_s[MAX_GROUP_PRODUCTS][4], c_first[MAX_GROUP_PRODUCTS][4];

@@ -179,6 +179,8 @@ int noalloc_mult(int level, const tblis_tensor* A, const label_type* idx_A,
     }
     else
     {
+        if (level >= 1 && thread_algorithm() != 0 && !fmm_table(thread_algorithm(), level))
+            return TBLIS_STRA_ERR_UNSUPPORTED;
         const ProductTable& tab = product_table(level);
         const int H = tab.H;
         DmmaArgs a;
@@ -189,7 +191,7 @@ int noalloc_mult(int level, const tblis_tensor* A, const label_type* idx_A,
         a.rsA = rsA; a.ksA = ksA; a.ksB = ksB; a.csB = csB; a.rsC = rsC; a.csC = csC;
         a.bA = bA; a.bB = bB; a.bC = bC;
         a.m = g.m; a.n = g.n; a.k = g.k; a.mC = g.m; a.nC = g.n; a.batch = g.batch;
-        a.ms = (g.m + H - 1) / H; a.ns = (g.n + H - 1) / H; a.ks = (g.k + H - 1) / H;
+        a.ms = (g.m + H - 1) / H; a.ns = (g.n + tab.Hn - 1) / tab.Hn; a.ks = (g.k + tab.Hk - 1) / tab.Hk;
         a.tiles_m = (int)((a.ms + 127) / 128);
         a.tiles_n = (int)((a.ns + 127) / 128);
         a.work = a.batch * (int64_t)a.tiles_m * a.tiles_n;
@@ -198,6 +200,7 @@ int noalloc_mult(int level, const tblis_tensor* A, const label_type* idx_A,
         a.b_kfast = (g.unit_ksB != 0 && (g.unit_csB == 0 || g.unit_ksB < g.unit_csB)) ? 1 : 0;
         a.nprod = (int)tab.prod.size();
         a.H = a.Hc = H;
+        a.Hk = tab.Hk; a.Hn = tab.Hn;
         int terms = 1;
         for (int p = 0; p < a.nprod; p++)
         {
@@ -218,7 +221,11 @@ int noalloc_mult(int level, const tblis_tensor* A, const label_type* idx_A,
         // No error flag (it would need memory): a bounded wait that runs out
         // still ends the kernel cleanly.
         cudaError_t e = launch_fused(a, st, sms, nullptr, 0);
-        if (e == cudaErrorNotSupported) e = launch_dmma(a, terms, st, sms);
+        if (e == cudaErrorNotSupported)
+        {
+            if (tab.Hk != H || tab.Hn != H) return TBLIS_STRA_ERR_UNSUPPORTED;
+            e = launch_dmma(a, terms, st, sms);
+        }
         if (e != cudaSuccess) { cudaGetLastError(); return TBLIS_STRA_ERR_CUDA; }
     }
     double one = 1.0;

@@ -426,7 +426,7 @@ __device__ __forceinline__ void packed_ws_body(const Src& src, int* err, long lo
         const int64_t nk = a.k_pad / BK;
         // Offset tables of the tile's rows (columns) in every block row (column)
         // h < H of the C block grid, shared by all products of the work item.
-        const int H = a.H;
+        const int H = a.H, Hn = a.Hn > 0 ? a.Hn : a.H;
         for (int i = tid; i < 4 * BM; i += NT)
         {
             const int h = i / BM, r = i % BM;
@@ -437,7 +437,7 @@ __device__ __forceinline__ void packed_ws_body(const Src& src, int* err, long lo
         {
             const int h = i / BN, c = i % BN;
             const int64_t loc = tn * BN + c, gj = h * a.ns + loc;
-            colC[i] = (h < H && loc < a.ns && gj < a.n) ? a.csC[gj] : OFF_INVALID;
+            colC[i] = (h < Hn && loc < a.ns && gj < a.n) ? a.csC[gj] : OFF_INVALID;
         }
         __syncthreads();
 
@@ -630,7 +630,8 @@ cudaError_t launch_pack_multi(const PackMultiArgs& a, cudaStream_t stream)
 cudaError_t launch_packed_gemm(const PackedGemmArgs& a, cudaStream_t stream, int num_sms)
 {
     if (a.batch <= 0 || a.tiles_m <= 0 || a.tiles_n <= 0) return cudaSuccess;
-    if (a.nprod < 1 || a.nprod > MAX_GROUP_PRODUCTS || a.H < 1 || a.H > 4) return cudaErrorInvalidValue;
+    if (a.nprod < 1 || a.nprod > MAX_GROUP_PRODUCTS || a.H < 1 || a.H > 4 || a.Hn < 0 || a.Hn > 4)
+        return cudaErrorInvalidValue;
     for (int p = 0; p < a.nprod; p++)
         if (a.nc[p] < 1 || a.nc[p] > 4) return cudaErrorInvalidValue;
     const cudaError_t err = launch_packed_ws_cfg<PG0>(a, stream, num_sms);

@@ -5,7 +5,10 @@
 #include <cstring>
 #include <limits>
 #include <map>
+#include <memory>
+#include <mutex>
 #include <numeric>
+#include <string>
 #include <tuple>
 #include <vector>
 
@@ -397,11 +400,117 @@ const int W[4][7] = {{1, 0, 0, 1, -1, 0, 1},
                      {0, 1, 0, 1, 0, 0, 0},
                      {1, -1, 1, 0, 0, 1, 0}};
 
-ProductTable make_table(int level)
+FmmAlgorithm strassen_algorithm()
 {
-    ProductTable t;
+    FmmAlgorithm a;
+    a.name = "strassen";
+    a.mb = a.kb = a.nb = 2;
+    a.rank = 7;
+    for (int i = 0; i < 4; i++)
+        for (int r = 0; r < 7; r++)
+        {
+            a.U.push_back(U[i][r]);
+            a.V.push_back(V[i][r]);
+            a.W.push_back(W[i][r]);
+        }
+    return a;
+}
+
+// The classical product of an mb x kb by kb x nb block grid: one product per
+// (row, summed slice, column), each adding into one C block.
+FmmAlgorithm classical_algorithm(int mb, int kb, int nb)
+{
+    FmmAlgorithm a;
+    a.name = "classical" + std::to_string(mb) + std::to_string(kb) + std::to_string(nb);
+    a.mb = mb; a.kb = kb; a.nb = nb;
+    a.rank = mb * kb * nb;
+    a.U.assign((size_t)(mb * kb * a.rank), 0);
+    a.V.assign((size_t)(kb * nb * a.rank), 0);
+    a.W.assign((size_t)(mb * nb * a.rank), 0);
+    int r = 0;
+    for (int i = 0; i < mb; i++)
+        for (int t = 0; t < kb; t++)
+            for (int j = 0; j < nb; j++, r++)
+            {
+                a.U[(size_t)((i * kb + t) * a.rank + r)] = 1;
+                a.V[(size_t)((t * nb + j) * a.rank + r)] = 1;
+                a.W[(size_t)((i * nb + j) * a.rank + r)] = 1;
+            }
+    return a;
+}
+
+// Strassen on the leading 2 x 2 x 2 blocks of a grid grown by one block along
+// `axis` (0 rows of A and C, 1 the summed dimension, 2 columns of B and C),
+// plus the classical products that the extra block needs: <3,2,2>, <2,3,2>
+// and <2,2,3> with 7 + 4 = 11 products (against 12 classical).
+FmmAlgorithm strassen_plus_classical(int axis)
+{
+    const FmmAlgorithm s = strassen_algorithm();
+    FmmAlgorithm a;
+    a.mb = axis == 0 ? 3 : 2; a.kb = axis == 1 ? 3 : 2; a.nb = axis == 2 ? 3 : 2;
+    a.name = "strassen" + std::to_string(a.mb) + std::to_string(a.kb) + std::to_string(a.nb);
+    a.rank = 11;
+    a.U.assign((size_t)(a.mb * a.kb * 11), 0);
+    a.V.assign((size_t)(a.kb * a.nb * 11), 0);
+    a.W.assign((size_t)(a.mb * a.nb * 11), 0);
+    for (int r = 0; r < 7; r++)
+        for (int i = 0; i < 4; i++)
+        {
+            const int br = i / 2, bc = i % 2;
+            a.U[(size_t)((br * a.kb + bc) * 11 + r)] = s.U[(size_t)(i * 7 + r)];
+            a.V[(size_t)((br * a.nb + bc) * 11 + r)] = s.V[(size_t)(i * 7 + r)];
+            a.W[(size_t)((br * a.nb + bc) * 11 + r)] = s.W[(size_t)(i * 7 + r)];
+        }
+    // the 4 classical products of the extra block row / slice / column
+    int r = 7;
+    for (int x = 0; x < 2; x++)
+        for (int y = 0; y < 2; y++, r++)
+        {
+            int ai, aj, bi, bj, ci, cj;
+            if (axis == 0)      { ai = 2; aj = x; bi = x; bj = y; ci = 2; cj = y; }   // C(2,y) += A(2,x) B(x,y)
+            else if (axis == 1) { ai = x; aj = 2; bi = 2; bj = y; ci = x; cj = y; }   // C(x,y) += A(x,2) B(2,y)
+            else                { ai = x; aj = y; bi = y; bj = 2; ci = x; cj = 2; }   // C(x,2) += A(x,y) B(y,2)
+            a.U[(size_t)((ai * a.kb + aj) * 11 + r)] = 1;
+            a.V[(size_t)((bi * a.nb + bj) * 11 + r)] = 1;
+            a.W[(size_t)((ci * a.nb + cj) * 11 + r)] = 1;
+        }
+    return a;
+}
+
+// Exactness of an algorithm: sum_r U[A(i,t)][r] V[B(t',j)][r] W[C(i',j')][r]
+// is 1 when t = t', i = i', j = j' and 0 otherwise (the matrix product).
+bool algorithm_exact(const FmmAlgorithm& a)
+{
+    const int R = a.rank;
+    if (a.mb < 1 || a.kb < 1 || a.nb < 1 || R < 1) return false;
+    if (a.U.size() != (size_t)(a.mb * a.kb * R) || a.V.size() != (size_t)(a.kb * a.nb * R) ||
+        a.W.size() != (size_t)(a.mb * a.nb * R))
+        return false;
+    for (int ia = 0; ia < a.mb * a.kb; ia++)
+        for (int ib = 0; ib < a.kb * a.nb; ib++)
+            for (int ic = 0; ic < a.mb * a.nb; ic++)
+            {
+                long long sum = 0;
+                for (int r = 0; r < R; r++)
+                    sum += (long long)a.U[(size_t)(ia * R + r)] * a.V[(size_t)(ib * R + r)] * a.W[(size_t)(ic * R + r)];
+                const bool want = (ia % a.kb == ib / a.nb) && (ia / a.kb == ic / a.nb) && (ib % a.nb == ic % a.nb);
+                if (sum != (want ? 1 : 0)) return false;
+            }
+    return true;
+}
+
+// Level-L table of an algorithm: product p has digits p_0 .. p_{L-1} (outer
+// level most significant); a block of the Hm x Hk (A), Hk x Hn (B) and
+// Hm x Hn (C) grids has row = sum_l row_l * base^(L-1-l), so for Strassen
+// the 4 x 4 ids 4*row+col match src/stra_internal/3t/stra_mult_2level.cxx:341-353.
+// False when a sum or a C update has more than 4 blocks.
+bool build_table(const FmmAlgorithm& alg, int level, int id, ProductTable& t)
+{
+    t = ProductTable();
     t.level = level;
-    t.H = 1 << level;
+    t.algorithm = id;
+    t.H = t.Hk = t.Hn = 1;
+    for (int l = 0; l < level; l++) { t.H *= alg.mb; t.Hk *= alg.kb; t.Hn *= alg.nb; }
     if (level == 0)
     {
         Product p;
@@ -409,65 +518,155 @@ ProductTable make_table(int level)
         p.a[0] = {0, 0, 1}; p.b[0] = {0, 0, 1}; p.c[0] = {0, 0, 1};
         p.c_first[0] = 1;
         t.prod.push_back(p);
-        return t;
+        return true;
     }
-    // Level L product index p = p_outer * 7^(L-1) + ... ; sub-block (r, c) of
-    // the H x H grid has r = sum_l r_l * 2^(L-1-l) (outer level most
-    // significant), matching the 4x4 ids 4*row+col of
-    // src/stra_internal/3t/stra_mult_2level.cxx:341-353.
     int np = 1;
-    for (int l = 0; l < level; l++) np *= 7;
+    for (int l = 0; l < level; l++) np *= alg.rank;
     for (int p = 0; p < np; p++)
     {
-        int digits[2] = {0, 0};
+        std::vector<int> digits((size_t)level);
         int rem = p;
-        for (int l = level - 1; l >= 0; l--) { digits[l] = rem % 7; rem /= 7; }
+        for (int l = level - 1; l >= 0; l--) { digits[(size_t)l] = rem % alg.rank; rem /= alg.rank; }
         Product pr;
-        auto expand = [&](const int (*Mx)[7], Term* out, int8_t& count) {
-            // Kronecker product of the per-level coefficient columns.
+        auto expand = [&](const std::vector<int>& Mx, int rows, int cols, Term* out, int8_t& count) {
             struct Acc { int r, c, s; };
             std::vector<Acc> cur = {{0, 0, 1}};
             for (int l = 0; l < level; l++)
             {
                 std::vector<Acc> nxt;
                 for (auto& a : cur)
-                    for (int id = 0; id < 4; id++)
+                    for (int id2 = 0; id2 < rows * cols; id2++)
                     {
-                        int v = Mx[id][digits[l]];
+                        const int v = Mx[(size_t)(id2 * alg.rank + digits[(size_t)l])];
                         if (!v) continue;
-                        nxt.push_back({a.r * 2 + id / 2, a.c * 2 + id % 2, a.s * v});
+                        nxt.push_back({a.r * rows + id2 / cols, a.c * cols + id2 % cols, a.s * v});
                     }
                 cur = nxt;
             }
+            if (cur.size() > 4) return false;
+            for (auto& a : cur)
+                if (a.s != 1 && a.s != -1) return false;
             count = (int8_t)cur.size();
             for (size_t i = 0; i < cur.size(); i++)
                 out[i] = {(int8_t)cur[i].r, (int8_t)cur[i].c, (int8_t)cur[i].s};
+            return true;
         };
-        expand(U, pr.a, pr.na);
-        expand(V, pr.b, pr.nb);
-        expand(W, pr.c, pr.nc);
+        if (!expand(alg.U, alg.mb, alg.kb, pr.a, pr.na) || !expand(alg.V, alg.kb, alg.nb, pr.b, pr.nb) ||
+            !expand(alg.W, alg.mb, alg.nb, pr.c, pr.nc))
+            return false;
+        if (pr.na == 0 || pr.nb == 0 || pr.nc == 0) continue;   // a product that contributes nothing
         t.prod.push_back(pr);
     }
     // Mark the first product touching each C block (beta applied there once).
-    std::vector<int> seen(t.H * t.H, 0);
+    std::vector<int> seen((size_t)(t.H * t.Hn), 0);
     for (auto& pr : t.prod)
         for (int i = 0; i < pr.nc; i++)
         {
-            int id = pr.c[i].r * t.H + pr.c[i].c;
-            pr.c_first[i] = seen[id] ? 0 : 1;
-            seen[id] = 1;
+            const int id2 = pr.c[i].r * t.Hn + pr.c[i].c;
+            pr.c_first[i] = seen[(size_t)id2] ? 0 : 1;
+            seen[(size_t)id2] = 1;
         }
-    return t;
+    // every C block must be touched, or beta would not reach it
+    for (int v : seen)
+        if (!v) return false;
+    return true;
 }
+
+struct Registry
+{
+    std::mutex mu;
+    std::vector<FmmAlgorithm> algs;
+    // tables per (algorithm, level 1..2); null where the kernels cannot run it
+    std::vector<std::unique_ptr<ProductTable>> tab[3];
+    Registry()
+    {
+        add(strassen_algorithm());
+        add(classical_algorithm(2, 2, 2));
+        add(strassen_plus_classical(0));
+        add(strassen_plus_classical(1));
+        add(strassen_plus_classical(2));
+    }
+    int add(const FmmAlgorithm& a)
+    {
+        const int id = (int)algs.size();
+        algs.push_back(a);
+        for (int level = 1; level <= 2; level++)
+        {
+            auto t = std::make_unique<ProductTable>();
+            const bool ok = build_table(a, level, id, *t) && t->H <= 4 && t->Hk <= 4 && t->Hn <= 4 &&
+                            !t->prod.empty() && t->prod.size() <= 49;
+            tab[level].push_back(ok ? std::move(t) : nullptr);
+        }
+        return id;
+    }
+};
+
+Registry& registry()
+{
+    static Registry r;
+    return r;
+}
+
+thread_local int t_fmm = 0;
 
 }  // namespace
 
+int register_algorithm(const FmmAlgorithm& a)
+{
+    if (!algorithm_exact(a)) return -TBLIS_STRA_ERR_ARG;
+    Registry& r = registry();
+    std::lock_guard<std::mutex> lk(r.mu);
+    if (r.algs.size() >= 64) return -TBLIS_STRA_ERR_TOO_LARGE;
+    const int id = r.add(a);
+    if (!r.tab[1][(size_t)id])
+    {
+        // keep the id (ids never move) but the kernels cannot run it
+        return -TBLIS_STRA_ERR_UNSUPPORTED;
+    }
+    return id;
+}
+
+const FmmAlgorithm* algorithm_by_id(int id)
+{
+    Registry& r = registry();
+    std::lock_guard<std::mutex> lk(r.mu);
+    if (id < 0 || id >= (int)r.algs.size()) return nullptr;
+    return &r.algs[(size_t)id];
+}
+
+const ProductTable* fmm_table(int id, int level)
+{
+    if (level == 0) return &strassen_table(0);
+    if (level < 1 || level > 2) return nullptr;
+    Registry& r = registry();
+    std::lock_guard<std::mutex> lk(r.mu);
+    if (id < 0 || id >= (int)r.algs.size()) return nullptr;
+    return r.tab[level][(size_t)id].get();
+}
+
+void set_thread_algorithm(int id) { t_fmm = id; }
+int thread_algorithm() { return t_fmm; }
+
+const ProductTable& strassen_table(int level)
+{
+    struct Tables
+    {
+        ProductTable t[3];
+        Tables()
+        {
+            const FmmAlgorithm s = strassen_algorithm();
+            for (int l = 0; l < 3; l++) build_table(s, l, 0, t[l]);
+        }
+    };
+    static const Tables tables;
+    return tables.t[level < 0 ? 0 : level > 2 ? 2 : level];
+}
+
 const ProductTable& product_table(int level)
 {
-    static const ProductTable t0 = make_table(0);
-    static const ProductTable t1 = make_table(1);
-    static const ProductTable t2 = make_table(2);
-    return level == 0 ? t0 : level == 1 ? t1 : t2;
+    if (level >= 1 && t_fmm != 0)
+        if (const ProductTable* t = fmm_table(t_fmm, level)) return *t;
+    return strassen_table(level);
 }
 
 namespace {
@@ -510,7 +709,7 @@ PackGroup make_group(int level, const int (*M)[7], int group)
 // Expand a group's sums and compare them with the product table's terms.
 bool group_matches(const PackGroup& pg, int level, int operand, int group)
 {
-    const ProductTable& t = product_table(level);
+    const ProductTable& t = strassen_table(level);
     for (int q = 0; q < 7; q++)
     {
         const Product& pr = t.prod[(size_t)(group * 7 + q)];
@@ -556,6 +755,7 @@ const PackGroup* pack_group(int level, int operand, int group)
     };
     static const Groups groups;
     if (level < 1 || level > 2 || !groups.ok[level] || operand < 0 || operand > 1) return nullptr;
+    if (thread_algorithm() != 0) return nullptr;   // the factored sums are Strassen's
     if (group < 0 || group >= (int)groups.g[level][operand].size()) return nullptr;
     return &groups.g[level][operand][(size_t)group];
 }

@@ -94,15 +94,52 @@ struct Product
 struct ProductTable
 {
     int level = 0;
-    int H = 1;            // 2^level sub-blocks per dimension
+    int H = 1;            // block rows of A and C (2^level for Strassen)
+    int Hk = 1, Hn = 1;   // block columns of A (= rows of B) and of B and C
+    int algorithm = 0;    // registry id of the fast-multiplication algorithm
     std::vector<Product> prod;
 };
+
+// A fast matrix-multiplication algorithm <mb, kb, nb; rank>: on an mb x kb
+// block grid of A, kb x nb of B and mb x nb of C, product r is
+//   M_r = (sum_i U[i][r] A_i) (sum_j V[j][r] B_j),   C_q += W[q][r] M_r,
+// block id = row * (grid columns) + column, coefficient matrices row-major
+// (rows = block ids, columns = products), the layout of the reference's
+// coefficient files (src/stra_internal/3t/strassen:1-14; the generator
+// src/stra_internal/3m/my_stra_gen.py takes the same U/V/W for other shapes).
+struct FmmAlgorithm
+{
+    std::string name;
+    int mb = 2, kb = 2, nb = 2, rank = 7;
+    std::vector<int> U, V, W;
+};
+
+// Built-in algorithms: 0 Strassen <2,2,2;7>; 1 the classical <2,2,2;8>;
+// 2-4 Strassen beside the classical product on the third block row, column
+// or summed slice: <3,2,2;11>, <2,3,2;11>, <2,2,3;11>.  register_algorithm
+// adds more (checked: the coefficients must multiply matrices exactly) and
+// returns the new id, or a negative TBLIS_STRA_* status.
+constexpr int FMM_BUILTIN = 5;
+int register_algorithm(const FmmAlgorithm& a);
+const FmmAlgorithm* algorithm_by_id(int id);
+// The product table of algorithm `id` at `level` (its Kronecker power), or
+// nullptr when the kernels cannot run it: block grid beyond 4 x 4, more than
+// 49 products, or a sum or C update of more than 4 blocks.
+const ProductTable* fmm_table(int id, int level);
+
+// The calling thread's algorithm (tblis_stra_set_algorithm); product_table()
+// below serves it at every level >= 1.
+void set_thread_algorithm(int id);
+int thread_algorithm();
 
 // 〈2,2,2〉 Strassen coefficients (U for A, V for B, W for C; rows = sub-block
 // id 0..3 = (id/2, id%2), columns = products), as listed in
 // src/stra_internal/3t/strassen:1-14, and their Kronecker square for level 2
-// (the 49-product grid of src/stra_internal/3t/stra_mult_2level.cxx:341-1485).
+// (the 49-product grid of src/stra_internal/3t/stra_mult_2level.cxx:341-1485);
+// at level >= 1 with another algorithm selected on the calling thread, that
+// algorithm's table (callers check fmm_table() first).
 const ProductTable& product_table(int level);
+const ProductTable& strassen_table(int level);
 
 // The operand sums of 7 consecutive products (all of L=1, or products
 // 7G .. 7G+6 of L=2) in factored form, so one pass over the operand forms all

@@ -158,6 +158,14 @@ def _load() -> ctypes.CDLL:
     lib.tblis_stra_measure_dmma_peak.restype = ctypes.c_int
     lib.tblis_stra_mult_noalloc.argtypes = [ctypes.c_int, T, S, T, S, T, S, ctypes.c_void_p]
     lib.tblis_stra_mult_noalloc.restype = ctypes.c_int
+    lib.tblis_stra_set_algorithm.argtypes = [ctypes.c_int]
+    lib.tblis_stra_set_algorithm.restype = ctypes.c_int
+    lib.tblis_stra_get_algorithm.restype = ctypes.c_int
+    PI = ctypes.POINTER(ctypes.c_int)
+    lib.tblis_stra_algorithm_info.argtypes = [ctypes.c_int, PI, PI, PI, PI, PI]
+    lib.tblis_stra_algorithm_info.restype = ctypes.c_int
+    lib.tblis_stra_register_algorithm.argtypes = [ctypes.c_int] * 4 + [PI, PI, PI, PI]
+    lib.tblis_stra_register_algorithm.restype = ctypes.c_int
     lib.tblis_get_num_threads.restype = ctypes.c_uint
     lib.tblis_set_num_threads.argtypes = [ctypes.c_uint]
     return lib
@@ -392,6 +400,70 @@ class Batch:
 
 
 KERNEL_KINDS = {"fused": 0, "pack": 1, "packed_gemm": 2, "aux": 3, "split_gemm": 4}
+
+
+ALGORITHMS = {"strassen": 0, "classical222": 1, "strassen322": 2, "strassen232": 3, "strassen223": 4}
+
+
+def set_algorithm(id_or_name) -> None:
+    """Fast matrix-multiplication algorithm of the Strassen levels on this
+    thread (an id, or a built-in name of ALGORITHMS)."""
+    _check(lib.tblis_stra_set_algorithm(ALGORITHMS.get(id_or_name, id_or_name)))
+
+
+def get_algorithm() -> int:
+    return int(lib.tblis_stra_get_algorithm())
+
+
+def algorithm_info(alg) -> dict:
+    """Shape, rank and highest runnable level of an algorithm."""
+    v = [ctypes.c_int() for _ in range(5)]
+    _check(lib.tblis_stra_algorithm_info(ALGORITHMS.get(alg, alg), *[ctypes.byref(x) for x in v]))
+    mb, kb, nb, rank, levels = (x.value for x in v)
+    return {"mb": mb, "kb": kb, "nb": nb, "rank": rank, "levels": levels}
+
+
+def register_algorithm(mb: int, kb: int, nb: int, U, V, W) -> int:
+    """Adds an algorithm from its coefficient matrices (rows = block ids,
+    columns = products) and returns its id."""
+    import numpy as np
+    U, V, W = (np.ascontiguousarray(np.asarray(X), dtype=np.int32) for X in (U, V, W))
+    rank = U.shape[1]
+    if U.shape != (mb * kb, rank) or V.shape != (kb * nb, rank) or W.shape != (mb * nb, rank):
+        raise ValueError("coefficient matrices do not match the shape")
+    out = ctypes.c_int()
+    P = ctypes.POINTER(ctypes.c_int)
+    _check(lib.tblis_stra_register_algorithm(mb, kb, nb, rank, U.ctypes.data_as(P), V.ctypes.data_as(P),
+                                             W.ctypes.data_as(P), ctypes.byref(out)))
+    return out.value
+
+
+def parse_coefficients(text: str):
+    """U, V, W from the reference's coefficient-file format
+    (src/stra_internal/3t/strassen:1-14): three blocks of integer rows (one
+    row per block id, one column per product) separated by '#' lines."""
+    import numpy as np
+    blocks, cur = [], []
+    for line in text.splitlines():
+        if line.strip().startswith("#"):
+            if cur:
+                blocks.append(cur)
+            cur = []
+        elif line.strip():
+            cur.append([int(x) for x in line.split()])
+    if cur:
+        blocks.append(cur)
+    if len(blocks) != 3:
+        raise ValueError(f"expected U, V and W blocks, found {len(blocks)}")
+    return tuple(np.array(b, dtype=np.int32) for b in blocks)
+
+
+def load_algorithm_file(path: str, mb: int, kb: int, nb: int) -> int:
+    """Registers the <mb, kb, nb> algorithm of a coefficient file in the
+    reference's format (as its generator reads them) and returns its id."""
+    with open(path) as f:
+        U, V, W = parse_coefficients(f.read())
+    return register_algorithm(mb, kb, nb, U, V, W)
 
 
 def set_wait_limit(cycles: int) -> None:
