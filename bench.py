@@ -199,9 +199,10 @@ def sampled_exact_error(torch, A, B, C, nsamples=4096, seed=7):
     extent equal; FP32 values are promoted exactly."""
     from oracle import oracle
     import numpy as np
-    e = A.shape[0]
     rng = np.random.default_rng(seed)
-    idx = rng.integers(0, e, size=(nsamples, 4))
+    # (a, b, c, d): a, c from A(e,f,a,c); b, d from B(f,b,d,e)
+    hi = (A.shape[2], B.shape[1], A.shape[3], B.shape[2])
+    idx = np.stack([rng.integers(0, h, size=nsamples) for h in hi], axis=1)
     worst, num, den = 0.0, 0.0, 0.0
     for lo in range(0, nsamples, 512):
         part = torch.as_tensor(idx[lo:lo + 512], device=A.device)
@@ -283,6 +284,47 @@ def batched_form(torch, tsb, device, stream, count, barrier_sync, max_over_ranks
         out[name] = res
         del tens
         torch.cuda.empty_cache()
+    return out
+
+
+def precision_sweep(torch, tsb, device, stream, barrier_sync, max_over_ranks):
+    """The precision form over its sizes and both input sets: C(abcd) +=
+    A(efac) B(fbde) in FP32 at NIm = NJn = NPk in {4096, 8192, 16384}, entries
+    U[-1,1] or sign * 10^U[-3,3] (log-uniform magnitudes in [1e-3, 1e3]),
+    L = 0/1/2 with 6 and 3 split-BF16 terms; effective TFLOP/s (median of 3)
+    and the normwise error of 1024 sampled entries against exact
+    (long-double) dot products of the same FP32 values."""
+    out = {}
+    for dist in ("uniform", "loguniform"):
+        for lo, hi in ((64, 64), (64, 128), (128, 128)):
+            npk = lo * hi
+            flops = 2.0 * float(npk) ** 3
+            g = torch.Generator(device=device).manual_seed(7)
+            ext = dict(a=lo, b=lo, e=lo, c=hi, d=hi, f=hi)
+
+            def operand(idx):
+                t = colmajor(torch, [ext[x] for x in idx], device, g).float()
+                if dist == "loguniform":
+                    mag = torch.empty_like(t).uniform_(-3.0, 3.0, generator=g)
+                    t = torch.sign(t) * torch.pow(10.0, mag)
+                return t
+
+            A, B = operand(IDX_A), operand(IDX_B)
+            C = colmajor(torch, [ext[x] for x in IDX_C], device, fill=0.0).float()
+            for terms in (6, 3):
+                tsb.set_fp32_terms(terms)
+                for lv in (0, 1, 2):
+                    def run():
+                        tsb.contract(lv, 1.0, A, IDX_A, B, IDX_B, 0.0, C, IDX_C, stream=stream)
+                    run()
+                    barrier_sync()
+                    ts = sorted(max_over_ranks(time_steps(torch, run, 1, stream)) for _ in range(3))
+                    _, nw = sampled_exact_error(torch, A, B, C, nsamples=1024)
+                    out[f"{dist}_N{npk}_L{lv}_{terms}terms"] = {"tflops": flops / ts[1] / 1e12,
+                                                                 "sampled_normwise_err": nw}
+            tsb.set_fp32_terms(6)
+            del A, B, C
+            torch.cuda.empty_cache()
     return out
 
 
@@ -700,6 +742,7 @@ def main():
         precision["best_6terms_vs_fp64_L0"] = best6 / levels["L0"]
         del A32, B32, C32, Cref
         torch.cuda.empty_cache()
+        precision["sweep"] = precision_sweep(torch, tsb, device, stream, barrier_sync, max_over_ranks)
 
     # ---- differentiation form: forward + backward through the autograd binding
     differentiation = None
