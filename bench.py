@@ -250,8 +250,14 @@ def batched_form(torch, tsb, device, stream, count, barrier_sync, max_over_ranks
         # autotuned (level, variant, tile) vs the plain grouped fused launch at L=0
         # FP64: against the plain grouped fused launch; FP32: against the
         # split schedule problem by problem
+        # against the plain one-launch fused kernel / problem-by-problem split
+        # schedule, and against the best fixed L=0 schedule (the grouped packed
+        # GEMM over chunks of problems, FP64; the grouped split GEMM, FP32)
         modes = [("autotuned", -1, None)]
-        modes.append(("fused_L0", 0, ["fused"]) if dtype == torch.float64 else ("split_L0", 0, ["split"]))
+        if dtype == torch.float64:
+            modes += [("fused_L0", 0, ["fused"]), ("packed_grouped_L0", 0, ["packed_grouped"])]
+        else:
+            modes += [("split_L0", 0, ["split"]), ("split_grouped_L0", 0, ["split_grouped"])]
         for mode, lv, allowed in modes:
             probs = [(1.0, A, ia, B, ib, 0.0, C, ic, lv) for A, ia, B, ib, C, ic in tens]
             tsb.set_batch_schedules(allowed)
@@ -278,7 +284,7 @@ def batched_form(torch, tsb, device, stream, count, barrier_sync, max_over_ranks
             torch.cuda.synchronize()
             worst = max(worst, float(torch.linalg.norm((C.double() - R).flatten()) / torch.linalg.norm(R.flatten())))
         res["spot_normwise_err"] = worst
-        for base in ("fused_L0", "split_L0"):
+        for base in ("fused_L0", "split_L0", "packed_grouped_L0", "split_grouped_L0"):
             if base in res:
                 res["autotuned_vs_" + base] = res["autotuned"]["tflops_effective"] / res[base]["tflops_effective"]
         out[name] = res
