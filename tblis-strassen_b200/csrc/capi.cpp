@@ -1695,7 +1695,14 @@ bool slice_geometry(const tblis_tensor* T, int pos, int64_t& sigma, int64_t& hei
 }
 
 constexpr size_t PIPELINE_MIN_BYTES = (size_t)64 << 20;
-constexpr int PIPELINE_CHUNKS = 4;
+#ifndef TSB_PIPELINE_CHUNKS
+#define TSB_PIPELINE_CHUNKS 4
+#endif
+#ifndef TSB_PIPELINE_CUTS
+#define TSB_PIPELINE_CUTS 2
+#endif
+constexpr int PIPELINE_CHUNKS = TSB_PIPELINE_CHUNKS;   // pieces of the split operand
+constexpr int PIPELINE_CUTS = TSB_PIPELINE_CUTS;       // pieces of the other operand (second cut)
 constexpr int NOT_PIPELINED = -1;
 
 int run_plan(int level, int impl, const GemmView& g, const DevPlan& t, void* const dptr[3], cudaStream_t st,
@@ -1775,7 +1782,7 @@ int mult_pipelined(int level, int impl, const tblis_tensor* const T[3], const la
         qc = (int)d;
         pw = pwhole;
     }
-    const int halves = qc >= 0 ? 2 : 1;
+    const int halves = qc >= 0 ? (int)std::min<int64_t>(PIPELINE_CUTS, T[2]->len[qc]) : 1;
 
     CopyStreams cs;
     int s = copy_streams(device, cs);
