@@ -60,8 +60,8 @@ constexpr int PCH = 16;                  // producer elements per batch of loads
 // Register split: threads x launch registers is the CTA's pool; the producer
 // gives back what the consumers take (checked against the compiled count on
 // the host before every launch).
-constexpr int PROD_REGS = 96;
-constexpr int CONS_REGS = 200;
+constexpr int PROD_REGS = 136;
+constexpr int CONS_REGS = 176;
 
 struct FusedCtrl
 {
@@ -117,7 +117,9 @@ __device__ __forceinline__ void decode_work(const DmmaArgs& a, int64_t w, int64_
 // One operand sum of one ring slot: X(r, k) = sum_t sign_t * X[row_t(r) + k_t(k)]
 // over the terms of the product's sum, stored at tile_pos(k, r).  `rows` is
 // the row (column) offset table [FHMAX][FT] of the tile, `ktab` this k-step's
-// k offset table [FHMAX][FBK]; invalid entries read as zero.
+// k offset table [FHMAX][FBK]; invalid entries read as zero.  The loads of two
+// terms are issued together, so a thread keeps 2 * PCH loads in flight (the
+// gathers are latency-bound, not bandwidth-bound).
 template <bool KFAST>
 __device__ __forceinline__ void produce_tile(const double* __restrict__ X, const int64_t* rows, const int64_t* ktab,
                                              int nt, const int8_t* t_row, const int8_t* t_k, const int8_t* t_s,
@@ -130,22 +132,28 @@ __device__ __forceinline__ void produce_tile(const double* __restrict__ X, const
 #pragma unroll
         for (int e = 0; e < PCH; e++) v[e] = 0.0;
 #pragma unroll 1
-        for (int t = 0; t < nt; t++)
+        for (int t = 0; t < nt; t += 2)
         {
-            const int64_t* rt = rows + t_row[t] * FT;
-            const int64_t* kt = ktab + t_k[t] * FBK;
-            const bool neg = t_s[t] < 0;
-            double x[PCH];
+            const bool two = t + 1 < nt;
+            const int64_t* rt0 = rows + t_row[t] * FT;
+            const int64_t* kt0 = ktab + t_k[t] * FBK;
+            const int64_t* rt1 = rows + t_row[two ? t + 1 : t] * FT;
+            const int64_t* kt1 = ktab + t_k[two ? t + 1 : t] * FBK;
+            const double s0 = t_s[t] < 0 ? -1.0 : 1.0;
+            const double s1 = two ? (t_s[t + 1] < 0 ? -1.0 : 1.0) : 0.0;
+            double x0[PCH], x1[PCH];
 #pragma unroll
             for (int e = 0; e < PCH; e++)
             {
                 int kk, r;
                 lane_map<FBK, FT>(KFAST, ptid + (c0 + e) * PT, kk, r);
-                const int64_t ro = rt[r], ko = kt[kk];
-                x[e] = (ro != OFF_INVALID && ko != OFF_INVALID) ? __ldg(X + (ro + ko)) : 0.0;
+                const int64_t ro0 = rt0[r], ko0 = kt0[kk], ro1 = rt1[r], ko1 = kt1[kk];
+                x0[e] = (ro0 != OFF_INVALID && ko0 != OFF_INVALID) ? __ldg(X + (ro0 + ko0)) : 0.0;
+                x1[e] = (two && ro1 != OFF_INVALID && ko1 != OFF_INVALID) ? __ldg(X + (ro1 + ko1)) : 0.0;
             }
+            // exact: s0, s1 are +-1 or 0
 #pragma unroll
-            for (int e = 0; e < PCH; e++) v[e] += neg ? -x[e] : x[e];
+            for (int e = 0; e < PCH; e++) v[e] += s0 * x0[e] + s1 * x1[e];
         }
 #pragma unroll
         for (int e = 0; e < PCH; e++)
@@ -197,6 +205,19 @@ stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
         // ---------------- producer warpgroup ----------------
         asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" :: "n"(PROD_REGS));
         const int ptid = tid;
+        // This thread's 2 entries of the k offset tables kA, kB for k-step s:
+        // they depend on the k-step only (not on the product or the tile), so
+        // the next k-step's are loaded while the current one is produced.
+        static_assert(2 * FHMAX * FBK == 2 * PT, "two table entries per producer thread");
+        auto ktab_entry = [&](int64_t s, int j) -> int64_t {
+            const int i = ptid + j * PT;
+            const int op = i / (FHMAX * FBK), e = i % (FHMAX * FBK);
+            const int h = e / FBK, kk = e % FBK;
+            const int64_t kl = s * FBK + kk, gk = h * a.ks + kl;
+            if (!(h < Hk && kl < a.ks && gk < a.k)) return OFF_INVALID;
+            return op == 0 ? a.ksA[gk] : a.ksB[gk];
+        };
+        int64_t kv0 = nk > 0 ? ktab_entry(0, 0) : OFF_INVALID, kv1 = nk > 0 ? ktab_entry(0, 1) : OFF_INVALID;
         uint32_t it = 0;
         bool ok = true;      // this thread's waits so far
         bool stop = false;   // set only right after a collective check, so uniform
@@ -226,16 +247,14 @@ stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
                     // the tile's row tables are complete); a wait that ran out
                     // in any of them ends the loops for all of them.
                     if (bar_any<1, PT>(!ok)) { stop = true; break; }
-                    for (int i = ptid; i < 2 * FHMAX * FBK; i += PT)
-                    {
-                        const int op = i / (FHMAX * FBK), e = i % (FHMAX * FBK);
-                        const int h = e / FBK, kk = e % FBK;
-                        const int64_t kl = s * FBK + kk, gk = h * a.ks + kl;
-                        const bool in = h < Hk && kl < a.ks && gk < a.k;
-                        if (op == 0) kA[e] = in ? a.ksA[gk] : OFF_INVALID;
-                        else         kB[e] = in ? a.ksB[gk] : OFF_INVALID;
-                    }
+                    kA[ptid] = kv0;                  // kA and kB are one array of 2 * PT entries
+                    kA[ptid + PT] = kv1;
                     bar_sync<1, PT>();
+                    {
+                        const int64_t sn = s + 1 < nk ? s + 1 : 0;
+                        kv0 = ktab_entry(sn, 0);
+                        kv1 = ktab_entry(sn, 1);
+                    }
                     const uint32_t slot = it % FSTAGES;
                     const uint32_t use = it / FSTAGES;   // earlier uses of this slot
                     it++;
@@ -342,27 +361,20 @@ stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
                     const double cb = first ? a.beta : 1.0;
 #pragma unroll
                     for (int mi = 0; mi < MI; mi++)
-                    {
-                        double cv[2][NI][2];
 #pragma unroll
                         for (int hr = 0; hr < 2; hr++)
                         {
                             const int64_t ro = rt[wm + mi * 16 + g + hr * 8];
+                            if (ro == OFF_INVALID) continue;
+                            double cv[NI][2];
 #pragma unroll
                             for (int ni = 0; ni < NI; ni++)
 #pragma unroll
                                 for (int hc = 0; hc < 2; hc++)
                                 {
                                     const int64_t co = ct[wn + ni * 8 + t4 * 2 + hc];
-                                    cv[hr][ni][hc] = (read_c && ro != OFF_INVALID && co != OFF_INVALID)
-                                                         ? a.C[ro + co] : 0.0;
+                                    cv[ni][hc] = (read_c && co != OFF_INVALID) ? a.C[ro + co] : 0.0;
                                 }
-                        }
-#pragma unroll
-                        for (int hr = 0; hr < 2; hr++)
-                        {
-                            const int64_t ro = rt[wm + mi * 16 + g + hr * 8];
-                            if (ro == OFF_INVALID) continue;
 #pragma unroll
                             for (int ni = 0; ni < NI; ni++)
 #pragma unroll
@@ -370,10 +382,9 @@ stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
                                 {
                                     const int64_t co = ct[wn + ni * 8 + t4 * 2 + hc];
                                     if (co == OFF_INVALID) continue;
-                                    a.C[ro + co] = coef * acc[mi][ni][hr * 2 + hc] + cb * cv[hr][ni][hc];
+                                    a.C[ro + co] = coef * acc[mi][ni][hr * 2 + hc] + cb * cv[ni][hc];
                                 }
                         }
-                    }
                 }
             }
         }
