@@ -12,23 +12,34 @@
 // in order, so C blocks shared by products need no atomics and beta is
 // applied once, by the first product touching a block):
 //
-//   producer warpgroup (warps 0-3): for each k-step of 32 gathers the 2, or
-//     up to 4 at L = 2, A blocks (and B blocks) of the product's signed sums
-//     through the scatter vectors into registers, forms S = sum_i u_i A_i and
-//     T = sum_j v_j B_j, and stores them into a ring slot in the swizzled
-//     k-major layout of the DMMA fragments (tile_pos), so each operand sum is
-//     formed once per staged tile rather than per fragment read; the slot's
-//     "full" mbarrier then completes.  Its registers are cut to PROD_REGS.
+//   producer warpgroup (warps 0-3, registers cut with setmaxnreg): fills a
+//     3-slot ring, one k-step per slot, through the scatter vectors, in one of
+//     two modes:
+//       RAW (sums of at most 2 blocks: L <= 1): cp.async gathers of the raw
+//         blocks of each operand sum (16 k per slot) into the swizzled k-major
+//         fragment layout (tile_pos); the slot's "full" mbarrier completes when
+//         the copies land (cp.async.mbarrier.arrive), so the producer never
+//         waits on data and runs ahead to the next slot;
+//       SUM (up to 4 blocks: L = 2): the blocks are loaded into registers,
+//         S = sum_i u_i A_i and T = sum_j v_j B_j are formed once per staged
+//         tile (32 k per slot) and stored into the slot.
 //   consumer warpgroups (warps 4-11): 2 x 4 warps of 64 x 32 (m16n8k4 DMMA
-//     fragments read as 128-bit pairs), registers raised to CONS_REGS; after a
-//     slot is read each warp arrives on its "empty" mbarrier; after the last
-//     k-step of a product the epilogue adds +-alpha*S*T into the product's C
-//     blocks.
+//     fragments read as 128-bit pairs; in RAW mode the 2 blocks' fragments are
+//     summed with their signs as they are read); after a slot is read each warp
+//     arrives on its "empty" mbarrier; after the last k-step of a product the
+//     epilogue adds +-alpha*S*T into the product's C blocks.
 //
-// The producer runs up to STAGES k-steps ahead, across product and tile
+// Measured at 16384^3 (no-workspace calls): RAW L=0 29.7, L=1 19.8 effective
+// TFLOP/s, against 12.6 at L=1 for the SUM mode, whose register-held gathers
+// are latency-bound; both modes are bound by the element-wise gathers through
+// the scatter vectors (8-byte requests to L2), which the packed schedule
+// turns into 32 KB bulk copies by packing the sums once in HBM.
+//
+// The producer runs up to 3 k-steps ahead, across product and tile
 // boundaries.  Every wait is bounded; a wait that runs out makes both roles
 // leave their loops at the next tile (a collective OR over each role's named
-// barrier), and with no asynchronous copies in flight the CTA simply ends.
+// barrier); RAW-mode producers then let their own copies land before the CTA
+// ends.
 #include "kernels.cuh"
 #include "mbarrier.cuh"
 #include "tile_layout.cuh"
@@ -43,7 +54,6 @@ extern std::atomic<unsigned long long> g_launches;
 namespace {
 
 constexpr int FT = 128;                  // tile rows (A side) and columns (B side)
-constexpr int FBK = 32;                  // k per ring slot
 constexpr int FSTAGES = 3;
 constexpr int FHMAX = 4;                 // largest block grid side (level 2)
 constexpr int NPW = 4;                   // producer warps (one warpgroup)
@@ -54,14 +64,26 @@ constexpr int CT = 32 * NCW;             // consumer threads
 constexpr int CWM = 2, CWN = 4;
 constexpr int WTM = FT / CWM, WTN = FT / CWN;   // 64 x 32 warp tile
 constexpr int MI = WTM / 16, NI = WTN / 8;      // 4 x 4 fragments
-constexpr int PE = FBK * FT / PT;        // elements of one operand tile per producer thread (32)
-constexpr int PCH = 16;                  // producer elements per batch of loads
+constexpr int FBK_MAX = 32;
+constexpr int PCH = 16;                  // SUM mode: producer elements per batch of loads
 
-// Register split: threads x launch registers is the CTA's pool; the producer
-// gives back what the consumers take (checked against the compiled count on
-// the host before every launch).
-constexpr int PROD_REGS = 136;
-constexpr int CONS_REGS = 176;
+// Per-mode geometry.  Register split: threads x launch registers is the CTA's
+// pool; the producer gives back what the consumers take (checked against the
+// compiled count on the host before every launch; both splits compile without
+// spills).
+template <bool RAW>
+struct FMode
+{
+    static constexpr int BK = RAW ? 16 : 32;               // k per ring slot
+    static constexpr int NT = RAW ? 2 : 1;                 // blocks per operand held in a slot
+    static constexpr int PE = BK * FT / PT;                // elements of one operand block per producer thread
+    static constexpr int KENT = 2 * FHMAX * BK / PT;       // k-table entries per producer thread
+    static constexpr int PROD_REGS = RAW ? 80 : 128;
+    static constexpr int CONS_REGS = RAW ? 200 : 184;
+    static constexpr size_t SLOT_DOUBLES = size_t(BK) * FT * 2 * NT;
+    static_assert(2 * FHMAX * BK == KENT * PT, "k-table entries split evenly over the producers");
+    static_assert(RAW || PE % PCH == 0, "producer batches cover a block");
+};
 
 struct FusedCtrl
 {
@@ -69,13 +91,13 @@ struct FusedCtrl
     int abort;
 };
 
-constexpr size_t SLOT_DOUBLES = size_t(FBK) * FT * 2;                  // S and T tiles
-constexpr size_t RING_BYTES = FSTAGES * SLOT_DOUBLES * 8;
+constexpr size_t RING_BYTES = FSTAGES * size_t(FBK_MAX) * FT * 2 * 8;   // either mode's 3 slots
+static_assert(FSTAGES * FMode<true>::SLOT_DOUBLES * 8 == RING_BYTES &&
+              FSTAGES * FMode<false>::SLOT_DOUBLES * 8 == RING_BYTES, "both modes fill the ring");
 constexpr size_t TAB_BYTES = size_t(4) * FHMAX * FT * 8                 // rowA, colB, rowC, colC
-                             + size_t(2) * FHMAX * FBK * 8;             // k tables of A and B
+                             + size_t(2) * FHMAX * FBK_MAX * 8;         // k tables of A and B
 constexpr size_t FUSED_SMEM = RING_BYTES + TAB_BYTES + sizeof(FusedCtrl);
 static_assert(FUSED_SMEM <= 227 * 1024, "shared memory budget");
-static_assert(PE % PCH == 0, "producer batches cover a tile");
 
 __device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, double b0)
 {
@@ -114,17 +136,18 @@ __device__ __forceinline__ void decode_work(const DmmaArgs& a, int64_t w, int64_
     tn = (tw % (GROUP * a.tiles_n)) / gsize;
 }
 
-// One operand sum of one ring slot: X(r, k) = sum_t sign_t * X[row_t(r) + k_t(k)]
+// SUM mode: one operand sum of one ring slot: X(r, k) = sum_t sign_t * X[row_t(r) + k_t(k)]
 // over the terms of the product's sum, stored at tile_pos(k, r).  `rows` is
 // the row (column) offset table [FHMAX][FT] of the tile, `ktab` this k-step's
-// k offset table [FHMAX][FBK]; invalid entries read as zero.  The loads of two
+// k offset table [FHMAX][BK]; invalid entries read as zero.  The loads of two
 // terms are issued together, so a thread keeps 2 * PCH loads in flight (the
 // gathers are latency-bound, not bandwidth-bound).
-template <bool KFAST>
+template <bool KFAST, int BK>
 __device__ __forceinline__ void produce_tile(const double* __restrict__ X, const int64_t* rows, const int64_t* ktab,
                                              int nt, const int8_t* t_row, const int8_t* t_k, const int8_t* t_s,
                                              double* dst, int ptid)
 {
+    constexpr int PE = BK * FT / PT;
 #pragma unroll 1
     for (int c0 = 0; c0 < PE; c0 += PCH)
     {
@@ -136,9 +159,9 @@ __device__ __forceinline__ void produce_tile(const double* __restrict__ X, const
         {
             const bool two = t + 1 < nt;
             const int64_t* rt0 = rows + t_row[t] * FT;
-            const int64_t* kt0 = ktab + t_k[t] * FBK;
+            const int64_t* kt0 = ktab + t_k[t] * BK;
             const int64_t* rt1 = rows + t_row[two ? t + 1 : t] * FT;
-            const int64_t* kt1 = ktab + t_k[two ? t + 1 : t] * FBK;
+            const int64_t* kt1 = ktab + t_k[two ? t + 1 : t] * BK;
             const double s0 = t_s[t] < 0 ? -1.0 : 1.0;
             const double s1 = two ? (t_s[t + 1] < 0 ? -1.0 : 1.0) : 0.0;
             double x0[PCH], x1[PCH];
@@ -146,7 +169,7 @@ __device__ __forceinline__ void produce_tile(const double* __restrict__ X, const
             for (int e = 0; e < PCH; e++)
             {
                 int kk, r;
-                lane_map<FBK, FT>(KFAST, ptid + (c0 + e) * PT, kk, r);
+                lane_map<BK, FT>(KFAST, ptid + (c0 + e) * PT, kk, r);
                 const int64_t ro0 = rt0[r], ko0 = kt0[kk], ro1 = rt1[r], ko1 = kt1[kk];
                 x0[e] = (ro0 != OFF_INVALID && ko0 != OFF_INVALID) ? __ldg(X + (ro0 + ko0)) : 0.0;
                 x1[e] = (two && ro1 != OFF_INVALID && ko1 != OFF_INVALID) ? __ldg(X + (ro1 + ko1)) : 0.0;
@@ -159,25 +182,57 @@ __device__ __forceinline__ void produce_tile(const double* __restrict__ X, const
         for (int e = 0; e < PCH; e++)
         {
             int kk, r;
-            lane_map<FBK, FT>(KFAST, ptid + (c0 + e) * PT, kk, r);
+            lane_map<BK, FT>(KFAST, ptid + (c0 + e) * PT, kk, r);
             dst[tile_pos(kk, r, FT)] = v[e];
         }
     }
 }
 
-template <bool KA, bool KB>
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void* src, int src_bytes)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" :: "r"(dst), "l"(src), "r"(src_bytes));
+}
+
+// RAW mode: the raw blocks of one operand sum into a slot, block t at
+// dst + t * BK * FT, element (r, k) at tile_pos(k, r); invalid entries are
+// zero-filled (source size 0).
+template <bool KFAST, int BK>
+__device__ __forceinline__ void issue_tiles(const double* __restrict__ X, const int64_t* rows, const int64_t* ktab,
+                                            int nt, const int8_t* t_row, const int8_t* t_k, double* dst, int ptid)
+{
+    constexpr int PE = BK * FT / PT;
+    for (int t = 0; t < nt; t++)
+    {
+        const int64_t* rt = rows + t_row[t] * FT;
+        const int64_t* kt = ktab + t_k[t] * BK;
+        const uint32_t base = smem_addr(dst + (size_t)t * BK * FT);
+#pragma unroll
+        for (int e = 0; e < PE; e++)
+        {
+            int kk, r;
+            lane_map<BK, FT>(KFAST, ptid + e * PT, kk, r);
+            const int64_t ro = rt[r], ko = kt[kk];
+            const bool ok = ro != OFF_INVALID && ko != OFF_INVALID;
+            cp_async8(base + (uint32_t)tile_pos(kk, r, FT) * 8, ok ? X + (ro + ko) : X, ok ? 8 : 0);
+        }
+    }
+}
+
+template <bool RAW, bool KA, bool KB>
 __global__ void __launch_bounds__(FTHREADS, 1)
 stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
 {
+    using M = FMode<RAW>;
+    constexpr int BK = M::BK;
     extern __shared__ __align__(128) unsigned char smem[];
     double* ring = reinterpret_cast<double*>(smem);
     int64_t* rowA = reinterpret_cast<int64_t*>(smem + RING_BYTES);
     int64_t* colB = rowA + FHMAX * FT;
     int64_t* rowC = colB + FHMAX * FT;
     int64_t* colC = rowC + FHMAX * FT;
-    int64_t* kA = colC + FHMAX * FT;         // [FHMAX][FBK]
-    int64_t* kB = kA + FHMAX * FBK;
-    FusedCtrl* ctl = reinterpret_cast<FusedCtrl*>(kB + FHMAX * FBK);
+    int64_t* kA = colC + FHMAX * FT;         // [FHMAX][BK]
+    int64_t* kB = kA + FHMAX * BK;           // [FHMAX][BK]
+    FusedCtrl* ctl = reinterpret_cast<FusedCtrl*>(colC + FHMAX * FT + 2 * FHMAX * FBK_MAX);
     volatile int* abort_flag = &ctl->abort;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -195,7 +250,7 @@ stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
 
     const int64_t tiles = (int64_t)a.tiles_m * a.tiles_n;
     const int64_t work = a.batch * tiles;
-    const int64_t nk = (a.ks + FBK - 1) / FBK;
+    const int64_t nk = (a.ks + BK - 1) / BK;
     const int H = a.H;                           // block rows of A and C
     const int Hk = a.Hk > 0 ? a.Hk : a.H;        // block columns of A, rows of B
     const int Hn = a.Hn > 0 ? a.Hn : a.H;        // block columns of B and C
@@ -203,21 +258,23 @@ stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
     if (warp < NPW)
     {
         // ---------------- producer warpgroup ----------------
-        asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" :: "n"(PROD_REGS));
+        asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" :: "n"(M::PROD_REGS));
         const int ptid = tid;
-        // This thread's 2 entries of the k offset tables kA, kB for k-step s:
-        // they depend on the k-step only (not on the product or the tile), so
-        // the next k-step's are loaded while the current one is produced.
-        static_assert(2 * FHMAX * FBK == 2 * PT, "two table entries per producer thread");
+        // This thread's entries of the k offset tables kA, kB for k-step s
+        // (KENT of them): they depend on the k-step only (not on the product or
+        // the tile), so the next k-step's are loaded while the current one is
+        // produced.
         auto ktab_entry = [&](int64_t s, int j) -> int64_t {
             const int i = ptid + j * PT;
-            const int op = i / (FHMAX * FBK), e = i % (FHMAX * FBK);
-            const int h = e / FBK, kk = e % FBK;
-            const int64_t kl = s * FBK + kk, gk = h * a.ks + kl;
+            const int op = i / (FHMAX * BK), e = i % (FHMAX * BK);
+            const int h = e / BK, kk = e % BK;
+            const int64_t kl = s * BK + kk, gk = h * a.ks + kl;
             if (!(h < Hk && kl < a.ks && gk < a.k)) return OFF_INVALID;
             return op == 0 ? a.ksA[gk] : a.ksB[gk];
         };
-        int64_t kv0 = nk > 0 ? ktab_entry(0, 0) : OFF_INVALID, kv1 = nk > 0 ? ktab_entry(0, 1) : OFF_INVALID;
+        int64_t kv[M::KENT];
+#pragma unroll
+        for (int j = 0; j < M::KENT; j++) kv[j] = nk > 0 ? ktab_entry(0, j) : OFF_INVALID;
         uint32_t it = 0;
         bool ok = true;      // this thread's waits so far
         bool stop = false;   // set only right after a collective check, so uniform
@@ -247,13 +304,13 @@ stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
                     // the tile's row tables are complete); a wait that ran out
                     // in any of them ends the loops for all of them.
                     if (bar_any<1, PT>(!ok)) { stop = true; break; }
-                    kA[ptid] = kv0;                  // kA and kB are one array of 2 * PT entries
-                    kA[ptid + PT] = kv1;
+#pragma unroll
+                    for (int j = 0; j < M::KENT; j++) kA[ptid + j * PT] = kv[j];   // kA, kB: one array
                     bar_sync<1, PT>();
                     {
                         const int64_t sn = s + 1 < nk ? s + 1 : 0;
-                        kv0 = ktab_entry(sn, 0);
-                        kv1 = ktab_entry(sn, 1);
+#pragma unroll
+                        for (int j = 0; j < M::KENT; j++) kv[j] = ktab_entry(sn, j);
                     }
                     const uint32_t slot = it % FSTAGES;
                     const uint32_t use = it / FSTAGES;   // earlier uses of this slot
@@ -264,19 +321,32 @@ stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
                         ok = false;
                         continue;
                     }
-                    double* S = ring + slot * SLOT_DOUBLES;
-                    double* T = S + FBK * FT;
-                    produce_tile<KA>(a.A, rowA, kA, P.na, P.a_r, P.a_c, P.a_s, S, ptid);
-                    produce_tile<KB>(a.B, colB, kB, P.nb, P.b_c, P.b_r, P.b_s, T, ptid);
-                    mbar_arrive(smem_addr(&ctl->full[slot]));   // release: the stores above are visible
+                    double* S = ring + slot * M::SLOT_DOUBLES;
+                    double* T = S + M::NT * BK * FT;
+                    if constexpr (RAW)
+                    {
+                        issue_tiles<KA, BK>(a.A, rowA, kA, P.na, P.a_r, P.a_c, S, ptid);
+                        issue_tiles<KB, BK>(a.B, colB, kB, P.nb, P.b_c, P.b_r, T, ptid);
+                        // the slot's full barrier completes when every producer's copies have landed
+                        asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n"
+                                     :: "r"(smem_addr(&ctl->full[slot])) : "memory");
+                    }
+                    else
+                    {
+                        produce_tile<KA, BK>(a.A, rowA, kA, P.na, P.a_r, P.a_c, P.a_s, S, ptid);
+                        produce_tile<KB, BK>(a.B, colB, kB, P.nb, P.b_c, P.b_r, P.b_s, T, ptid);
+                        mbar_arrive(smem_addr(&ctl->full[slot]));   // release: the stores above are visible
+                    }
                 }
             }
         }
+        if constexpr (RAW)
+            asm volatile("cp.async.wait_all;\n" ::: "memory");   // this thread's copies land before it leaves
     }
     else
     {
         // ---------------- consumer warpgroups ----------------
-        asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" :: "n"(CONS_REGS));
+        asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" :: "n"(M::CONS_REGS));
         const int ctid = tid - PT;
         const int cw = warp - NPW;
         const int g = lane >> 2, t4 = lane & 3;
@@ -316,10 +386,17 @@ stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
                     ok = __all_sync(0xffffffffu, mbar_wait(smem_addr(&ctl->full[slot]), (cit / FSTAGES) & 1,
                                                            abort_flag, err, 2, limit));
                     if (!ok) break;
-                    const double* Ab = ring + slot * SLOT_DOUBLES;
-                    const double* Bb = Ab + FBK * FT;
-#pragma unroll 2
-                    for (int k4 = 0; k4 < FBK; k4 += 4)
+                    const double* Ab = ring + slot * M::SLOT_DOUBLES;
+                    const double* Bb = Ab + M::NT * BK * FT;
+                    // RAW mode: the second block of a sum, with its sign
+                    // relative to the first (the first's sign moves to the
+                    // C coefficient, as products' signs multiply)
+                    const DevProduct& Pc = a.prod[p];
+                    const bool a2 = RAW && Pc.na > 1, b2 = RAW && Pc.nb > 1;
+                    const double ra = a2 && (Pc.a_s[1] * Pc.a_s[0] < 0) ? -1.0 : 1.0;
+                    const double rb = b2 && (Pc.b_s[1] * Pc.b_s[0] < 0) ? -1.0 : 1.0;
+#pragma unroll
+                    for (int k4 = 0; k4 < BK; k4 += 4)
                     {
                         const int kr = k4 + t4;
                         const int pg = 2 * ((g + swz_c(kr)) & 7);
@@ -327,14 +404,26 @@ stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
 #pragma unroll
                         for (int mi = 0; mi < MI; mi++)
                         {
-                            const double2 v = *reinterpret_cast<const double2*>(Ab + kr * FT + wm + mi * 16 + pg);
+                            const int pos = kr * FT + wm + mi * 16 + pg;
+                            const double2 v = *reinterpret_cast<const double2*>(Ab + pos);
                             af[mi][0] = v.x; af[mi][1] = v.y;
+                            if (a2)
+                            {
+                                const double2 u = *reinterpret_cast<const double2*>(Ab + BK * FT + pos);
+                                af[mi][0] = fma(ra, u.x, af[mi][0]); af[mi][1] = fma(ra, u.y, af[mi][1]);
+                            }
                         }
 #pragma unroll
                         for (int nj = 0; nj < NI / 2; nj++)
                         {
-                            const double2 v = *reinterpret_cast<const double2*>(Bb + kr * FT + wn + nj * 16 + pg);
+                            const int pos = kr * FT + wn + nj * 16 + pg;
+                            const double2 v = *reinterpret_cast<const double2*>(Bb + pos);
                             bf[2 * nj] = v.x; bf[2 * nj + 1] = v.y;
+                            if (b2)
+                            {
+                                const double2 u = *reinterpret_cast<const double2*>(Bb + BK * FT + pos);
+                                bf[2 * nj] = fma(rb, u.x, bf[2 * nj]); bf[2 * nj + 1] = fma(rb, u.y, bf[2 * nj + 1]);
+                            }
                         }
 #pragma unroll
                         for (int mi = 0; mi < MI; mi++)
@@ -355,7 +444,10 @@ stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
                 {
                     const int64_t* rt = rowC + P.c_r[t] * FT;
                     const int64_t* ct = colC + P.c_c[t] * FT;
-                    const double coef = P.c_s[t] < 0 ? -a.alpha : a.alpha;
+                    // RAW mode formed the sums as A_0 +- A_1 (B likewise): the
+                    // signs of the first blocks multiply into the coefficient
+                    const bool lead_neg = RAW && ((P.a_s[0] < 0) != (P.b_s[0] < 0));
+                    const double coef = ((P.c_s[t] < 0) != lead_neg) ? -a.alpha : a.alpha;
                     const bool first = P.c_first[t] != 0;
                     const bool read_c = !first || a.beta != 0.0;
                     const double cb = first ? a.beta : 1.0;
@@ -393,23 +485,34 @@ stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
 
 }  // namespace
 
-size_t fused_smem_bytes() { return FUSED_SMEM; }
-
 cudaError_t launch_fused(const DmmaArgs& in, cudaStream_t stream, int num_sms, int* err, long long wait_limit)
 {
     if (in.batch <= 0 || in.ms <= 0 || in.ns <= 0) return cudaSuccess;
-    // direct C updates on an H x H grid of up to 4 x 4 blocks only
+    // direct C updates on grids of up to 4 x 4 blocks only
     if (in.H < 1 || in.H > FHMAX || in.Hc != in.H || in.mC != in.m || in.nC != in.n) return cudaErrorNotSupported;
     if (in.Hk < 0 || in.Hk > FHMAX || in.Hn < 0 || in.Hn > FHMAX) return cudaErrorNotSupported;
     if (in.nprod < 1 || in.nprod > MAX_PRODUCTS) return cudaErrorInvalidValue;
-    auto kern = in.a_kfast ? (in.b_kfast ? stra_fused_kernel<true, true> : stra_fused_kernel<true, false>)
-                           : (in.b_kfast ? stra_fused_kernel<false, true> : stra_fused_kernel<false, false>);
+    // RAW mode when every operand sum has at most 2 blocks (L <= 1), else SUM
+    bool raw = true;
+    for (int p = 0; p < in.nprod; p++)
+        if (in.prod[p].na > FMode<true>::NT || in.prod[p].nb > FMode<true>::NT) raw = false;
+    using Kern = void (*)(DmmaArgs, int*, long long);
+    Kern kern;
+    if (raw)
+        kern = in.a_kfast ? (in.b_kfast ? stra_fused_kernel<true, true, true> : stra_fused_kernel<true, true, false>)
+                          : (in.b_kfast ? stra_fused_kernel<true, false, true> : stra_fused_kernel<true, false, false>);
+    else
+        kern = in.a_kfast ? (in.b_kfast ? stra_fused_kernel<false, true, true> : stra_fused_kernel<false, true, false>)
+                          : (in.b_kfast ? stra_fused_kernel<false, false, true> : stra_fused_kernel<false, false, false>);
     // The register split must fit the pool the CTA is launched with.
+    const size_t need = raw ? (size_t)FMode<true>::PROD_REGS * PT + (size_t)FMode<true>::CONS_REGS * CT
+                            : (size_t)FMode<false>::PROD_REGS * PT + (size_t)FMode<false>::CONS_REGS * CT;
     cudaFuncAttributes fa;
-    cudaError_t e = cudaFuncGetAttributes(&fa, kern);
+    cudaError_t e = cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(kern));
     if (e != cudaSuccess) return e;
-    if ((size_t)fa.numRegs * FTHREADS < (size_t)PROD_REGS * PT + (size_t)CONS_REGS * CT) return cudaErrorNotSupported;
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FUSED_SMEM);
+    if ((size_t)fa.numRegs * FTHREADS < need) return cudaErrorNotSupported;
+    e = cudaFuncSetAttribute(reinterpret_cast<const void*>(kern), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)FUSED_SMEM);
     if (e != cudaSuccess) return e;
     DmmaArgs args = in;
     args.tiles_m = (int)((args.ms + FT - 1) / FT);

@@ -56,6 +56,32 @@ def test_wait_timeout_fp64_then_recovery(tsb, cuda, level):
     assert err <= oracle.error_bound(level, 512, np.abs(A).max(), np.abs(B).max())
 
 
+@pytest.mark.parametrize("level", [0, 1, 2])
+def test_wait_timeout_fused_no_workspace_then_recovery(tsb, cuda, level):
+    """The fused no-workspace kernel (raw-block copies at L <= 1, register
+    sums at L = 2): a one-cycle bound, TBLIS_STRA_ERR_TIMEOUT, then a correct
+    call on the same context."""
+    import torch
+    A, B, ref = _problem()
+    dA, dB = _dev(torch, A, cuda), _dev(torch, B, cuda)
+    C = torch.zeros_like(dA)
+    tsb.set_workspace_limit(0)
+    try:
+        tsb.set_wait_limit(1)
+        try:
+            with pytest.raises(tsb.TblisStraError) as ei:
+                tsb.contract(level, 1.0, dA, "ik", dB, "kj", 0.0, C, "ij", drop_in=True)
+            assert ei.value.status == ERR_TIMEOUT
+        finally:
+            tsb.set_wait_limit(0)
+        C.zero_()
+        tsb.contract(level, 1.0, dA, "ik", dB, "kj", 0.0, C, "ij", drop_in=True)
+    finally:
+        tsb.set_workspace_limit(None)
+    err = float(np.abs(C.cpu().numpy() - ref).max())
+    assert err <= oracle.error_bound(level, 512, np.abs(A).max(), np.abs(B).max())
+
+
 @pytest.mark.parametrize("level", [0, 1])
 def test_wait_timeout_split_bf16_then_recovery(tsb, cuda, level):
     import torch
