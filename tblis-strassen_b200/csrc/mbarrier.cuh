@@ -47,15 +47,28 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t addr, uint32_t bytes)
 
 // Bounded wait (at most `limit` clock cycles) for the phase of the given
 // parity; false on timeout or abort.
+//
+// try_wait may suspend the thread for a system-dependent time before it
+// reports an incomplete phase.  With CAP_SUSPEND, a bound shorter than the
+// default caps that suspension at 1 ns, so the bound, not the suspension, is
+// what ends the wait (kernels whose copies can land inside one suspension --
+// cp.async gathers of a few KB -- otherwise never see a short bound run out).
+// Without it the wait keeps the plain form, which costs no registers.
+template <bool CAP_SUSPEND = false>
 __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity, volatile int* abort_flag,
                                           int* err, int code, long long limit)
 {
     const long long start = clock64();
+    const bool short_bound = CAP_SUSPEND && limit < MBAR_WAIT_LIMIT;
     while (true)
     {
         uint32_t done;
-        asm volatile("{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-                     "selp.u32 %0, 1, 0, p;\n}\n" : "=r"(done) : "r"(addr), "r"(parity) : "memory");
+        if (short_bound)
+            asm volatile("{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
+                         "selp.u32 %0, 1, 0, p;\n}\n" : "=r"(done) : "r"(addr), "r"(parity), "r"(1u) : "memory");
+        else
+            asm volatile("{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                         "selp.u32 %0, 1, 0, p;\n}\n" : "=r"(done) : "r"(addr), "r"(parity) : "memory");
         if (done) return true;
         if (*abort_flag) return false;
         if (clock64() - start > limit)
