@@ -48,12 +48,13 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t addr, uint32_t bytes)
 // Bounded wait (at most `limit` clock cycles) for the phase of the given
 // parity; false on timeout or abort.
 //
-// try_wait may suspend the thread for a system-dependent time before it
-// reports an incomplete phase.  With CAP_SUSPEND, a bound shorter than the
-// default caps that suspension at 1 ns, so the bound, not the suspension, is
-// what ends the wait (kernels whose copies can land inside one suspension --
-// cp.async gathers of a few KB -- otherwise never see a short bound run out).
-// Without it the wait keeps the plain form, which costs no registers.
+// try_wait may suspend the thread inside the instruction until the phase
+// completes or a system-dependent time runs out, so a bound shorter than that
+// time may never be seen to run out.  With CAP_SUSPEND, a bound shorter than
+// the default polls with test_wait instead, which never suspends, so the bound
+// is what ends the wait (the fused kernel, whose waits are all shorter than
+// one such suspension, relies on this for its timeout path).  Without it the
+// wait keeps the plain form, which costs no registers.
 template <bool CAP_SUSPEND = false>
 __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity, volatile int* abort_flag,
                                           int* err, int code, long long limit)
@@ -64,8 +65,8 @@ __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity, volati
     {
         uint32_t done;
         if (short_bound)
-            asm volatile("{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
-                         "selp.u32 %0, 1, 0, p;\n}\n" : "=r"(done) : "r"(addr), "r"(parity), "r"(1u) : "memory");
+            asm volatile("{\n.reg .pred p;\nmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                         "selp.u32 %0, 1, 0, p;\n}\n" : "=r"(done) : "r"(addr), "r"(parity) : "memory");
         else
             asm volatile("{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
                          "selp.u32 %0, 1, 0, p;\n}\n" : "=r"(done) : "r"(addr), "r"(parity) : "memory");
