@@ -302,6 +302,25 @@ int tblis_stra_plan_query(const tblis_tensor* A, const label_type* idx_A,
                           int64_t* ksA, int64_t* ksB,
                           int64_t* bA, int64_t* bB, int64_t* bC);
 
+/* Which no-workspace ABC kernel a contraction at Strassen level `level` gets
+ * (host only; no counterpart in the reference).  *pairs = 1 when the
+ * element-pair form applies: the unit-stride mode of A and of B is a
+ * contracted mode, so the kernel stages tiles as contiguous 16-byte pairs (by
+ * cp.async, or by tensor-map copies where the tiles are boxes) in a layout
+ * whose DMMA fragment reads are conflict-free; 0 when it gathers tiles
+ * element by element through the scatter vectors.  `tables` (may be NULL;
+ * 265 ints) receives the plan: the bank-conflict count of the consumers'
+ * reads (0 = none), the producer (1 pair copies, 0 tensor maps), the
+ * tensor-map ranks of A and B, 1 when B is read in 16-byte pairs, the swizzle
+ * spans of A and B (bytes, 0 = none), the slot k bit each pair spans in A and
+ * B, the per-lane read offsets aoff[32][2] and boff[32][4] (doubles), the
+ * fragment row and column permutations sigA[8] and sigB[8], the unswizzled
+ * row positions of the slot's 16 k in A's and B's tiles, and the 8 pair
+ * bases of A and of B in copy order. */
+int tblis_stra_fused_pairs_query(int level, const tblis_tensor* A, const label_type* idx_A,
+                                 const tblis_tensor* B, const label_type* idx_B,
+                                 const tblis_tensor* C, const label_type* idx_C, int* pairs, int* tables);
+
 /* Contraction that allocates no device memory (no counterpart in the
  * reference, which allocates host workspace freely).  For callers that cannot
  * call cudaMalloc: an application whose own pool has reserved the whole
@@ -394,7 +413,9 @@ void tblis_stra_batch_destroy(tblis_stra_batch batch);
  * times whole calls with omp_get_wtime, test/test_strassen.cxx:74-95).  With
  * timing on, every kernel launch is bracketed by CUDA events on its stream;
  * tblis_stra_kernel_timing() waits for them and returns, for one kernel kind
- * (0 fused DMMA, 1 pack, 2 packed DMMA GEMM, 3 elementwise helpers), the number
+ * (0 fused DMMA with gathered tiles, 1 pack, 2 packed DMMA GEMM, 3 elementwise
+ * helpers, 4 split-BF16 GEMM, 5 fused DMMA with tensor-map tile copies, 6 fused
+ * DMMA with 16-byte pair copies), the number
  * of launches and their summed time since timing was (re)enabled.
  * tblis_stra_set_kernel_timing() also clears the records. */
 int tblis_stra_set_kernel_timing(int on);

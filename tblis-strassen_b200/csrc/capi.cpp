@@ -481,7 +481,7 @@ int run_fp64(int level, int impl, const GemmView& g, const DevPlan& t,
             TSB_CUDA(cudaMemsetAsync(ferr.p, 0, sizeof(int), st));
             err = static_cast<int*>(ferr.p);
         }
-        cudaError_t e = launch_fused(a, st, sms, err, wait_limit_cycles());
+        cudaError_t e = launch_fused(a, st, sms, err, wait_limit_cycles(), &g);
         if (e == cudaErrorNotSupported)
         {
             if (tab.Hk != H || tab.Hn != H) return TBLIS_STRA_ERR_UNSUPPORTED;   // square grids only there
@@ -2290,6 +2290,25 @@ int tblis_stra_plan_query(const tblis_tensor* A, const label_type* idx_A,
     };
     cp(rsA, g.rsA); cp(rsC, g.rsC); cp(csB, g.csB); cp(csC, g.csC);
     cp(ksA, g.ksA); cp(ksB, g.ksB); cp(bA, g.bA); cp(bB, g.bB); cp(bC, g.bC);
+    return TBLIS_STRA_SUCCESS;
+}
+
+int tblis_stra_fused_pairs_query(int level, const tblis_tensor* A, const label_type* idx_A,
+                                 const tblis_tensor* B, const label_type* idx_B,
+                                 const tblis_tensor* C, const label_type* idx_C, int* pairs, int* tables)
+{
+    if (level < 0 || level > 2) return TBLIS_STRA_ERR_ARG;
+    if (!pairs) return TBLIS_STRA_ERR_NULL;
+    tsb::GemmView g;
+    int s = tsb::plan_contraction(A, idx_A, B, idx_B, C, idx_C, g, false);
+    if (s) return s;
+    const tsb::ProductTable& tab = tsb::product_table(level);
+    bool sums_of_two = true;
+    for (const tsb::Product& p : tab.prod)
+        if (p.na > 2 || p.nb > 2) sums_of_two = false;
+    const int64_t ms = (g.m + tab.H - 1) / tab.H, ns = (g.n + tab.Hn - 1) / tab.Hn,
+                  ks = (g.k + tab.Hk - 1) / tab.Hk;
+    *pairs = sums_of_two && tsb::fused_pairs_plan(g, tab.H, tab.Hn, tab.Hk, ms, ns, ks, tables) ? 1 : 0;
     return TBLIS_STRA_SUCCESS;
 }
 

@@ -40,7 +40,7 @@
 // leave their loops at the next tile (a collective OR over each role's named
 // barrier); RAW-mode producers then let their own copies land before the CTA
 // ends.
-#include "kernels.cuh"
+#include "fused_common.cuh"
 #include "mbarrier.cuh"
 #include "tile_layout.cuh"
 #include "timing.hpp"
@@ -53,17 +53,8 @@ extern std::atomic<unsigned long long> g_launches;
 
 namespace {
 
-constexpr int FT = 128;                  // tile rows (A side) and columns (B side)
-constexpr int FSTAGES = 3;
-constexpr int FHMAX = 4;                 // largest block grid side (level 2)
-constexpr int NPW = 4;                   // producer warps (one warpgroup)
-constexpr int NCW = 8;                   // consumer warps: 2 (M) x 4 (N)
-constexpr int FTHREADS = 32 * (NPW + NCW);
-constexpr int PT = 32 * NPW;             // producer threads
-constexpr int CT = 32 * NCW;             // consumer threads
-constexpr int CWM = 2, CWN = 4;
-constexpr int WTM = FT / CWM, WTN = FT / CWN;   // 64 x 32 warp tile
-constexpr int MI = WTM / 16, NI = WTN / 8;      // 4 x 4 fragments
+using namespace fused;
+
 constexpr int FBK_MAX = 32;
 constexpr int PCH = 16;                  // SUM mode: producer elements per batch of loads
 
@@ -85,12 +76,6 @@ struct FMode
     static_assert(RAW || PE % PCH == 0, "producer batches cover a block");
 };
 
-struct FusedCtrl
-{
-    uint64_t full[FSTAGES], empty[FSTAGES];
-    int abort;
-};
-
 constexpr size_t RING_BYTES = FSTAGES * size_t(FBK_MAX) * FT * 2 * 8;   // either mode's 3 slots
 static_assert(FSTAGES * FMode<true>::SLOT_DOUBLES * 8 == RING_BYTES &&
               FSTAGES * FMode<false>::SLOT_DOUBLES * 8 == RING_BYTES, "both modes fill the ring");
@@ -98,43 +83,6 @@ constexpr size_t TAB_BYTES = size_t(4) * FHMAX * FT * 8                 // rowA,
                              + size_t(2) * FHMAX * FBK_MAX * 8;         // k tables of A and B
 constexpr size_t FUSED_SMEM = RING_BYTES + TAB_BYTES + sizeof(FusedCtrl);
 static_assert(FUSED_SMEM <= 227 * 1024, "shared memory budget");
-
-__device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, double b0)
-{
-    asm("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 "
-        "{%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
-        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
-        : "d"(a0), "d"(a1), "d"(b0));
-}
-
-// Named barrier `id` over `count` threads with an OR over `flag`.
-template <int ID, int COUNT>
-__device__ __forceinline__ bool bar_any(bool flag)
-{
-    uint32_t out;
-    asm volatile("{\n.reg .pred q, p;\nsetp.ne.u32 q, %1, 0;\nbar.red.or.pred p, %2, %3, q;\n"
-                 "selp.u32 %0, 1, 0, p;\n}\n" : "=r"(out) : "r"((uint32_t)flag), "n"(ID), "n"(COUNT) : "memory");
-    return out != 0;
-}
-
-template <int ID, int COUNT>
-__device__ __forceinline__ void bar_sync()
-{
-    asm volatile("bar.sync %0, %1;\n" :: "n"(ID), "n"(COUNT) : "memory");
-}
-
-__device__ __forceinline__ void decode_work(const DmmaArgs& a, int64_t w, int64_t& b, int64_t& tm, int64_t& tn)
-{
-    const int64_t tiles = (int64_t)a.tiles_m * a.tiles_n;
-    b = w / tiles;
-    const int64_t tw = w - b * tiles;
-    const int64_t GROUP = 8;
-    const int64_t group = tw / (GROUP * a.tiles_n);
-    const int64_t first_m = group * GROUP;
-    const int64_t gsize = (a.tiles_m - first_m) < GROUP ? (a.tiles_m - first_m) : GROUP;
-    tm = first_m + (tw % gsize);
-    tn = (tw % (GROUP * a.tiles_n)) / gsize;
-}
 
 // SUM mode: one operand sum of one ring slot: X(r, k) = sum_t sign_t * X[row_t(r) + k_t(k)]
 // over the terms of the product's sum, stored at tile_pos(k, r).  `rows` is
@@ -359,15 +307,7 @@ stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
             if (bar_any<2, CT>(!ok)) break;
             int64_t b, tm, tn;
             decode_work(a, w, b, tm, tn);
-            const int64_t offC = a.bC[b];
-            for (int i = ctid; i < FHMAX * FT; i += CT)
-            {
-                const int h = i / FT, r = i % FT;
-                const int64_t li = tm * FT + r, gi = h * a.ms + li;
-                rowC[i] = (h < H && li < a.ms && gi < a.m) ? offC + a.rsC[gi] : OFF_INVALID;
-                const int64_t lj = tn * FT + r, gj = h * a.ns + lj;
-                colC[i] = (h < Hn && lj < a.ns && gj < a.n) ? a.csC[gj] : OFF_INVALID;
-            }
+            fill_c_tables(a, b, tm, tn, rowC, colC, ctid);
             bar_sync<2, CT>();
 
             for (int p = 0; p < a.nprod && ok; p++)
@@ -438,46 +378,12 @@ stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
                 if (!ok) break;
 
                 // C_t = (first ? beta*C_t : C_t) + sign_t*alpha*S*T for the
-                // product's C blocks t; loads of a row pair before its stores.
+                // product's C blocks t.  RAW mode formed the sums as
+                // A_0 +- A_1 (B likewise): the signs of the first blocks
+                // multiply into the coefficient.
                 const DevProduct& P = a.prod[p];
-                for (int t = 0; t < P.nc; t++)
-                {
-                    const int64_t* rt = rowC + P.c_r[t] * FT;
-                    const int64_t* ct = colC + P.c_c[t] * FT;
-                    // RAW mode formed the sums as A_0 +- A_1 (B likewise): the
-                    // signs of the first blocks multiply into the coefficient
-                    const bool lead_neg = RAW && ((P.a_s[0] < 0) != (P.b_s[0] < 0));
-                    const double coef = ((P.c_s[t] < 0) != lead_neg) ? -a.alpha : a.alpha;
-                    const bool first = P.c_first[t] != 0;
-                    const bool read_c = !first || a.beta != 0.0;
-                    const double cb = first ? a.beta : 1.0;
-#pragma unroll
-                    for (int mi = 0; mi < MI; mi++)
-#pragma unroll
-                        for (int hr = 0; hr < 2; hr++)
-                        {
-                            const int64_t ro = rt[wm + mi * 16 + g + hr * 8];
-                            if (ro == OFF_INVALID) continue;
-                            double cv[NI][2];
-#pragma unroll
-                            for (int ni = 0; ni < NI; ni++)
-#pragma unroll
-                                for (int hc = 0; hc < 2; hc++)
-                                {
-                                    const int64_t co = ct[wn + ni * 8 + t4 * 2 + hc];
-                                    cv[ni][hc] = (read_c && co != OFF_INVALID) ? a.C[ro + co] : 0.0;
-                                }
-#pragma unroll
-                            for (int ni = 0; ni < NI; ni++)
-#pragma unroll
-                                for (int hc = 0; hc < 2; hc++)
-                                {
-                                    const int64_t co = ct[wn + ni * 8 + t4 * 2 + hc];
-                                    if (co == OFF_INVALID) continue;
-                                    a.C[ro + co] = coef * acc[mi][ni][hr * 2 + hc] + cb * cv[ni][hc];
-                                }
-                        }
-                }
+                const bool lead_neg = RAW && ((P.a_s[0] < 0) != (P.b_s[0] < 0));
+                product_epilogue(a, P, lead_neg, rowC, colC, acc, wm, wn, g, 2 * t4, 2 * t4 + 1);
             }
         }
     }
@@ -485,9 +391,15 @@ stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
 
 }  // namespace
 
-cudaError_t launch_fused(const DmmaArgs& in, cudaStream_t stream, int num_sms, int* err, long long wait_limit)
+cudaError_t launch_fused(const DmmaArgs& in, cudaStream_t stream, int num_sms, int* err, long long wait_limit,
+                         const GemmView* g)
 {
     if (in.batch <= 0 || in.ms <= 0 || in.ns <= 0) return cudaSuccess;
+    if (g)
+    {
+        const cudaError_t e = launch_fused_pairs(in, *g, stream, num_sms, err, wait_limit);
+        if (e != cudaErrorNotSupported) return e;
+    }
     // direct C updates on grids of up to 4 x 4 blocks only
     if (in.H < 1 || in.H > FHMAX || in.Hc != in.H || in.mC != in.m || in.nC != in.n) return cudaErrorNotSupported;
     if (in.Hk < 0 || in.Hk > FHMAX || in.Hn < 0 || in.Hn > FHMAX) return cudaErrorNotSupported;

@@ -344,8 +344,28 @@ void dmma_tile_shape(int terms, int H, int Hc, int config, int* bm, int* bn);
 // once per staged tile (fused_kernel.cu): C updated directly (Hc == H,
 // mC == m, nC == n), H <= 4.  cudaErrorNotSupported when it cannot run
 // these arguments (the caller then uses launch_dmma).  `err` (may be null)
-// is set when a bounded wait runs out; wait_limit as PackedGemmArgs.
-cudaError_t launch_fused(const DmmaArgs& args, cudaStream_t stream, int num_sms, int* err, long long wait_limit);
+// is set when a bounded wait runs out; wait_limit as PackedGemmArgs.  With
+// the contraction's plan `g`, the element-pair form (fused_pairs.cu) runs
+// where its conditions hold, the gather form elsewhere.
+struct GemmView;
+cudaError_t launch_fused(const DmmaArgs& args, cudaStream_t stream, int num_sms, int* err, long long wait_limit,
+                         const GemmView* g = nullptr);
+// The element-pair form alone; cudaErrorNotSupported when its conditions do
+// not hold (fused_pairs.cu lists them).
+cudaError_t launch_fused_pairs(const DmmaArgs& args, const GemmView& g, cudaStream_t stream, int num_sms, int* err,
+                               long long wait_limit);
+// Whether the element-pair form applies to a plan cut into an H x Hk (A),
+// Hk x Hn (B) grid of blocks of extents ms, ns, ks (host only).  `tables`
+// (may be null; PAIRS_PLAN_INTS entries) receives: the bank-conflict count of
+// the consumers' reads, the producer (0 tensor-map boxes, 1 16-byte pair
+// copies), the tensor-map ranks of A and B (0 for pair copies), 1 when B is
+// read in pairs, the swizzle spans of A and B, the pair bits of A and B, then
+// the lane offsets aoff[32][2], boff[32][4], sigA[8], sigB[8], the
+// unswizzled row positions of the slot's 16 k in A's and B's tiles, and the
+// pair bases of A and B in copy order.
+constexpr int PAIRS_PLAN_INTS = 9 + 64 + 128 + 8 + 8 + 16 + 16 + 8 + 8;
+bool fused_pairs_plan(const GemmView& g, int H, int Hn, int Hk, int64_t ms, int64_t ns, int64_t ks,
+                      int tables[PAIRS_PLAN_INTS]);
 cudaError_t launch_dmma_grouped(const DmmaGroupArgs& g, int terms, int H, int Hc, int config,
                                 cudaStream_t stream, int num_sms);
 cudaError_t launch_scale(const ScaleArgs& args, cudaStream_t stream);

@@ -220,7 +220,7 @@ int noalloc_mult(int level, const tblis_tensor* A, const label_type* idx_A,
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         // No error flag (it would need memory): a bounded wait that runs out
         // still ends the kernel cleanly.
-        cudaError_t e = launch_fused(a, st, sms, nullptr, 0);
+        cudaError_t e = launch_fused(a, st, sms, nullptr, 0, &g);
         if (e == cudaErrorNotSupported)
         {
             if (tab.Hk != H || tab.Hn != H) return TBLIS_STRA_ERR_UNSUPPORTED;

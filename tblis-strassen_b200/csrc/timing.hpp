@@ -16,7 +16,9 @@ enum KernelKind
     KK_PACKED_GEMM = 2,  // packed_gemm_kernel
     KK_AUX = 3,          // scale / sum-gather / scatter-add
     KK_SPLIT_GEMM = 4,   // split_gemm_kernel (tcgen05, FP32 via bf16 planes)
-    KK_COUNT = 5
+    KK_FUSED_TMA = 5,    // stra_fused_pair_kernel, tensor-map producer
+    KK_FUSED_PAIRS = 6,  // stra_fused_pair_kernel, 16-byte pair-copy producer
+    KK_COUNT = 7
 };
 
 bool timing_enabled();

@@ -116,6 +116,9 @@ def _load() -> ctypes.CDLL:
     P64 = ctypes.POINTER(ctypes.c_int64)
     lib.tblis_stra_plan_query.argtypes = [T, S, T, S, T, S, P64, ctypes.POINTER(ctypes.c_double)] + [P64] * 9
     lib.tblis_stra_plan_query.restype = ctypes.c_int
+    lib.tblis_stra_fused_pairs_query.argtypes = [ctypes.c_int, T, S, T, S, T, S, ctypes.POINTER(ctypes.c_int),
+                                                 ctypes.POINTER(ctypes.c_int)]
+    lib.tblis_stra_fused_pairs_query.restype = ctypes.c_int
     lib.tblis_stra_set_workspace_limit.argtypes = [ctypes.c_size_t]
     lib.tblis_stra_set_workspace_limit.restype = ctypes.c_int
     lib.tblis_stra_get_workspace_limit.restype = ctypes.c_size_t
@@ -399,7 +402,8 @@ class Batch:
             pass
 
 
-KERNEL_KINDS = {"fused": 0, "pack": 1, "packed_gemm": 2, "aux": 3, "split_gemm": 4}
+KERNEL_KINDS = {"fused": 0, "pack": 1, "packed_gemm": 2, "aux": 3, "split_gemm": 4, "fused_tma": 5,
+                "fused_pairs": 6}
 
 
 ALGORITHMS = {"strassen": 0, "classical222": 1, "strassen322": 2, "strassen232": 3, "strassen223": 4}
@@ -563,6 +567,37 @@ def plan_query(A, idx_A, B, idx_B, C, idx_C, scatter: bool = True):
                                          ctypes.byref(vc2.t), ic, sizes, ab, *ptrs))
         for nm, a, L in zip(names, arrs, lens):
             out[nm] = a[:L]
+    return out
+
+
+def fused_pairs_query(level, A, idx_A, B, idx_B, C, idx_C):
+    """How the no-workspace ABC kernel stages this contraction's tiles at
+    `level` (host only, no GPU needed): a dict with ``pairs`` (bool: the
+    element-pair form applies; otherwise the gather form runs) and its plan:
+    ``producer`` ("pairs": 16-byte copies of contiguous k pairs; "tma":
+    tensor-map boxes), ``conflicts`` (bank conflicts of the consumers' reads,
+    0 = none), ``rank_A``, ``rank_B`` (tensor-map ranks, 0 for pair copies),
+    ``b_pairs`` (B read in 16-byte pairs), ``swz_A``, ``swz_B`` (swizzle
+    spans in bytes, 0 = none), ``bit_A``, ``bit_B`` (the slot k bit each
+    16-byte pair spans), the per-lane read offsets ``aoff`` (32 x 2) and
+    ``boff`` (32 x 4) in doubles, the fragment permutations ``sigA``,
+    ``sigB``, the unswizzled row positions ``koffA``, ``koffB`` of the
+    slot's 16 k and the pair bases ``pbaseA``, ``pbaseB`` in copy order."""
+    va, vb, vc = _View(A, 1.0), _View(B, 1.0), _View(C, 0.0)
+    ia, ib, ic = _labels(idx_A, va.t.ndim), _labels(idx_B, vb.t.ndim), _labels(idx_C, vc.t.ndim)
+    ok = ctypes.c_int(0)
+    tab = (ctypes.c_int * 265)()
+    _check(lib.tblis_stra_fused_pairs_query(level, ctypes.byref(va.t), ia, ctypes.byref(vb.t), ib,
+                                            ctypes.byref(vc.t), ic, ctypes.byref(ok), tab))
+    t = list(tab)
+    out = {"pairs": bool(ok.value)}
+    if out["pairs"]:
+        out.update(conflicts=t[0], producer=("tma", "pairs")[t[1]], rank_A=t[2], rank_B=t[3],
+                   b_pairs=bool(t[4]), swz_A=t[5], swz_B=t[6], bit_A=t[7], bit_B=t[8],
+                   aoff=[t[9 + 2 * i:11 + 2 * i] for i in range(32)],
+                   boff=[t[73 + 4 * i:77 + 4 * i] for i in range(32)],
+                   sigA=t[201:209], sigB=t[209:217], koffA=t[217:233], koffB=t[233:249],
+                   pbaseA=t[249:257], pbaseB=t[257:265])
     return out
 
 

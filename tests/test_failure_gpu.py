@@ -1,6 +1,7 @@
 """Failure detection on the GPU, in forms that fault, trap or hang nothing.
 
-* Bounded waits: the warp-specialised kernels (packed FP64 GEMM, split-BF16
+* Bounded waits: the warp-specialised kernels (packed FP64 GEMM, the fused
+  no-workspace kernels in their gather and element-pair forms, split-BF16
   tcgen05 GEMM) bound every pipeline wait.  A test shortens the bound to one
   SM clock cycle (tblis_stra_set_wait_limit), so the first wait whose copy or
   MMA has not landed yet runs out; the kernel then stops issuing work, lets
@@ -77,6 +78,36 @@ def test_wait_timeout_fused_no_workspace_then_recovery(tsb, cuda, level):
         C.zero_()
         tsb.contract(level, 1.0, dA, "ik", dB, "kj", 0.0, C, "ij", drop_in=True)
     finally:
+        tsb.set_workspace_limit(None)
+    err = float(np.abs(C.cpu().numpy() - ref).max())
+    assert err <= oracle.error_bound(level, 512, np.abs(A).max(), np.abs(B).max())
+
+
+@pytest.mark.parametrize("level", [0, 1])
+def test_wait_timeout_pair_kernel_then_recovery(tsb, cuda, level):
+    """The element-pair form of the no-workspace kernel (A stored k-major, so
+    its k pairs are contiguous): a one-cycle bound, TBLIS_STRA_ERR_TIMEOUT,
+    then a correct call on the same context."""
+    import torch
+    A, B, ref = _problem()
+    At = np.asfortranarray(A.T)              # A(k, i): k contiguous
+    dA, dB = _dev(torch, At, cuda), _dev(torch, B, cuda)
+    C = torch.zeros((512, 512), dtype=torch.float64, device=cuda).t().contiguous().t()
+    tsb.set_workspace_limit(0)
+    tsb.set_kernel_timing(True)
+    try:
+        tsb.set_wait_limit(1)
+        try:
+            with pytest.raises(tsb.TblisStraError) as ei:
+                tsb.contract(level, 1.0, dA, "ki", dB, "kj", 0.0, C, "ij", drop_in=True)
+            assert ei.value.status == ERR_TIMEOUT
+        finally:
+            tsb.set_wait_limit(0)
+        C.zero_()
+        tsb.contract(level, 1.0, dA, "ki", dB, "kj", 0.0, C, "ij", drop_in=True)
+        assert tsb.kernel_timing("fused_pairs")[0] == 2
+    finally:
+        tsb.set_kernel_timing(False)
         tsb.set_workspace_limit(None)
     err = float(np.abs(C.cpu().numpy() - ref).max())
     assert err <= oracle.error_bound(level, 512, np.abs(A).max(), np.abs(B).max())
