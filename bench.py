@@ -487,7 +487,8 @@ def kernel_probe(args):
         t.record()
         t.synchronize()
         ms = s.elapsed_time(t)
-        parts = {k: tsb.kernel_timing(k) for k in ("fused", "pack", "packed_gemm", "aux", "split_gemm")}
+        parts = {k: tsb.kernel_timing(k) for k in ("fused", "fused_pairs", "fused_tma", "pack", "packed_gemm", "aux",
+                                                   "split_gemm")}
         tsb.set_kernel_timing(False)
         print("   kernels: " + ", ".join(f"{k} {n}x {v:.2f} ms" for k, (n, v) in parts.items() if n))
         print(f"L{lv} impl{args.variant} {args.dtype}{'/' + str(args.terms) + ' terms' if args.dtype == 'f32' else ''} "
@@ -646,17 +647,26 @@ def main():
         levels[f"L{lv}"] = flops * max(2, args.steps // 2) / tl / 1e12
 
     # ---- the no-workspace ABC kernel (all products in one persistent launch,
-    #      operand sums formed per staged tile), through the regular call with
-    #      no workspace allowed and through the allocation-free entry point
+    #      operand sums formed in the consumers from the staged raw blocks),
+    #      through the regular call with no workspace allowed (at this level
+    #      and at L=0) and through the allocation-free entry point
     no_workspace = {}
     tsb.set_workspace_limit(0)
     try:
-        for _ in range(2):
-            step()
-        barrier_sync()
         nw = max(2, args.steps // 4)
-        tf = max_over_ranks(time_steps(torch, step, nw, stream))
-        no_workspace[f"L{args.level}_workspace0"] = flops * nw / tf / 1e12
+        for lv in sorted({0, args.level}):
+            for _ in range(2):
+                step(lv, 1)
+            barrier_sync()
+            tsb.set_kernel_timing(True)
+            tf = max_over_ranks(time_steps(torch, lambda: step(lv, 1), nw, stream))
+            ran = [k for k in ("fused", "fused_pairs", "fused_tma") if tsb.kernel_timing(k)[0] > 0]
+            tsb.set_kernel_timing(False)
+            no_workspace[f"L{lv}_workspace0"] = flops * nw / tf / 1e12
+            no_workspace[f"L{lv}_kernel"] = {"fused": "stra_fused_kernel (gathers)",
+                                              "fused_pairs": "stra_fused_pair_kernel (16-byte pair copies)",
+                                              "fused_tma": "stra_fused_pair_kernel (tensor-map boxes)"}.get(
+                                                  ran[0] if ran else "", "none")
     finally:
         tsb.set_workspace_limit(None)
     noalloc = tsb.noalloc_mult

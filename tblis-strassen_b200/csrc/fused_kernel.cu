@@ -29,11 +29,13 @@
 //     arrives on its "empty" mbarrier; after the last k-step of a product the
 //     epilogue adds +-alpha*S*T into the product's C blocks.
 //
-// Measured at 16384^3 (no-workspace calls): RAW L=0 29.7, L=1 19.8 effective
-// TFLOP/s, against 12.6 at L=1 for the SUM mode, whose register-held gathers
-// are latency-bound; both modes are bound by the element-wise gathers through
-// the scatter vectors (8-byte requests to L2), which the packed schedule
-// turns into 32 KB bulk copies by packing the sums once in HBM.
+// Measured at 16384^3 (no-workspace calls, effective TFLOP/s): RAW L=0 33.1,
+// L=1 19.8 on the headline contraction's layout (30.9 at L=1 on k-major GEMM
+// operands), SUM L=2 10.1; both modes are bound by the element-wise gathers
+// through the scatter vectors (8-byte requests to L2).  Where the unit-stride
+// modes of A and B are contracted modes, the element-pair form
+// (fused_pairs.cu: 16-byte pair copies or tensor-map boxes into a planned
+// conflict-free layout) runs instead: 33.3 and 32.2 at L=0 and L=1 there.
 //
 // The producer runs up to 3 k-steps ahead, across product and tile
 // boundaries.  Every wait is bounded; a wait that runs out makes both roles

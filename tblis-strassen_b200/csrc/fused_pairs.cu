@@ -12,15 +12,17 @@
 // loads along that mode (src/stra_nodes/stra_packm.hpp:367-683).
 //
 // Two producers fill the same layout (the host picks one):
-//   PAIRS: the producer warpgroup copies each k pair of the unit-stride mode
-//     (two consecutive doubles) with one 16-byte cp.async, addressed through
-//     the row and k offset tables of the tile (any row layout, ragged blocks
-//     included: entries past the extents read as zero); the slot's "full"
-//     mbarrier completes when the copies land.
-//   TMA: one thread copies each block tile as one tensor-map box
-//     (cp.async.bulk.tensor), where the tile is a box of the operand (each
-//     row and k mode's extent divides the tile or is a multiple of it, at
-//     most 5 dimensions, unit-stride k mode at dimension 0).
+//   TMA: where every tile is a box of its operand whose rows are one
+//     128-byte run of the unit-stride k mode (each row and k mode's extent
+//     divides the tile or is a multiple of it, at most 5 dimensions, the
+//     unit-stride k mode at dimension 0), four lanes of one producer warp
+//     copy the product's (up to 2 + 2) block tiles, one tensor-map box
+//     (cp.async.bulk.tensor) each, on the slot's "full" mbarrier;
+//   PAIRS: elsewhere, the producer warpgroup copies each k pair of the
+//     unit-stride mode (two consecutive doubles) with one 16-byte cp.async,
+//     addressed through the row and k offset tables of the tile (any row
+//     layout, ragged blocks included: entries past the extents read as
+//     zero); the slot's "full" mbarrier completes when the copies land.
 // Layout of one 128 x 16 tile (16 KB): row r at 16 r doubles; inside a row,
 // the 16 k in the order of a bit permutation of the slot's k index that puts
 // the pair bit at position 0; then the 16-byte chunks of every 128-byte row
@@ -135,7 +137,7 @@ __device__ __forceinline__ void box_coords(const TmaCoords& co, int64_t row, int
             int64_t x = 0;
             for (int p = 0; p < co.nparts[d]; p++)
             {
-                int64_t y = v / co.div[d][p];
+                int64_t y = co.div[d][p] == 1 ? v : v / co.div[d][p];
                 if (co.mod[d][p]) y %= co.mod[d][p];
                 x += y * co.mult[d][p];
             }
@@ -243,8 +245,15 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
         asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" :: "n"(Regs<PROD>::PROD_REGS));
         if constexpr (PROD == PROD_TMA)
         {
-            // ---------------- producer: one thread issues the boxes ----------------
-            if (tid != 0) return;
+            // ---------------- producer warp 0: lanes issue the boxes ----------------
+            // Lane 0 waits for the slot and posts its byte count; then lanes
+            // 0 and 1 copy the A blocks of the product's sum, lanes 2 and 3 the
+            // B blocks, each computing its own box coordinates.
+            if (warp != 0) return;
+            if (lane == 0)
+                for (int m = 0; m < 2; m++)
+                    asm volatile("prefetch.tensormap [%0];\n" :: "l"(reinterpret_cast<unsigned long long>(&tp.map[m]))
+                                 : "memory");
             uint32_t it = 0;
             bool ok = true;
             for (int64_t w = blockIdx.x; w < work && ok; w += gridDim.x)
@@ -257,36 +266,40 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
                     for (int64_t s = 0; s < nk; s++)
                     {
                         const uint32_t slot = it % FSTAGES, use = it / FSTAGES;
-                        if (use > 0 && !mbar_wait<true>(smem_addr(&ctl->empty[slot]), (use & 1) ^ 1, abort_flag,
-                                                        err, 1, limit))
-                        {
-                            ok = false;
-                            break;
-                        }
+                        bool got = true;
+                        if (lane == 0 && use > 0)
+                            got = mbar_wait<true>(smem_addr(&ctl->empty[slot]), (use & 1) ^ 1, abort_flag, err, 1, limit);
+                        ok = __shfl_sync(0xffffffffu, got, 0);
+                        if (!ok) break;
                         it++;
                         const uint32_t full = smem_addr(&ctl->full[slot]);
-                        mbar_expect_tx(full, (uint32_t)((P.na + P.nb) * BOX_DOUBLES * 8));
+                        if (lane == 0) mbar_expect_tx(full, (uint32_t)((P.na + P.nb) * BOX_DOUBLES * 8));
+                        __syncwarp();
                         double* S = ring + slot * TSLOT_DOUBLES;
-                        double* T = S + TNT * BOX_DOUBLES;
                         int c[5];
-                        for (int t = 0; t < P.na; t++)
+                        if (lane < P.na)
                         {
-                            box_coords(tp.co[0], P.a_r[t] * a.ms + tm * FT, P.a_c[t] * a.ks + s * TBK, b, c);
-                            tma_box(smem_addr(S + t * BOX_DOUBLES), &tp.map[0], c, tp.co[0].ndim, full);
+                            box_coords(tp.co[0], P.a_r[lane] * a.ms + tm * FT, P.a_c[lane] * a.ks + s * TBK, b, c);
+                            tma_box(smem_addr(S + lane * BOX_DOUBLES), &tp.map[0], c, tp.co[0].ndim, full);
                         }
-                        for (int t = 0; t < P.nb; t++)
+                        else if (lane >= TNT && lane - TNT < P.nb)
                         {
+                            const int t = lane - TNT;
                             box_coords(tp.co[1], P.b_c[t] * a.ns + tn * FT, P.b_r[t] * a.ks + s * TBK, b, c);
-                            tma_box(smem_addr(T + t * BOX_DOUBLES), &tp.map[1], c, tp.co[1].ndim, full);
+                            tma_box(smem_addr(S + (TNT + t) * BOX_DOUBLES), &tp.map[1], c, tp.co[1].ndim, full);
                         }
                     }
                 }
             }
             // Copies in flight land before the CTA leaves: bounded waits on
             // the last uses of the slots.
-            volatile int never = 0;
-            for (uint32_t i = it > (uint32_t)FSTAGES ? it - FSTAGES : 0; i < it; i++)
-                mbar_wait(smem_addr(&ctl->full[i % FSTAGES]), (i / FSTAGES) & 1, &never, nullptr, 0, MBAR_WAIT_LIMIT);
+            if (lane == 0)
+            {
+                volatile int never = 0;
+                for (uint32_t i = it > (uint32_t)FSTAGES ? it - FSTAGES : 0; i < it; i++)
+                    mbar_wait(smem_addr(&ctl->full[i % FSTAGES]), (i / FSTAGES) & 1, &never, nullptr, 0,
+                              MBAR_WAIT_LIMIT);
+            }
             return;
         }
         else
@@ -922,12 +935,39 @@ bool encode_box(const Layout& lay, const double* base, CUtensorMap& map)
 }
 
 // The plan of both operands for a grid of H x Hk (A), Hk x Hn (B) blocks of
-// extents ms, ns, ks: the pair-copy form where its conditions hold, else the
-// TMA form where the tiles are boxes; false when neither applies.
+// extents ms, ns, ks; false when the element-pair kernel does not apply.
+// Tensor-map boxes where every tile is a box whose rows are one 128-byte run
+// of the operand (16 k of its unit-stride mode: one request per row); 16-byte
+// pair copies elsewhere.  Measured at 16384^3 (effective TFLOP/s, L0 / L1):
+// k-major GEMM operands (128-byte rows) 34.5 / 34.7 by boxes, 33.4 / 34.2 by
+// pairs; the headline contraction's layout (32-byte runs: each box 512 small
+// requests) 17.9 / 20.3 by boxes, 33.3 / 32.2 by pairs.
 bool plan_operands(const GemmView& g, int H, int Hn, int Hk, int64_t ms, int64_t ns, int64_t ks, Plan& pl)
 {
     if (g.type != TYPE_DOUBLE) return false;
     std::memset(&pl.tp, 0, sizeof pl.tp);
+    // Tiles of the TMA form must not cross block boundaries (a grid of one
+    // block along an index has none: its ragged end lies past the tensor).
+    if (!((H > 1 && ms % FT) || (Hn > 1 && ns % FT) || (Hk > 1 && ks % TBK)))
+    {
+        const std::vector<int64_t>* LA[3] = {&g.mode_len[0], &g.mode_len[4], &g.mode_len[6]};
+        const std::vector<int64_t>* SA[3] = {&g.mode_stride[0], &g.mode_stride[4], &g.mode_stride[6]};
+        const std::vector<int64_t>* LB[3] = {&g.mode_len[2], &g.mode_len[5], &g.mode_len[7]};
+        const std::vector<int64_t>* SB[3] = {&g.mode_stride[2], &g.mode_stride[5], &g.mode_stride[7]};
+        int bA = -1, bB = -1;
+        auto wide = [](std::vector<Layout> v) {
+            v.erase(std::remove_if(v.begin(), v.end(), [](const Layout& l) { return l.box[0] != (uint32_t)TBK; }),
+                    v.end());
+            return v;
+        };
+        const std::vector<Layout> la = wide(tma_layouts(LA, SA, bA));
+        const std::vector<Layout> lb = wide(tma_layouts(LB, SB, bB));
+        if (choose_plan(la, bA, lb, bB, pl))
+        {
+            pl.prod = PROD_TMA;
+            return true;
+        }
+    }
     int bitA = 0, bitB = 0;
     if (pair_bit(g.mode_len[4], g.mode_stride[4], g.mode_stride[0], g.mode_stride[6], Hk, ks, bitA,
                  pl.tp.pbase[0]) &&
@@ -946,19 +986,7 @@ bool plan_operands(const GemmView& g, int H, int Hn, int Hk, int64_t ms, int64_t
         pl.tp.pbit[1] = (int8_t)bitB;
         return true;
     }
-    // Tiles of the TMA form must not cross block boundaries (a grid of one
-    // block along an index has none: its ragged end lies past the tensor).
-    if ((H > 1 && ms % FT) || (Hn > 1 && ns % FT) || (Hk > 1 && ks % TBK)) return false;
-    const std::vector<int64_t>* LA[3] = {&g.mode_len[0], &g.mode_len[4], &g.mode_len[6]};
-    const std::vector<int64_t>* SA[3] = {&g.mode_stride[0], &g.mode_stride[4], &g.mode_stride[6]};
-    const std::vector<int64_t>* LB[3] = {&g.mode_len[2], &g.mode_len[5], &g.mode_len[7]};
-    const std::vector<int64_t>* SB[3] = {&g.mode_stride[2], &g.mode_stride[5], &g.mode_stride[7]};
-    int bA = -1, bB = -1;
-    const std::vector<Layout> la = tma_layouts(LA, SA, bA);
-    const std::vector<Layout> lb = tma_layouts(LB, SB, bB);
-    if (!choose_plan(la, bA, lb, bB, pl)) return false;
-    pl.prod = PROD_TMA;
-    return true;
+    return false;
 }
 
 }  // namespace

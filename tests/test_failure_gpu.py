@@ -84,33 +84,47 @@ def test_wait_timeout_fused_no_workspace_then_recovery(tsb, cuda, level):
 
 
 @pytest.mark.parametrize("level", [0, 1])
-def test_wait_timeout_pair_kernel_then_recovery(tsb, cuda, level):
-    """The element-pair form of the no-workspace kernel (A stored k-major, so
-    its k pairs are contiguous): a one-cycle bound, TBLIS_STRA_ERR_TIMEOUT,
-    then a correct call on the same context."""
+@pytest.mark.parametrize("producer", ["tma", "pairs"])
+def test_wait_timeout_pair_kernel_then_recovery(tsb, cuda, level, producer):
+    """The element-pair form of the no-workspace kernel, with each of its
+    producers: a one-cycle bound, TBLIS_STRA_ERR_TIMEOUT, then a correct call
+    on the same context.  Tensor-map boxes: A(k, i), B(k, j) (128-byte runs);
+    pair copies: the headline contraction's layout at 512^3."""
     import torch
-    A, B, ref = _problem()
-    At = np.asfortranarray(A.T)              # A(k, i): k contiguous
-    dA, dB = _dev(torch, At, cuda), _dev(torch, B, cuda)
-    C = torch.zeros((512, 512), dtype=torch.float64, device=cuda).t().contiguous().t()
+    if producer == "tma":
+        A, B, ref = _problem()
+        hA, hB = np.asfortranarray(A.T), B            # A(k, i): k contiguous
+        ia, ib, ic, shape_c, k, mA, mB = "ki", "kj", "ij", (512, 512), 512, np.abs(A).max(), np.abs(B).max()
+    else:
+        ext = dict(a=16, b=16, c=32, d=32, e=16, f=32)
+        ia, ib, ic = "efac", "fbde", "abcd"
+        hA = oracle.uniform([ext[c] for c in ia], 60)
+        hB = oracle.uniform([ext[c] for c in ib], 61)
+        shape_c = tuple(ext[c] for c in ic)
+        ref = np.zeros(shape_c, order="F")
+        oracle.contract(1.0, hA, ia, hB, ib, 0.0, ref, ic)
+        k, mA, mB = 512, np.abs(hA).max(), np.abs(hB).max()
+    dA, dB = _dev(torch, hA, cuda), _dev(torch, hB, cuda)
+    C = _dev(torch, np.zeros(shape_c, order="F"), cuda)
+    kind = "fused_tma" if producer == "tma" else "fused_pairs"
     tsb.set_workspace_limit(0)
     tsb.set_kernel_timing(True)
     try:
         tsb.set_wait_limit(1)
         try:
             with pytest.raises(tsb.TblisStraError) as ei:
-                tsb.contract(level, 1.0, dA, "ki", dB, "kj", 0.0, C, "ij", drop_in=True)
+                tsb.contract(level, 1.0, dA, ia, dB, ib, 0.0, C, ic, drop_in=True)
             assert ei.value.status == ERR_TIMEOUT
         finally:
             tsb.set_wait_limit(0)
         C.zero_()
-        tsb.contract(level, 1.0, dA, "ki", dB, "kj", 0.0, C, "ij", drop_in=True)
-        assert tsb.kernel_timing("fused_pairs")[0] == 2
+        tsb.contract(level, 1.0, dA, ia, dB, ib, 0.0, C, ic, drop_in=True)
+        assert tsb.kernel_timing(kind)[0] == 2
     finally:
         tsb.set_kernel_timing(False)
         tsb.set_workspace_limit(None)
     err = float(np.abs(C.cpu().numpy() - ref).max())
-    assert err <= oracle.error_bound(level, 512, np.abs(A).max(), np.abs(B).max())
+    assert err <= oracle.error_bound(level, k, mA, mB)
 
 
 @pytest.mark.parametrize("level", [0, 1])

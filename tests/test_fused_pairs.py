@@ -20,7 +20,8 @@ the reference's contraction, src/internal/3t/mult.cxx:100-165) on layouts the
 planner accepts -- the headline contraction's (C(abcd) += A(efac) B(fbde)),
 a transposed GEMM whose B is read in pairs, ragged extents whose last rows
 and k lie past the tensors (read as zero) and a batched case -- with the
-kernel-timing record confirming that the pair kernel ran.
+kernel-timing record confirming which producer ran (tensor-map boxes where
+tile rows are 128-byte runs, 16-byte pair copies elsewhere).
 """
 import numpy as np
 import pytest
@@ -47,41 +48,46 @@ def _query(tsb, level, ia, ib, ic, ext, lead=None):
     return tsb.fused_pairs_query(level, A, ia, B, ib, C, ic)
 
 
+# (level, idx_A, idx_B, idx_C, extents, padded leading extent of A and B, producer)
 ACCEPTED = [
-    # the headline contraction's layout (k modes contiguous in different operands)
-    (0, "efac", "fbde", "abcd", dict(a=64, b=64, c=64, d=64, e=64, f=64), None),
-    (1, "efac", "fbde", "abcd", dict(a=64, b=64, c=64, d=64, e=64, f=64), None),
-    (1, "efac", "fbde", "abcd", dict(a=128, b=128, c=128, d=128, e=128, f=128), None),
-    (1, "efac", "fbde", "abcd", dict(a=9, b=7, c=10, d=5, e=8, f=12), None),
-    # transposed GEMM: k contiguous in both operands (B read in pairs)
-    (1, "ki", "kj", "ij", dict(i=512, j=256, k=512), None),
-    (0, "ki", "kj", "ij", dict(i=255, j=383, k=46), None),
-    (1, "ki", "kj", "ij", dict(i=255, j=255, k=63), 64),
-    (1, "ki", "kj", "ij", dict(i=300, j=200, k=64), None),
+    # the headline contraction's layout (k modes contiguous in different
+    # operands, 32-byte runs): pair copies
+    (0, "efac", "fbde", "abcd", dict(a=64, b=64, c=64, d=64, e=64, f=64), None, "pairs"),
+    (1, "efac", "fbde", "abcd", dict(a=64, b=64, c=64, d=64, e=64, f=64), None, "pairs"),
+    (1, "efac", "fbde", "abcd", dict(a=128, b=128, c=128, d=128, e=128, f=128), None, "pairs"),
+    (1, "efac", "fbde", "abcd", dict(a=9, b=7, c=10, d=5, e=8, f=12), None, "pairs"),
+    # k-major GEMM operands: 128-byte runs, tensor-map boxes (B read in pairs)
+    (1, "ki", "kj", "ij", dict(i=512, j=256, k=512), None, "tma"),
+    (0, "ki", "kj", "ij", dict(i=255, j=383, k=46), None, "tma"),
+    (1, "ki", "kj", "ij", dict(i=255, j=255, k=63), 64, "tma"),
+    # block rows of 150: not whole tiles, so pair copies
+    (1, "ki", "kj", "ij", dict(i=300, j=200, k=64), None, "pairs"),
     # batch label in all three operands
-    (1, "kib", "kjb", "ijb", dict(i=256, j=256, k=64, b=3), None),
+    (1, "kib", "kjb", "ijb", dict(i=256, j=256, k=64, b=3), None, "tma"),
 ]
 
 REJECTED = [
-    (1, "ik", "kj", "ij", dict(i=512, j=512, k=512), None),     # A's unit stride is a row mode
-    (2, "efac", "fbde", "abcd", dict(a=64, b=64, c=64, d=64, e=64, f=64), None),   # sums of 4 blocks
-    (1, "ki", "kj", "ij", dict(i=256, j=256, k=62), None),     # k blocks of 31: slots would straddle them
-    (0, "ki", "kj", "ij", dict(i=256, j=256, k=47), None),     # odd column stride: pairs not 16-byte aligned
+    (1, "ik", "kj", "ij", dict(i=512, j=512, k=512), None, None),     # A's unit stride is a row mode
+    (2, "efac", "fbde", "abcd", dict(a=64, b=64, c=64, d=64, e=64, f=64), None, None),   # sums of 4 blocks
+    (1, "ki", "kj", "ij", dict(i=256, j=256, k=62), None, None),     # k blocks of 31: slots would straddle them
+    (0, "ki", "kj", "ij", dict(i=256, j=256, k=47), None, None),     # odd column stride: pairs not 16-byte aligned
 ]
 
 
 @pytest.mark.parametrize("case", ACCEPTED)
 def test_planner_accepts_pair_tiles_conflict_free(tsb, case):
-    level, ia, ib, ic, ext, lead = case
+    level, ia, ib, ic, ext, lead, producer = case
     q = _query(tsb, level, ia, ib, ic, ext, lead)
     assert q["pairs"], case
-    assert q["producer"] == "pairs"
+    assert q["producer"] == producer
     assert q["conflicts"] == 0, q
+    if producer == "tma":
+        assert 1 <= q["rank_A"] <= 5 and 1 <= q["rank_B"] <= 5
 
 
 @pytest.mark.parametrize("case", REJECTED)
 def test_planner_rejects(tsb, case):
-    level, ia, ib, ic, ext, lead = case
+    level, ia, ib, ic, ext, lead, _ = case
     assert not _query(tsb, level, ia, ib, ic, ext, lead)["pairs"], case
 
 
@@ -156,7 +162,7 @@ def _bank_conflicts(reads, width, phase_lanes):
 
 @pytest.mark.parametrize("case", ACCEPTED)
 def test_lane_tables_pair_the_same_k_and_cover_the_slot(tsb, case):
-    level, ia, ib, ic, ext, lead = case
+    level, ia, ib, ic, ext, lead, _ = case
     q = _query(tsb, level, ia, ib, ic, ext, lead)
     steps, a_reads, b_reads = _replay(q)
     for (g, t4), seq in steps.items():
@@ -178,7 +184,9 @@ def test_producer_copies_land_where_consumers_read(tsb, case):
     element of the tile is written once, the pair's second element (its k
     with the pair bit set) lands 8 bytes after the first, and a quarter warp's
     8 copies hit 8 different 16-byte bank groups."""
-    level, ia, ib, ic, ext, lead = case
+    level, ia, ib, ic, ext, lead, producer = case
+    if producer != "pairs":
+        pytest.skip("tiles copied as tensor-map boxes")
     q = _query(tsb, level, ia, ib, ic, ext, lead)
     for op in "AB":
         koff, span, bit, pbase = q["koff" + op], q["swz_" + op], q["bit_" + op], q["pbase" + op]
@@ -238,7 +246,9 @@ def _operand(shape, seed, lead):
 def test_pair_kernel_matches_oracle(tsb, cuda, case):
     import torch
     level, alpha, beta, ia, ib, ic, ext, lead = case
-    assert _query(tsb, level, ia, ib, ic, ext, lead)["pairs"]
+    q = _query(tsb, level, ia, ib, ic, ext, lead)
+    assert q["pairs"]
+    kind = "fused_pairs" if q["producer"] == "pairs" else "fused_tma"
     i = GPU_CASES.index(case)
     A = _operand([ext[c] for c in ia], 300 + 3 * i, lead)
     B = _operand([ext[c] for c in ib], 301 + 3 * i, lead)
@@ -251,7 +261,7 @@ def test_pair_kernel_matches_oracle(tsb, cuda, case):
     try:
         tsb.contract(level, alpha, dA, ia, dB, ib, beta, dC, ic)
         torch.cuda.synchronize()
-        launches, _ = tsb.kernel_timing("fused_pairs")
+        launches, _ = tsb.kernel_timing(kind)
     finally:
         tsb.set_kernel_timing(False)
         tsb.set_workspace_limit(None)
