@@ -440,10 +440,20 @@ def kernel_probe(args):
     dev = torch.device("cuda:0")
     gen = torch.Generator(device=dev).manual_seed(0)
     e = args.extent
-    shape = (e,) * 4
-    A = colmajor(torch, shape, dev, gen)
-    B = colmajor(torch, shape, dev, gen)
-    C = colmajor(torch, shape, dev, fill=0.0)
+    ia, ib, ic = IDX_A, IDX_B, IDX_C
+    if args.layout == "kmajor":
+        # the GEMM C(i,j) = A(k,i) B(k,j) with m = n = k = extent^2, both
+        # operands stored with k contiguous
+        n = e * e
+        A = torch.empty((n, n), dtype=torch.float64, device=dev).uniform_(-1, 1, generator=gen).t()
+        B = torch.empty((n, n), dtype=torch.float64, device=dev).uniform_(-1, 1, generator=gen).t()
+        C = torch.zeros((n, n), dtype=torch.float64, device=dev).t()
+        ia, ib, ic = "ki", "kj", "ij"
+    else:
+        shape = (e,) * 4
+        A = colmajor(torch, shape, dev, gen)
+        B = colmajor(torch, shape, dev, gen)
+        C = colmajor(torch, shape, dev, fill=0.0)
     if args.dtype == "f32":
         A, B, C = A.float(), B.float(), C.float()
         tsb.set_fp32_terms(args.terms)
@@ -476,14 +486,14 @@ def kernel_probe(args):
         return
     levels = [int(x) for x in args.kernels.split(",")]
     for lv in levels:
-        tsb.contract(lv, 1.0, A, IDX_A, B, IDX_B, 1.0, C, IDX_C, impl=args.variant)
+        tsb.contract(lv, 1.0, A, ia, B, ib, 1.0, C, ic, impl=args.variant)
     torch.cuda.synchronize()
     flops = 2.0 * float(e * e) ** 3
     for lv in levels:
         s, t = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         tsb.set_kernel_timing(True)
         s.record()
-        tsb.contract(lv, 1.0, A, IDX_A, B, IDX_B, 1.0, C, IDX_C, impl=args.variant)
+        tsb.contract(lv, 1.0, A, ia, B, ib, 1.0, C, ic, impl=args.variant)
         t.record()
         t.synchronize()
         ms = s.elapsed_time(t)
@@ -492,7 +502,7 @@ def kernel_probe(args):
         tsb.set_kernel_timing(False)
         print("   kernels: " + ", ".join(f"{k} {n}x {v:.2f} ms" for k, (n, v) in parts.items() if n))
         print(f"L{lv} impl{args.variant} {args.dtype}{'/' + str(args.terms) + ' terms' if args.dtype == 'f32' else ''} "
-              f"extent {e}: {ms:.3f} ms  {flops / ms / 1e9:.2f} TFLOP/s effective")
+              f"{args.layout} extent {e}: {ms:.3f} ms  {flops / ms / 1e9:.2f} TFLOP/s effective")
 
 
 def rank_sync(torch, dist, device):
@@ -551,6 +561,8 @@ def main():
                     help="--kernels probe: device workspace limit in bytes (0 = fully fused kernel)")
     ap.add_argument("--product-parallel", type=int, default=-1, choices=[-1, 0, 1],
                     help="--kernels probe: product-parallel schedule (-1 automatic, 0 never, 1 when it fits)")
+    ap.add_argument("--layout", choices=["config1", "kmajor"], default="config1",
+                    help="--kernels probe: the headline contraction, or the GEMM A(k,i) B(k,j) of m=n=k=extent^2")
     ap.add_argument("--kernels", default=None,
                     help="comma-separated levels: run one warm-up and one timed call per level "
                          "and print per-level times (profiling driver; no JSON line)")

@@ -265,7 +265,7 @@ stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
                     const uint32_t slot = it % FSTAGES;
                     const uint32_t use = it / FSTAGES;   // earlier uses of this slot
                     it++;
-                    if (!ok || (use > 0 && !mbar_wait<true>(smem_addr(&ctl->empty[slot]), (use & 1) ^ 1, abort_flag, err,
+                    if (!ok || (use > 0 && !mbar_wait(smem_addr(&ctl->empty[slot]), (use & 1) ^ 1, abort_flag, err,
                                                       1, limit)))
                     {
                         ok = false;
@@ -325,7 +325,7 @@ stra_fused_kernel(const __grid_constant__ DmmaArgs a, int* err, long long limit)
                 for (int64_t s = 0; s < nk; s++)
                 {
                     const uint32_t slot = cit % FSTAGES;
-                    ok = __all_sync(0xffffffffu, mbar_wait<true>(smem_addr(&ctl->full[slot]), (cit / FSTAGES) & 1,
+                    ok = __all_sync(0xffffffffu, mbar_wait(smem_addr(&ctl->full[slot]), (cit / FSTAGES) & 1,
                                                            abort_flag, err, 2, limit));
                     if (!ok) break;
                     const double* Ab = ring + slot * M::SLOT_DOUBLES;

@@ -268,7 +268,7 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
                         const uint32_t slot = it % FSTAGES, use = it / FSTAGES;
                         bool got = true;
                         if (lane == 0 && use > 0)
-                            got = mbar_wait<true>(smem_addr(&ctl->empty[slot]), (use & 1) ^ 1, abort_flag, err, 1, limit);
+                            got = mbar_wait(smem_addr(&ctl->empty[slot]), (use & 1) ^ 1, abort_flag, err, 1, limit);
                         ok = __shfl_sync(0xffffffffu, got, 0);
                         if (!ok) break;
                         it++;
@@ -367,7 +367,7 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
                         }
                         const uint32_t slot = it % FSTAGES, use = it / FSTAGES;
                         it++;
-                        if (!ok || (use > 0 && !mbar_wait<true>(smem_addr(&ctl->empty[slot]), (use & 1) ^ 1,
+                        if (!ok || (use > 0 && !mbar_wait(smem_addr(&ctl->empty[slot]), (use & 1) ^ 1,
                                                                 abort_flag, err, 1, limit)))
                         {
                             ok = false;
@@ -462,7 +462,7 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
             for (int64_t s = 0; s < nk; s++)
             {
                 const uint32_t slot = cit % FSTAGES;
-                ok = __all_sync(0xffffffffu, mbar_wait<true>(smem_addr(&ctl->full[slot]), (cit / FSTAGES) & 1,
+                ok = __all_sync(0xffffffffu, mbar_wait(smem_addr(&ctl->full[slot]), (cit / FSTAGES) & 1,
                                                              abort_flag, err, 2, limit));
                 if (!ok) break;
                 const double* Ab = ring + slot * TSLOT_DOUBLES;

@@ -48,28 +48,37 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t addr, uint32_t bytes)
 // Bounded wait (at most `limit` clock cycles) for the phase of the given
 // parity; false on timeout or abort.
 //
-// try_wait may suspend the thread inside the instruction until the phase
-// completes or a system-dependent time runs out, so a bound shorter than that
-// time may never be seen to run out.  With CAP_SUSPEND, a bound shorter than
-// the default polls with test_wait instead, which never suspends, so the bound
-// is what ends the wait (the fused kernel, whose waits are all shorter than
-// one such suspension, relies on this for its timeout path).  Without it the
-// wait keeps the plain form, which costs no registers.
-template <bool CAP_SUSPEND = false>
+// try_wait may hold a thread inside the instruction until the phase completes
+// or a system-dependent time passes, so a bound shorter than that time would
+// only be seen to run out when a wait outlasted it.  A bound shorter than the
+// default therefore polls with test_wait (which never suspends) in a loop of
+// its own, so the default loop keeps its registers.
 __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity, volatile int* abort_flag,
                                           int* err, int code, long long limit)
 {
     const long long start = clock64();
-    const bool short_bound = CAP_SUSPEND && limit < MBAR_WAIT_LIMIT;
+    if (limit < MBAR_WAIT_LIMIT)
+    {
+        while (true)
+        {
+            uint32_t done;
+            asm volatile("{\n.reg .pred p;\nmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                         "selp.u32 %0, 1, 0, p;\n}\n" : "=r"(done) : "r"(addr), "r"(parity) : "memory");
+            if (done) return true;
+            if (*abort_flag) return false;
+            if (clock64() - start > limit)
+            {
+                *abort_flag = 1;
+                if (err) atomicExch(err, code);
+                return false;
+            }
+        }
+    }
     while (true)
     {
         uint32_t done;
-        if (short_bound)
-            asm volatile("{\n.reg .pred p;\nmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-                         "selp.u32 %0, 1, 0, p;\n}\n" : "=r"(done) : "r"(addr), "r"(parity) : "memory");
-        else
-            asm volatile("{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-                         "selp.u32 %0, 1, 0, p;\n}\n" : "=r"(done) : "r"(addr), "r"(parity) : "memory");
+        asm volatile("{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                     "selp.u32 %0, 1, 0, p;\n}\n" : "=r"(done) : "r"(addr), "r"(parity) : "memory");
         if (done) return true;
         if (*abort_flag) return false;
         if (clock64() - start > limit)
