@@ -249,7 +249,8 @@ int tblis_stra_set_fp32_terms(int terms);
 int tblis_stra_get_fp32_terms(void);
 
 /* Bound, in SM clock cycles, on each wait of the warp-specialised kernels
- * (the packed FP64 GEMM and the split-BF16 tcgen05 GEMM) for a copy, an MMA
+ * (the packed FP64 GEMM, the fused no-workspace kernels and the split-BF16
+ * tcgen05 GEMM) for a copy, an MMA
  * stage or a drained accumulator; 0 (the default) means about one second.
  * When a wait runs out, the kernel stops issuing work, lets its own copies
  * and MMAs land, frees its tensor memory and ends; blocking calls then return
@@ -259,6 +260,16 @@ int tblis_stra_get_fp32_terms(void);
  * kernels.  Returns 0 or TBLIS_STRA_ERR_ARG (negative cycles). */
 int tblis_stra_set_wait_limit(long long cycles);
 long long tblis_stra_get_wait_limit(void);
+/* Failure test hook (no counterpart in the reference): with injection on, the
+ * calling thread's next calls make every pipeline wait of those kernels
+ * behave as a wait on a flag that nothing sets -- it runs out after the wait
+ * bound (tblis_stra_set_wait_limit, or 1000 cycles when that is 0) whatever
+ * the state of its copy or MMA, and the kernel takes its timeout path as
+ * above (blocking calls return TBLIS_STRA_ERR_TIMEOUT).  The waits with which
+ * a kernel lets its own copies and MMAs land before it ends are not
+ * affected.  Off by default; returns 0. */
+int tblis_stra_set_wait_injection(int on);
+int tblis_stra_get_wait_injection(void);
 
 /* Largest single device allocation (bytes) a call of the calling thread may
  * make for its scatter-vector tables, workspace, staging buffers and flags

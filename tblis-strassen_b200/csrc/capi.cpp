@@ -56,6 +56,7 @@ thread_local size_t t_ws_limit = SIZE_MAX;   // device workspace the ABC schedul
 thread_local int t_fp32_terms = 6;           // split-BF16 product terms for FP32 (3 or 6)
 thread_local int t_product_parallel = -1;    // product-parallel ABC: -1 auto, 0 never, 1 when it fits
 thread_local long long t_wait_limit = 0;     // pipeline wait bound in SM cycles (0: the kernels' default)
+thread_local bool t_wait_inject = false;     // pipeline waits run out whatever the state of their phase
 thread_local size_t t_alloc_limit = SIZE_MAX;  // largest single device allocation a call may make
 unsigned g_num_threads = 1;
 thread_local std::string t_detail;           // what the last failing CUDA call was
@@ -1080,7 +1081,11 @@ int run_fp64_ksplit_enqueue(const GemmView& g, const int64_t* const tb[9], const
 // pageable memory may return before its DMA completes, and kernels on
 // non-blocking streams are not ordered after it, so tables read by such
 // kernels go through a private non-blocking stream per device, synchronised.
-long long wait_limit_cycles() { return t_wait_limit; }
+long long wait_limit_cycles()
+{
+    if (!t_wait_inject) return t_wait_limit;
+    return t_wait_limit > 0 ? -t_wait_limit : -1000;
+}
 size_t alloc_limit_bytes() { return t_alloc_limit; }
 
 int upload_complete(void* dst, const void* src, size_t bytes)
@@ -2227,6 +2232,13 @@ int tblis_stra_set_wait_limit(long long cycles)
     return TBLIS_STRA_SUCCESS;
 }
 long long tblis_stra_get_wait_limit(void) { return tsb::t_wait_limit; }
+
+int tblis_stra_set_wait_injection(int on)
+{
+    tsb::t_wait_inject = on != 0;
+    return TBLIS_STRA_SUCCESS;
+}
+int tblis_stra_get_wait_injection(void) { return tsb::t_wait_inject ? 1 : 0; }
 
 int tblis_stra_set_alloc_limit(size_t bytes)
 {

@@ -11,12 +11,15 @@ namespace tsb {
 constexpr long long MBAR_WAIT_LIMIT = 2000000000LL;   // clock cycles (~1 s)
 
 // The bound a kernel applies to its pipeline waits: `requested` cycles when
-// positive (tblis_stra_set_wait_limit), else MBAR_WAIT_LIMIT.  Waits that only
+// positive (tblis_stra_set_wait_limit), MBAR_WAIT_LIMIT when 0; a negative
+// value -c asks every pipeline wait to treat its phase as never completing
+// and run out after c cycles (tblis_stra_set_wait_injection: the wait on a
+// flag that nothing sets, for failure tests).  Waits that only
 // let a CTA's own copies or MMAs land before it exits always use
 // MBAR_WAIT_LIMIT, so no CTA leaves with work in flight.
 __host__ __device__ __forceinline__ long long wait_cycles(long long requested)
 {
-    return requested > 0 ? requested : MBAR_WAIT_LIMIT;
+    return requested != 0 ? requested : MBAR_WAIT_LIMIT;
 }
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p)
@@ -57,6 +60,15 @@ __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity, volati
                                           int* err, int code, long long limit)
 {
     const long long start = clock64();
+    if (limit < 0)
+    {
+        // injected: the phase is treated as never completing
+        while (clock64() - start <= -limit)
+            if (*abort_flag) return false;
+        *abort_flag = 1;
+        if (err) atomicExch(err, code);
+        return false;
+    }
     if (limit < MBAR_WAIT_LIMIT)
     {
         while (true)

@@ -119,6 +119,9 @@ def _load() -> ctypes.CDLL:
     lib.tblis_stra_fused_pairs_query.argtypes = [ctypes.c_int, T, S, T, S, T, S, ctypes.POINTER(ctypes.c_int),
                                                  ctypes.POINTER(ctypes.c_int)]
     lib.tblis_stra_fused_pairs_query.restype = ctypes.c_int
+    lib.tblis_stra_set_wait_injection.argtypes = [ctypes.c_int]
+    lib.tblis_stra_set_wait_injection.restype = ctypes.c_int
+    lib.tblis_stra_get_wait_injection.restype = ctypes.c_int
     lib.tblis_stra_set_workspace_limit.argtypes = [ctypes.c_size_t]
     lib.tblis_stra_set_workspace_limit.restype = ctypes.c_int
     lib.tblis_stra_get_workspace_limit.restype = ctypes.c_size_t
@@ -476,6 +479,14 @@ def set_wait_limit(cycles: int) -> None:
     ends the kernel cleanly and blocking calls raise status
     TBLIS_STRA_ERR_TIMEOUT."""
     _check(lib.tblis_stra_set_wait_limit(cycles))
+
+
+def set_wait_injection(on: bool) -> None:
+    """Failure test hook: with injection on, every pipeline wait of this
+    thread's next calls runs out after the wait bound whatever the state of
+    its copy or MMA (a wait on a flag that nothing sets), so the kernels take
+    their timeout path and blocking calls raise TBLIS_STRA_ERR_TIMEOUT."""
+    _check(lib.tblis_stra_set_wait_injection(1 if on else 0))
 
 
 def get_wait_limit() -> int:

@@ -103,6 +103,26 @@ def test_product_parallel_knob(tsb):
     assert tsb.get_product_parallel() == -1
 
 
+def test_failure_knobs(tsb):
+    """Wait bound, wait injection and allocation ceiling: per-thread settings
+    with their defaults restored (no GPU needed)."""
+    assert tsb.get_wait_limit() == 0
+    tsb.set_wait_limit(12345)
+    assert tsb.get_wait_limit() == 12345
+    with pytest.raises(tsb.TblisStraError):
+        tsb.set_wait_limit(-1)
+    tsb.set_wait_limit(0)
+    lib = tsb.lib
+    assert lib.tblis_stra_get_wait_injection() == 0
+    tsb.set_wait_injection(True)
+    assert lib.tblis_stra_get_wait_injection() == 1
+    tsb.set_wait_injection(False)
+    assert lib.tblis_stra_get_wait_injection() == 0
+    tsb.set_alloc_limit(1 << 20)
+    assert tsb.get_alloc_limit() == 1 << 20
+    tsb.set_alloc_limit(None)
+
+
 def test_status_strings(tsb):
     for s in range(12):
         assert tsb.status_string(s) != "unknown status"

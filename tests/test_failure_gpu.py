@@ -3,11 +3,14 @@
 * Bounded waits: the warp-specialised kernels (packed FP64 GEMM, the fused
   no-workspace kernels in their gather and element-pair forms, split-BF16
   tcgen05 GEMM) bound every pipeline wait.  A test shortens the bound to one
-  SM clock cycle (tblis_stra_set_wait_limit), so the first wait whose copy or
-  MMA has not landed yet runs out; the kernel then stops issuing work, lets
-  its own copies and MMAs land, frees its tensor memory and ends, and the
-  blocking call reports TBLIS_STRA_ERR_TIMEOUT.  The next call with the
-  default bound must succeed on the same context and match the oracle.
+  SM clock cycle (tblis_stra_set_wait_limit) and turns on the wait injection
+  (tblis_stra_set_wait_injection), under which each pipeline wait behaves as
+  a wait on a flag that nothing sets, so the first one runs out whatever the
+  timing of the copies (at these sizes a copy has often landed before its
+  wait starts); the kernel then stops issuing work, lets its own copies and
+  MMAs land, frees its tensor memory and ends, and the blocking call reports
+  TBLIS_STRA_ERR_TIMEOUT.  The next call with the default bound and no
+  injection must succeed on the same context and match the oracle.
 * Allocation failure: a per-thread ceiling on single device allocations
   (tblis_stra_set_alloc_limit) makes the library's own allocations fail as an
   out-of-memory device would; the call returns TBLIS_STRA_ERR_ALLOC and C is
@@ -45,12 +48,14 @@ def test_wait_timeout_fp64_then_recovery(tsb, cuda, level):
     dA, dB = _dev(torch, A, cuda), _dev(torch, B, cuda)
     C = torch.zeros_like(dA)
     tsb.set_wait_limit(1)
+    tsb.set_wait_injection(True)
     try:
         with pytest.raises(tsb.TblisStraError) as ei:
             tsb.contract(level, 1.0, dA, "ik", dB, "kj", 0.0, C, "ij", drop_in=True)
         assert ei.value.status == ERR_TIMEOUT
     finally:
         tsb.set_wait_limit(0)
+        tsb.set_wait_injection(False)
     C.zero_()
     tsb.contract(level, 1.0, dA, "ik", dB, "kj", 0.0, C, "ij", drop_in=True)
     err = float(np.abs(C.cpu().numpy() - ref).max())
@@ -69,12 +74,14 @@ def test_wait_timeout_fused_no_workspace_then_recovery(tsb, cuda, level):
     tsb.set_workspace_limit(0)
     try:
         tsb.set_wait_limit(1)
+        tsb.set_wait_injection(True)
         try:
             with pytest.raises(tsb.TblisStraError) as ei:
                 tsb.contract(level, 1.0, dA, "ik", dB, "kj", 0.0, C, "ij", drop_in=True)
             assert ei.value.status == ERR_TIMEOUT
         finally:
             tsb.set_wait_limit(0)
+            tsb.set_wait_injection(False)
         C.zero_()
         tsb.contract(level, 1.0, dA, "ik", dB, "kj", 0.0, C, "ij", drop_in=True)
     finally:
@@ -111,12 +118,14 @@ def test_wait_timeout_pair_kernel_then_recovery(tsb, cuda, level, producer):
     tsb.set_kernel_timing(True)
     try:
         tsb.set_wait_limit(1)
+        tsb.set_wait_injection(True)
         try:
             with pytest.raises(tsb.TblisStraError) as ei:
                 tsb.contract(level, 1.0, dA, ia, dB, ib, 0.0, C, ic, drop_in=True)
             assert ei.value.status == ERR_TIMEOUT
         finally:
             tsb.set_wait_limit(0)
+            tsb.set_wait_injection(False)
         C.zero_()
         tsb.contract(level, 1.0, dA, ia, dB, ib, 0.0, C, ic, drop_in=True)
         assert tsb.kernel_timing(kind)[0] == 2
@@ -137,12 +146,14 @@ def test_wait_timeout_split_bf16_then_recovery(tsb, cuda, level):
     dA, dB = _dev(torch, np.asfortranarray(A32), cuda), _dev(torch, np.asfortranarray(B32), cuda)
     C = torch.zeros_like(dA)
     tsb.set_wait_limit(1)
+    tsb.set_wait_injection(True)
     try:
         with pytest.raises(tsb.TblisStraError) as ei:
             tsb.contract(level, 1.0, dA, "ik", dB, "kj", 0.0, C, "ij", drop_in=True)
         assert ei.value.status == ERR_TIMEOUT
     finally:
         tsb.set_wait_limit(0)
+        tsb.set_wait_injection(False)
     C.zero_()
     tsb.contract(level, 1.0, dA, "ik", dB, "kj", 0.0, C, "ij", drop_in=True)
     got = C.double().cpu().numpy()
