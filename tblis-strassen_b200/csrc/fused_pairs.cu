@@ -51,6 +51,8 @@
 #include <atomic>
 #include <climits>
 #include <cstring>
+#include <map>
+#include <utility>
 #include <vector>
 
 namespace tsb {
@@ -989,13 +991,39 @@ bool plan_operands(const GemmView& g, int H, int Hn, int Hk, int64_t ms, int64_t
     return false;
 }
 
+// Plans by contraction shape (the operands' mode extents and strides, the
+// block grid), per calling thread: the layout and lane-table search costs
+// about half a millisecond, the kernel at small sizes less.  Failures are
+// kept too.  At most 64 entries (cleared when full).
+bool cached_plan(const GemmView& g, int H, int Hn, int Hk, int64_t ms, int64_t ns, int64_t ks, Plan& pl)
+{
+    thread_local std::map<std::vector<int64_t>, std::pair<bool, Plan>> plans;
+    std::vector<int64_t> key = {g.type, H, Hn, Hk, ms, ns, ks};
+    for (int v : {0, 2, 4, 5, 6, 7})
+    {
+        key.push_back((int64_t)g.mode_len[v].size());
+        key.insert(key.end(), g.mode_len[v].begin(), g.mode_len[v].end());
+        key.insert(key.end(), g.mode_stride[v].begin(), g.mode_stride[v].end());
+    }
+    auto it = plans.find(key);
+    if (it != plans.end())
+    {
+        pl = it->second.second;
+        return it->second.first;
+    }
+    if (plans.size() >= 64) plans.clear();
+    const bool ok = plan_operands(g, H, Hn, Hk, ms, ns, ks, pl);
+    plans.emplace(std::move(key), std::make_pair(ok, pl));
+    return ok;
+}
+
 }  // namespace
 
 bool fused_pairs_plan(const GemmView& g, int H, int Hn, int Hk, int64_t ms, int64_t ns, int64_t ks,
                       int tables[PAIRS_PLAN_INTS])
 {
     Plan pl;
-    if (!plan_operands(g, H, Hn, Hk, ms, ns, ks, pl)) return false;
+    if (!cached_plan(g, H, Hn, Hk, ms, ns, ks, pl)) return false;
     if (tables)
     {
         int i = 0;
@@ -1035,7 +1063,7 @@ cudaError_t launch_fused_pairs(const DmmaArgs& in, const GemmView& g, cudaStream
         return cudaErrorNotSupported;
     const int Hn = in.Hn > 0 ? in.Hn : in.H, Hk = in.Hk > 0 ? in.Hk : in.H;
     Plan pl;
-    if (!plan_operands(g, in.H, Hn, Hk, in.ms, in.ns, in.ks, pl)) return cudaErrorNotSupported;
+    if (!cached_plan(g, in.H, Hn, Hk, in.ms, in.ns, in.ks, pl)) return cudaErrorNotSupported;
     FusedPairs& tp = pl.tp;
     if (pl.prod == PROD_TMA)
     {
