@@ -319,15 +319,18 @@ int tblis_stra_plan_query(const tblis_tensor* A, const label_type* idx_A,
  * contracted mode, so the kernel stages tiles as contiguous 16-byte pairs (by
  * cp.async, or by tensor-map copies where the tiles are boxes) in a layout
  * whose DMMA fragment reads are conflict-free; 0 when it gathers tiles
- * element by element through the scatter vectors.  `tables` (may be NULL;
- * 265 ints) receives the plan: the bank-conflict count of the consumers'
- * reads (0 = none), the producer (1 pair copies, 0 tensor maps), the
- * tensor-map ranks of A and B, 1 when B is read in 16-byte pairs, the swizzle
- * spans of A and B (bytes, 0 = none), the slot k bit each pair spans in A and
- * B, the per-lane read offsets aoff[32][2] and boff[32][4] (doubles), the
+ * element by element through the scatter vectors.  Levels 0 and 1 (operand
+ * sums of up to 2 blocks) stage 16 k per ring slot, level 2 (up to 4 blocks)
+ * 8 k.  `tables` (may be NULL; 266 ints) receives the plan: the
+ * bank-conflict count of the consumers' reads (0 = none), the producer (1
+ * pair copies, 0 tensor maps), the tensor-map ranks of A and B, 1 when B is
+ * read in 16-byte pairs, the swizzle spans of A and B (bytes, 0 = none), the
+ * slot k bit each pair spans in A and B, the per-lane read offsets
+ * aoff[32][2] and boff[32][4] (doubles; the first tb/8 and tb/4 used), the
  * fragment row and column permutations sigA[8] and sigB[8], the unswizzled
- * row positions of the slot's 16 k in A's and B's tiles, and the 8 pair
- * bases of A and of B in copy order. */
+ * row positions of the slot's k in A's and B's tiles (16 each, the first tb
+ * used), the pair bases of A and of B in copy order (8 each, the first tb/2
+ * used), and tb, the k per slot (16 or 8). */
 int tblis_stra_fused_pairs_query(int level, const tblis_tensor* A, const label_type* idx_A,
                                  const tblis_tensor* B, const label_type* idx_B,
                                  const tblis_tensor* C, const label_type* idx_C, int* pairs, int* tables);

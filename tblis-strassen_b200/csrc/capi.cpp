@@ -2315,12 +2315,13 @@ int tblis_stra_fused_pairs_query(int level, const tblis_tensor* A, const label_t
     int s = tsb::plan_contraction(A, idx_A, B, idx_B, C, idx_C, g, false);
     if (s) return s;
     const tsb::ProductTable& tab = tsb::product_table(level);
-    bool sums_of_two = true;
-    for (const tsb::Product& p : tab.prod)
-        if (p.na > 2 || p.nb > 2) sums_of_two = false;
+    int most = 1;   // blocks in the longest operand sum: 16-k slots up to 2, 8-k slots up to 4
+    for (const tsb::Product& p : tab.prod) most = std::max(most, std::max((int)p.na, (int)p.nb));
     const int64_t ms = (g.m + tab.H - 1) / tab.H, ns = (g.n + tab.Hn - 1) / tab.Hn,
                   ks = (g.k + tab.Hk - 1) / tab.Hk;
-    *pairs = sums_of_two && tsb::fused_pairs_plan(g, tab.H, tab.Hn, tab.Hk, ms, ns, ks, tables) ? 1 : 0;
+    *pairs = most <= 4 && tsb::fused_pairs_plan(g, tab.H, tab.Hn, tab.Hk, ms, ns, ks, most <= 2 ? 16 : 8, tables)
+                 ? 1
+                 : 0;
     return TBLIS_STRA_SUCCESS;
 }
 

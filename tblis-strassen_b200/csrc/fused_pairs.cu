@@ -64,11 +64,28 @@ using namespace fused;
 namespace {
 
 constexpr int PROD_TMA = 0, PROD_PAIRS = 1;
-constexpr int TBK = 16;                                   // k per ring slot
-constexpr int ROW = 16;                                   // doubles per tile row in shared memory
-constexpr int TNT = 2;                                    // blocks per operand in a slot
-constexpr int BOX_DOUBLES = TBK * FT;                     // one 128 x 16 tile: 16 KB
-constexpr int TSLOT_DOUBLES = 2 * TNT * BOX_DOUBLES;      // A0 A1 B0 B1
+// A ring slot holds, per operand, the blocks of the product's sum: 2 tiles of
+// 128 x 16 (sums of up to 2 blocks, Strassen levels 0 and 1) or 4 tiles of
+// 128 x 8 (up to 4 blocks, level 2), 64 KB either way.  TB, the slot's k, is
+// the kernel's template parameter; a tile row holds TB doubles.
+constexpr int TBK = 16;                                   // k per ring slot, at most
+constexpr int TSLOT_DOUBLES = 2 * 32 * FT;                // A0..A(NT-1) B0..B(NT-1)
+template <int TB>
+struct SlotShape
+{
+    static constexpr int NT = 32 / TB;                    // blocks per operand in a slot
+    static constexpr int ROW = TB;                        // doubles per tile row in shared memory
+    static constexpr int BOX = TB * FT;                   // one tile, doubles
+    static constexpr int LPR = TB / 2;                    // producer lanes per tile row (one pair each)
+    static constexpr int RPW = 32 / LPR;                  // tile rows per producer warp and pass
+    static constexpr int RPP = NPW * RPW;                 // tile rows per pass of the producer warpgroup
+    static constexpr int NIP = FT / RPP;                  // passes per tile
+    static constexpr int NQ = TB / 8;                     // pairs of MMA k-steps per slot
+    static constexpr int KTAB = 2 * FHMAX * TB;           // k-table entries (kA, kB)
+    static constexpr int KENT = (KTAB + PT - 1) / PT;     // per producer thread
+    static_assert(TB == 8 || TB == 16, "slot k");
+    static_assert(2 * NT * BOX == TSLOT_DOUBLES && NIP * RPP == FT, "slot shape");
+};
 constexpr size_t TRING_BYTES = size_t(FSTAGES) * TSLOT_DOUBLES * 8;
 constexpr size_t CTAB_BYTES = size_t(2) * FHMAX * FT * 8;                        // rowC, colC
 constexpr size_t PTAB_BYTES = size_t(2) * FHMAX * FT * 8 + size_t(2) * FHMAX * TBK * 8;   // rowA, colB, kA, kB
@@ -86,8 +103,6 @@ struct Regs
     static constexpr int PROD_REGS = PROD == PROD_PAIRS ? 80 : 64;
     static constexpr int CONS_REGS = PROD == PROD_PAIRS ? 208 : 216;
 };
-constexpr int KENT = 2 * FHMAX * TBK / PT;                // k-table entries per producer thread (PAIRS)
-static_assert(KENT * PT == 2 * FHMAX * TBK, "k tables split evenly over the producers");
 
 // How a tile origin gives the box coordinates of one operand (TMA form):
 // coordinate d is the sum over its parts p of ((v / div) % mod) * mult (no
@@ -112,15 +127,16 @@ struct FusedPairs
     // Consumer lane tables, in doubles inside a tile, swizzle applied: lane
     // (g, t4) of a warp at tile row (column) 0 reads A's pair of steps 2q,
     // 2q+1 at aoff[lane][q] and B's step j at boff[lane][j] (in pairs: the
-    // pair of steps 2q, 2q+1 at boff[lane][2q]).  Tile row r + 8 i is 128 i
-    // doubles further: shifts by multiples of 8 rows commute with the swizzle.
+    // pair of steps 2q, 2q+1 at boff[lane][2q]); q < TB / 8.  Tile row r + 8 i
+    // is 8 i TB doubles further: shifts by multiples of 8 rows commute with
+    // the swizzle (spans up to 128 bytes for 16-double rows, 64 for 8).
     int16_t aoff[32][2];
     int16_t boff[32][4];
     int8_t sigA[8];      // fragment row g -> row within its group of 8
     int8_t sigB[8];      // fragment column g -> column within its group of 8
     // PAIRS producer: unswizzled position of each slot k in a tile row, the
-    // swizzle span (bytes), the pair bit of the slot k index and the pair
-    // bases in copy order (consecutive lanes take consecutive pairs).
+    // swizzle span (bytes), the pair bit of the slot k index and the TB / 2
+    // pair bases in copy order (consecutive lanes take consecutive pairs).
     int8_t koff[2][TBK];
     int16_t swz[2];
     int8_t pbit[2];
@@ -206,7 +222,14 @@ __device__ __forceinline__ double2 ld2(const double* p)
     return *reinterpret_cast<const double2*>(p);
 }
 
-template <int PROD, bool BPAIR>
+// x with its sign bit XORed with bit 31 of m (m is 0 or 0x80000000): a
+// block's sign relative to the first of its sum, applied exactly.
+__device__ __forceinline__ double flip(double x, uint32_t m)
+{
+    return __hiloint2double(__double2hiint(x) ^ (int)m, __double2loint(x));
+}
+
+template <int PROD, bool BPAIR, int TB>
 __global__ void __launch_bounds__(FTHREADS, 1)
 stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant__ FusedPairs tp, int* err,
                        long long limit)
@@ -220,9 +243,9 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
     int64_t* colC = rowC + FHMAX * FT;
     int64_t* rowA = colC + FHMAX * FT;       // PAIRS producer tables
     int64_t* colB = rowA + FHMAX * FT;
-    int64_t* kA = colB + FHMAX * FT;         // [FHMAX][TBK], kB follows
-    int64_t* kB = kA + FHMAX * TBK;
-    FusedCtrl* ctl = reinterpret_cast<FusedCtrl*>(PROD == PROD_PAIRS ? reinterpret_cast<unsigned char*>(kB + FHMAX * TBK)
+    int64_t* kA = colB + FHMAX * FT;         // [FHMAX][TB], kB follows (room for TBK)
+    int64_t* kB = kA + FHMAX * TB;
+    FusedCtrl* ctl = reinterpret_cast<FusedCtrl*>(PROD == PROD_PAIRS ? reinterpret_cast<unsigned char*>(kA + 2 * FHMAX * TBK)
                                                                      : reinterpret_cast<unsigned char*>(rowA));
     volatile int* abort_flag = &ctl->abort;
 
@@ -240,7 +263,9 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
     __syncthreads();
 
     const int64_t work = a.batch * (int64_t)a.tiles_m * a.tiles_n;
-    const int64_t nk = (a.ks + TBK - 1) / TBK;
+    using SS = SlotShape<TB>;
+    constexpr int NT = SS::NT, ROW = SS::ROW, BOX = SS::BOX;
+    const int64_t nk = (a.ks + TB - 1) / TB;
 
     if (warp < NPW)
     {
@@ -251,6 +276,7 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
             // Lane 0 waits for the slot and posts its byte count; then lanes
             // 0 and 1 copy the A blocks of the product's sum, lanes 2 and 3 the
             // B blocks, each computing its own box coordinates.
+            static_assert(TB == TBK, "tensor-map boxes fill 16-k slots");
             if (warp != 0) return;
             if (lane == 0)
                 for (int m = 0; m < 2; m++)
@@ -275,20 +301,20 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
                         if (!ok) break;
                         it++;
                         const uint32_t full = smem_addr(&ctl->full[slot]);
-                        if (lane == 0) mbar_expect_tx(full, (uint32_t)((P.na + P.nb) * BOX_DOUBLES * 8));
+                        if (lane == 0) mbar_expect_tx(full, (uint32_t)((P.na + P.nb) * BOX * 8));
                         __syncwarp();
                         double* S = ring + slot * TSLOT_DOUBLES;
                         int c[5];
                         if (lane < P.na)
                         {
-                            box_coords(tp.co[0], P.a_r[lane] * a.ms + tm * FT, P.a_c[lane] * a.ks + s * TBK, b, c);
-                            tma_box(smem_addr(S + lane * BOX_DOUBLES), &tp.map[0], c, tp.co[0].ndim, full);
+                            box_coords(tp.co[0], P.a_r[lane] * a.ms + tm * FT, P.a_c[lane] * a.ks + s * TB, b, c);
+                            tma_box(smem_addr(S + lane * BOX), &tp.map[0], c, tp.co[0].ndim, full);
                         }
-                        else if (lane >= TNT && lane - TNT < P.nb)
+                        else if (lane >= NT && lane - NT < P.nb)
                         {
-                            const int t = lane - TNT;
-                            box_coords(tp.co[1], P.b_c[t] * a.ns + tn * FT, P.b_r[t] * a.ks + s * TBK, b, c);
-                            tma_box(smem_addr(S + (TNT + t) * BOX_DOUBLES), &tp.map[1], c, tp.co[1].ndim, full);
+                            const int t = lane - NT;
+                            box_coords(tp.co[1], P.b_c[t] * a.ns + tn * FT, P.b_r[t] * a.ks + s * TB, b, c);
+                            tma_box(smem_addr(S + (NT + t) * BOX), &tp.map[1], c, tp.co[1].ndim, full);
                         }
                     }
                 }
@@ -307,11 +333,12 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
         else
         {
             // ---------------- producer warpgroup: 16-byte pair copies ----------------
-            // Thread (warp w, lane l) copies pair kp = l % 8 of tile rows
-            // r0 + 16 i (i < 8), r0 = 4 w + l / 8: a row's 8 pairs go to 8
-            // consecutive lanes (one 16-byte chunk each of one 128-byte row).
+            // Thread (warp w, lane l) copies pair kp = l % P of tile rows
+            // r0 + (4 * 32 / P) i, r0 = (32 / P) w + l / P, P = TB / 2 pairs
+            // per row: a row's pairs go to consecutive lanes (one 16-byte
+            // chunk each of one TB-double row).
             const int ptid = tid;
-            const int kp = lane & 7, r0 = warp * 4 + (lane >> 3);
+            const int kp = lane % SS::LPR, r0 = warp * SS::RPW + lane / SS::LPR;
             const int klA = tp.pbase[0][kp], klB = tp.pbase[1][kp];
             const int kla2 = klA | (1 << tp.pbit[0]), klb2 = klB | (1 << tp.pbit[1]);
             const int dA = (swizzle((tp.koff[0][klA] + ROW * (r0 & 7)) * 8, tp.swz[0]) >> 3) + ROW * (r0 & ~7);
@@ -324,15 +351,15 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
             // the current one is copied.
             auto ktab_entry = [&](int64_t s, int j) -> int64_t {
                 const int i = ptid + j * PT;
-                const int op = i / (FHMAX * TBK), e = i % (FHMAX * TBK);
-                const int h = e / TBK, kk = e % TBK;
-                const int64_t kl = s * TBK + kk, gk = h * a.ks + kl;
-                if (!(h < Hk && kl < a.ks && gk < a.k)) return OFF_INVALID;
+                const int op = i / (FHMAX * TB), e = i % (FHMAX * TB);
+                const int h = e / TB, kk = e % TB;
+                const int64_t kl = s * TB + kk, gk = h * a.ks + kl;
+                if (!(i < SS::KTAB && h < Hk && kl < a.ks && gk < a.k)) return OFF_INVALID;
                 return op == 0 ? a.ksA[gk] : a.ksB[gk];
             };
-            int64_t kv[KENT];
+            int64_t kv[SS::KENT];
 #pragma unroll
-            for (int j = 0; j < KENT; j++) kv[j] = nk > 0 ? ktab_entry(0, j) : OFF_INVALID;
+            for (int j = 0; j < SS::KENT; j++) kv[j] = nk > 0 ? ktab_entry(0, j) : OFF_INVALID;
             uint32_t it = 0;
             bool ok = true;      // this thread's waits so far
             bool stop = false;   // set only right after a collective check, so uniform
@@ -360,12 +387,13 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
                         // that ran out in any of them ends the loops for all.
                         if (bar_any<1, PT>(!ok)) { stop = true; break; }
 #pragma unroll
-                        for (int j = 0; j < KENT; j++) kA[ptid + j * PT] = kv[j];   // kA, kB: one array
+                        for (int j = 0; j < SS::KENT; j++)   // kA, kB: one array
+                            if (SS::KENT * PT == SS::KTAB || ptid + j * PT < SS::KTAB) kA[ptid + j * PT] = kv[j];
                         bar_sync<1, PT>();
                         {
                             const int64_t sn = s + 1 < nk ? s + 1 : 0;
 #pragma unroll
-                            for (int j = 0; j < KENT; j++) kv[j] = ktab_entry(sn, j);
+                            for (int j = 0; j < SS::KENT; j++) kv[j] = ktab_entry(sn, j);
                         }
                         const uint32_t slot = it % FSTAGES, use = it / FSTAGES;
                         it++;
@@ -376,34 +404,34 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
                             continue;
                         }
                         const uint32_t S = smem_addr(ring + slot * TSLOT_DOUBLES);
-                        const uint32_t T = S + TNT * BOX_DOUBLES * 8;
+                        const uint32_t T = S + NT * BOX * 8;
                         for (int t = 0; t < P.na; t++)
                         {
                             const int64_t* rt = rowA + P.a_r[t] * FT;
-                            const int64_t* kt = kA + P.a_c[t] * TBK;
+                            const int64_t* kt = kA + P.a_c[t] * TB;
                             const int64_t ko = kt[klA];
                             const int nb = kt[kla2] != OFF_INVALID ? 16 : 8;
 #pragma unroll
-                            for (int i = 0; i < 8; i++)
+                            for (int i = 0; i < SS::NIP; i++)
                             {
-                                const int64_t ro = rt[r0 + 16 * i];
+                                const int64_t ro = rt[r0 + SS::RPP * i];
                                 const bool v = ro != OFF_INVALID && ko != OFF_INVALID;
-                                cp_async16(S + (uint32_t)(t * BOX_DOUBLES + dA + 16 * ROW * i) * 8,
+                                cp_async16(S + (uint32_t)(t * BOX + dA + SS::RPP * ROW * i) * 8,
                                            v ? a.A + (ro + ko) : a.A, v ? nb : 0);
                             }
                         }
                         for (int t = 0; t < P.nb; t++)
                         {
                             const int64_t* ct = colB + P.b_c[t] * FT;
-                            const int64_t* kt = kB + P.b_r[t] * TBK;
+                            const int64_t* kt = kB + P.b_r[t] * TB;
                             const int64_t ko = kt[klB];
                             const int nb = kt[klb2] != OFF_INVALID ? 16 : 8;
 #pragma unroll
-                            for (int i = 0; i < 8; i++)
+                            for (int i = 0; i < SS::NIP; i++)
                             {
-                                const int64_t co = ct[r0 + 16 * i];
+                                const int64_t co = ct[r0 + SS::RPP * i];
                                 const bool v = co != OFF_INVALID && ko != OFF_INVALID;
-                                cp_async16(T + (uint32_t)(t * BOX_DOUBLES + dB + 16 * ROW * i) * 8,
+                                cp_async16(T + (uint32_t)(t * BOX + dB + SS::RPP * ROW * i) * 8,
                                            v ? a.B + (co + ko) : a.B, v ? nb : 0);
                             }
                         }
@@ -429,10 +457,11 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
     // This lane's reads inside a tile: A's pairs of steps at rows wm + sa
     // (+16 mi, +8 for the fragment's second row), B's steps at columns
     // wn + sigB[g] (+8 ni).
-    const int a_off0 = tp.aoff[lane][0] + wm * ROW, a_off1 = tp.aoff[lane][1] + wm * ROW;
-    int b_off[4];
+    int a_off[SS::NQ], b_off[2 * SS::NQ];
 #pragma unroll
-    for (int j = 0; j < 4; j++) b_off[j] = tp.boff[lane][j] + wn * ROW;
+    for (int q = 0; q < SS::NQ; q++) a_off[q] = tp.aoff[lane][q] + wm * ROW;
+#pragma unroll
+    for (int j = 0; j < 2 * SS::NQ; j++) b_off[j] = tp.boff[lane][j] + wn * ROW;
     const int col0 = tp.sigB[2 * t4], col1 = tp.sigB[2 * t4 + 1];
 
     uint32_t cit = 0;
@@ -455,11 +484,16 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
 #pragma unroll
                     for (int e = 0; e < 4; e++) acc[mi][ni][e] = 0.0;
             const DevProduct& P = a.prod[p];
-            // the second block of a sum, with its sign relative to the first
-            // (the first's sign moves to the C coefficient)
-            const bool a2 = P.na > 1, b2 = P.nb > 1;
-            const double ra = a2 && (P.a_s[1] * P.a_s[0] < 0) ? -1.0 : 1.0;
-            const double rb = b2 && (P.b_s[1] * P.b_s[0] < 0) ? -1.0 : 1.0;
+            // the other blocks of a sum, with their signs relative to the
+            // first (the first's sign moves to the C coefficient)
+            const int na = P.na, nb = P.nb;
+            uint32_t ma[NT], mb[NT];
+#pragma unroll
+            for (int t = 1; t < NT; t++)
+            {
+                ma[t] = t < na && P.a_s[t] * P.a_s[0] < 0 ? 0x80000000u : 0u;
+                mb[t] = t < nb && P.b_s[t] * P.b_s[0] < 0 ? 0x80000000u : 0u;
+            }
 
             for (int64_t s = 0; s < nk; s++)
             {
@@ -468,25 +502,26 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
                                                              abort_flag, err, 2, limit));
                 if (!ok) break;
                 const double* Ab = ring + slot * TSLOT_DOUBLES;
-                const double* Bb = Ab + TNT * BOX_DOUBLES;
+                const double* Bb = Ab + NT * BOX;
 #pragma unroll
-                for (int q = 0; q < 2; q++)
+                for (int q = 0; q < SS::NQ; q++)
                 {
-                    const int ao = q ? a_off1 : a_off0;
                     double2 va[MI][2];
 #pragma unroll
                     for (int mi = 0; mi < MI; mi++)
 #pragma unroll
                         for (int h = 0; h < 2; h++)
                         {
-                            const double* pa = Ab + (mi * 16 + h * 8) * ROW + ao;
+                            const double* pa = Ab + (mi * 16 + h * 8) * ROW + a_off[q];
                             va[mi][h] = ld2(pa);
-                            if (a2)
-                            {
-                                const double2 u = ld2(pa + BOX_DOUBLES);
-                                va[mi][h].x = fma(ra, u.x, va[mi][h].x);
-                                va[mi][h].y = fma(ra, u.y, va[mi][h].y);
-                            }
+#pragma unroll
+                            for (int t = 1; t < NT; t++)
+                                if (t < na)
+                                {
+                                    const double2 u = ld2(pa + t * BOX);
+                                    va[mi][h].x += flip(u.x, ma[t]);
+                                    va[mi][h].y += flip(u.y, ma[t]);
+                                }
                         }
                     double vb[NI][2];
 #pragma unroll
@@ -496,12 +531,14 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
                         {
                             const double* pb = Bb + ni * 8 * ROW + b_off[2 * q];
                             double2 v = ld2(pb);
-                            if (b2)
-                            {
-                                const double2 u = ld2(pb + BOX_DOUBLES);
-                                v.x = fma(rb, u.x, v.x);
-                                v.y = fma(rb, u.y, v.y);
-                            }
+#pragma unroll
+                            for (int t = 1; t < NT; t++)
+                                if (t < nb)
+                                {
+                                    const double2 u = ld2(pb + t * BOX);
+                                    v.x += flip(u.x, mb[t]);
+                                    v.y += flip(u.y, mb[t]);
+                                }
                             vb[ni][0] = v.x;
                             vb[ni][1] = v.y;
                         }
@@ -511,7 +548,9 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
                             {
                                 const double* pb = Bb + ni * 8 * ROW + b_off[2 * q + jj];
                                 vb[ni][jj] = *pb;
-                                if (b2) vb[ni][jj] = fma(rb, pb[BOX_DOUBLES], vb[ni][jj]);
+#pragma unroll
+                                for (int t = 1; t < NT; t++)
+                                    if (t < nb) vb[ni][jj] += flip(pb[t * BOX], mb[t]);
                             }
                     }
 #pragma unroll
@@ -680,50 +719,57 @@ std::vector<Layout> tma_layouts(const std::vector<int64_t>* L[3], const std::vec
     return out;
 }
 
-// Layouts of the pair-copy form: the pair bit at row position 0, the other 3
-// slot k bits in every order, every swizzle span.
-std::vector<Layout> pair_layouts(int bit)
+// Layouts of the pair-copy form for slots of tb k (16 or 8): the pair bit
+// at row position 0, the other slot k bits in every order, every swizzle
+// span that commutes with shifts by 8 rows (up to 128 bytes for 16-double
+// rows, 64 for 8).
+std::vector<Layout> pair_layouts(int bit, int tb)
 {
     std::vector<Layout> out;
+    const int nbits = tb == 16 ? 4 : 3;
     int rest[3], nr = 0;
-    for (int b = 0; b < 4; b++)
+    for (int b = 0; b < nbits; b++)
         if (b != bit) rest[nr++] = b;
-    std::sort(rest, rest + 3);
+    std::sort(rest, rest + nr);
     do
     {
         for (int span : {0, 32, 64, 128})
         {
+            if (span > tb * 8) continue;
             Layout lay;
             std::memset(&lay.co, 0, sizeof lay.co);
             lay.swz = span;
-            for (int kl = 0; kl < TBK; kl++)
-                lay.koff[kl] = ((kl >> bit) & 1) | (((kl >> rest[0]) & 1) << 1) | (((kl >> rest[1]) & 1) << 2) |
-                               (((kl >> rest[2]) & 1) << 3);
+            for (int kl = 0; kl < tb; kl++)
+            {
+                int pos = (kl >> bit) & 1;
+                for (int i = 0; i < nr; i++) pos |= ((kl >> rest[i]) & 1) << (i + 1);
+                lay.koff[kl] = pos;
+            }
             out.push_back(lay);
         }
-    } while (std::next_permutation(rest, rest + 3));
+    } while (std::next_permutation(rest, rest + nr));
     return out;
 }
 
-// Bank conflicts of one operand's reads for a lane mapping kappa(t, j) and a
-// permutation sig of the 8 fragment rows (columns): 16-byte reads of the
-// pairs (steps 2q, 2q+1) by quarter warps when `pairs`, else 8-byte reads of
-// each step by half warps.  Row offsets are multiples of 8 rows and do not
-// change the banks.
+// Bank conflicts of one operand's reads for a lane mapping kappa(t, j), a
+// permutation sig of the 8 fragment rows (columns) and rows of tb doubles:
+// 16-byte reads of the pairs (steps 2q, 2q+1) by quarter warps when `pairs`,
+// else 8-byte reads of each step by half warps.  Row offsets are multiples of
+// 8 rows and do not change the banks.
 template <class Kappa>
-int read_conflicts(const Layout& lay, const int sig[8], Kappa kappa, bool pairs)
+int read_conflicts(const Layout& lay, const int sig[8], Kappa kappa, bool pairs, int tb)
 {
     int cost = 0;
     if (pairs)
     {
         for (int Q = 0; Q < 4; Q++)
-            for (int q = 0; q < 2; q++)
+            for (int q = 0; q < tb / 8; q++)
             {
                 int cnt[8] = {0}, mx = 0;
                 for (int g = 2 * Q; g < 2 * Q + 2; g++)
                     for (int t = 0; t < 4; t++)
                     {
-                        const int byte = swizzle((lay.koff[kappa(t, 2 * q)] + ROW * sig[g]) * 8, lay.swz);
+                        const int byte = swizzle((lay.koff[kappa(t, 2 * q)] + tb * sig[g]) * 8, lay.swz);
                         mx = std::max(mx, ++cnt[(byte >> 4) & 7]);
                     }
                 cost += mx - 1;
@@ -732,13 +778,13 @@ int read_conflicts(const Layout& lay, const int sig[8], Kappa kappa, bool pairs)
     else
     {
         for (int Hh = 0; Hh < 2; Hh++)
-            for (int j = 0; j < 4; j++)
+            for (int j = 0; j < tb / 4; j++)
             {
                 int cnt[16] = {0}, mx = 0;
                 for (int g = 4 * Hh; g < 4 * Hh + 4; g++)
                     for (int t = 0; t < 4; t++)
                     {
-                        const int byte = swizzle((lay.koff[kappa(t, j)] + ROW * sig[g]) * 8, lay.swz);
+                        const int byte = swizzle((lay.koff[kappa(t, j)] + tb * sig[g]) * 8, lay.swz);
                         mx = std::max(mx, ++cnt[(byte >> 3) & 15]);
                     }
                 cost += mx - 1;
@@ -751,6 +797,7 @@ int read_conflicts(const Layout& lay, const int sig[8], Kappa kappa, bool pairs)
 struct Plan
 {
     int prod = PROD_PAIRS;
+    int tb = TBK;        // k per slot
     Layout la, lb;
     FusedPairs tp;       // lane tables filled (tensor maps and coordinates not yet)
     bool bpair = false;
@@ -758,15 +805,16 @@ struct Plan
     int bitA = 0, bitB = 0;
 };
 
-// Lane tables of the consumers.  Step j (0..3) of lane t (0..3) in a group of
-// 4 MMA k-steps takes slot k kappa(t, j): bit 0 of j is A's pair bit (so
-// steps 2q, 2q+1 read one 16-byte pair of A); bit 1 of j and the two bits of
-// t take the other k bits in a chosen order.  B is read in pairs as well when
-// its pair bit is A's, else by element.  The search takes, for each lane
-// mapping, the layout of each operand and the permutation of its fragment
-// rows (columns; permutations of the 3 bits of g) with the fewest bank
-// conflicts, and keeps the best mapping.
-bool choose_plan(const std::vector<Layout>& LA, int bitA0, const std::vector<Layout>& LB, int bitB0, Plan& pl)
+// Lane tables of the consumers for slots of tb k.  Step j (0 .. tb/4 - 1) of
+// lane t (0..3) in a group of tb / 4 MMA k-steps takes slot k kappa(t, j):
+// bit 0 of j is A's pair bit (so steps 2q, 2q+1 read one 16-byte pair of A);
+// bit 1 of j (16-k slots) and the two bits of t take the other k bits in a
+// chosen order.  B is read in pairs as well when its pair bit is A's, else by
+// element.  The search takes, for each lane mapping, the layout of each
+// operand and the permutation of its fragment rows (columns; permutations of
+// the 3 bits of g) with the fewest bank conflicts, and keeps the best mapping.
+bool choose_plan(const std::vector<Layout>& LA, int bitA0, const std::vector<Layout>& LB, int bitB0, int tb,
+                 Plan& pl)
 {
     if (LA.empty() || LB.empty()) return false;
     static const int perm[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
@@ -775,36 +823,38 @@ bool choose_plan(const std::vector<Layout>& LA, int bitA0, const std::vector<Lay
         for (int g = 0; g < 8; g++)
             sigs[pi][g] = (((g >> 0) & 1) << perm[pi][0]) | (((g >> 1) & 1) << perm[pi][1]) |
                           (((g >> 2) & 1) << perm[pi][2]);
+    const int nbits = tb == 16 ? 4 : 3;
     const bool bpair = bitA0 == bitB0;
     int best = INT_MAX;
-    for (int b1 = 0; b1 < 4; b1++)
+    for (int b1 = nbits == 4 ? 0 : -1; b1 < (nbits == 4 ? 4 : 0); b1++)
     {
         if (b1 == bitA0) continue;
         int rest[2], nr = 0;
-        for (int b = 0; b < 4; b++)
+        for (int b = 0; b < nbits; b++)
             if (b != bitA0 && b != b1) rest[nr++] = b;
         for (int order = 0; order < 2; order++)
         {
             const int t0 = rest[order], t1 = rest[1 - order];
             auto kappa = [&](int t, int j) {
-                return ((j & 1) << bitA0) | ((j >> 1) << b1) | ((t & 1) << t0) | ((t >> 1) << t1);
+                return ((j & 1) << bitA0) | (b1 >= 0 ? (j >> 1) << b1 : 0) | ((t & 1) << t0) | ((t >> 1) << t1);
             };
             int ca = INT_MAX, cb = INT_MAX, ia = 0, ib = 0, pa = 0, pb = 0;
             for (size_t i = 0; i < LA.size(); i++)
                 for (int pi = 0; pi < 6; pi++)
                 {
-                    const int c = read_conflicts(LA[i], sigs[pi], kappa, true);
+                    const int c = read_conflicts(LA[i], sigs[pi], kappa, true, tb);
                     if (c < ca) { ca = c; ia = (int)i; pa = pi; }
                 }
             for (size_t i = 0; i < LB.size(); i++)
                 for (int pi = 0; pi < 6; pi++)
                 {
-                    const int c = read_conflicts(LB[i], sigs[pi], kappa, bpair);
+                    const int c = read_conflicts(LB[i], sigs[pi], kappa, bpair, tb);
                     if (c < cb) { cb = c; ib = (int)i; pb = pi; }
                 }
             if (ca + cb < best)
             {
                 best = ca + cb;
+                pl.tb = tb;
                 pl.la = LA[ia];
                 pl.lb = LB[ib];
                 pl.bpair = bpair;
@@ -812,15 +862,17 @@ bool choose_plan(const std::vector<Layout>& LA, int bitA0, const std::vector<Lay
                 pl.bitA = bitA0;
                 pl.bitB = bitB0;
                 FusedPairs& tp = pl.tp;
+                std::memset(tp.aoff, 0, sizeof tp.aoff);
+                std::memset(tp.boff, 0, sizeof tp.boff);
                 for (int lane = 0; lane < 32; lane++)
                 {
                     const int g = lane >> 2, t = lane & 3;
-                    for (int q = 0; q < 2; q++)
+                    for (int q = 0; q < tb / 8; q++)
                         tp.aoff[lane][q] =
-                            (int16_t)(swizzle((pl.la.koff[kappa(t, 2 * q)] + ROW * sigs[pa][g]) * 8, pl.la.swz) / 8);
-                    for (int j = 0; j < 4; j++)
+                            (int16_t)(swizzle((pl.la.koff[kappa(t, 2 * q)] + tb * sigs[pa][g]) * 8, pl.la.swz) / 8);
+                    for (int j = 0; j < tb / 4; j++)
                         tp.boff[lane][j] =
-                            (int16_t)(swizzle((pl.lb.koff[kappa(t, j)] + ROW * sigs[pb][g]) * 8, pl.lb.swz) / 8);
+                            (int16_t)(swizzle((pl.lb.koff[kappa(t, j)] + tb * sigs[pb][g]) * 8, pl.lb.swz) / 8);
                 }
                 for (int g = 0; g < 8; g++)
                 {
@@ -833,19 +885,19 @@ bool choose_plan(const std::vector<Layout>& LA, int bitA0, const std::vector<Lay
     return true;
 }
 
-// The pair bit of one operand for the pair-copy form: its k modes (planner
-// order) hold a unit-stride mode u (of even extent unless it is the top k
-// mode) whose lower modes span 2^b
-// slot k (b < 4), so slot k kl and kl + 2^b (bit b of kl clear) are adjacent
-// doubles.  Every other stride (k, row and batch modes) is even, so each
-// pair starts on 16 bytes (with a 16-byte aligned base), and slots start on
-// multiples of 16 k (one block along k, or block extents of whole slots).
-// `pbase` receives the 8 pair bases of a slot ordered by their offset in the
-// operand, so that consecutive lanes copy neighbouring pairs.
+// The pair bit of one operand for the pair-copy form with slots of tb k: its
+// k modes (planner order) hold a unit-stride mode u (of even extent unless it
+// is the top k mode) whose lower modes span 2^b slot k (2^b < tb), so slot k
+// kl and kl + 2^b (bit b of kl clear) are adjacent doubles.  Every other
+// stride (k, row and batch modes) is even, so each pair starts on 16 bytes
+// (with a 16-byte aligned base), and slots start on multiples of tb k (one
+// block along k, or block extents of whole slots).  `pbase` receives the tb/2
+// pair bases of a slot ordered by their offset in the operand, so that
+// consecutive lanes copy neighbouring pairs.
 bool pair_bit(const std::vector<int64_t>& kl, const std::vector<int64_t>& ks, const std::vector<int64_t>& rs,
-              const std::vector<int64_t>& bs, int Hk, int64_t kblk, int& bit, int8_t pbase[8])
+              const std::vector<int64_t>& bs, int Hk, int64_t kblk, int tb, int& bit, int8_t pbase[8])
 {
-    if (Hk > 1 && kblk % TBK) return false;
+    if (Hk > 1 && kblk % tb) return false;
     int u = -1, top = -1;
     for (size_t i = 0; i < kl.size(); i++)
     {
@@ -857,7 +909,7 @@ bool pair_bit(const std::vector<int64_t>& kl, const std::vector<int64_t>& ks, co
     if (u < 0 || (kl[u] % 2 && u != top)) return false;
     int64_t below = 1;
     for (int i = 0; i < u; i++) below *= kl[i];
-    if (below > 8 || (below & (below - 1))) return false;
+    if (below > tb / 2 || (below & (below - 1))) return false;
     for (size_t i = 0; i < kl.size(); i++)
         if ((int)i != u && kl[i] > 1 && ks[i] % 2) return false;
     for (size_t i = 0; i < rs.size(); i++)
@@ -868,7 +920,7 @@ bool pair_bit(const std::vector<int64_t>& kl, const std::vector<int64_t>& ks, co
     while ((int64_t(1) << bit) < below) bit++;
     // offsets of the pair bases of the first slot (mixed radix over the modes)
     std::vector<std::pair<int64_t, int>> bases;
-    for (int k = 0; k < TBK; k++)
+    for (int k = 0; k < tb; k++)
     {
         if ((k >> bit) & 1) continue;
         int64_t rest = k, off = 0;
@@ -880,7 +932,7 @@ bool pair_bit(const std::vector<int64_t>& kl, const std::vector<int64_t>& ks, co
         bases.emplace_back(off, k);
     }
     std::stable_sort(bases.begin(), bases.end());
-    for (int i = 0; i < 8; i++) pbase[i] = (int8_t)bases[i].second;
+    for (int i = 0; i < 8; i++) pbase[i] = i < tb / 2 ? (int8_t)bases[i].second : 0;
     return true;
 }
 
@@ -923,7 +975,7 @@ bool encode_box(const Layout& lay, const double* base, CUtensorMap& map)
     }
     // a box is one 16 KB tile, written densely (dimension 0's bytes equal the
     // swizzle span, or no swizzle)
-    if (box_elems != (size_t)BOX_DOUBLES) return false;
+    if (box_elems != (size_t)SlotShape<TBK>::BOX) return false;
     if (lay.swz != 0 && lay.swz != (int)lay.box[0] * 8) return false;
     const CUtensorMapSwizzle sw = lay.swz == 32    ? CU_TENSOR_MAP_SWIZZLE_32B
                                   : lay.swz == 64  ? CU_TENSOR_MAP_SWIZZLE_64B
@@ -937,20 +989,22 @@ bool encode_box(const Layout& lay, const double* base, CUtensorMap& map)
 }
 
 // The plan of both operands for a grid of H x Hk (A), Hk x Hn (B) blocks of
-// extents ms, ns, ks; false when the element-pair kernel does not apply.
+// extents ms, ns, ks and slots of tb k (16: sums of up to 2 blocks, 8: up to
+// 4); false when the element-pair kernel does not apply.  Slots of 8 k are
+// filled by pair copies only.
 // Tensor-map boxes where every tile is a box whose rows are one 128-byte run
 // of the operand (16 k of its unit-stride mode: one request per row); 16-byte
 // pair copies elsewhere.  Measured at 16384^3 (effective TFLOP/s, L0 / L1):
 // k-major GEMM operands (128-byte rows) 34.5 / 34.7 by boxes, 33.4 / 34.2 by
 // pairs; the headline contraction's layout (32-byte runs: each box 512 small
 // requests) 17.9 / 20.3 by boxes, 33.3 / 32.2 by pairs.
-bool plan_operands(const GemmView& g, int H, int Hn, int Hk, int64_t ms, int64_t ns, int64_t ks, Plan& pl)
+bool plan_operands(const GemmView& g, int H, int Hn, int Hk, int64_t ms, int64_t ns, int64_t ks, int tb, Plan& pl)
 {
-    if (g.type != TYPE_DOUBLE) return false;
+    if (g.type != TYPE_DOUBLE || (tb != 16 && tb != 8)) return false;
     std::memset(&pl.tp, 0, sizeof pl.tp);
     // Tiles of the TMA form must not cross block boundaries (a grid of one
     // block along an index has none: its ragged end lies past the tensor).
-    if (!((H > 1 && ms % FT) || (Hn > 1 && ns % FT) || (Hk > 1 && ks % TBK)))
+    if (tb == TBK && !((H > 1 && ms % FT) || (Hn > 1 && ns % FT) || (Hk > 1 && ks % TBK)))
     {
         const std::vector<int64_t>* LA[3] = {&g.mode_len[0], &g.mode_len[4], &g.mode_len[6]};
         const std::vector<int64_t>* SA[3] = {&g.mode_stride[0], &g.mode_stride[4], &g.mode_stride[6]};
@@ -964,24 +1018,24 @@ bool plan_operands(const GemmView& g, int H, int Hn, int Hk, int64_t ms, int64_t
         };
         const std::vector<Layout> la = wide(tma_layouts(LA, SA, bA));
         const std::vector<Layout> lb = wide(tma_layouts(LB, SB, bB));
-        if (choose_plan(la, bA, lb, bB, pl))
+        if (choose_plan(la, bA, lb, bB, TBK, pl))
         {
             pl.prod = PROD_TMA;
             return true;
         }
     }
     int bitA = 0, bitB = 0;
-    if (pair_bit(g.mode_len[4], g.mode_stride[4], g.mode_stride[0], g.mode_stride[6], Hk, ks, bitA,
+    if (pair_bit(g.mode_len[4], g.mode_stride[4], g.mode_stride[0], g.mode_stride[6], Hk, ks, tb, bitA,
                  pl.tp.pbase[0]) &&
-        pair_bit(g.mode_len[5], g.mode_stride[5], g.mode_stride[2], g.mode_stride[7], Hk, ks, bitB,
+        pair_bit(g.mode_len[5], g.mode_stride[5], g.mode_stride[2], g.mode_stride[7], Hk, ks, tb, bitB,
                  pl.tp.pbase[1]) &&
-        choose_plan(pair_layouts(bitA), bitA, pair_layouts(bitB), bitB, pl))
+        choose_plan(pair_layouts(bitA, tb), bitA, pair_layouts(bitB, tb), bitB, tb, pl))
     {
         pl.prod = PROD_PAIRS;
         for (int op = 0; op < 2; op++)
         {
             const Layout& lay = op ? pl.lb : pl.la;
-            for (int kl = 0; kl < TBK; kl++) pl.tp.koff[op][kl] = (int8_t)lay.koff[kl];
+            for (int kl = 0; kl < TBK; kl++) pl.tp.koff[op][kl] = kl < tb ? (int8_t)lay.koff[kl] : 0;
             pl.tp.swz[op] = (int16_t)lay.swz;
         }
         pl.tp.pbit[0] = (int8_t)bitA;
@@ -995,10 +1049,10 @@ bool plan_operands(const GemmView& g, int H, int Hn, int Hk, int64_t ms, int64_t
 // block grid), per calling thread: the layout and lane-table search costs
 // about half a millisecond, the kernel at small sizes less.  Failures are
 // kept too.  At most 64 entries (cleared when full).
-bool cached_plan(const GemmView& g, int H, int Hn, int Hk, int64_t ms, int64_t ns, int64_t ks, Plan& pl)
+bool cached_plan(const GemmView& g, int H, int Hn, int Hk, int64_t ms, int64_t ns, int64_t ks, int tb, Plan& pl)
 {
     thread_local std::map<std::vector<int64_t>, std::pair<bool, Plan>> plans;
-    std::vector<int64_t> key = {g.type, H, Hn, Hk, ms, ns, ks};
+    std::vector<int64_t> key = {g.type, H, Hn, Hk, ms, ns, ks, tb};
     for (int v : {0, 2, 4, 5, 6, 7})
     {
         key.push_back((int64_t)g.mode_len[v].size());
@@ -1012,18 +1066,18 @@ bool cached_plan(const GemmView& g, int H, int Hn, int Hk, int64_t ms, int64_t n
         return it->second.first;
     }
     if (plans.size() >= 64) plans.clear();
-    const bool ok = plan_operands(g, H, Hn, Hk, ms, ns, ks, pl);
+    const bool ok = plan_operands(g, H, Hn, Hk, ms, ns, ks, tb, pl);
     plans.emplace(std::move(key), std::make_pair(ok, pl));
     return ok;
 }
 
 }  // namespace
 
-bool fused_pairs_plan(const GemmView& g, int H, int Hn, int Hk, int64_t ms, int64_t ns, int64_t ks,
+bool fused_pairs_plan(const GemmView& g, int H, int Hn, int Hk, int64_t ms, int64_t ns, int64_t ks, int tb,
                       int tables[PAIRS_PLAN_INTS])
 {
     Plan pl;
-    if (!cached_plan(g, H, Hn, Hk, ms, ns, ks, pl)) return false;
+    if (!cached_plan(g, H, Hn, Hk, ms, ns, ks, tb, pl)) return false;
     if (tables)
     {
         int i = 0;
@@ -1046,6 +1100,7 @@ bool fused_pairs_plan(const GemmView& g, int H, int Hn, int Hk, int64_t ms, int6
         for (int kl = 0; kl < TBK; kl++) tables[i++] = pl.lb.koff[kl];
         for (int p = 0; p < 8; p++) tables[i++] = pl.tp.pbase[0][p];
         for (int p = 0; p < 8; p++) tables[i++] = pl.tp.pbase[1][p];
+        tables[i++] = pl.tb;
     }
     return true;
 }
@@ -1057,13 +1112,15 @@ cudaError_t launch_fused_pairs(const DmmaArgs& in, const GemmView& g, cudaStream
     if (in.H < 1 || in.H > FHMAX || in.Hc != in.H || in.mC != in.m || in.nC != in.n) return cudaErrorNotSupported;
     if (in.Hk < 0 || in.Hk > FHMAX || in.Hn < 0 || in.Hn > FHMAX) return cudaErrorNotSupported;
     if (in.nprod < 1 || in.nprod > MAX_PRODUCTS) return cudaErrorInvalidValue;
-    for (int p = 0; p < in.nprod; p++)
-        if (in.prod[p].na > TNT || in.prod[p].nb > TNT) return cudaErrorNotSupported;
+    int most = 1;   // blocks in the longest operand sum
+    for (int p = 0; p < in.nprod; p++) most = std::max(most, (int)std::max(in.prod[p].na, in.prod[p].nb));
+    if (most > SlotShape<8>::NT) return cudaErrorNotSupported;
+    const int tb = most <= SlotShape<16>::NT ? 16 : 8;
     if (reinterpret_cast<uintptr_t>(in.A) % 16 || reinterpret_cast<uintptr_t>(in.B) % 16)
         return cudaErrorNotSupported;
     const int Hn = in.Hn > 0 ? in.Hn : in.H, Hk = in.Hk > 0 ? in.Hk : in.H;
     Plan pl;
-    if (!cached_plan(g, in.H, Hn, Hk, in.ms, in.ns, in.ks, pl)) return cudaErrorNotSupported;
+    if (!cached_plan(g, in.H, Hn, Hk, in.ms, in.ns, in.ks, tb, pl)) return cudaErrorNotSupported;
     FusedPairs& tp = pl.tp;
     if (pl.prod == PROD_TMA)
     {
@@ -1073,8 +1130,11 @@ cudaError_t launch_fused_pairs(const DmmaArgs& in, const GemmView& g, cudaStream
     }
     using Kern = void (*)(DmmaArgs, FusedPairs, int*, long long);
     Kern kern = pl.prod == PROD_PAIRS
-                    ? (pl.bpair ? stra_fused_pair_kernel<PROD_PAIRS, true> : stra_fused_pair_kernel<PROD_PAIRS, false>)
-                    : (pl.bpair ? stra_fused_pair_kernel<PROD_TMA, true> : stra_fused_pair_kernel<PROD_TMA, false>);
+                    ? (pl.tb == 8 ? (pl.bpair ? stra_fused_pair_kernel<PROD_PAIRS, true, 8>
+                                              : stra_fused_pair_kernel<PROD_PAIRS, false, 8>)
+                                  : (pl.bpair ? stra_fused_pair_kernel<PROD_PAIRS, true, 16>
+                                              : stra_fused_pair_kernel<PROD_PAIRS, false, 16>))
+                    : (pl.bpair ? stra_fused_pair_kernel<PROD_TMA, true, 16> : stra_fused_pair_kernel<PROD_TMA, false, 16>);
     const size_t need = pl.prod == PROD_PAIRS
                             ? (size_t)Regs<PROD_PAIRS>::PROD_REGS * PT + (size_t)Regs<PROD_PAIRS>::CONS_REGS * CT
                             : (size_t)Regs<PROD_TMA>::PROD_REGS * PT + (size_t)Regs<PROD_TMA>::CONS_REGS * CT;

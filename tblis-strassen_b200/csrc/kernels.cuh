@@ -355,16 +355,18 @@ cudaError_t launch_fused(const DmmaArgs& args, cudaStream_t stream, int num_sms,
 cudaError_t launch_fused_pairs(const DmmaArgs& args, const GemmView& g, cudaStream_t stream, int num_sms, int* err,
                                long long wait_limit);
 // Whether the element-pair form applies to a plan cut into an H x Hk (A),
-// Hk x Hn (B) grid of blocks of extents ms, ns, ks (host only).  `tables`
-// (may be null; PAIRS_PLAN_INTS entries) receives: the bank-conflict count of
-// the consumers' reads, the producer (0 tensor-map boxes, 1 16-byte pair
-// copies), the tensor-map ranks of A and B (0 for pair copies), 1 when B is
-// read in pairs, the swizzle spans of A and B, the pair bits of A and B, then
-// the lane offsets aoff[32][2], boff[32][4], sigA[8], sigB[8], the
-// unswizzled row positions of the slot's 16 k in A's and B's tiles, and the
-// pair bases of A and B in copy order.
-constexpr int PAIRS_PLAN_INTS = 9 + 64 + 128 + 8 + 8 + 16 + 16 + 8 + 8;
-bool fused_pairs_plan(const GemmView& g, int H, int Hn, int Hk, int64_t ms, int64_t ns, int64_t ks,
+// Hk x Hn (B) grid of blocks of extents ms, ns, ks with ring slots of tb k
+// (16 for operand sums of up to 2 blocks, 8 for up to 4; host only).
+// `tables` (may be null; PAIRS_PLAN_INTS entries) receives: the bank-conflict
+// count of the consumers' reads, the producer (0 tensor-map boxes, 1 16-byte
+// pair copies), the tensor-map ranks of A and B (0 for pair copies), 1 when B
+// is read in pairs, the swizzle spans of A and B, the pair bits of A and B,
+// then the lane offsets aoff[32][2], boff[32][4], sigA[8], sigB[8], the
+// unswizzled row positions of the slot's k in A's and B's tiles (16 each,
+// the first tb used), the pair bases of A and B in copy order (8 each, the
+// first tb / 2 used) and tb.
+constexpr int PAIRS_PLAN_INTS = 9 + 64 + 128 + 8 + 8 + 16 + 16 + 8 + 8 + 1;
+bool fused_pairs_plan(const GemmView& g, int H, int Hn, int Hk, int64_t ms, int64_t ns, int64_t ks, int tb,
                       int tables[PAIRS_PLAN_INTS]);
 cudaError_t launch_dmma_grouped(const DmmaGroupArgs& g, int terms, int H, int Hc, int config,
                                 cudaStream_t stream, int num_sms);

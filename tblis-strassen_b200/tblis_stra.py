@@ -593,22 +593,26 @@ def fused_pairs_query(level, A, idx_A, B, idx_B, C, idx_C):
     16-byte pair spans), the per-lane read offsets ``aoff`` (32 x 2) and
     ``boff`` (32 x 4) in doubles, the fragment permutations ``sigA``,
     ``sigB``, the unswizzled row positions ``koffA``, ``koffB`` of the
-    slot's 16 k and the pair bases ``pbaseA``, ``pbaseB`` in copy order."""
+    slot's k, the pair bases ``pbaseA``, ``pbaseB`` in copy order and ``tb``,
+    the k per ring slot (16 for levels 0 and 1, 8 for level 2, whose operand
+    sums have up to 4 blocks); the lists are cut to the entries in use."""
     va, vb, vc = _View(A, 1.0), _View(B, 1.0), _View(C, 0.0)
     ia, ib, ic = _labels(idx_A, va.t.ndim), _labels(idx_B, vb.t.ndim), _labels(idx_C, vc.t.ndim)
     ok = ctypes.c_int(0)
-    tab = (ctypes.c_int * 265)()
+    tab = (ctypes.c_int * 266)()
     _check(lib.tblis_stra_fused_pairs_query(level, ctypes.byref(va.t), ia, ctypes.byref(vb.t), ib,
                                             ctypes.byref(vc.t), ic, ctypes.byref(ok), tab))
     t = list(tab)
     out = {"pairs": bool(ok.value)}
     if out["pairs"]:
+        tb = t[265]
+        nq, nj, np_ = tb // 8, tb // 4, tb // 2
         out.update(conflicts=t[0], producer=("tma", "pairs")[t[1]], rank_A=t[2], rank_B=t[3],
                    b_pairs=bool(t[4]), swz_A=t[5], swz_B=t[6], bit_A=t[7], bit_B=t[8],
-                   aoff=[t[9 + 2 * i:11 + 2 * i] for i in range(32)],
-                   boff=[t[73 + 4 * i:77 + 4 * i] for i in range(32)],
-                   sigA=t[201:209], sigB=t[209:217], koffA=t[217:233], koffB=t[233:249],
-                   pbaseA=t[249:257], pbaseB=t[257:265])
+                   aoff=[t[9 + 2 * i:9 + 2 * i + nq] for i in range(32)],
+                   boff=[t[73 + 4 * i:73 + 4 * i + nj] for i in range(32)],
+                   sigA=t[201:209], sigB=t[209:217], koffA=t[217:217 + tb], koffB=t[233:233 + tb],
+                   pbaseA=t[249:249 + np_], pbaseB=t[257:257 + np_], tb=tb)
     return out
 
 

@@ -3,12 +3,14 @@
 CPU tests (no GPU): the host planner (tblis_stra_fused_pairs_query) decides
 where the unit-stride mode of A and of B is a contracted mode, so that tiles
 can be staged as contiguous 16-byte k pairs, and picks the shared-memory
-layout and the consumers' lane tables.  The tests replay the kernel's
-address arithmetic on those tables -- tile row r at 16 r doubles, the slot's
-16 k at the planned row positions, the swizzle of the chosen span (16-byte
+layout and the consumers' lane tables.  A ring slot holds tb = 16 k of up to
+2 blocks per operand (levels 0 and 1) or tb = 8 k of up to 4 blocks (level 2,
+whose operand sums have up to 4 blocks).  The tests replay the kernel's
+address arithmetic on those tables -- tile row r at tb r doubles, the slot's
+tb k at the planned row positions, the swizzle of the chosen span (16-byte
 chunk bits XOR the row bits above bit 7), fragment rows and columns permuted
 by sigA/sigB -- and check that
-  * in every MMA step both operands' lanes take the same k, and the 16 k of a
+  * in every MMA step both operands' lanes take the same k, and the tb k of a
     slot are each taken once per fragment row and column;
   * every read lands on the fragment row (column) the epilogue writes back;
   * every producer copy lands where the consumers read that element;
@@ -19,7 +21,8 @@ GPU tests: parity of the kernel with the oracle (the plain-C restatement of
 the reference's contraction, src/internal/3t/mult.cxx:100-165) on layouts the
 planner accepts -- the headline contraction's (C(abcd) += A(efac) B(fbde)),
 a transposed GEMM whose B is read in pairs, ragged extents whose last rows
-and k lie past the tensors (read as zero) and a batched case -- with the
+and k lie past the tensors (read as zero) and a batched case, at levels 0, 1
+and 2 -- with the
 kernel-timing record confirming which producer ran (tensor-map boxes where
 tile rows are 128-byte runs, 16-byte pair copies elsewhere).
 """
@@ -27,8 +30,6 @@ import numpy as np
 import pytest
 
 from oracle import oracle
-
-ROW = 16
 
 
 def _view(shape, lead=None):
@@ -64,11 +65,18 @@ ACCEPTED = [
     (1, "ki", "kj", "ij", dict(i=300, j=200, k=64), None, "pairs"),
     # batch label in all three operands
     (1, "kib", "kjb", "ijb", dict(i=256, j=256, k=64, b=3), None, "tma"),
+    # level 2: sums of up to 4 blocks, 8 k per slot, pair copies only
+    (2, "efac", "fbde", "abcd", dict(a=64, b=64, c=64, d=64, e=64, f=64), None, "pairs"),
+    (2, "efac", "fbde", "abcd", dict(a=9, b=7, c=10, d=5, e=8, f=12), None, "pairs"),
+    (2, "efac", "fbde", "abcd", dict(a=9, b=7, c=10, d=5, e=4, f=16), None, "pairs"),
+    (2, "ki", "kj", "ij", dict(i=512, j=512, k=512), None, "pairs"),
+    (2, "ki", "kj", "ij", dict(i=255, j=255, k=127), 128, "pairs"),
+    (2, "kib", "kjb", "ijb", dict(i=256, j=256, k=64, b=3), None, "pairs"),
 ]
 
 REJECTED = [
     (1, "ik", "kj", "ij", dict(i=512, j=512, k=512), None, None),     # A's unit stride is a row mode
-    (2, "efac", "fbde", "abcd", dict(a=64, b=64, c=64, d=64, e=64, f=64), None, None),   # sums of 4 blocks
+    (2, "ki", "kj", "ij", dict(i=256, j=256, k=48), None, None),     # k blocks of 12: not whole 8-k slots
     (1, "ki", "kj", "ij", dict(i=256, j=256, k=62), None, None),     # k blocks of 31: slots would straddle them
     (0, "ki", "kj", "ij", dict(i=256, j=256, k=47), None, None),     # odd column stride: pairs not 16-byte aligned
 ]
@@ -80,6 +88,7 @@ def test_planner_accepts_pair_tiles_conflict_free(tsb, case):
     q = _query(tsb, level, ia, ib, ic, ext, lead)
     assert q["pairs"], case
     assert q["producer"] == producer
+    assert q["tb"] == (8 if level == 2 else 16)
     assert q["conflicts"] == 0, q
     if producer == "tma":
         assert 1 <= q["rank_A"] <= 5 and 1 <= q["rank_B"] <= 5
@@ -100,10 +109,11 @@ def _swizzle(byte, span):
     return byte ^ (((byte >> 7) & ((1 << s) - 1)) << 4)
 
 
-def _decode(off, koff, span):
-    """(row, slot k) of the double at offset `off` (doubles) of a tile."""
+def _decode(off, koff, span, tb):
+    """(row, slot k) of the double at offset `off` (doubles) of a tile whose
+    rows hold tb doubles."""
     u = _swizzle(off * 8, span) // 8
-    row, pos = divmod(u, ROW)
+    row, pos = divmod(u, tb)
     return row, koff.index(pos)
 
 
@@ -112,30 +122,31 @@ def _replay(q):
     warp at tile row and column 0).  Returns, per lane (g, t4), the list over
     steps of (kA, kB), and the offsets read by A's and B's loads grouped by
     instruction."""
-    assert sorted(q["koffA"]) == list(range(16)) and sorted(q["koffB"]) == list(range(16))
+    tb = q["tb"]
+    assert sorted(q["koffA"]) == list(range(tb)) and sorted(q["koffB"]) == list(range(tb))
     sa_of, sb_of = q["sigA"], q["sigB"]
     assert sorted(sa_of) == list(range(8)) and sorted(sb_of) == list(range(8))
     steps, a_reads, b_reads = {}, {}, {}
     for lane in range(32):
         g = lane >> 2
         seq = []
-        for qq in range(2):
+        for qq in range(tb // 8):
             ao = q["aoff"][lane][qq]
             assert ao % 2 == 0                      # 16-byte aligned pair
             a_reads.setdefault(qq, []).append((lane, ao))
             for jj in range(2):
-                ra, ka = _decode(ao + jj, q["koffA"], q["swz_A"])
+                ra, ka = _decode(ao + jj, q["koffA"], q["swz_A"], tb)
                 assert ra == sa_of[g]
                 if q["b_pairs"]:
                     bo = q["boff"][lane][2 * qq]
                     assert bo % 2 == 0
                     if jj == 0:
                         b_reads.setdefault(qq, []).append((lane, bo))
-                    rb, kb = _decode(bo + jj, q["koffB"], q["swz_B"])
+                    rb, kb = _decode(bo + jj, q["koffB"], q["swz_B"], tb)
                 else:
                     bo = q["boff"][lane][2 * qq + jj]
                     b_reads.setdefault(2 * qq + jj, []).append((lane, bo))
-                    rb, kb = _decode(bo, q["koffB"], q["swz_B"])
+                    rb, kb = _decode(bo, q["koffB"], q["swz_B"], tb)
                 assert rb == sb_of[g]
                 seq.append((ka, kb))
         steps[(g, lane & 3)] = seq
@@ -168,47 +179,57 @@ def test_lane_tables_pair_the_same_k_and_cover_the_slot(tsb, case):
     for (g, t4), seq in steps.items():
         for kA, kB in seq:
             assert kA == kB, (g, t4, seq)
-    # each MMA step sums over the 4 lanes t4 of a row g; over its 4 steps the
-    # 16 k of the slot are each taken once
+    # each MMA step sums over the 4 lanes t4 of a row g; over its tb / 4
+    # steps the tb k of the slot are each taken once
+    tb = q["tb"]
     for g in range(8):
-        ks = [steps[(g, t4)][s][0] for t4 in range(4) for s in range(4)]
-        assert sorted(ks) == list(range(16)), (g, ks)
+        ks = [steps[(g, t4)][s][0] for t4 in range(4) for s in range(tb // 4)]
+        assert sorted(ks) == list(range(tb)), (g, ks)
     assert _bank_conflicts(a_reads, 16, 8) == 0
     assert _bank_conflicts(b_reads, 16 if q["b_pairs"] else 8, 8 if q["b_pairs"] else 16) == 0
 
 
 @pytest.mark.parametrize("case", ACCEPTED)
 def test_producer_copies_land_where_consumers_read(tsb, case):
-    """The pair producer: thread (warp w, lane l) copies pair pbase[l % 8] of
-    tile rows 4 w + l / 8 + 16 i to swizzle((koff + 16 r) * 8) / 8.  Every
-    element of the tile is written once, the pair's second element (its k
-    with the pair bit set) lands 8 bytes after the first, and a quarter warp's
-    8 copies hit 8 different 16-byte bank groups."""
+    """The pair producer: with P = tb / 2 pairs per tile row, thread (warp w,
+    lane l) copies pair pbase[l % P] of tile rows (32 / P) w + l / P +
+    (128 / P) i to swizzle((koff + tb r) * 8) / 8.  Every element of the tile
+    is written once, the pair's second element (its k with the pair bit set)
+    lands 8 bytes after the first, and a quarter warp's 8 copies hit 8
+    different 16-byte bank groups."""
     level, ia, ib, ic, ext, lead, producer = case
     if producer != "pairs":
         pytest.skip("tiles copied as tensor-map boxes")
     q = _query(tsb, level, ia, ib, ic, ext, lead)
+    tb = q["tb"]
+    P = tb // 2
+    rpw, rpp = 32 // P, 4 * 32 // P
     for op in "AB":
         koff, span, bit, pbase = q["koff" + op], q["swz_" + op], q["bit_" + op], q["pbase" + op]
-        assert sorted(pbase + [k | (1 << bit) for k in pbase]) == list(range(16))
+        assert len(pbase) == P
+        assert sorted(pbase + [k | (1 << bit) for k in pbase]) == list(range(tb))
         written = {}
         for warp in range(4):
             for lane in range(32):
-                kp, r0 = lane & 7, warp * 4 + (lane >> 3)
+                kp, r0 = lane % P, warp * rpw + lane // P
                 kl = pbase[kp]
                 assert not (kl >> bit) & 1
-                d0 = (_swizzle((koff[kl] + ROW * (r0 & 7)) * 8, span) >> 3) + ROW * (r0 & ~7)
-                for i in range(8):
-                    off = d0 + 16 * ROW * i
+                d0 = (_swizzle((koff[kl] + tb * (r0 & 7)) * 8, span) >> 3) + tb * (r0 & ~7)
+                for i in range(128 // rpp):
+                    off = d0 + rpp * tb * i
                     assert off % 2 == 0
                     for half, k in ((0, kl), (1, kl | (1 << bit))):
-                        assert _decode(off + half, koff, span) == (r0 + 16 * i, k)
+                        assert _decode(off + half, koff, span, tb) == (r0 + rpp * i, k)
                         assert off + half not in written
                         written[off + half] = True
-        assert len(written) == 128 * 16
-        # quarter warps of one copy instruction: lanes 8x .. 8x+7 share a row
-        for r7 in range(8):
-            units = {(_swizzle((koff[pbase[kp]] + ROW * r7) * 8, span) >> 4) & 7 for kp in range(8)}
+        assert len(written) == 128 * tb
+        # quarter warps of one copy instruction: 8 consecutive lanes cover
+        # 8 / P rows
+        for quarter in range(4 * 4):
+            units = set()
+            for lane in range(8 * (quarter % 4), 8 * (quarter % 4) + 8):
+                kp, r = lane % P, (quarter // 4) * rpw + lane // P
+                units.add((_swizzle((koff[pbase[kp]] + tb * (r & 7)) * 8, span) >> 4) & 7)
             assert len(units) == 8
 
 
@@ -231,6 +252,12 @@ GPU_CASES = [
     (1, 1.0, -1.0, "ki", "kj", "ij", dict(i=255, j=255, k=63), 64),
     (1, 1.0, 1.0, "ki", "kj", "ij", dict(i=300, j=200, k=64), None),
     (1, 2.0, 0.5, "kib", "kjb", "ijb", dict(i=256, j=256, k=64, b=3), None),
+    # level 2: sums of up to 4 blocks per operand, 8 k per slot
+    (2, 1.0, 1.0, "efac", "fbde", "abcd", dict(a=32, b=16, c=32, d=32, e=16, f=8), None),
+    (2, 1.5, 0.5, "efac", "fbde", "abcd", dict(a=9, b=7, c=10, d=5, e=8, f=12), None),
+    (2, -0.5, 0.25, "ki", "kj", "ij", dict(i=512, j=256, k=512), None),
+    (2, 1.0, -1.0, "ki", "kj", "ij", dict(i=255, j=255, k=127), 128),
+    (2, 2.0, 0.5, "kib", "kjb", "ijb", dict(i=256, j=256, k=64, b=3), None),
 ]
 
 
@@ -274,7 +301,8 @@ def test_pair_kernel_matches_oracle(tsb, cuda, case):
 
 
 @pytest.mark.gpu
-def test_pair_kernel_noalloc_entry_point(tsb, cuda):
+@pytest.mark.parametrize("level", [1, 2])
+def test_pair_kernel_noalloc_entry_point(tsb, cuda, level):
     """The allocation-free entry point reaches the same kernel."""
     import torch
     ia, ib, ic = "efac", "fbde", "abcd"
@@ -287,11 +315,11 @@ def test_pair_kernel_noalloc_entry_point(tsb, cuda):
     dC = torch.zeros_like(_dev(torch, ref, cuda))
     tsb.set_kernel_timing(True)
     try:
-        tsb.noalloc_mult(1, 1.0, dA, ia, dB, ib, 0.0, dC, ic)
+        tsb.noalloc_mult(level, 1.0, dA, ia, dB, ib, 0.0, dC, ic)
         torch.cuda.synchronize()
         launches, _ = tsb.kernel_timing("fused_pairs")
     finally:
         tsb.set_kernel_timing(False)
     assert launches == 1
-    bound = oracle.error_bound(1, 16 * 8, float(np.abs(A).max()), float(np.abs(B).max()))
+    bound = oracle.error_bound(level, 16 * 8, float(np.abs(A).max()), float(np.abs(B).max()))
     assert float(np.abs(dC.cpu().numpy() - ref).max()) <= bound
