@@ -666,7 +666,7 @@ def main():
     tsb.set_workspace_limit(0)
     try:
         nw = max(2, args.steps // 4)
-        for lv in sorted({0, args.level}):
+        for lv in sorted({0, args.level, 2}):
             for _ in range(2):
                 step(lv, 1)
             barrier_sync()

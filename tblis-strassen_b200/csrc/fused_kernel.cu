@@ -35,7 +35,8 @@
 // through the scatter vectors (8-byte requests to L2).  Where the unit-stride
 // modes of A and B are contracted modes, the element-pair form
 // (fused_pairs.cu: 16-byte pair copies or tensor-map boxes into a planned
-// conflict-free layout) runs instead: 33.3 and 32.2 at L=0 and L=1 there.
+// conflict-free layout) runs instead: 33.3, 32.2 and 23.9 at L=0, 1 and 2
+// there.
 //
 // The producer runs up to 3 k-steps ahead, across product and tile
 // boundaries.  Every wait is bounded; a wait that runs out makes both roles

@@ -23,18 +23,21 @@
 //     addressed through the row and k offset tables of the tile (any row
 //     layout, ragged blocks included: entries past the extents read as
 //     zero); the slot's "full" mbarrier completes when the copies land.
-// Layout of one 128 x 16 tile (16 KB): row r at 16 r doubles; inside a row,
-// the 16 k in the order of a bit permutation of the slot's k index that puts
-// the pair bit at position 0; then the 16-byte chunks of every 128-byte row
-// XORed with bits of the row (the TMA swizzle of span 32, 64 or 128 bytes,
-// or none).  The TMA form is limited to layouts a tensor map writes densely
-// (dimension 0's box bytes equal to the swizzle span).
+// A ring slot (64 KB) holds the blocks of the product's sums: 128 x 16 tiles,
+// up to 2 per operand (Strassen levels 0 and 1), or 128 x 8 tiles, up to 4
+// per operand (level 2, whose sums have up to 4 blocks; pair copies only).
+// Layout of one 128 x TB tile: row r at TB r doubles; inside a row, the TB k
+// in the order of a bit permutation of the slot's k index that puts the pair
+// bit at position 0; then the 16-byte chunks of every 128 bytes XORed with
+// bits of the row (the TMA swizzle of span 32, 64 or 128 bytes, or none; at
+// most 64 for 8-double rows).  The TMA form is limited to layouts a tensor
+// map writes densely (dimension 0's box bytes equal to the swizzle span).
 //
 // Consumers (warps 4-11, 2 x 4 warps of 64 x 32): which k a lane takes in
-// which MMA step is a permutation of the slot's 16 k (a sum over k may take
+// which MMA step is a permutation of the slot's TB k (a sum over k may take
 // them in any order), chosen with the permutations of each warp's 8 fragment
-// rows and columns so that the reads are conflict-free; both blocks of an
-// operand sum are read and added with their relative sign; the epilogue adds
+// rows and columns so that the reads are conflict-free; the blocks of an
+// operand sum are read and added with their relative signs; the epilogue adds
 // +-alpha * (S T) into the product's C blocks as the gather form does.
 //
 // Every wait is bounded; after a wait runs out both roles leave their loops
