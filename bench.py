@@ -660,8 +660,8 @@ def main():
 
     # ---- the no-workspace ABC kernel (all products in one persistent launch,
     #      operand sums formed in the consumers from the staged raw blocks),
-    #      through the regular call with no workspace allowed (at this level
-    #      and at L=0) and through the allocation-free entry point
+    #      through the regular call with no workspace allowed (at this level,
+    #      at L=0 and at L=2) and through the allocation-free entry point
     no_workspace = {}
     tsb.set_workspace_limit(0)
     try:
