@@ -259,6 +259,7 @@ cudaError_t launch_scatter_add(const ScatterAddArgs& a, cudaStream_t stream)
 {
     const int64_t total = a.batch * a.ms * a.ns;
     if (total <= 0) return cudaSuccess;
+    if (a.nc < 0 || a.nc > 4) return cudaErrorInvalidValue;
     timing_begin(KK_AUX, stream);
     scatter_add_kernel<<<grid_for(total), THREADS, 0, stream>>>(a);
     timing_end(KK_AUX, stream);

@@ -120,28 +120,26 @@ __device__ __forceinline__ void write_planes(const float (*buf)[SK + 1], void* o
     {
         const int q = tid + 256 * i;
         const int r = q / (SK / 8), g = q % (SK / 8);
-        unsigned short hv[8], mv[8], lv[8];
+        // two values per conversion (cvt.rn.bf16x2.f32); the residuals are
+        // exact in FP32, and bf16 -> FP32 is a shift
+        uint32_t hv[4], mv[4], lv[4];
 #pragma unroll
-        for (int j = 0; j < 8; j++)
+        for (int j = 0; j < 4; j++)
         {
-            const float x = buf[r][g * 8 + j];
-            const __nv_bfloat16 h = __float2bfloat16_rn(x);
-            const float r1 = x - __bfloat162float(h);
-            const __nv_bfloat16 m = __float2bfloat16_rn(r1);
-            const float r2 = r1 - __bfloat162float(m);
-            const __nv_bfloat16 l = __float2bfloat16_rn(r2);
-            hv[j] = __bfloat16_as_ushort(h);
-            mv[j] = __bfloat16_as_ushort(m);
-            lv[j] = __bfloat16_as_ushort(l);
+            const float x0 = buf[r][g * 8 + 2 * j], x1 = buf[r][g * 8 + 2 * j + 1];
+            const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+            const float a0 = x0 - __low2float(h), a1 = x1 - __high2float(h);
+            const __nv_bfloat162 m = __floats2bfloat162_rn(a0, a1);
+            const __nv_bfloat162 l = __floats2bfloat162_rn(a0 - __low2float(m), a1 - __high2float(m));
+            hv[j] = *reinterpret_cast<const uint32_t*>(&h);
+            mv[j] = *reinterpret_cast<const uint32_t*>(&m);
+            lv[j] = *reinterpret_cast<const uint32_t*>(&l);
         }
         const int off = swz(half * PR + r, g * 8);
-        auto pack = [](const unsigned short* v) {
-            return make_uint4(v[0] | (unsigned)v[1] << 16, v[2] | (unsigned)v[3] << 16,
-                              v[4] | (unsigned)v[5] << 16, v[6] | (unsigned)v[7] << 16);
-        };
-        *reinterpret_cast<uint4*>(blk + off) = pack(hv);
-        *reinterpret_cast<uint4*>(blk + plane_stride + off) = pack(mv);
-        if (planes > 2) *reinterpret_cast<uint4*>(blk + 2 * plane_stride + off) = pack(lv);
+        *reinterpret_cast<uint4*>(blk + off) = make_uint4(hv[0], hv[1], hv[2], hv[3]);
+        *reinterpret_cast<uint4*>(blk + plane_stride + off) = make_uint4(mv[0], mv[1], mv[2], mv[3]);
+        if (planes > 2)
+            *reinterpret_cast<uint4*>(blk + 2 * plane_stride + off) = make_uint4(lv[0], lv[1], lv[2], lv[3]);
     }
 }
 
