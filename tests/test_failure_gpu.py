@@ -90,13 +90,13 @@ def test_wait_timeout_fused_no_workspace_then_recovery(tsb, cuda, level):
     assert err <= oracle.error_bound(level, 512, np.abs(A).max(), np.abs(B).max())
 
 
-@pytest.mark.parametrize("level", [0, 1])
-@pytest.mark.parametrize("producer", ["tma", "pairs"])
+@pytest.mark.parametrize("level,producer", [(0, "tma"), (1, "tma"), (0, "pairs"), (1, "pairs"), (2, "pairs")])
 def test_wait_timeout_pair_kernel_then_recovery(tsb, cuda, level, producer):
     """The element-pair form of the no-workspace kernel, with each of its
-    producers: a one-cycle bound, TBLIS_STRA_ERR_TIMEOUT, then a correct call
-    on the same context.  Tensor-map boxes: A(k, i), B(k, j) (128-byte runs);
-    pair copies: the headline contraction's layout at 512^3."""
+    producers and both slot shapes (16 k per slot at L <= 1, 8 k at L = 2):
+    a one-cycle bound, TBLIS_STRA_ERR_TIMEOUT, then a correct call on the same
+    context.  Tensor-map boxes: A(k, i), B(k, j) (128-byte runs); pair
+    copies: the headline contraction's layout at 512^3."""
     import torch
     if producer == "tma":
         A, B, ref = _problem()
