@@ -488,14 +488,19 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
                     for (int e = 0; e < 4; e++) acc[mi][ni][e] = 0.0;
             const DevProduct& P = a.prod[p];
             // the other blocks of a sum, with their signs relative to the
-            // first (the first's sign moves to the C coefficient)
+            // first (the first's sign moves to the C coefficient): added as
+            // fma(+-1, u, v) with 2 blocks per sum, as sign-bit flips (fewer
+            // registers) with 4
             const int na = P.na, nb = P.nb;
             uint32_t ma[NT], mb[NT];
+            double ra[NT], rb[NT];
 #pragma unroll
             for (int t = 1; t < NT; t++)
             {
                 ma[t] = t < na && P.a_s[t] * P.a_s[0] < 0 ? 0x80000000u : 0u;
                 mb[t] = t < nb && P.b_s[t] * P.b_s[0] < 0 ? 0x80000000u : 0u;
+                ra[t] = ma[t] ? -1.0 : 1.0;
+                rb[t] = mb[t] ? -1.0 : 1.0;
             }
 
             for (int64_t s = 0; s < nk; s++)
@@ -522,8 +527,16 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
                                 if (t < na)
                                 {
                                     const double2 u = ld2(pa + t * BOX);
-                                    va[mi][h].x += flip(u.x, ma[t]);
-                                    va[mi][h].y += flip(u.y, ma[t]);
+                                    if (TB == 16)
+                                    {
+                                        va[mi][h].x = fma(ra[t], u.x, va[mi][h].x);
+                                        va[mi][h].y = fma(ra[t], u.y, va[mi][h].y);
+                                    }
+                                    else
+                                    {
+                                        va[mi][h].x += flip(u.x, ma[t]);
+                                        va[mi][h].y += flip(u.y, ma[t]);
+                                    }
                                 }
                         }
                     double vb[NI][2];
@@ -539,8 +552,16 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
                                 if (t < nb)
                                 {
                                     const double2 u = ld2(pb + t * BOX);
-                                    v.x += flip(u.x, mb[t]);
-                                    v.y += flip(u.y, mb[t]);
+                                    if (TB == 16)
+                                    {
+                                        v.x = fma(rb[t], u.x, v.x);
+                                        v.y = fma(rb[t], u.y, v.y);
+                                    }
+                                    else
+                                    {
+                                        v.x += flip(u.x, mb[t]);
+                                        v.y += flip(u.y, mb[t]);
+                                    }
                                 }
                             vb[ni][0] = v.x;
                             vb[ni][1] = v.y;
@@ -553,7 +574,9 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
                                 vb[ni][jj] = *pb;
 #pragma unroll
                                 for (int t = 1; t < NT; t++)
-                                    if (t < nb) vb[ni][jj] += flip(pb[t * BOX], mb[t]);
+                                    if (t < nb)
+                                        vb[ni][jj] = TB == 16 ? fma(rb[t], pb[t * BOX], vb[ni][jj])
+                                                              : vb[ni][jj] + flip(pb[t * BOX], mb[t]);
                             }
                     }
 #pragma unroll
