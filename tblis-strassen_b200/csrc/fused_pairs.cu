@@ -489,8 +489,10 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
             const DevProduct& P = a.prod[p];
             // the other blocks of a sum, with their signs relative to the
             // first (the first's sign moves to the C coefficient): added as
-            // fma(+-1, u, v) with 2 blocks per sum, as sign-bit flips (fewer
-            // registers) with 4
+            // fma(+-1, u, v) with 2 blocks per sum or B read in pairs, as
+            // sign-bit flips (fewer registers: no spills) with 4 blocks and B
+            // read by element
+            constexpr bool FMA_SUMS = TB == 16 || BPAIR;
             const int na = P.na, nb = P.nb;
             uint32_t ma[NT], mb[NT];
             double ra[NT], rb[NT];
@@ -527,7 +529,7 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
                                 if (t < na)
                                 {
                                     const double2 u = ld2(pa + t * BOX);
-                                    if (TB == 16)
+                                    if (FMA_SUMS)
                                     {
                                         va[mi][h].x = fma(ra[t], u.x, va[mi][h].x);
                                         va[mi][h].y = fma(ra[t], u.y, va[mi][h].y);
@@ -552,7 +554,7 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
                                 if (t < nb)
                                 {
                                     const double2 u = ld2(pb + t * BOX);
-                                    if (TB == 16)
+                                    if (FMA_SUMS)
                                     {
                                         v.x = fma(rb[t], u.x, v.x);
                                         v.y = fma(rb[t], u.y, v.y);
@@ -575,7 +577,7 @@ stra_fused_pair_kernel(const __grid_constant__ DmmaArgs a, const __grid_constant
 #pragma unroll
                                 for (int t = 1; t < NT; t++)
                                     if (t < nb)
-                                        vb[ni][jj] = TB == 16 ? fma(rb[t], pb[t * BOX], vb[ni][jj])
+                                        vb[ni][jj] = FMA_SUMS ? fma(rb[t], pb[t * BOX], vb[ni][jj])
                                                               : vb[ni][jj] + flip(pb[t * BOX], mb[t]);
                             }
                     }
