@@ -171,10 +171,10 @@ def _bank_conflicts(reads, width, phase_lanes):
     return total
 
 
-@pytest.mark.parametrize("case", ACCEPTED)
-def test_lane_tables_pair_the_same_k_and_cover_the_slot(tsb, case):
-    level, ia, ib, ic, ext, lead, _ = case
-    q = _query(tsb, level, ia, ib, ic, ext, lead)
+def check_lane_tables(q):
+    """The consumers' reads of a plan: both operands take the same k in every
+    MMA step, each row (column) g takes the slot's tb k once over its tb / 4
+    steps, and no quarter (half) warp hits one bank at two addresses."""
     steps, a_reads, b_reads = _replay(q)
     for (g, t4), seq in steps.items():
         for kA, kB in seq:
@@ -189,18 +189,13 @@ def test_lane_tables_pair_the_same_k_and_cover_the_slot(tsb, case):
     assert _bank_conflicts(b_reads, 16 if q["b_pairs"] else 8, 8 if q["b_pairs"] else 16) == 0
 
 
-@pytest.mark.parametrize("case", ACCEPTED)
-def test_producer_copies_land_where_consumers_read(tsb, case):
-    """The pair producer: with P = tb / 2 pairs per tile row, thread (warp w,
-    lane l) copies pair pbase[l % P] of tile rows (32 / P) w + l / P +
-    (128 / P) i to swizzle((koff + tb r) * 8) / 8.  Every element of the tile
-    is written once, the pair's second element (its k with the pair bit set)
-    lands 8 bytes after the first, and a quarter warp's 8 copies hit 8
-    different 16-byte bank groups."""
-    level, ia, ib, ic, ext, lead, producer = case
-    if producer != "pairs":
-        pytest.skip("tiles copied as tensor-map boxes")
-    q = _query(tsb, level, ia, ib, ic, ext, lead)
+def check_producer_copies(q):
+    """The pair producer of a plan: with P = tb / 2 pairs per tile row,
+    thread (warp w, lane l) copies pair pbase[l % P] of tile rows (32 / P) w +
+    l / P + (128 / P) i to swizzle((koff + tb r) * 8) / 8.  Every element of
+    the tile is written once, the pair's second element (its k with the pair
+    bit set) lands 8 bytes after the first, and a quarter warp's 8 copies hit
+    8 different 16-byte bank groups."""
     tb = q["tb"]
     P = tb // 2
     rpw, rpp = 32 // P, 4 * 32 // P
@@ -231,6 +226,20 @@ def test_producer_copies_land_where_consumers_read(tsb, case):
                 kp, r = lane % P, (quarter // 4) * rpw + lane // P
                 units.add((_swizzle((koff[pbase[kp]] + tb * (r & 7)) * 8, span) >> 4) & 7)
             assert len(units) == 8
+
+
+@pytest.mark.parametrize("case", ACCEPTED)
+def test_lane_tables_pair_the_same_k_and_cover_the_slot(tsb, case):
+    level, ia, ib, ic, ext, lead, _ = case
+    check_lane_tables(_query(tsb, level, ia, ib, ic, ext, lead))
+
+
+@pytest.mark.parametrize("case", ACCEPTED)
+def test_producer_copies_land_where_consumers_read(tsb, case):
+    level, ia, ib, ic, ext, lead, producer = case
+    if producer != "pairs":
+        pytest.skip("tiles copied as tensor-map boxes")
+    check_producer_copies(_query(tsb, level, ia, ib, ic, ext, lead))
 
 
 # ------------------------------------------------------------------ GPU parity
